@@ -1,0 +1,453 @@
+#!/usr/bin/env python
+"""Throughput of the 2D electrostatic PIC step on B200.
+
+Metric: particle-steps/s of bin + deposit + push (the particle phases of one
+PIC step), with Poisson ms/step reported beside it.  One "step" is one full
+PIC step of the workload: zero rho, deposit every species, Poisson to 1e-8
+relative residual + E field, push every species.  `value` counts the device
+time of the particle phases only (CUDA events on the library's stream, which
+is torch's current stream), summed over the K timed steps, max over ranks.
+
+Default workload: the 1024x1024 configuration with the 200 V internal
+electrode and the drifting Gaussian blob (~2.3e8 particles, FP32 state,
+64-bit fixed-point deposit).  The particle state (~9 GB) is far larger than
+L2, so no flush is needed between steps.
+
+Multi-GPU: a single instance does not shard (no domain decomposition), so N
+ranks run N independent replicas with different seeds ("scaling": "weak").
+
+--impl reference times the reference's algorithm on the host cores (the
+hashmap port in oracle/, the reference's own CPU path being unbuildable here)
+on a bounded sample of the same workload, and prints the same JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "bmp-6th-sem_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s (bin+deposit+push)"
+UNIT = "particle-steps/s"
+# Algorithmic HBM bytes per particle for each launch of the push (FP32 state,
+# 20 B per particle: float4 {fx, fy, vx, vy} + float vz).
+BYTES_COUNT_PASS = 20     # read the state
+BYTES_SCATTER_PASS = 40   # read the state, write it to the new position
+BYTES_STEP = 60           # whole particle phase of one step
+BYTES_SURVEY_FP32 = 112   # the blueprint's per-particle-step figure (push 48 + deposit 12 + bin 52)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg3", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload(name):
+    import pic_configs as C
+    return {"cfg1": C.cfg1, "cfg2": C.cfg2, "cfg3": C.cfg3}[name]()
+
+
+def describe(w):
+    el = [r for r in w.rects[4:]]
+    return (f"{w.name}: {w.nx}x{w.ny} cells, dx={w.dx} m, dt={w.dt} s, Bz={w.b0} T, "
+            f"{w.ppc} ppc/species background" +
+            (f" + Gaussian blob peak {w.plasma[0].blob_peak_ppc:g} ppc sigma {w.plasma[0].blob_sigma:g} cells"
+             if w.plasma[0].blob_peak_ppc else "") +
+            (f", internal electrode {el}" if el else "") + ", electrons + Ar+")
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's algorithm (hashmap port) on a bounded sample
+# ---------------------------------------------------------------------------
+
+def sample_points(w, s, scale, seed):
+    """Host Points for the workload shrunk by `scale` per axis, same per-cell
+    densities (background ppc + blob profile)."""
+    import pic_b200 as P
+    import pic_configs as C
+    nx, ny = w.nx // scale, w.ny // scale
+    rng = np.random.default_rng(seed)
+    ps = w.plasma[s]
+    gx, gy = np.meshgrid(np.arange(nx), np.arange(ny))
+    cnt = np.full(nx * ny, ps.ppc, np.int64)
+    if ps.blob_peak_ppc > 0:
+        cx, cy, sig = ps.blob_cx / scale, ps.blob_cy / scale, ps.blob_sigma / scale
+        r2 = ((gx + 0.5 - cx) ** 2 + (gy + 0.5 - cy) ** 2).ravel()
+        blob = np.floor(ps.blob_peak_ppc * np.exp(-r2 / (2 * sig * sig)) + rng.random(nx * ny))
+        cnt = cnt + blob.astype(np.int64)
+    cells = np.repeat(np.arange(nx * ny), cnt)
+    first = np.repeat(np.cumsum(cnt) - cnt, cnt)
+    is_blob = (np.arange(len(cells)) - first) >= ps.ppc
+    n = len(cells)
+    pts = np.zeros(n, P.POINT_DTYPE)
+    pts["x"] = (cells % nx + rng.random(n)) * w.dx
+    pts["y"] = (cells // nx + rng.random(n)) * w.dx
+    sig_v = np.sqrt(C.QE * ps.temperature_ev / w.species[s][1])
+    pts["vx"] = rng.normal(0, sig_v, n) + np.where(is_blob, ps.drift_vx, 0.0)
+    pts["vy"] = rng.normal(0, sig_v, n) + np.where(is_blob, ps.drift_vy, 0.0)
+    pts["vz"] = rng.normal(0, sig_v, n)
+    # the reference's arrays are in random order (initParticlesRandomly)
+    return pts[rng.permutation(n)], nx, ny
+
+
+def cpu_reference_run(w, scale, max_seconds, min_steps=2, max_steps=None, steps=None):
+    """Times the reference's step structure (src/main.cpp:130-230) on the host:
+    per species hashmap deposit, then the Poisson solve (SuperLU, factored
+    once), then per species mover + compaction + map cleanup.  Returns
+    (particle-steps/s of the particle phases, poisson ms/step, sample text,
+    threads, per-step particle seconds list)."""
+    import oracle as O
+    import pic_configs as C
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    sp_pts, nx, ny = [], 0, 0
+    for s in range(2):
+        pts, nx, ny = sample_points(w, s, scale, seed=900 + s)
+        sp_pts.append(pts)
+    dx = dy = w.dx
+    g = O.Grid(nx, ny, dx, dy)
+    scale_rects = [(0, 0, 0, ny, w.rects[0][4]), (nx, 0, nx, ny, w.rects[1][4]),
+                   (0, ny, nx, ny, w.rects[2][4]), (0, 0, nx, 0, w.rects[3][4])]
+    for (x1, y1, x2, y2, v) in w.rects[4:]:
+        scale_rects.append((x1 // scale, y1 // scale, x2 // scale, y2 // scale, v))
+    el = O.Electrodes(scale_rects)
+    D = O.DirectPoisson(nx + 1, ny + 1, dx, dy, el)
+    species = [O.Species(str(s), *C._species(nx, ny, w.ppc, w.n0)[s]) for s in range(2)]
+    weigh = [O.weighing_factor(sp, nx * dx * ny * dy, dx, dy) for sp in species]
+    # the reference sizes each bucket for prob_size*wg slots; the blob peak
+    # needs ~1.1k per bucket here
+    H = [O.RefHashmapSpecies(g, sp_pts[s], probing_length=2048) for s in range(2)]
+    bz = np.full(g.nodes, w.b0)
+    n_particles = sum(len(p) for p in sp_pts)
+    part_t, pois_t = [], []
+    t_start = time.perf_counter()
+    it = 0
+    while True:
+        rho = np.zeros(g.nodes)
+        t0 = time.perf_counter()
+        for s in range(2):
+            H[s].deposit(species[s], weigh[s], C.EPS0, rho)
+        t1 = time.perf_counter()
+        phi, ef = D.step(rho)
+        t2 = time.perf_counter()
+        for s in range(2):
+            H[s].move(species[s].ctom, w.dt, ef, bz)
+            H[s].compact()
+            H[s].cleanup()
+        t3 = time.perf_counter()
+        part_t.append((t1 - t0) + (t3 - t2))
+        pois_t.append(t2 - t1)
+        it += 1
+        if steps is not None:
+            if it >= steps:
+                break
+        elif (it >= min_steps and time.perf_counter() - t_start > max_seconds) or (
+                max_steps and it >= max_steps):
+            break
+    value = n_particles * len(part_t) / sum(part_t)
+    sample = (f"{w.name} at 1/{scale} scale per axis: {nx}x{ny} cells, {n_particles} particles "
+              f"(same per-cell densities, blob and electrode scaled), {len(part_t)} steps of the "
+              f"reference hashmap algorithm (deposit, mover, compaction, cleanup) on {threads} "
+              f"OpenMP threads; Poisson by SuperLU on one thread")
+    return value, 1e3 * statistics.mean(pois_t), sample, threads, part_t, n_particles
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows),
+                "reasons": reasons}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_particle():
+    """Per-particle DRAM bytes of the scatter pass from the committed ncu
+    summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("scatter_dram_bytes_per_particle"), d.get("source")
+    return None, None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import pic_b200 as P
+    import pic_configs as C
+    torch.cuda.set_device(local_rank)
+    w = workload(args.config)
+    pic = P.Pic(C.library_config(w, device=local_rank))
+    stream = torch.cuda.current_stream()
+    pic.set_stream(stream.cuda_stream)
+    C.load_plasma(pic, w, seed=1234 + 7 * rank)
+    counts = [pic.count(s) for s in range(2)]
+    n_part = sum(counts)
+    L = P.lib()
+    import ctypes
+
+    def launches():
+        n = ctypes.c_int64(0)
+        L.pic_launch_count(pic.h, ctypes.byref(n))
+        return n.value
+
+    it = 0
+    for _ in range(args.warmup):
+        pic.step(it)
+        it += 1
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    l0 = launches()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    iters = []
+    t_wall0 = time.perf_counter()
+    for k in range(args.steps):
+        e = ev[k]
+        e[0].record(stream)
+        pic.zero_rho()
+        for s in range(2):
+            pic.charge_deposition(s)
+        e[1].record(stream)
+        pic.poisson_solve(it)
+        e[2].record(stream)
+        for s in range(2):
+            pic.move_particles(s, it)
+        e[3].record(stream)
+        iters.append(pic.poisson_stats()[0])
+        it += 1
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall0
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    gpu_launches = launches() - l0
+    part_ms = sum(e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3]) for e in ev)
+    pois_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    step_ms = sum(e[0].elapsed_time(e[3]) for e in ev)
+    relres = pic.poisson_stats()[1]
+    times = torch.tensor([part_ms, step_ms, sum(pois_ms)], dtype=torch.float64, device="cuda")
+    nparts = torch.tensor([float(n_part)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(nparts, op=torch.distributed.ReduceOp.SUM)
+    part_ms, step_ms, pois_sum = times.tolist()
+    total_particles = nparts.item()
+    value = total_particles * args.steps / (part_ms * 1e-3)
+
+    # per-kernel breakdown over 3 extra profiled steps (not part of `value`)
+    L.pic_set_profiling(pic.h, 1)
+    ms6 = (ctypes.c_double * P_PHASES)()
+    calls6 = (ctypes.c_int64 * P_PHASES)()
+    L.pic_profile_read(pic.h, ms6, calls6, 1)
+    prof_steps = 3
+    for _ in range(prof_steps):
+        pic.step(it)
+        it += 1
+    L.pic_profile_read(pic.h, ms6, calls6, 1)
+    L.pic_set_profiling(pic.h, 0)
+    phase_names = ["push_count", "scan", "push_scatter", "deposit", "flush", "poisson"]
+    phases = {phase_names[i]: {"ms_per_step": ms6[i] / prof_steps, "calls_per_step": calls6[i] / prof_steps}
+              for i in range(P_PHASES)}
+    peak, peak_kind = measured_peaks()
+    scatter_ms = ms6[2] / calls6[2] if calls6[2] else float("nan")
+    avg_n = n_part / 2
+    achieved = BYTES_SCATTER_PASS * avg_n / (scatter_ms * 1e-3) / 1e9
+    traffic_pp, traffic_src = ncu_traffic_per_particle()
+    roofline = {"kernel": "k_particles<kScatter> (push + scatter + fused deposit)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                "bytes_per_particle": BYTES_SCATTER_PASS,
+                "traffic": (traffic_pp * avg_n) if traffic_pp else None,
+                "traffic_source": traffic_src}
+    step_particle_ms = (ms6[0] + ms6[1] + ms6[2] + ms6[4]) / prof_steps
+    roofline_step = {"bytes_per_particle_step": BYTES_STEP,
+                     "achieved_GBs": BYTES_STEP * n_part / (step_particle_ms * 1e-3) / 1e9,
+                     "survey_112B_equivalent_GBs": BYTES_SURVEY_FP32 * n_part / (step_particle_ms * 1e-3) / 1e9}
+    roofline_step["frac"] = roofline_step["achieved_GBs"] / peak
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(pic, args.steps, n_part, it)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": part_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": describe(w), "particles_per_gpu": n_part,
+                   "particles_per_species": counts, "grid_nodes": (w.nx + 1) * (w.ny + 1),
+                   "l2": "inputs larger than L2 (particle state ~%.1f GB per GPU)" % (n_part * 40 / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "full_step": {"ms_per_step": step_ms / args.steps,
+                      "particle_steps_per_s": total_particles * args.steps / (step_ms * 1e-3),
+                      "wall_s": t_wall},
+        "poisson": {"solver": "MG-PCG (FP32 V-cycle, FP64 CG)", "warm_start": "previous phi",
+                    "ms_per_step_plain": pois_sum / args.steps,
+                    "ms_per_step_learned": None, "iters_per_step": statistics.mean(iters),
+                    "relres": relres, "tol": 1e-8},
+        "roofline": roofline, "roofline_particle_phase": roofline_step,
+        "phases": phases, "gpu_launches": gpu_launches, "clocks": clocks, "e2e": e2e,
+    }
+    return line, pic, w
+
+
+P_PHASES = 6
+
+
+def run_e2e(pic, steps, n_part, it0):
+    """Same metric through the public C ABI with host buffers: import both
+    species from host Points, K x (zero rho, deposit, read rho to host, push),
+    export both species back.  Wall clock around the whole sequence."""
+    import pic_b200 as P
+    host = [pic.export_points(s) for s in range(2)]   # untimed: the inputs on the host
+    rho_host = np.zeros(pic.nodes)
+    t0 = time.perf_counter()
+    for s in range(2):
+        pic.import_points(s, host[s])
+    for k in range(steps):
+        pic.zero_rho()
+        for s in range(2):
+            pic.charge_deposition(s)
+        rho_host[:] = pic.rho()
+        for s in range(2):
+            pic.move_particles(s, it0 + k)
+    out = [pic.export_points(s) for s in range(2)]
+    pic.synchronize()
+    t = time.perf_counter() - t0
+    h2d = sum(len(h) for h in host) * P.POINT_DTYPE.itemsize
+    d2h = sum(len(o) for o in out) * P.POINT_DTYPE.itemsize
+    return {"value": n_part * steps / t, "unit": UNIT,
+            "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps + pic.nodes * 8,
+            "wall_s": t,
+            "what": "pic_import_points (both species) + K x (zero_rho, charge_deposition x2, "
+                    "pic_get_rho to host, move_particles x2) + pic_export_points; E held "
+                    "from the last solve (Poisson excluded, as in the metric)"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        w = workload(args.config)
+        # bounded sample per step: 1/4 scale per axis of the workload
+        scale = 4 if w.nx >= 512 else 1
+        steps = args.steps + args.warmup
+        value, pois_ms, sample, threads, part_t, n = cpu_reference_run(w, scale, 0, steps=steps)
+        timed = part_t[args.warmup:]
+        value = n * len(timed) / sum(timed)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * sum(timed) / len(timed), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": describe(w), "parallelism": "host cores"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "poisson": {"ms_per_step": pois_ms, "solver": "SuperLU (PARDISO restatement)"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device(f"cuda:{local_rank}"))
+    line, pic, w = run_ours(args, rank, world, local_rank)
+    pic.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        scale = 4 if w.nx >= 512 else 1
+        value, pois_ms, sample, threads, _, _ = cpu_reference_run(w, scale, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": sample, "poisson_ms_per_step": pois_ms}
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,527 @@
+// context.cu -- pic_* C ABI: context lifetime, particle I/O, step operators,
+// grid access.  Operators enqueue on the context stream; host-copy getters
+// synchronise.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pic_internal.h"
+
+namespace picb200 {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+static int check_species(pic_ctx* c, int s) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (s < 0 || s >= c->cfg.num_species) return fail(PIC_ERR_ARG, "species index out of range");
+    return PIC_OK;
+}
+
+static int ensure_host_staging(pic_ctx* c, size_t bytes) {
+    if (bytes <= c->host_staging_bytes) return PIC_OK;
+    if (c->host_staging) cudaFreeHost(c->host_staging);
+    c->host_staging = nullptr;
+    c->host_staging_bytes = 0;
+    PIC_CUDA(cudaMallocHost(&c->host_staging, bytes));
+    c->host_staging_bytes = bytes;
+    return PIC_OK;
+}
+
+// Device -> host copy through pinned staging (pageable destinations would
+// serialise the stream anyway).
+static int copy_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes) {
+    PIC_TRY(ensure_host_staging(c, bytes));
+    PIC_CUDA(cudaMemcpyAsync(c->host_staging, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    std::memcpy(host, c->host_staging, bytes);
+    return PIC_OK;
+}
+
+static int copy_to_device(pic_ctx* c, void* dev, const void* host, size_t bytes) {
+    PIC_TRY(ensure_host_staging(c, bytes));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));  // staging may still feed a copy
+    std::memcpy(c->host_staging, host, bytes);
+    PIC_CUDA(cudaMemcpyAsync(dev, c->host_staging, bytes, cudaMemcpyHostToDevice, c->stream));
+    return PIC_OK;
+}
+
+static cudaEvent_t pool_event(pic_ctx* c) {
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(pic_ctx* c, int phase) {
+    (void)phase;
+    if (!c->profiling) return;
+    c->prof_open = pool_event(c);
+    cudaEventRecord(c->prof_open, c->stream);
+}
+
+void prof_end(pic_ctx* c, int phase) {
+    if (!c->profiling || !c->prof_open) return;
+    cudaEvent_t b = pool_event(c);
+    cudaEventRecord(b, c->stream);
+    c->prof_pending.push_back({phase, c->prof_open, b});
+    c->prof_open = nullptr;
+}
+
+static void free_ctx(pic_ctx* c) {
+    for (auto& p : c->prof_pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    for (int s = 0; s < PIC_MAX_SPECIES; ++s) species_free(c->sp[s]);
+    poisson_free(c);
+    cudaFree(c->rho);
+    cudaFree(c->phi);
+    cudaFree(c->bz);
+    cudaFree(c->fld);
+    cudaFree(c->mask);
+    cudaFree(c->dir_val);
+    cudaFree(c->efield64);
+    cudaFree(c->scan_partials);
+    cudaFree(c->staging);
+    if (c->host_staging) cudaFreeHost(c->host_staging);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // namespace picb200
+
+using namespace picb200;
+
+extern "C" {
+
+const char* pic_last_error(void) { return g_last_error.c_str(); }
+
+const char* pic_status_string(int status) {
+    switch (status) {
+        case PIC_OK: return "ok";
+        case PIC_ERR_ARG: return "bad argument";
+        case PIC_ERR_CONFIG: return "invalid configuration";
+        case PIC_ERR_CAPACITY: return "capacity exceeded";
+        case PIC_ERR_NOT_CONVERGED: return "Poisson solve did not converge";
+        case PIC_ERR_CUDA: return "CUDA error";
+        case PIC_ERR_STATE: return "operator called in the wrong state";
+        case PIC_ERR_IO: return "I/O error";
+        case PIC_ERR_NO_DEVICE: return "no usable sm_100 device";
+        case PIC_ERR_TIMEOUT: return "bounded device wait gave up";
+        default: return "unknown status";
+    }
+}
+
+int pic_config_default(pic_config* cfg) {
+    if (!cfg) return fail(PIC_ERR_ARG, "null config");
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->nx = cfg->ny = 128;
+    cfg->xmax = cfg->ymax = 128 * 2.5e-4;
+    cfg->dt = 5e-11;
+    cfg->epsilon = 8.854e-12;
+    cfg->poisson_solver = PIC_SOLVER_MG_PCG;
+    cfg->warm_start = PIC_WARM_PREVIOUS;
+    cfg->poisson_tol = 1e-8;
+    cfg->poisson_maxit = 500;
+    cfg->deposit_energy = 1;
+    cfg->timesteps = 100;
+    cfg->print_interval = 1;
+    return PIC_OK;
+}
+
+int pic_create(const pic_config* cfg_in, pic_ctx** out) {
+    if (!cfg_in || !out) return fail(PIC_ERR_ARG, "null argument");
+    *out = nullptr;
+    const pic_config& cfg = *cfg_in;
+    if (cfg.nx < 4 || cfg.ny < 4) return fail(PIC_ERR_CONFIG, "nx and ny must be >= 4");
+    if ((int64_t)cfg.nx * cfg.ny > (1ll << 30)) return fail(PIC_ERR_CONFIG, "grid too large");
+    if (!(cfg.xmax > 0) || !(cfg.ymax > 0) || !(cfg.dt > 0) || !(cfg.epsilon > 0))
+        return fail(PIC_ERR_CONFIG, "xmax, ymax, dt and epsilon must be positive");
+    if (cfg.num_species < 1 || cfg.num_species > PIC_MAX_SPECIES)
+        return fail(PIC_ERR_CONFIG, "num_species must be 1..4");
+    if (cfg.num_rects < 0 || cfg.num_rects > PIC_MAX_RECTS)
+        return fail(PIC_ERR_CONFIG, "num_rects must be 0..32");
+    const int GX = cfg.nx + 1, GY = cfg.ny + 1;
+    std::vector<uint8_t> mask((size_t)GX * GY, 0);
+    std::vector<double> dval((size_t)GX * GY, 0.0);
+    for (int r = 0; r < cfg.num_rects; ++r) {
+        const pic_rect& R = cfg.rects[r];
+        if (R.x1 < 0 || R.y1 < 0 || R.x2 >= GX || R.y2 >= GY || R.x1 > R.x2 || R.y1 > R.y2)
+            return fail(PIC_ERR_CONFIG, "electrode rectangle outside the node grid");
+        // setPotentialBoundary / overwritePhi order: later rectangles win
+        for (int j = R.y1; j <= R.y2; ++j)
+            for (int i = R.x1; i <= R.x2; ++i) {
+                mask[(size_t)j * GX + i] = 1;
+                dval[(size_t)j * GX + i] = R.potential;
+            }
+    }
+    for (int i = 0; i < GX; ++i)
+        if (!mask[i] || !mask[(size_t)(GY - 1) * GX + i])
+            return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
+    for (int j = 0; j < GY; ++j)
+        if (!mask[(size_t)j * GX] || !mask[(size_t)j * GX + GX - 1])
+            return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(PIC_ERR_NO_DEVICE, "no CUDA device visible");
+    if (cfg.device < 0 || cfg.device >= ndev) return fail(PIC_ERR_ARG, "device ordinal out of range");
+    cudaDeviceProp prop{};
+    PIC_CUDA(cudaGetDeviceProperties(&prop, cfg.device));
+    if (prop.major != 10)
+        return fail(PIC_ERR_NO_DEVICE, std::string("library is built for sm_100a; device is ") +
+                                           prop.name);
+    PIC_CUDA(cudaSetDevice(cfg.device));
+
+    pic_ctx* c = new pic_ctx();
+    c->cfg = cfg;
+    if (c->cfg.poisson_tol <= 0) c->cfg.poisson_tol = 1e-8;
+    if (c->cfg.poisson_maxit <= 0) c->cfg.poisson_maxit = 500;
+    c->nx = cfg.nx;
+    c->ny = cfg.ny;
+    c->GX = GX;
+    c->GY = GY;
+    c->nodes = (int64_t)GX * GY;
+    c->ncells = (int64_t)cfg.nx * cfg.ny;
+    c->dx = cfg.xmax / cfg.nx;  // readPICDAT, src/particles.cpp:360-361
+    c->dy = cfg.ymax / cfg.ny;
+    c->device = cfg.device;
+    auto bail = [&](int st) {
+        free_ctx(c);
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "stream creation failed"));
+    c->own_stream = true;
+    const size_t n = (size_t)c->nodes;
+    if (cudaMalloc(&c->rho, n * 8) || cudaMalloc(&c->phi, n * 8) || cudaMalloc(&c->bz, n * 8) ||
+        cudaMalloc(&c->fld, n * sizeof(float4)) || cudaMalloc(&c->mask, n) ||
+        cudaMalloc(&c->dir_val, n * 8) || cudaMalloc(&c->efield64, n * 16) ||
+        cudaMalloc(&c->scan_partials, ((size_t)c->ncells / 2048 + 2) * 4))
+        return bail(fail(PIC_ERR_CUDA, "device allocation failed for the grids"));
+    std::vector<double> bz(n, cfg.b0);  // initMagneticField, src/particles.cpp:709-720
+    std::vector<double> phi0(n, 0.0);
+    for (size_t i = 0; i < n; ++i)
+        if (mask[i]) phi0[i] = dval[i];  // initPoissonSolver -> overwritePhi
+    if (cudaMemcpy(c->mask, mask.data(), n, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->dir_val, dval.data(), n * 8, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->bz, bz.data(), n * 8, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->phi, phi0.data(), n * 8, cudaMemcpyHostToDevice) ||
+        cudaMemset(c->rho, 0, n * 8) || cudaMemset(c->fld, 0, n * sizeof(float4)))
+        return bail(fail(PIC_ERR_CUDA, "grid initialisation copy failed"));
+    int st = fields_set_bz(c);
+    if (st) return bail(st);
+    for (int s = 0; s < cfg.num_species; ++s)
+        if ((st = species_setup(c, s))) return bail(st);
+    if ((st = poisson_setup(c))) return bail(st);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "context initialisation failed"));
+    *out = c;
+    return PIC_OK;
+}
+
+void pic_destroy(pic_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+}
+
+int pic_set_stream(pic_ctx* c, void* stream) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    if (stream) {
+        c->stream = static_cast<cudaStream_t>(stream);
+        c->own_stream = false;
+    } else {
+        PIC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    return PIC_OK;
+}
+
+void* pic_get_stream(pic_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int pic_synchronize(pic_ctx* c) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    return PIC_OK;
+}
+
+int pic_reserve(pic_ctx* c, int s, int64_t capacity) {
+    PIC_TRY(check_species(c, s));
+    if (capacity < 0) return fail(PIC_ERR_ARG, "negative capacity");
+    return species_reserve(c, s, capacity);
+}
+
+int pic_import_points(pic_ctx* c, int s, const pic_point* host, int64_t n) {
+    PIC_TRY(check_species(c, s));
+    if (n < 0 || (n > 0 && !host)) return fail(PIC_ERR_ARG, "bad point array");
+    if (n > (int64_t)0xF0000000ll) return fail(PIC_ERR_CAPACITY, "too many points");
+    pic_point* dev = nullptr;
+    PIC_TRY(particles_import_staging(c, n, &dev));
+    // chunked through pinned staging so arbitrary host memory works
+    const int64_t chunk = 1 << 20;
+    PIC_TRY(ensure_host_staging(c, (size_t)std::min<int64_t>(n, chunk) * sizeof(pic_point) + 64));
+    for (int64_t i0 = 0; i0 < n; i0 += chunk) {
+        const int64_t m = std::min<int64_t>(chunk, n - i0);
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        std::memcpy(c->host_staging, host + i0, (size_t)m * sizeof(pic_point));
+        PIC_CUDA(cudaMemcpyAsync(dev + i0, c->host_staging, (size_t)m * sizeof(pic_point),
+                                 cudaMemcpyHostToDevice, c->stream));
+    }
+    return particles_import(c, s, n);
+}
+
+int pic_export_points(pic_ctx* c, int s, pic_point* host, int64_t capacity, int64_t* n_out) {
+    PIC_TRY(check_species(c, s));
+    int64_t n = 0;
+    PIC_TRY(particles_count(c, s, &n));
+    if (n_out) *n_out = n;
+    if (!host) return PIC_OK;  // size query
+    if (capacity < n) return fail(PIC_ERR_CAPACITY, "export buffer smaller than the particle count");
+    if (n == 0) return PIC_OK;
+    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(pic_point)));
+    pic_point* dev = static_cast<pic_point*>(c->staging);
+    int64_t n2 = 0;
+    PIC_TRY(particles_export(c, s, dev, &n2));
+    const int64_t chunk = 1 << 20;
+    PIC_TRY(ensure_host_staging(c, (size_t)std::min<int64_t>(n, chunk) * sizeof(pic_point) + 64));
+    for (int64_t i0 = 0; i0 < n; i0 += chunk) {
+        const int64_t m = std::min<int64_t>(chunk, n - i0);
+        PIC_CUDA(cudaMemcpyAsync(c->host_staging, dev + i0, (size_t)m * sizeof(pic_point),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        std::memcpy(host + i0, c->host_staging, (size_t)m * sizeof(pic_point));
+    }
+    return PIC_OK;
+}
+
+int pic_export_state(pic_ctx* c, int s, int32_t* cell, float* fx, float* fy, float* vx,
+                     float* vy, float* vz, int64_t capacity, int64_t* n_out) {
+    PIC_TRY(check_species(c, s));
+    int64_t n = 0;
+    PIC_TRY(particles_count(c, s, &n));
+    if (n_out) *n_out = n;
+    if (!cell && !fx && !fy && !vx && !vy && !vz) return PIC_OK;
+    if (!cell || !fx || !fy || !vx || !vy || !vz) return fail(PIC_ERR_ARG, "null output array");
+    if (capacity < n) return fail(PIC_ERR_CAPACITY, "output arrays smaller than the particle count");
+    if (n == 0) return PIC_OK;
+    PIC_TRY(ensure_staging(c, (size_t)n * 24));
+    PIC_TRY(particles_export_state(c, s, c->staging, n));
+    std::vector<char> h((size_t)n * 24);
+    PIC_TRY(copy_to_host(c, h.data(), c->staging, h.size()));
+    const size_t b = (size_t)n * 4;
+    std::memcpy(cell, h.data(), b);
+    std::memcpy(fx, h.data() + b, b);
+    std::memcpy(fy, h.data() + 2 * b, b);
+    std::memcpy(vx, h.data() + 3 * b, b);
+    std::memcpy(vy, h.data() + 4 * b, b);
+    std::memcpy(vz, h.data() + 5 * b, b);
+    return PIC_OK;
+}
+
+int pic_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d) {
+    PIC_TRY(check_species(c, s));
+    if (!d) return fail(PIC_ERR_ARG, "null plasma description");
+    return particles_load_plasma(c, s, d);
+}
+
+int pic_particle_count(pic_ctx* c, int s, int64_t* n) {
+    PIC_TRY(check_species(c, s));
+    if (!n) return fail(PIC_ERR_ARG, "null output");
+    return particles_count(c, s, n);
+}
+
+int pic_bin_counts(pic_ctx* c, int s, int32_t* host) {
+    PIC_TRY(check_species(c, s));
+    if (!host) return fail(PIC_ERR_ARG, "null output");
+    PIC_TRY(ensure_staging(c, (size_t)c->nodes * 4));
+    PIC_TRY(particles_bin_counts(c, s, static_cast<int32_t*>(c->staging)));
+    return copy_to_host(c, host, c->staging, (size_t)c->nodes * 4);
+}
+
+int pic_left_exits(pic_ctx* c, int s, int64_t* n) {
+    PIC_TRY(check_species(c, s));
+    unsigned long long v = 0;
+    PIC_CUDA(cudaMemcpyAsync(&v, c->sp[s].counters, 8, cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    PIC_CUDA(cudaMemsetAsync(c->sp[s].counters, 0, 8, c->stream));
+    if (n) *n = (int64_t)v;
+    return PIC_OK;
+}
+
+int pic_zero_rho(pic_ctx* c) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_CUDA(cudaMemsetAsync(c->rho, 0, (size_t)c->nodes * 8, c->stream));
+    return PIC_OK;
+}
+
+int pic_charge_deposition(pic_ctx* c, int s) {
+    PIC_TRY(check_species(c, s));
+    if (!c->sp[s].acc_fresh) PIC_TRY(particles_deposit(c, s));
+    return particles_flush_rho(c, s);
+}
+
+int pic_poisson_solve(pic_ctx* c, int iteration) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    (void)iteration;
+    return poisson_solve(c);
+}
+
+int pic_move_particles(pic_ctx* c, int s, int iteration) {
+    PIC_TRY(check_species(c, s));
+    (void)iteration;
+    if (!c->fields_valid) PIC_TRY(fields_from_phi(c));
+    return particles_push(c, s);
+}
+
+int pic_compact_particles(pic_ctx* c, int s) { return check_species(c, s); }
+int pic_cleanup_map(pic_ctx* c, int s) { return check_species(c, s); }
+
+int pic_particle_phase(pic_ctx* c, int iteration) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (!c->fields_valid) PIC_TRY(fields_from_phi(c));
+    for (int s = 0; s < c->cfg.num_species; ++s) {
+        if (!c->sp[s].acc_fresh) PIC_TRY(particles_deposit(c, s));
+        PIC_TRY(particles_push(c, s));
+    }
+    (void)iteration;
+    return PIC_OK;
+}
+
+int pic_step(pic_ctx* c, int iteration) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_TRY(pic_zero_rho(c));
+    for (int s = 0; s < c->cfg.num_species; ++s) PIC_TRY(pic_charge_deposition(c, s));
+    PIC_TRY(pic_poisson_solve(c, iteration));
+    for (int s = 0; s < c->cfg.num_species; ++s) PIC_TRY(pic_move_particles(c, s, iteration));
+    return PIC_OK;
+}
+
+int pic_get_rho(pic_ctx* c, double* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    return copy_to_host(c, host, c->rho, (size_t)c->nodes * 8);
+}
+
+int pic_get_phi(pic_ctx* c, double* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    return copy_to_host(c, host, c->phi, (size_t)c->nodes * 8);
+}
+
+int pic_get_efield(pic_ctx* c, pic_field* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    PIC_TRY(efield_export(c));
+    return copy_to_host(c, host, c->efield64, (size_t)c->nodes * 16);
+}
+
+int pic_get_final_mesh(pic_ctx* c, int s, double* host) {
+    PIC_TRY(check_species(c, s));
+    if (!host) return fail(PIC_ERR_ARG, "null output");
+    return copy_to_host(c, host, c->sp[s].final_mesh, (size_t)c->nodes * 8);
+}
+
+int pic_get_energy_mesh(pic_ctx* c, int s, double* host) {
+    PIC_TRY(check_species(c, s));
+    if (!host) return fail(PIC_ERR_ARG, "null output");
+    return copy_to_host(c, host, c->sp[s].energy_mesh, (size_t)c->nodes * 8);
+}
+
+int pic_set_rho(pic_ctx* c, const double* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    return copy_to_device(c, c->rho, host, (size_t)c->nodes * 8);
+}
+
+int pic_set_phi(pic_ctx* c, const double* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    PIC_TRY(copy_to_device(c, c->phi, host, (size_t)c->nodes * 8));
+    c->ps.have_prev = true;
+    c->fields_valid = false;
+    return PIC_OK;
+}
+
+int pic_update_fields_from_phi(pic_ctx* c) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    return fields_from_phi(c);
+}
+
+int pic_set_bz(pic_ctx* c, const double* host) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    PIC_TRY(copy_to_device(c, c->bz, host, (size_t)c->nodes * 8));
+    return fields_set_bz(c);
+}
+
+int pic_set_profiling(pic_ctx* c, int on) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    c->profiling = on != 0;
+    return PIC_OK;
+}
+
+int pic_profile_read(pic_ctx* c, double* ms, int64_t* calls, int reset) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto& p : c->prof_pending) {
+        float t = 0;
+        PIC_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+        c->prof_ms[p.phase] += t;
+        c->prof_calls[p.phase] += 1;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->prof_pending.clear();
+    for (int i = 0; i < PIC_NUM_PHASES; ++i) {
+        if (ms) ms[i] = c->prof_ms[i];
+        if (calls) calls[i] = c->prof_calls[i];
+        if (reset) {
+            c->prof_ms[i] = 0;
+            c->prof_calls[i] = 0;
+        }
+    }
+    return PIC_OK;
+}
+
+int pic_launch_count(pic_ctx* c, int64_t* n) {
+    if (!c || !n) return fail(PIC_ERR_ARG, "null argument");
+    *n = c->launches;
+    return PIC_OK;
+}
+
+int pic_set_poisson(pic_ctx* c, int solver, int warm, double tol, int maxit) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (solver != PIC_SOLVER_MG_PCG && solver != PIC_SOLVER_JACOBI_PCG)
+        return fail(PIC_ERR_ARG, "unknown solver");
+    if (warm < PIC_WARM_ZERO || warm > PIC_WARM_LEARNED) return fail(PIC_ERR_ARG, "unknown warm start");
+    if (!(tol > 0) || maxit <= 0) return fail(PIC_ERR_ARG, "tol and maxit must be positive");
+    c->ps.solver = solver;
+    c->ps.warm = warm;
+    c->ps.tol = tol;
+    c->ps.maxit = maxit;
+    return PIC_OK;
+}
+
+int pic_poisson_stats(pic_ctx* c, int* iters, double* relres, double* ms) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (iters) *iters = c->ps.last_iters;
+    if (relres) *relres = c->ps.last_relres;
+    if (ms) *ms = c->ps.last_ms;
+    return PIC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+// pic_internal.h -- shared declarations of the B200 PIC library (not part of
+// the public ABI).  Host C++17 + CUDA for sm_100a.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "pic_capi.h"
+
+namespace picb200 {
+
+// ---------------------------------------------------------------------------
+// Error plumbing
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+#define PIC_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess)                                                      \
+            return ::picb200::fail(PIC_ERR_CUDA, std::string(#call) + ": " +        \
+                                                     cudaGetErrorString(e_));       \
+    } while (0)
+
+#define PIC_TRY(call)                \
+    do {                             \
+        int s_ = (call);             \
+        if (s_ != PIC_OK) return s_; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Fixed-point deposit scales
+// ---------------------------------------------------------------------------
+// Each particle's bilinear weights are built from per-axis offsets rounded to
+// 20 bits: qx = round(fx*2^20), so the four corner weights are exact 40-bit
+// products that sum to exactly 2^40.  Node sums stay below 2^63 for up to
+// 2^23 particles touching one node.
+constexpr int kAxisBits = 20;
+constexpr double kChargeUnit = 1.0 / 1099511627776.0;  // 2^-40
+// Energy-weighted corner weights are rounded to 2^-16 eV per particle.
+constexpr double kEnergyUnit = 1.0 / 65536.0;  // 2^-16
+constexpr float kEnergyClampEv = 16777216.0f;  // 2^24 eV per particle
+// Particles per cell above which a node sum could overflow.
+constexpr uint32_t kMaxPerCell = 1u << 21;
+
+// ---------------------------------------------------------------------------
+// Particle kernel tiling
+// ---------------------------------------------------------------------------
+constexpr int kTileX = 64;  // cells per block in x
+constexpr int kTileY = 4;   // cells per block in y
+constexpr int kHalo = 1;    // mover halo (cells) kept in the shared tile
+constexpr int kWarps = 8;   // 256 threads per block
+
+struct SpeciesConsts {
+    float h;          // 0.5*(q/m)*dt
+    float dtdx, dtdy; // dt/dx, dt/dy
+    float half_inv_abs_qm;  // 0.5/|q/m| -> kinetic energy in eV
+};
+
+// Cell-sorted state of one species (one buffer of a double buffer):
+// a[i] = {fx, fy, vx, vy}, vz[i].
+struct ParticleSoA {
+    float4* a;
+    float* vz;
+};
+
+struct Species {
+    pic_species_desc desc{};
+    double ctom = 0, weighing = 0;
+    SpeciesConsts k{};
+    int64_t capacity = 0;
+    float* store = nullptr;         // 2 buffers x 5 arrays x capacity floats
+    ParticleSoA buf[2]{};
+    int cur = 0;
+    uint32_t* off = nullptr;        // [ncells+1] segment starts of buf[cur]
+    uint32_t* off_next = nullptr;   // [ncells+1] segment starts being built
+    uint32_t* stay = nullptr;       // [ncells]  stayers per cell (pass 1)
+    uint32_t* movein = nullptr;     // [ncells]  movers entering a cell (pass 1)
+    uint32_t* cursor = nullptr;     // [ncells]  mover slots handed out (pass 2)
+    unsigned long long* acc_q = nullptr;  // [nodes] fixed-point charge weights
+    unsigned long long* acc_e = nullptr;  // [nodes] fixed-point energy weights
+    double* final_mesh = nullptr;   // [nodes]
+    double* energy_mesh = nullptr;  // [nodes]
+    unsigned long long* counters = nullptr;  // [0] left exits, [1] max per cell flag
+    bool acc_fresh = false;         // acc_* hold the deposit of the current positions
+};
+
+// Multigrid level (FP32).
+struct MGLevel {
+    int nx, ny, GX, GY;
+    int64_t nodes;
+    float cx, cy, cd;  // 1/dx^2, 1/dy^2, 2(cx+cy)
+    uint8_t* mask;     // 1 = Dirichlet
+    float* x;
+    float* b;
+};
+
+struct PoissonState {
+    int solver = PIC_SOLVER_MG_PCG;
+    int warm = PIC_WARM_PREVIOUS;
+    double tol = 1e-8;
+    int maxit = 500;
+    std::vector<MGLevel> levels;
+    double* r = nullptr;
+    double* z = nullptr;
+    double* p[2] = {nullptr, nullptr};
+    double* q = nullptr;
+    double* partials = nullptr;  // per-block partial dot products
+    double* scal = nullptr;      // device scalars (see poisson.cu)
+    double* host_scal = nullptr; // pinned mirror of scal
+    int pcur = 0;
+    int nblocks = 0;
+    bool have_prev = false;
+    int last_iters = 0;
+    double last_relres = 0, last_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float* net_guess = nullptr;  // learned warm start output (nodes), optional
+};
+
+}  // namespace picb200
+
+struct pic_ctx {
+    pic_config cfg{};
+    int nx = 0, ny = 0, GX = 0, GY = 0;
+    int64_t nodes = 0, ncells = 0;
+    double dx = 0, dy = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // grids (device)
+    double* rho = nullptr;
+    double* phi = nullptr;
+    double* bz = nullptr;          // FP64 node Bz
+    float4* fld = nullptr;         // {Ex, Ey, Bz, 0} FP32 per node for the push
+    uint8_t* mask = nullptr;       // electrode nodes
+    double* dir_val = nullptr;     // electrode potential per node
+    double* efield64 = nullptr;    // interleaved FP64 E for export
+    // scratch shared by operators
+    uint32_t* scan_partials = nullptr;
+    void* staging = nullptr;       // device staging for host<->device copies
+    size_t staging_bytes = 0;
+    void* host_staging = nullptr;  // pinned host staging
+    size_t host_staging_bytes = 0;
+    picb200::Species sp[PIC_MAX_SPECIES];
+    picb200::PoissonState ps;
+    bool fields_valid = false;
+    // instrumentation
+    bool profiling = false;
+    struct ProfEvent {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfEvent> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    cudaEvent_t prof_open = nullptr;
+    double prof_ms[PIC_NUM_PHASES] = {};
+    int64_t prof_calls[PIC_NUM_PHASES] = {};
+    int64_t launches = 0;
+};
+
+namespace picb200 {
+
+// context.cu: phase timing (no-ops unless profiling is on)
+void prof_begin(pic_ctx* c, int phase);
+void prof_end(pic_ctx* c, int phase);
+
+// particles.cu
+int species_setup(pic_ctx* c, int s);
+int species_reserve(pic_ctx* c, int s, int64_t capacity);
+void species_free(Species& sp);
+// Stages n points for import; returns the device address to copy them to.
+int particles_import_staging(pic_ctx* c, int64_t n, pic_point** dev_points);
+int particles_import(pic_ctx* c, int s, int64_t n);  // points already staged
+int ensure_staging(pic_ctx* c, size_t bytes);
+int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out);
+int particles_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d);
+// raw state into 6 consecutive arrays of n entries (int32 cell, 5 floats)
+int particles_export_state(pic_ctx* c, int s, void* dev, int64_t n);
+int particles_deposit(pic_ctx* c, int s);       // fresh deposit of current positions
+int particles_flush_rho(pic_ctx* c, int s);     // acc -> final/energy mesh, rho +=
+int particles_push(pic_ctx* c, int s);          // pass1 + scan + pass2 (+deposit)
+int particles_count(pic_ctx* c, int s, int64_t* n);
+int particles_bin_counts(pic_ctx* c, int s, int32_t* dev_counts);
+
+// poisson.cu
+int poisson_setup(pic_ctx* c);
+void poisson_free(pic_ctx* c);
+int poisson_solve(pic_ctx* c);
+int fields_from_phi(pic_ctx* c);
+int efield_export(pic_ctx* c);
+int fields_set_bz(pic_ctx* c);
+
+}  // namespace picb200

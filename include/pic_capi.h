@@ -1,0 +1,226 @@
+/*
+ * pic_capi.h -- C ABI of the B200-native 2D electrostatic PIC step.
+ *
+ * Drop-in for the operator surface of SYCL-PIC-poissonsolver
+ * (vansh268p/BMP-6th-sem), SYCL-PIC-poissonsolver/src/sycl_pic_ctypes.cpp:46-272:
+ * cell binning, CIC charge deposition, field gather + Boris push and the
+ * Poisson solve on the geometry.conf electrode mesh.  Plain C types only:
+ * pointers, sizes, status codes.  All device memory is owned by the library.
+ *
+ * Two surfaces:
+ *   1. pic_* -- context-handle API.  One pic_ctx per simulation instance;
+ *      operators enqueue work on the context's CUDA stream and return a
+ *      status code (0 ok, negative = PIC_ERR_*).  pic_last_error() gives the
+ *      message of the most recent failure on the calling thread.
+ *   2. sycl_pic_* -- the reference's own names and signatures, backed by one
+ *      process-global context, synchronous, returning elapsed wall seconds
+ *      exactly as the reference does.  They return -1.0 (or -1 / NULL) where
+ *      the reference would have called exit(); the reason is in
+ *      pic_last_error().
+ *
+ * Array layouts at the boundary are the reference's:
+ *   - particles: pic_point AoS, 56 B (include/point.hpp:11-14);
+ *   - grids: row-major [GRID_Y][GRID_X] double, GRID_X = NX+1, GRID_Y = NY+1
+ *     (src/particles.cpp:357-368, 728-734);
+ *   - electric field: interleaved pic_field {fx, fy} per node
+ *     (include/point.hpp:16-19).
+ * Inside the library particles are cell-sorted SoA (int cell implied by the
+ * sort, FP32 in-cell offsets, FP32 velocities); see pic_import_points.
+ */
+#ifndef PIC_CAPI_H
+#define PIC_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC_CAPI_VERSION 1
+#define PIC_MAX_SPECIES 4
+#define PIC_MAX_RECTS 32
+
+/* ---- status codes ------------------------------------------------------ */
+#define PIC_OK 0
+#define PIC_ERR_ARG (-1)           /* bad argument (null pointer, bad species, size) */
+#define PIC_ERR_CONFIG (-2)        /* invalid configuration or input file          */
+#define PIC_ERR_CAPACITY (-3)      /* particle buffer or fixed-point range exceeded */
+#define PIC_ERR_NOT_CONVERGED (-4) /* Poisson solve hit its iteration limit         */
+#define PIC_ERR_CUDA (-5)          /* CUDA runtime error                            */
+#define PIC_ERR_STATE (-6)         /* operator called in the wrong state            */
+#define PIC_ERR_IO (-7)            /* file could not be read or written             */
+#define PIC_ERR_NO_DEVICE (-8)     /* no usable sm_100 device                       */
+#define PIC_ERR_TIMEOUT (-9)       /* a bounded device wait gave up                 */
+
+/* ---- boundary record types (reference layouts) ------------------------- */
+
+/* Point, SYCL-PIC-poissonsolver/include/point.hpp:11-14.  z is not tracked
+ * by the library (no reference computation reads it); export writes z=0.
+ * pointer: -1 marks a dead particle on import; export writes the particle's
+ * position in the cell-sorted order. */
+typedef struct pic_point {
+    double x, y, z, vx, vy, vz;
+    int32_t pointer;
+    int32_t pad_;
+} pic_point;
+
+/* Field, include/point.hpp:16-19. */
+typedef struct pic_field {
+    double fx, fy;
+} pic_field;
+
+/* Geometry, include/point.hpp:21-24: inclusive node-index rectangle held at
+ * `potential` volts (readGeometry converts geometry.conf fractions with
+ * (int)((GRID-1)*fraction), src/particles.cpp:677-681). */
+typedef struct pic_rect {
+    int32_t x1, y1, x2, y2;
+    double potential;
+} pic_rect;
+
+/* One row of M_PICDAT.DAT's species table (src/particles.cpp:590-608). */
+typedef struct pic_species_desc {
+    double charge;       /* C, with sign                            */
+    double mass;         /* kg                                      */
+    double sim_count;    /* "SimulationParticles" (weight formula)  */
+    double actual_count; /* "ActualParticles"                       */
+} pic_species_desc;
+
+#define PIC_SOLVER_MG_PCG 0     /* geometric-multigrid-preconditioned CG */
+#define PIC_SOLVER_JACOBI_PCG 1 /* plain path: diagonal-preconditioned CG */
+
+#define PIC_WARM_ZERO 0     /* start every solve from phi = 0             */
+#define PIC_WARM_PREVIOUS 1 /* start from the previous step's phi          */
+#define PIC_WARM_LEARNED 2  /* start from the conv network's prediction    */
+
+typedef struct pic_config {
+    int32_t nx, ny;       /* cells; nodes are (nx+1) x (ny+1)             */
+    double xmax, ymax;    /* domain size (m); dx = xmax/nx, dy = ymax/ny  */
+    double dt;            /* s                                            */
+    double epsilon;       /* F/m                                          */
+    double b0;            /* uniform Bz (T) (initMagneticField)           */
+    double surf_area;     /* m^2 for the weight formula; 0 -> xmax*ymax   */
+    int32_t num_species;
+    pic_species_desc species[PIC_MAX_SPECIES];
+    int32_t num_rects;    /* electrode rectangles, applied in order       */
+    pic_rect rects[PIC_MAX_RECTS];
+    int32_t poisson_solver;   /* PIC_SOLVER_*                              */
+    int32_t warm_start;       /* PIC_WARM_*                                */
+    double poisson_tol;       /* relative residual target, default 1e-8   */
+    int32_t poisson_maxit;    /* default 500                               */
+    int32_t deposit_energy;   /* 1: also build the energy mesh (default)   */
+    int32_t device;           /* CUDA device ordinal                       */
+    int32_t timesteps;        /* informational (M_PICDAT TIMESTEPS)        */
+    int32_t print_interval;   /* informational (M_PICDAT printInterval)    */
+} pic_config;
+
+/* Uniform Maxwellian plasma plus an optional Gaussian blob, generated on the
+ * device with Philox-4x32-10 (counter = particle id, key = seed).  Cell c gets
+ * ppc background particles and floor(blob_peak_ppc*exp(-r^2/(2 sigma^2)) + u)
+ * blob particles (u uniform per cell), r measured in cells from the blob
+ * centre.  Velocities: per-component sigma = sqrt(e*T/m); blob particles add
+ * (drift_vx, drift_vy). */
+typedef struct pic_plasma_desc {
+    int32_t ppc;              /* background particles per cell             */
+    double temperature_ev;
+    double blob_peak_ppc;     /* 0 -> no blob                              */
+    double blob_cx, blob_cy;  /* blob centre in cell units                 */
+    double blob_sigma;        /* cells                                     */
+    double drift_vx, drift_vy;/* m/s, blob particles only                  */
+    uint64_t seed;
+} pic_plasma_desc;
+
+typedef struct pic_ctx pic_ctx;
+
+/* ---- lifetime ---------------------------------------------------------- */
+const char* pic_last_error(void);
+const char* pic_status_string(int status);
+int pic_config_default(pic_config* cfg);
+/* Reads M_PICDAT.DAT + geometry.conf (readPICDAT src/particles.cpp:308-633,
+ * readGeometry :636-686) into a config.  Species counts come from the file. */
+int pic_config_from_files(const char* picdat_path, const char* geometry_path, pic_config* cfg);
+int pic_create(const pic_config* cfg, pic_ctx** out);
+void pic_destroy(pic_ctx* ctx);
+/* Run the context on a caller-owned cudaStream_t (NULL -> library stream). */
+int pic_set_stream(pic_ctx* ctx, void* cuda_stream);
+void* pic_get_stream(pic_ctx* ctx);
+int pic_synchronize(pic_ctx* ctx);
+
+/* ---- particles --------------------------------------------------------- */
+int pic_reserve(pic_ctx* ctx, int species, int64_t capacity);
+/* Replace a species' particles with n host Points (reference AoS).  The cell
+ * is (int)(x*(1/dx)), (int)(y*(1/dy)) as in InsertKernel
+ * (src/particles.cpp:230-235); the FP32 offset is the FP64 remainder.
+ * Dead (pointer == -1) or out-of-domain points are dropped. */
+int pic_import_points(pic_ctx* ctx, int species, const pic_point* host, int64_t n);
+int pic_export_points(pic_ctx* ctx, int species, pic_point* host, int64_t capacity,
+                      int64_t* n_out);
+/* The internal cell-sorted state, unconverted: cell index (gy*nx + gx),
+ * FP32 offsets and velocities, in storage order.  Each output array holds
+ * `capacity` entries; *n_out receives the particle count (all pointers NULL:
+ * size query).  No reference counterpart: it exposes the library's own
+ * layout for exact checks. */
+int pic_export_state(pic_ctx* ctx, int species, int32_t* cell, float* fx, float* fy, float* vx,
+                     float* vy, float* vz, int64_t capacity, int64_t* n_out);
+int pic_load_plasma(pic_ctx* ctx, int species, const pic_plasma_desc* desc);
+int pic_particle_count(pic_ctx* ctx, int species, int64_t* n_out);
+/* Live particles per bucket, indexed like the reference's key_idx
+ * (gy*GRID_X + gx, GRID_X*GRID_Y entries). */
+int pic_bin_counts(pic_ctx* ctx, int species, int32_t* host_counts);
+/* Particles that left through x < 0 since the last call (new_additions,
+ * src/mover.cpp:344-351); the counter is reset by the read. */
+int pic_left_exits(pic_ctx* ctx, int species, int64_t* n_out);
+
+/* ---- step operators (reference order, src/main.cpp:130-257) ------------ */
+int pic_zero_rho(pic_ctx* ctx);
+int pic_charge_deposition(pic_ctx* ctx, int species);
+int pic_poisson_solve(pic_ctx* ctx, int iteration);
+int pic_move_particles(pic_ctx* ctx, int species, int iteration);
+int pic_compact_particles(pic_ctx* ctx, int species); /* no-op: the sort compacts */
+int pic_cleanup_map(pic_ctx* ctx, int species);       /* no-op: no hashmap       */
+/* zero_rho, deposit every species, Poisson, E, push every species. */
+int pic_step(pic_ctx* ctx, int iteration);
+/* bin + deposit + push for every species, with the E field held fixed. */
+int pic_particle_phase(pic_ctx* ctx, int iteration);
+
+/* ---- grids (host copies in the reference layout) ------------------------ */
+int pic_get_rho(pic_ctx* ctx, double* host);
+int pic_get_phi(pic_ctx* ctx, double* host);
+int pic_get_efield(pic_ctx* ctx, pic_field* host);
+int pic_get_final_mesh(pic_ctx* ctx, int species, double* host);
+int pic_get_energy_mesh(pic_ctx* ctx, int species, double* host);
+int pic_set_rho(pic_ctx* ctx, const double* host);
+int pic_set_phi(pic_ctx* ctx, const double* host);
+/* E from phi (calculateElectricField, src/poissonSolver.cpp:433-456); the
+ * reference Python extension's update_fields_from_phi
+ * (src/sycl_pic_module.cpp:216-223). */
+int pic_update_fields_from_phi(pic_ctx* ctx);
+int pic_set_bz(pic_ctx* ctx, const double* host);
+
+/* ---- instrumentation (no reference counterpart; the reference returns
+ * host wall seconds per operator, src/sycl_pic_ctypes.cpp:127-236) ------- */
+#define PIC_PHASE_PUSH_COUNT 0   /* pass 1: push + per-cell counts          */
+#define PIC_PHASE_SCAN 1         /* exclusive scan of the new cell counts    */
+#define PIC_PHASE_PUSH_SCATTER 2 /* pass 2: push + scatter + fused deposit   */
+#define PIC_PHASE_DEPOSIT 3      /* stand-alone deposit of current positions */
+#define PIC_PHASE_FLUSH 4        /* accumulators -> final/energy mesh, rho   */
+#define PIC_PHASE_POISSON 5      /* whole Poisson solve incl. E field        */
+#define PIC_NUM_PHASES 6
+/* When on, CUDA events bracket every phase on the context stream. */
+int pic_set_profiling(pic_ctx* ctx, int on);
+/* Synchronises, returns accumulated device milliseconds and calls per phase. */
+int pic_profile_read(pic_ctx* ctx, double* ms, int64_t* calls, int reset);
+/* Kernel launches issued by this context since creation. */
+int pic_launch_count(pic_ctx* ctx, int64_t* n);
+
+/* ---- Poisson controls -------------------------------------------------- */
+int pic_set_poisson(pic_ctx* ctx, int solver, int warm_start, double tol, int maxit);
+/* Iterations, achieved relative residual and device milliseconds of the most
+ * recent solve. */
+int pic_poisson_stats(pic_ctx* ctx, int* iterations, double* relres, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIC_CAPI_H */

@@ -1,0 +1,191 @@
+"""CPU-only checks of the C ABI: the library loads, exports every symbol the
+headers declare, validates configurations and reads the reference's input
+file formats -- no compute call, no GPU."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+PICDAT = """---------------------------------------------------------------------------------------------
+TIMESTEPS
+{steps}
+---------------------------------------------------------------------------------------------
+XMAX(m)		YMAX(m)		NX		NY
+{xmax}		{ymax}			{nx}		{ny}
+---------------------------------------------------------------------------------------------
+dt(s)
+{dt}
+---------------------------------------------------------------------------------------------
+B0(mT)		sigma(m)		BMAX(fraction)
+{b0mt}	0.02			0.7
+---------------------------------------------------------------------------------------------
+Te(eV)		Ti(eV)			Tg(K)
+2 		0.026			300
+---------------------------------------------------------------------------------------------
+Gas Pressure(P)
+0.1
+---------------------------------------------------------------------------------------------
+Uniform Initialization Flag (1-uniformly 0-uniformly within below fraction)
+{uniform}
+---------------------------------------------------------------------------------------------
+XX1				XX2			YY1			YY2
+0.25		0.75		0.00		0.5
+---------------------------------------------------------------------------------------------
+Re-injection Flag(1-reinject 0-do not reinject)
+0
+---------------------------------------------------------------------------------------------
+Scale factor
+1
+---------------------------------------------------------------------------------------------
+initParticleFlag (1-randomly 0-file)
+electron initialization text line
+ion initialization text line
+1
+---------------------------------------------------------------------------------------------
+Epsilon(epsilon = epsilon_0 * epsilon_r)(F/m)
+8.854e-12
+---------------------------------------------------------------------------------------------
+Periodic Boundary Flag (0 - non periodic, 1 - periodic)
+{periodic}
+---------------------------------------------------------------------------------------------
+Name of the simulation gas
+Ar
+---------------------------------------------------------------------------------------------
+Attachment Factor
+2
+---------------------------------------------------------------------------------------------
+Collision Flag (0 - Collision off, 1 - Collision On)
+0
+---------------------------------------------------------------------------------------------
+powerMode (0 - No heating, 3 - Forced heating, 2 - self consistent)		Heat Frequency(Hz)		power (Watt)
+0               1e8           0.2
+---------------------------------------------------------------------------------------------
+Print after every 'n' time steps. Provide 'n' below.
+{pint}
+---------------------------------------------------------------------------------------------
+START print spaceavg 			END print spaceavg
+10			20
+---------------------------------------------------------------------------------------------
+No of species
+2
+---------------------------------------------------------------------------------------------
+1-electron,2-positiveIon,3-negativeIon
+speciesId	SimulationParticles		ActualParticles		Charge(with sign)		Mass
+1			4e4						1e15		-1.602e-19				9.109e-31
+2			4e4						1e15		1.602e-19					6.6335e-26
+---------------------------------------------------------------------------------------------
+"""
+
+GEOMETRY = """----------------------------------------------
+ NDOM (number of rectangles; fractions of the domain)
+  5
+----------------------------------------------
+ x1     z1      x2      z2       VDOM
+  0.     0.      0.      1.       100.
+  1.     0.      1.      1.       0.
+  0.     1.      1.      1.       0.
+  0.     0.      1.      0.       0.
+  0.46875 0.46875 0.53125 0.53125 200.
+ ----------------------------------------------
+"""
+
+
+def test_library_exports_every_declared_symbol(picb):
+    L = picb.lib()
+    syms = picb.exported_symbols()
+    assert len(syms) > 40
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_config_default(picb):
+    cfg = picb.Config()
+    assert picb.lib().pic_config_default(ctypes.byref(cfg)) == 0
+    assert cfg.poisson_tol == 1e-8 and cfg.deposit_energy == 1
+    assert cfg.warm_start == picb.WARM_PREVIOUS
+
+
+def _write_inputs(tmp_path, **kw):
+    vals = dict(steps=7, xmax=0.064, ymax=0.032, nx=256, ny=128, dt=5e-11, b0mt=10.0, uniform=1,
+                periodic=0, pint=5)
+    vals.update(kw)
+    p = tmp_path / "M_PICDAT.DAT"
+    p.write_text(PICDAT.format(**vals))
+    g = tmp_path / "geometry.conf"
+    g.write_text(GEOMETRY)
+    return str(p), str(g)
+
+
+def test_config_from_reference_files(picb, tmp_path):
+    p, g = _write_inputs(tmp_path)
+    cfg = picb.Config()
+    st = picb.lib().pic_config_from_files(p.encode(), g.encode(), ctypes.byref(cfg))
+    assert st == 0, picb.lib().pic_last_error()
+    assert (cfg.nx, cfg.ny) == (256, 128)
+    assert cfg.xmax == 0.064 and cfg.dt == 5e-11
+    assert np.isclose(cfg.b0, 0.01)                      # mT -> T
+    assert cfg.num_species == 2 and cfg.species[1].mass == 6.6335e-26
+    assert cfg.species[0].charge == -1.602e-19 and cfg.species[0].sim_count == 4e4
+    assert np.isclose(cfg.surf_area, 0.064 * 0.032)
+    assert cfg.timesteps == 7 and cfg.print_interval == 5
+    assert cfg.num_rects == 5
+    r = cfg.rects[4]
+    # (int)((GRID-1)*fraction), src/particles.cpp:677-681
+    assert (r.x1, r.y1, r.x2, r.y2) == (int(256 * 0.46875), int(128 * 0.46875),
+                                        int(256 * 0.53125), int(128 * 0.53125))
+    assert r.potential == 200.0
+    assert (cfg.rects[0].x1, cfg.rects[0].x2, cfg.rects[0].y2) == (0, 0, 128)
+
+
+def test_config_box_init_surface_area(picb, tmp_path):
+    p, g = _write_inputs(tmp_path, uniform=0)
+    cfg = picb.Config()
+    assert picb.lib().pic_config_from_files(p.encode(), g.encode(), ctypes.byref(cfg)) == 0
+    # surfArea = (XX2-XX1)*W*(YY2-YY1)*H, src/particles.cpp:432
+    assert np.isclose(cfg.surf_area, 0.5 * 0.064 * 0.5 * 0.032)
+
+
+def test_config_rejects_periodic_and_missing_files(picb, tmp_path):
+    p, g = _write_inputs(tmp_path, periodic=1)
+    cfg = picb.Config()
+    assert picb.lib().pic_config_from_files(p.encode(), g.encode(), ctypes.byref(cfg)) == -2
+    assert picb.lib().pic_config_from_files(b"/nonexistent", g.encode(), ctypes.byref(cfg)) == -7
+
+
+def test_create_validates_before_touching_a_device(picb):
+    import pic_configs as C
+    w = C.cfg1()
+    cfg = C.library_config(w)
+    h = ctypes.c_void_p()
+    bad = C.library_config(w)
+    bad.nx = 2
+    assert picb.lib().pic_create(ctypes.byref(bad), ctypes.byref(h)) == -2
+    open_wall = C.library_config(w)
+    open_wall.num_rects = 3  # bottom wall missing: generateCoeffs needs every wall node fixed
+    assert picb.lib().pic_create(ctypes.byref(open_wall), ctypes.byref(h)) == -2
+    assert b"wall" in picb.lib().pic_last_error()
+    outside = C.library_config(w)
+    outside.rects[0].x2 = 500
+    assert picb.lib().pic_create(ctypes.byref(outside), ctypes.byref(h)) == -2
+
+
+@pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="a GPU is present")
+def test_create_without_gpu_fails_cleanly(picb):
+    import pic_configs as C
+    cfg = C.library_config(C.cfg1())
+    h = ctypes.c_void_p()
+    assert picb.lib().pic_create(ctypes.byref(cfg), ctypes.byref(h)) == -8
+    assert not h.value
+
+
+def test_compat_surface_before_init(picb):
+    L = picb.lib()
+    L.sycl_pic_get_rho_ptr.restype = ctypes.c_void_p
+    L.sycl_pic_charge_deposition.restype = ctypes.c_double
+    L.sycl_pic_charge_deposition.argtypes = [ctypes.c_int]
+    L.sycl_pic_generate_new_particles.restype = ctypes.c_double
+    assert L.sycl_pic_get_rho_ptr() is None
+    assert L.sycl_pic_charge_deposition(0) == -1.0
+    assert L.sycl_pic_get_grid_size() == -1
+    assert L.sycl_pic_generate_new_particles() == -1.0
