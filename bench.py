@@ -247,7 +247,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     w = workload(args.config)
     pic = P.Pic(C.library_config(w, device=local_rank))
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) torch stream: the library runs on it and the
+    # CUDA events below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     pic.set_stream(stream.cuda_stream)
     C.load_plasma(pic, w, seed=1234 + 7 * rank)
     counts = [pic.count(s) for s in range(2)]
@@ -313,12 +316,12 @@ def run_ours(args, rank, world, local_rank):
     L.pic_set_profiling(pic.h, 1)
     ms6 = (ctypes.c_double * P_PHASES)()
     calls6 = (ctypes.c_int64 * P_PHASES)()
-    L.pic_profile_read(pic.h, ms6, calls6, 1)
+    L.pic_profile_read(pic.h, ctypes.cast(ms6, ctypes.c_void_p), ctypes.cast(calls6, ctypes.c_void_p), 1)
     prof_steps = 3
     for _ in range(prof_steps):
         pic.step(it)
         it += 1
-    L.pic_profile_read(pic.h, ms6, calls6, 1)
+    L.pic_profile_read(pic.h, ctypes.cast(ms6, ctypes.c_void_p), ctypes.cast(calls6, ctypes.c_void_p), 1)
     L.pic_set_profiling(pic.h, 0)
     phase_names = ["push_count", "scan", "push_scatter", "deposit", "flush", "poisson"]
     phases = {phase_names[i]: {"ms_per_step": ms6[i] / prof_steps, "calls_per_step": calls6[i] / prof_steps}

@@ -154,9 +154,9 @@ __device__ __forceinline__ float energy_ev(float vx, float vy, float vz, float h
     return fminf(__fmul_rn(v2, half_inv_abs_qm), kEnergyClampEv);
 }
 
-// Energy-weighted corner weight in units of 2^-16 eV: en * q/2^40 * 2^16.
+// Energy-weighted corner weight in units of 2^-24 eV: en * q/2^40 * 2^24.
 __device__ __forceinline__ unsigned long long energy_fixed(float en, unsigned long long q) {
-    return __float2ull_rn(__fmul_rn(en, __fmul_rn((float)q, 0x1p-24f)));
+    return __float2ull_rn(__fmul_rn(en, __fmul_rn((float)q, 0x1p-16f)));
 }
 
 __device__ __forceinline__ void tile_add(unsigned long long* tq, unsigned long long* te, int tx,
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
             const bool mover = valid && p.alive && !stay;
             const unsigned sm = __ballot_sync(kFull, stay);
             const unsigned mm = __ballot_sync(kFull, mover);
-            if (MODE != kDeposit) {
+            if (MODE == kScatter) {
                 const unsigned lm = __ballot_sync(kFull, valid && !p.alive && p.left);
                 left_exits += __popc(lm);
             }
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
             }
         }
     }
-    if (MODE != kDeposit && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
+    if (MODE == kScatter && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
     if (kDep) {
         __syncthreads();
         for (int i = threadIdx.x; i < kNTX * kNTY; i += kThreads) {
@@ -724,6 +724,8 @@ void species_free(Species& sp) {
 int species_reserve(pic_ctx* c, int s, int64_t capacity) {
     Species& sp = c->sp[s];
     if (capacity <= sp.capacity) return PIC_OK;
+    // multiples of 64 particles keep both buffers' float4 arrays 256-byte aligned
+    capacity = (capacity + 63) & ~(int64_t)63;
     if (capacity > (int64_t)0xF0000000ll)
         return fail(PIC_ERR_CAPACITY, "a species holds at most 4.0e9 particles (32-bit offsets)");
     int64_t live = 0;

@@ -41,11 +41,13 @@ int fail(int status, const std::string& msg);
 // 2^23 particles touching one node.
 constexpr int kAxisBits = 20;
 constexpr double kChargeUnit = 1.0 / 1099511627776.0;  // 2^-40
-// Energy-weighted corner weights are rounded to 2^-16 eV per particle.
-constexpr double kEnergyUnit = 1.0 / 65536.0;  // 2^-16
-constexpr float kEnergyClampEv = 16777216.0f;  // 2^24 eV per particle
-// Particles per cell above which a node sum could overflow.
-constexpr uint32_t kMaxPerCell = 1u << 21;
+// Energy-weighted corner weights are rounded to 2^-24 eV; a particle's energy
+// is clamped at 2^20 eV (1 MeV), so one contribution stays below 2^44.
+constexpr double kEnergyUnit = 1.0 / 16777216.0;  // 2^-24
+constexpr float kEnergyClampEv = 1048576.0f;       // 2^20 eV per particle
+// Particles per cell above which a node sum could overflow (4 cells touch a
+// node: 2^18 contributions of < 2^44 stay below 2^62).
+constexpr uint32_t kMaxPerCell = 1u << 16;
 
 // ---------------------------------------------------------------------------
 // Particle kernel tiling

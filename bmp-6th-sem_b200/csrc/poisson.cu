@@ -568,63 +568,85 @@ int poisson_solve(pic_ctx* c) {
     }
     float* r32 = ps.levels[0].b;
     float* z32 = ps.levels[0].x;
-    k_pcg_setup<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->dir_val, c->rho, c->phi, ps.r,
-                                                   r32, ps.partials, nb, arrive, ps.scal);
-    k_fix_bb<<<1, 1, 0, c->stream>>>(ps.scal);
-    c->launches += 4;  // overwrite, setup, fix, true residual
-    PIC_CUDA(cudaGetLastError());
-    PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost,
-                             c->stream));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    // r = b - A x, ||r||^2 and ||b_red||^2 into the device scalars
+    auto setup = [&]() -> int {
+        k_pcg_setup<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->dir_val, c->rho, c->phi,
+                                                       ps.r, r32, ps.partials, nb, arrive, ps.scal);
+        k_fix_bb<<<1, 1, 0, c->stream>>>(ps.scal);
+        c->launches += 2;
+        PIC_CUDA(cudaGetLastError());
+        PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        return PIC_OK;
+    };
+    PIC_TRY(setup());
+    c->launches += 1;  // overwrite
     const double bb = ps.host_scal[S_BB];
     double rr = ps.host_scal[S_RR];
     const double target = ps.tol * ps.tol * bb;
-    int it = 0;
+    int it = 0, restarts = 0;
     int status = PIC_OK;
     const bool jacobi = ps.solver == PIC_SOLVER_JACOBI_PCG;
-    while (rr > target && bb > 0) {
-        if (it >= ps.maxit) {
-            status = PIC_ERR_NOT_CONVERGED;
-            break;
+    double true_rr = rr;
+    for (;;) {
+        bool first = true;
+        while (rr > target && bb > 0) {
+            if (it >= ps.maxit) {
+                status = PIC_ERR_NOT_CONVERGED;
+                break;
+            }
+            if (!jacobi) PIC_TRY(vcycle(c));
+            k_pcg_rz<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, ps.r, z32, 1.0 / g.cd,
+                                                        jacobi ? 1 : 0, ps.z, ps.partials, nb,
+                                                        arrive, ps.scal);
+            double* p_old = ps.p[ps.pcur];
+            double* p_new = ps.p[ps.pcur ^ 1];
+            k_pcg_p_ap<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, ps.z, p_old, p_new, ps.q,
+                                                          first ? 1 : 0, ps.partials, nb, arrive,
+                                                          ps.scal);
+            ps.pcur ^= 1;
+            k_pcg_update<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, p_new, ps.q, c->phi,
+                                                            ps.r, r32, ps.partials, nb, arrive,
+                                                            ps.scal);
+            k_shift_rz<<<1, 1, 0, c->stream>>>(ps.scal);
+            c->launches += 4;
+            PIC_CUDA(cudaGetLastError());
+            PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_RR, ps.scal + S_RR, sizeof(double),
+                                     cudaMemcpyDeviceToHost, c->stream));
+            PIC_CUDA(cudaStreamSynchronize(c->stream));
+            rr = ps.host_scal[S_RR];
+            first = false;
+            ++it;
+            if (!std::isfinite(rr)) {
+                status = PIC_ERR_NOT_CONVERGED;
+                break;
+            }
         }
-        if (!jacobi) PIC_TRY(vcycle(c));
-        k_pcg_rz<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, ps.r, z32, 1.0 / g.cd,
-                                                    jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive,
-                                                    ps.scal);
-        double* p_old = ps.p[ps.pcur];
-        double* p_new = ps.p[ps.pcur ^ 1];
-        k_pcg_p_ap<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, ps.z, p_old, p_new, ps.q,
-                                                      it == 0 ? 1 : 0, ps.partials, nb, arrive,
-                                                      ps.scal);
-        ps.pcur ^= 1;
-        k_pcg_update<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, p_new, ps.q, c->phi, ps.r,
-                                                        r32, ps.partials, nb, arrive, ps.scal);
-        k_shift_rz<<<1, 1, 0, c->stream>>>(ps.scal);
-        c->launches += 4;
-        PIC_CUDA(cudaGetLastError());
-        PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_RR, ps.scal + S_RR, sizeof(double),
+        // the recursively updated residual can drift from b - A x: check the
+        // true residual and restart from the current iterate if it is above
+        // the target
+        k_true_residual<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->rho, c->phi, ps.partials,
+                                                           nb, arrive, ps.scal);
+        c->launches += 1;
+        PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_TRUE_RR, ps.scal + S_TRUE_RR, sizeof(double),
                                  cudaMemcpyDeviceToHost, c->stream));
         PIC_CUDA(cudaStreamSynchronize(c->stream));
+        true_rr = ps.host_scal[S_TRUE_RR];
+        if (status != PIC_OK || bb <= 0 || true_rr <= target || restarts >= 3) break;
+        ++restarts;
+        PIC_TRY(setup());
         rr = ps.host_scal[S_RR];
-        ++it;
-        if (!std::isfinite(rr)) {
-            status = PIC_ERR_NOT_CONVERGED;
-            break;
-        }
     }
-    k_true_residual<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->rho, c->phi, ps.partials, nb,
-                                                       arrive, ps.scal);
     PIC_TRY(fields_from_phi(c));
     prof_end(c, PIC_PHASE_POISSON);
     PIC_CUDA(cudaEventRecord(ps.ev1, c->stream));
-    PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_TRUE_RR, ps.scal + S_TRUE_RR, sizeof(double),
-                             cudaMemcpyDeviceToHost, c->stream));
     PIC_CUDA(cudaStreamSynchronize(c->stream));
     float ms = 0;
     PIC_CUDA(cudaEventElapsedTime(&ms, ps.ev0, ps.ev1));
     ps.last_ms = ms;
     ps.last_iters = it;
-    ps.last_relres = bb > 0 ? std::sqrt(ps.host_scal[S_TRUE_RR] / bb) : 0.0;
+    ps.last_relres = bb > 0 ? std::sqrt(true_rr / bb) : 0.0;
     ps.have_prev = true;
     if (status != PIC_OK)
         return fail(status, "Poisson PCG did not reach the tolerance within poisson_maxit");
