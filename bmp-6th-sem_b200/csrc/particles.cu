@@ -55,9 +55,13 @@ constexpr float kAxisScale = (float)(1u << kAxisBits);
 constexpr float kOneBelow = 0x1.fffffep-1f;   // largest float < 1
 
 enum Mode { kCount = 0, kScatter = 1, kDeposit = 2 };
+constexpr int kDirs = 9;      // 3x3 neighbourhood, d = (sy+1)*3 + (sx+1)
+constexpr int kStay = 4;      // d of a particle that keeps its cell
+constexpr int kFar = 9;       // moved more than one cell in x or y
 
 struct KArgs {
     int nx, ny, GX;
+    int64_t ncells;
     SpeciesConsts k;
     const float4* __restrict__ fld;
     const float4* __restrict__ src_a;
@@ -65,10 +69,10 @@ struct KArgs {
     float4* __restrict__ dst_a;
     float* __restrict__ dst_vz;
     const uint32_t* __restrict__ off;
-    const uint32_t* __restrict__ off_next;
-    uint32_t* stay;
-    uint32_t* movein;
-    uint32_t* cursor;
+    uint32_t* dcount;   // [9][ncells]
+    const uint32_t* __restrict__ sub;  // [10][ncells]
+    uint32_t* farin;
+    uint32_t* farcur;
     unsigned long long* acc_q;
     unsigned long long* acc_e;
     unsigned long long* counters;  // [0] left exits, [1] cell overflow, [2] scatter guard
@@ -86,7 +90,8 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 struct Pushed {
     float fx, fy, vx, vy;
     int gx, gy;
-    bool alive, left;
+    int dir;  // 0..8 near (4 = same cell), kFar, or -1 when absorbed
+    bool left;
 };
 
 // Bilinear gather of E and Bz from the cell's four nodes plus the Boris push
@@ -121,30 +126,65 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     const float ngx = __fadd_rn((float)gx, sx), ngy = __fadd_rn((float)gy, sy);
     // Absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H).  Written so
     // that NaN lands outside.
-    o.alive = (ngx >= 0.0f) && (ngx < (float)nx) && (ngy >= 0.0f) && (ngy < (float)ny);
+    const bool alive = (ngx >= 0.0f) && (ngx < (float)nx) && (ngy >= 0.0f) && (ngy < (float)ny);
     o.left = !(ngx >= 0.0f);
-    o.gx = o.alive ? (int)ngx : 0;
-    o.gy = o.alive ? (int)ngy : 0;
+    o.gx = alive ? (int)ngx : gx;
+    o.gy = alive ? (int)ngy : gy;
+    const int ix = o.gx - gx, iy = o.gy - gy;
+    o.dir = !alive ? -1 : ((ix < -1 || ix > 1 || iy < -1 || iy > 1) ? kFar : (iy + 1) * 3 + (ix + 1));
     o.fx = fminf(__fsub_rn(px, sx), kOneBelow);
     o.fy = fminf(__fsub_rn(py, sy), kOneBelow);
     return o;
 }
 
+// round(f * 2^20) for f in [0, 1): exact scaling, then the 1.5*2^23 addition
+// rounds to nearest-even in the mantissa (integer ALU, no conversion unit).
+__device__ __forceinline__ uint32_t axis_fixed(float f) {
+    const float t = __fadd_rn(__fmul_rn(f, kAxisScale), 12582912.0f);
+    return __float_as_uint(t) - 0x4B400000u;
+}
+
 // Fixed-point corner weights of a particle at offsets (fx, fy): exact 40-bit
-// products summing to 2^40.
+// products summing to exactly 2^40; e_* are the energy-weighted weights in
+// units of 2^-24 eV (en * q/2^40 * 2^24, rounded half up).
 struct Weights {
     unsigned long long q00, q10, q01, q11;
+    unsigned long long e00, e10, e01, e11;
 };
 
-__device__ __forceinline__ Weights fixed_weights(float fx, float fy) {
-    const uint32_t ax = __float2uint_rn(__fmul_rn(fx, kAxisScale));
-    const uint32_t ay = __float2uint_rn(__fmul_rn(fy, kAxisScale));
+// (m * w) >> sh with round-half-up, sh in [19, 165]; m*w < 2^64.
+__device__ __forceinline__ unsigned long long shr_round(unsigned long long v, int sh) {
+    if (sh > 64) return 0ull;
+    if (sh == 64) return v >> 63;
+    return (v >> sh) + ((v >> (sh - 1)) & 1ull);
+}
+
+template <bool ENERGY>
+__device__ __forceinline__ Weights fixed_weights(float fx, float fy, float en) {
+    const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
     const uint32_t bx = kAxisOne - ax, by = kAxisOne - ay;
     Weights w;
     w.q00 = (unsigned long long)bx * by;
     w.q10 = (unsigned long long)ax * by;
     w.q01 = (unsigned long long)bx * ay;
     w.q11 = (unsigned long long)ax * ay;
+    if (ENERGY) {
+        // en = man * 2^(ex-150) (en >= 0, <= 2^20): e = man*qx*qy >> (166-ex)
+        const uint32_t bits = __float_as_uint(en);
+        int ex = (int)(bits >> 23);
+        uint32_t man = bits & 0x7FFFFFu;
+        if (ex) man |= 0x800000u;
+        else ex = 1;
+        const int sh = 166 - ex;
+        const unsigned long long ma = (unsigned long long)man * ax;
+        const unsigned long long mb = (unsigned long long)man * bx;
+        w.e00 = shr_round(mb * by, sh);
+        w.e10 = shr_round(ma * by, sh);
+        w.e01 = shr_round(mb * ay, sh);
+        w.e11 = shr_round(ma * ay, sh);
+    } else {
+        w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
+    }
     return w;
 }
 
@@ -154,13 +194,8 @@ __device__ __forceinline__ float energy_ev(float vx, float vy, float vz, float h
     return fminf(__fmul_rn(v2, half_inv_abs_qm), kEnergyClampEv);
 }
 
-// Energy-weighted corner weight in units of 2^-24 eV: en * q/2^40 * 2^24.
-__device__ __forceinline__ unsigned long long energy_fixed(float en, unsigned long long q) {
-    return __float2ull_rn(__fmul_rn(en, __fmul_rn((float)q, 0x1p-16f)));
-}
-
 __device__ __forceinline__ void tile_add(unsigned long long* tq, unsigned long long* te, int tx,
-                                         int ty, const Weights& w, float en, bool energy) {
+                                         int ty, const Weights& w, bool energy) {
     unsigned long long* q = tq + ty * kNTX + tx;
     atomicAdd(q, w.q00);
     atomicAdd(q + 1, w.q10);
@@ -168,40 +203,57 @@ __device__ __forceinline__ void tile_add(unsigned long long* tq, unsigned long l
     atomicAdd(q + kNTX + 1, w.q11);
     if (energy) {
         unsigned long long* e = te + ty * kNTX + tx;
-        atomicAdd(e, energy_fixed(en, w.q00));
-        atomicAdd(e + 1, energy_fixed(en, w.q10));
-        atomicAdd(e + kNTX, energy_fixed(en, w.q01));
-        atomicAdd(e + kNTX + 1, energy_fixed(en, w.q11));
+        atomicAdd(e, w.e00);
+        atomicAdd(e + 1, w.e10);
+        atomicAdd(e + kNTX, w.e01);
+        atomicAdd(e + kNTX + 1, w.e11);
     }
 }
 
-__device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w,
-                                           float en) {
+__device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w) {
     const int64_t n = (int64_t)gy * A.GX + gx;
     atomicAdd(A.acc_q + n, w.q00);
     atomicAdd(A.acc_q + n + 1, w.q10);
     atomicAdd(A.acc_q + n + A.GX, w.q01);
     atomicAdd(A.acc_q + n + A.GX + 1, w.q11);
     if (A.energy) {
-        atomicAdd(A.acc_e + n, energy_fixed(en, w.q00));
-        atomicAdd(A.acc_e + n + 1, energy_fixed(en, w.q10));
-        atomicAdd(A.acc_e + n + A.GX, energy_fixed(en, w.q01));
-        atomicAdd(A.acc_e + n + A.GX + 1, energy_fixed(en, w.q11));
+        atomicAdd(A.acc_e + n, w.e00);
+        atomicAdd(A.acc_e + n + 1, w.e10);
+        atomicAdd(A.acc_e + n + A.GX, w.e01);
+        atomicAdd(A.acc_e + n + A.GX + 1, w.e11);
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
+__device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, const Pushed& p,
+                                               float vz) {
+    if (dst < A.cap) {
+        __stcs(A.dst_a + dst, make_float4(p.fx, p.fy, p.vx, p.vy));
+        __stcs(A.dst_vz + dst, vz);
+    } else {
+        atomicOr(A.counters + 2, 1ull);
+    }
+}
+
+// One kernel body for the three uses:
+//   kCount   -- push, count leavers per direction (plain stores), far movers
+//               per target (atomics);
+//   kScatter -- push again, place every particle at its deterministic slot
+//               (sub-segment of its target cell for its direction + rank by
+//               ballot), deposit the new positions;
+//   kDeposit -- deposit the current positions (no push).
+template <int MODE, bool ENERGY>
+__global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
     constexpr bool kDep = (MODE != kCount);
     __shared__ unsigned long long tile_q[kDep ? kNTX * kNTY : 1];
-    __shared__ unsigned long long tile_e[kDep ? kNTX * kNTY : 1];
+    __shared__ unsigned long long tile_e[(kDep && ENERGY) ? kNTX * kNTY : 1];
+    __shared__ uint32_t base_s[kWarps][kDirs];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
     const int ox = tgx0 - kHalo, oy = tgy0 - kHalo;  // node tile origin
     if (kDep) {
         for (int i = threadIdx.x; i < kNTX * kNTY; i += kThreads) {
             tile_q[i] = 0ull;
-            tile_e[i] = 0ull;
+            if (ENERGY) tile_e[i] = 0ull;
         }
         __syncthreads();
     }
@@ -214,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
         const int64_t c = (int64_t)gy * A.nx + gx;
         const uint32_t beg = A.off[c], end = A.off[c + 1];
         if (beg == end) {
-            if (MODE == kCount && lane == 0) A.stay[c] = 0;
+            if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = 0u;
             continue;
         }
         const int64_t n0 = (int64_t)gy * A.GX + gx;
@@ -225,88 +277,102 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
             f01 = __ldg(A.fld + n0 + A.GX);
             f11 = __ldg(A.fld + n0 + A.GX + 1);
         }
-        uint32_t nstay = 0;
-        uint32_t stay_base = (MODE == kScatter) ? A.off_next[c] : 0u;
+        // running count per direction (registers: the loops below unroll)
+        uint32_t run[kDirs];
+#pragma unroll
+        for (int d = 0; d < kDirs; ++d) run[d] = 0u;
+        // destination base per direction: start of the target cell's
+        // sub-segment fed from this direction (per warp, in shared memory)
+        if (MODE == kScatter) {
+            __syncwarp();
+            if (lane < kDirs) {
+                const int tx = gx + lane % 3 - 1, ty = gy + lane / 3 - 1;
+                base_s[warp][lane] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
+                                         ? __ldg(A.sub + (int64_t)lane * A.ncells + (int64_t)ty * A.nx + tx)
+                                         : 0u;
+            }
+            __syncwarp();
+        }
         unsigned long long sq00 = 0, sq10 = 0, sq01 = 0, sq11 = 0;
         unsigned long long se00 = 0, se10 = 0, se01 = 0, se11 = 0;
 
+        // software pipeline: the next chunk's loads are issued before the
+        // current chunk is processed
+        uint32_t i = beg + lane;
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        float vz = 0.f;
+        if (i < end) {
+            a = __ldcs(A.src_a + i);
+            if (MODE != kCount) vz = __ldcs(A.src_vz + i);
+        }
         for (uint32_t i0 = beg; i0 < end; i0 += 32) {
-            const uint32_t i = i0 + lane;
             const bool valid = i < end;
-            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-            float vz = 0.f;
-            if (valid) {
-                a = __ldcs(A.src_a + i);
-                if (MODE != kCount) vz = __ldcs(A.src_vz + i);
+            const uint32_t inext = i + 32;
+            float4 an = make_float4(0.f, 0.f, 0.f, 0.f);
+            float vzn = 0.f;
+            if (inext < end) {
+                an = __ldcs(A.src_a + inext);
+                if (MODE != kCount) vzn = __ldcs(A.src_vz + inext);
             }
             Pushed p;
             if (MODE == kDeposit) {
                 p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
-                p.gx = gx; p.gy = gy; p.alive = true; p.left = false;
+                p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
             } else {
                 p = push_one(a, f00, f10, f01, f11, A.k, gx, gy, A.nx, A.ny);
             }
-            const bool stay = valid && p.alive && p.gx == gx && p.gy == gy;
-            const bool mover = valid && p.alive && !stay;
-            const unsigned sm = __ballot_sync(kFull, stay);
-            const unsigned mm = __ballot_sync(kFull, mover);
+            const int dir = valid ? p.dir : -1;
             if (MODE == kScatter) {
-                const unsigned lm = __ballot_sync(kFull, valid && !p.alive && p.left);
+                const unsigned lm = __ballot_sync(kFull, dir < 0 && valid && p.left);
                 left_exits += __popc(lm);
             }
+            // rank among this cell's particles leaving in the same direction
+            uint32_t rank = 0;
+#pragma unroll
+            for (int d = 0; d < kDirs; ++d) {
+                const unsigned m = __ballot_sync(kFull, dir == d);
+                if (dir == d) rank = run[d] + __popc(m & lt);
+                run[d] += __popc(m);
+            }
             float en = 0.f;
-            if (kDep && A.energy && (stay || mover)) en = energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm);
-            if (MODE == kScatter && stay) {
-                const uint32_t dst = stay_base + __popc(sm & lt);
-                if (dst < A.cap) {
-                    __stcs(A.dst_a + dst, make_float4(p.fx, p.fy, p.vx, p.vy));
-                    __stcs(A.dst_vz + dst, vz);
-                } else {
-                    atomicOr(A.counters + 2, 1ull);
-                }
-            }
-            if (kDep && stay) {
-                const Weights w = fixed_weights(p.fx, p.fy);
-                sq00 += w.q00; sq10 += w.q10; sq01 += w.q01; sq11 += w.q11;
-                if (A.energy) {
-                    se00 += energy_fixed(en, w.q00);
-                    se10 += energy_fixed(en, w.q10);
-                    se01 += energy_fixed(en, w.q01);
-                    se11 += energy_fixed(en, w.q11);
-                }
-            }
-            nstay += __popc(sm);
-            stay_base += __popc(sm);
-            if (mm) {
-                if (mover) {
-                    const uint32_t nc = (uint32_t)p.gy * (uint32_t)A.nx + (uint32_t)p.gx;
-                    const unsigned peers = __match_any_sync(mm, nc);
-                    const int leader = __ffs(peers) - 1;
-                    if (MODE == kCount) {
-                        if (lane == leader) atomicAdd(A.movein + nc, (uint32_t)__popc(peers));
-                    } else {
-                        uint32_t base = 0;
-                        if (lane == leader) base = atomicAdd(A.cursor + nc, (uint32_t)__popc(peers));
-                        base = __shfl_sync(peers, base, leader);
-                        const uint32_t dst = A.off_next[nc] + A.stay[nc] + base + __popc(peers & lt);
-                        if (dst < A.cap) {
-                            __stcs(A.dst_a + dst, make_float4(p.fx, p.fy, p.vx, p.vy));
-                            __stcs(A.dst_vz + dst, vz);
-                        } else {
-                            atomicOr(A.counters + 2, 1ull);
-                        }
-                        const Weights w = fixed_weights(p.fx, p.fy);
-                        const int tx = p.gx - ox, ty = p.gy - oy;
-                        if (tx >= 0 && tx < kNTX - 1 && ty >= 0 && ty < kNTY - 1)
-                            tile_add(tile_q, tile_e, tx, ty, w, en, A.energy);
-                        else
-                            global_add(A, p.gx, p.gy, w, en);
+            if (kDep && ENERGY && dir >= 0) en = energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm);
+            if (dir == kStay) {
+                if (MODE == kScatter) store_particle(A, base_s[warp][kStay] + rank, p, vz);
+                if (kDep) {
+                    const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
+                    sq00 += w.q00; sq10 += w.q10; sq01 += w.q01; sq11 += w.q11;
+                    if (ENERGY) {
+                        se00 += w.e00; se10 += w.e10; se01 += w.e01; se11 += w.e11;
                     }
                 }
+            } else if (dir >= 0) {
+                const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
+                if (dir == kFar) {
+                    if (MODE == kCount) atomicAdd(A.farin + nc, 1u);
+                    if (MODE == kScatter)
+                        store_particle(A, __ldg(A.sub + (int64_t)kFar * A.ncells + nc) +
+                                              atomicAdd(A.farcur + nc, 1u), p, vz);
+                } else if (MODE == kScatter) {
+                    store_particle(A, base_s[warp][dir] + rank, p, vz);
+                }
+                if (MODE == kScatter) {
+                    const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
+                    const int tx = p.gx - ox, ty = p.gy - oy;
+                    if (tx >= 0 && tx < kNTX - 1 && ty >= 0 && ty < kNTY - 1)
+                        tile_add(tile_q, tile_e, tx, ty, w, ENERGY);
+                    else
+                        global_add(A, p.gx, p.gy, w);
+                }
             }
+            i = inext;
+            a = an;
+            vz = vzn;
         }
         if (MODE == kCount) {
-            if (lane == 0) A.stay[c] = nstay;
+            if (lane == 0) {
+#pragma unroll
+                for (int d = 0; d < kDirs; ++d) A.dcount[(int64_t)d * A.ncells + c] = run[d];
+            }
         } else {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -314,21 +380,21 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
                 sq10 += __shfl_xor_sync(kFull, sq10, o);
                 sq01 += __shfl_xor_sync(kFull, sq01, o);
                 sq11 += __shfl_xor_sync(kFull, sq11, o);
-                if (A.energy) {
+                if (ENERGY) {
                     se00 += __shfl_xor_sync(kFull, se00, o);
                     se10 += __shfl_xor_sync(kFull, se10, o);
                     se01 += __shfl_xor_sync(kFull, se01, o);
                     se11 += __shfl_xor_sync(kFull, se11, o);
                 }
             }
-            if (lane == 0 && nstay) {
+            if (lane == 0 && run[kStay]) {
                 const int tx = gx - ox, ty = gy - oy;
                 unsigned long long* q = tile_q + ty * kNTX + tx;
                 atomicAdd(q, sq00);
                 atomicAdd(q + 1, sq10);
                 atomicAdd(q + kNTX, sq01);
                 atomicAdd(q + kNTX + 1, sq11);
-                if (A.energy) {
+                if (ENERGY) {
                     unsigned long long* e = tile_e + ty * kNTX + tx;
                     atomicAdd(e, se00);
                     atomicAdd(e + 1, se10);
@@ -347,7 +413,7 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
             const int64_t n = (int64_t)nyn * A.GX + nxn;
             const unsigned long long q = tile_q[i];
             if (q) atomicAdd(A.acc_q + n, q);
-            if (A.energy) {
+            if (ENERGY) {
                 const unsigned long long e = tile_e[i];
                 if (e) atomicAdd(A.acc_e + n, e);
             }
@@ -355,19 +421,47 @@ __global__ void __launch_bounds__(kThreads) k_particles(KArgs A) {
     }
 }
 
-// ---- exclusive scan of per-cell counts ------------------------------------
+// ---- exclusive scan of the new per-cell counts ------------------------------
+//
+// Cell t receives, from each direction d, the particles that left cell
+// t - dir(d) in direction d, plus its far movers.  Its new segment is laid
+// out by direction (d = 0..8, then far), so every particle has a
+// deterministic slot except far movers (atomic cursor).
 
-__device__ __forceinline__ uint32_t cell_count(const uint32_t* stay, const uint32_t* movein,
-                                               int64_t c, int64_t ncells) {
-    return c < ncells ? stay[c] + movein[c] : 0u;
+struct ScanArgs {
+    const uint32_t* dcount;
+    uint32_t* farin;
+    uint32_t* farcur;
+    uint32_t* sub;
+    uint32_t* off_next;
+    int nx, ny;
+    int64_t ncells;
+};
+
+__device__ __forceinline__ void incoming(const ScanArgs& S, int64_t t, uint32_t (&in)[kDirs + 1]) {
+    const int tx = (int)(t % S.nx), ty = (int)(t / S.nx);
+#pragma unroll
+    for (int d = 0; d < kDirs; ++d) {
+        const int sx = tx - (d % 3 - 1), sy = ty - (d / 3 - 1);
+        in[d] = (sx >= 0 && sy >= 0 && sx < S.nx && sy < S.ny)
+                    ? S.dcount[(int64_t)d * S.ncells + (int64_t)sy * S.nx + sx]
+                    : 0u;
+    }
+    in[kDirs] = S.farin[t];
 }
 
-__global__ void __launch_bounds__(256) k_scan_partials(const uint32_t* stay, const uint32_t* movein,
-                                                       int64_t ncells, uint32_t* partials) {
+__global__ void __launch_bounds__(256) k_scan_partials(ScanArgs S, uint32_t* partials) {
     __shared__ uint32_t red[8];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     uint32_t s = 0;
-    for (int j = threadIdx.x; j < kScanTile; j += 256) s += cell_count(stay, movein, base + j, ncells);
+    for (int j = threadIdx.x; j < kScanTile; j += 256) {
+        const int64_t t = base + j;
+        if (t >= S.ncells) break;
+        uint32_t in[kDirs + 1];
+        incoming(S, t, in);
+#pragma unroll
+        for (int d = 0; d <= kDirs; ++d) s += in[d];
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -378,17 +472,14 @@ __global__ void __launch_bounds__(256) k_scan_partials(const uint32_t* stay, con
     }
 }
 
-// off_next[c] = sum of counts before c; off_next[ncells] = total.  Zeroes
-// movein and cursor for the next step and flags cells above kMaxPerCell.
-__global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* stay, uint32_t* movein,
-                                                    uint32_t* cursor, int64_t ncells,
-                                                    const uint32_t* partials, int nparts,
-                                                    uint32_t* off_next,
+// off_next[t] = particles in cells before t; sub[d][t] = start of the part of
+// t's segment fed from direction d; off_next[ncells] = total.  Zeroes the far
+// counters for the next step and flags cells above kMaxPerCell.
+__global__ void __launch_bounds__(256) k_scan_apply(ScanArgs S, const uint32_t* partials,
                                                     unsigned long long* counters) {
     __shared__ uint32_t red[8];
     __shared__ uint32_t wsum[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // prefix over the partial sums of earlier blocks
     uint32_t pre = 0;
     for (int j = threadIdx.x; j < (int)blockIdx.x; j += 256) pre += partials[j];
     for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(kFull, pre, o);
@@ -398,13 +489,19 @@ __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* stay, uint32
     for (int w = 0; w < 8; ++w) block_pre += red[w];
     // each thread owns 8 consecutive cells
     const int64_t c0 = (int64_t)blockIdx.x * kScanTile + threadIdx.x * 8;
-    uint32_t v[8];
+    uint32_t tot[8];
     uint32_t tsum = 0, vmax = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        v[j] = cell_count(stay, movein, c0 + j, ncells);
-        tsum += v[j];
-        vmax = max(vmax, v[j]);
+        tot[j] = 0;
+        if (c0 + j < S.ncells) {
+            uint32_t in[kDirs + 1];
+            incoming(S, c0 + j, in);
+#pragma unroll
+            for (int d = 0; d <= kDirs; ++d) tot[j] += in[d];
+        }
+        tsum += tot[j];
+        vmax = max(vmax, tot[j]);
     }
     uint32_t incl = tsum;
 #pragma unroll
@@ -419,14 +516,22 @@ __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* stay, uint32
     uint32_t run = block_pre + wpre + incl - tsum;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const int64_t c = c0 + j;
-        if (c < ncells) {
-            off_next[c] = run;
-            movein[c] = 0;
-            cursor[c] = 0;
+        const int64_t t = c0 + j;
+        if (t < S.ncells) {
+            S.off_next[t] = run;
+            uint32_t in[kDirs + 1];
+            incoming(S, t, in);
+            uint32_t r = run;
+#pragma unroll
+            for (int d = 0; d <= kDirs; ++d) {
+                S.sub[(int64_t)d * S.ncells + t] = r;
+                r += in[d];
+            }
+            S.farin[t] = 0;
+            S.farcur[t] = 0;
         }
-        run += v[j];
-        if (c == ncells - 1) off_next[ncells] = run;
+        run += tot[j];
+        if (t == S.ncells - 1) S.off_next[S.ncells] = run;
     }
     if (vmax > kMaxPerCell) atomicOr(counters + 1, 1ull);
 }
@@ -437,7 +542,7 @@ __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* stay, uint32
 // gx = (int)(x * (1/dx)) in FP64 (src/particles.cpp:230-235).
 __global__ void k_import_convert(const pic_point* __restrict__ pts, int64_t n, int nx, int ny,
                                  double inv_dx, double inv_dy, float4* tmp_a, float* tmp_vz,
-                                 uint32_t* cell_of, uint32_t* movein) {
+                                 uint32_t* cell_of, uint32_t* farin) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const pic_point p = pts[i];
@@ -454,18 +559,18 @@ __global__ void k_import_convert(const pic_point* __restrict__ pts, int64_t n, i
         }
     }
     cell_of[i] = cell;
-    if (cell != 0xffffffffu) atomicAdd(movein + cell, 1u);
+    if (cell != 0xffffffffu) atomicAdd(farin + cell, 1u);
 }
 
 __global__ void k_import_scatter(const float4* __restrict__ tmp_a, const float* __restrict__ tmp_vz,
                                  const uint32_t* __restrict__ cell_of, int64_t n,
-                                 const uint32_t* __restrict__ off, uint32_t* cursor,
+                                 const uint32_t* __restrict__ off, uint32_t* farcur,
                                  float4* dst_a, float* dst_vz) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t c = cell_of[i];
     if (c == 0xffffffffu) return;
-    const uint32_t d = off[c] + atomicAdd(cursor + c, 1u);
+    const uint32_t d = off[c] + atomicAdd(farcur + c, 1u);
     dst_a[d] = tmp_a[i];
     dst_vz[d] = tmp_vz[i];
 }
@@ -584,10 +689,11 @@ __device__ __forceinline__ uint32_t blob_count(const PlasmaArgs& P, int64_t c) {
     return (uint32_t)floor(m + (double)u01(r.x));
 }
 
-__global__ void k_plasma_counts(PlasmaArgs P, int64_t ncells, uint32_t* movein) {
+// counts enter as the "stay" direction of each cell
+__global__ void k_plasma_counts(PlasmaArgs P, int64_t ncells, uint32_t* stay_count) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
-    movein[c] = (uint32_t)P.ppc + blob_count(P, c);
+    stay_count[c] = (uint32_t)P.ppc + blob_count(P, c);
 }
 
 __global__ void k_plasma_generate(PlasmaArgs P, const uint32_t* __restrict__ off, int64_t ncells,
@@ -622,9 +728,9 @@ inline unsigned grid1d(int64_t n, int threads) { return (unsigned)((n + threads 
 int scan_counts(pic_ctx* c, Species& sp) {
     const int64_t ncells = c->ncells;
     const int nparts = (int)((ncells + kScanTile - 1) / kScanTile);
-    k_scan_partials<<<nparts, 256, 0, c->stream>>>(sp.stay, sp.movein, ncells, c->scan_partials);
-    k_scan_apply<<<nparts, 256, 0, c->stream>>>(sp.stay, sp.movein, sp.cursor, ncells,
-                                                c->scan_partials, nparts, sp.off_next, sp.counters);
+    ScanArgs S{sp.dcount, sp.farin, sp.farcur, sp.sub, sp.off_next, c->nx, c->ny, ncells};
+    k_scan_partials<<<nparts, 256, 0, c->stream>>>(S, c->scan_partials);
+    k_scan_apply<<<nparts, 256, 0, c->stream>>>(S, c->scan_partials, sp.counters);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
@@ -634,6 +740,7 @@ KArgs make_args(pic_ctx* c, Species& sp) {
     A.nx = c->nx;
     A.ny = c->ny;
     A.GX = c->GX;
+    A.ncells = c->ncells;
     A.k = sp.k;
     A.fld = c->fld;
     A.src_a = sp.buf[sp.cur].a;
@@ -641,10 +748,10 @@ KArgs make_args(pic_ctx* c, Species& sp) {
     A.dst_a = sp.buf[sp.cur ^ 1].a;
     A.dst_vz = sp.buf[sp.cur ^ 1].vz;
     A.off = sp.off;
-    A.off_next = sp.off_next;
-    A.stay = sp.stay;
-    A.movein = sp.movein;
-    A.cursor = sp.cursor;
+    A.dcount = sp.dcount;
+    A.sub = sp.sub;
+    A.farin = sp.farin;
+    A.farcur = sp.farcur;
     A.acc_q = sp.acc_q;
     A.acc_e = sp.acc_e;
     A.counters = sp.counters;
@@ -684,9 +791,10 @@ int species_setup(pic_ctx* c, int s) {
     const size_t nc = (size_t)c->ncells;
     PIC_CUDA(cudaMalloc(&sp.off, (nc + 1) * sizeof(uint32_t)));
     PIC_CUDA(cudaMalloc(&sp.off_next, (nc + 1) * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.stay, nc * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.movein, nc * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.cursor, nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.dcount, 9 * nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.sub, 10 * nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.farin, nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.farcur, nc * sizeof(uint32_t)));
     PIC_CUDA(cudaMalloc(&sp.acc_q, (size_t)c->nodes * sizeof(unsigned long long)));
     PIC_CUDA(cudaMalloc(&sp.acc_e, (size_t)c->nodes * sizeof(unsigned long long)));
     PIC_CUDA(cudaMalloc(&sp.final_mesh, (size_t)c->nodes * sizeof(double)));
@@ -694,9 +802,10 @@ int species_setup(pic_ctx* c, int s) {
     PIC_CUDA(cudaMalloc(&sp.counters, 4 * sizeof(unsigned long long)));
     PIC_CUDA(cudaMemsetAsync(sp.off, 0, (nc + 1) * sizeof(uint32_t), c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.off_next, 0, (nc + 1) * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.stay, 0, nc * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.movein, 0, nc * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.cursor, 0, nc * sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, 9 * nc * sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.sub, 0, 10 * nc * sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, nc * sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.farcur, 0, nc * sizeof(uint32_t), c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.final_mesh, 0, (size_t)c->nodes * 8, c->stream));
@@ -710,9 +819,10 @@ void species_free(Species& sp) {
     cudaFree(sp.store);
     cudaFree(sp.off);
     cudaFree(sp.off_next);
-    cudaFree(sp.stay);
-    cudaFree(sp.movein);
-    cudaFree(sp.cursor);
+    cudaFree(sp.dcount);
+    cudaFree(sp.sub);
+    cudaFree(sp.farin);
+    cudaFree(sp.farcur);
     cudaFree(sp.acc_q);
     cudaFree(sp.acc_e);
     cudaFree(sp.final_mesh);
@@ -783,20 +893,22 @@ int particles_import(pic_ctx* c, int s, int64_t n) {
         reinterpret_cast<uint32_t*>(static_cast<char*>(c->staging) + aligned_points_bytes(n));
     const ParticleSoA tmp = sp.buf[sp.cur ^ 1];
     const ParticleSoA dst = sp.buf[sp.cur];
-    PIC_CUDA(cudaMemsetAsync(sp.movein, 0, (size_t)c->ncells * 4, c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.stay, 0, (size_t)c->ncells * 4, c->stream));
+    // every imported particle enters as a "far mover" of its cell
+    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, (size_t)c->ncells * 4, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, (size_t)c->ncells * 4 * 9, c->stream));
     if (n > 0)
         k_import_convert<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, n, c->nx, c->ny,
                                                                 1.0 / c->dx, 1.0 / c->dy, tmp.a,
-                                                                tmp.vz, cell_of, sp.movein);
+                                                                tmp.vz, cell_of, sp.farin);
     PIC_TRY(scan_counts(c, sp));
     if (n > 0)
         k_import_scatter<<<grid1d(n, 256), 256, 0, c->stream>>>(tmp.a, tmp.vz, cell_of, n,
-                                                                sp.off_next, sp.cursor, dst.a,
+                                                                sp.sub + 9 * c->ncells,
+                                                                sp.farcur, dst.a,
                                                                 dst.vz);
     PIC_CUDA(cudaGetLastError());
     std::swap(sp.off, sp.off_next);
-    PIC_CUDA(cudaMemsetAsync(sp.cursor, 0, (size_t)c->ncells * 4, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.farcur, 0, (size_t)c->ncells * 4, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     unsigned long long flags[2] = {0, 0};
@@ -871,8 +983,10 @@ int particles_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d) {
     P.drift_vy = (float)d->drift_vy;
     P.key = make_uint2((uint32_t)d->seed, (uint32_t)(d->seed >> 32));
     P.species = (uint32_t)s;
-    k_plasma_counts<<<grid1d(c->ncells, 256), 256, 0, c->stream>>>(P, c->ncells, sp.movein);
-    PIC_CUDA(cudaMemsetAsync(sp.stay, 0, (size_t)c->ncells * 4, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, (size_t)c->ncells * 4 * 9, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, (size_t)c->ncells * 4, c->stream));
+    k_plasma_counts<<<grid1d(c->ncells, 256), 256, 0, c->stream>>>(P, c->ncells,
+                                                                   sp.dcount + 4 * c->ncells);
     PIC_TRY(scan_counts(c, sp));
     std::swap(sp.off, sp.off_next);
     int64_t n = 0;
@@ -908,7 +1022,10 @@ int particles_deposit(pic_ctx* c, int s) {
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     KArgs A = make_args(c, sp);
     prof_begin(c, PIC_PHASE_DEPOSIT);
-    k_particles<kDeposit><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+    if (A.energy)
+        k_particles<kDeposit, true><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+    else
+        k_particles<kDeposit, false><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
     prof_end(c, PIC_PHASE_DEPOSIT);
     c->launches += 1;
     PIC_CUDA(cudaGetLastError());
@@ -940,7 +1057,7 @@ int particles_push(pic_ctx* c, int s) {
     KArgs A = make_args(c, sp);
     const dim3 g = tile_grid(c);
     prof_begin(c, PIC_PHASE_PUSH_COUNT);
-    k_particles<kCount><<<g, kThreads, 0, c->stream>>>(A);
+    k_particles<kCount, false><<<g, kThreads, 0, c->stream>>>(A);
     prof_end(c, PIC_PHASE_PUSH_COUNT);
     PIC_CUDA(cudaGetLastError());
     prof_begin(c, PIC_PHASE_SCAN);
@@ -950,7 +1067,10 @@ int particles_push(pic_ctx* c, int s) {
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     prof_begin(c, PIC_PHASE_PUSH_SCATTER);
-    k_particles<kScatter><<<g, kThreads, 0, c->stream>>>(A);
+    if (A.energy)
+        k_particles<kScatter, true><<<g, kThreads, 0, c->stream>>>(A);
+    else
+        k_particles<kScatter, false><<<g, kThreads, 0, c->stream>>>(A);
     prof_end(c, PIC_PHASE_PUSH_SCATTER);
     c->launches += 4;
     PIC_CUDA(cudaGetLastError());

@@ -80,9 +80,12 @@ struct Species {
     int cur = 0;
     uint32_t* off = nullptr;        // [ncells+1] segment starts of buf[cur]
     uint32_t* off_next = nullptr;   // [ncells+1] segment starts being built
-    uint32_t* stay = nullptr;       // [ncells]  stayers per cell (pass 1)
-    uint32_t* movein = nullptr;     // [ncells]  movers entering a cell (pass 1)
-    uint32_t* cursor = nullptr;     // [ncells]  mover slots handed out (pass 2)
+    uint32_t* dcount = nullptr;     // [9][ncells] particles leaving cell s in direction d
+                                    //   (d = (sy+1)*3 + (sx+1); d = 4 stays)
+    uint32_t* sub = nullptr;        // [10][ncells] start of cell t's sub-segment fed
+                                    //   from direction d (9: far movers)
+    uint32_t* farin = nullptr;      // [ncells] far movers (jump > 1 cell) entering a cell
+    uint32_t* farcur = nullptr;     // [ncells] far-mover slots handed out
     unsigned long long* acc_q = nullptr;  // [nodes] fixed-point charge weights
     unsigned long long* acc_e = nullptr;  // [nodes] fixed-point energy weights
     double* final_mesh = nullptr;   // [nodes]
