@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-energy", action="store_true",
+                    help="skip the energy-weighted mesh (deposit_energy = 0)")
     return ap.parse_args()
 
 
@@ -246,7 +248,7 @@ def run_ours(args, rank, world, local_rank):
     import pic_configs as C
     torch.cuda.set_device(local_rank)
     w = workload(args.config)
-    pic = P.Pic(C.library_config(w, device=local_rank))
+    pic = P.Pic(C.library_config(w, device=local_rank, deposit_energy=not args.no_energy))
     # a dedicated (non-default) torch stream: the library runs on it and the
     # CUDA events below are recorded on it
     stream = torch.cuda.Stream()
@@ -353,7 +355,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": describe(w), "particles_per_gpu": n_part,
                    "particles_per_species": counts, "grid_nodes": (w.nx + 1) * (w.ny + 1),
                    "l2": "inputs larger than L2 (particle state ~%.1f GB per GPU)" % (n_part * 40 / 1e9),
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "energy_mesh": not args.no_energy},
         "full_step": {"ms_per_step": step_ms / args.steps,
                       "particle_steps_per_s": total_particles * args.steps / (step_ms * 1e-3),
                       "wall_s": t_wall},

@@ -46,8 +46,6 @@ namespace picb200 {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kNTX = kTileX + 1 + 2 * kHalo;  // node tile width
-constexpr int kNTY = kTileY + 1 + 2 * kHalo;  // node tile height
 constexpr int kThreads = kWarps * 32;
 constexpr int kScanTile = 2048;               // cells per scan block
 constexpr uint32_t kAxisOne = 1u << kAxisBits;
@@ -194,33 +192,24 @@ __device__ __forceinline__ float energy_ev(float vx, float vy, float vz, float h
     return fminf(__fmul_rn(v2, half_inv_abs_qm), kEnergyClampEv);
 }
 
-__device__ __forceinline__ void tile_add(unsigned long long* tq, unsigned long long* te, int tx,
-                                         int ty, const Weights& w, bool energy) {
-    unsigned long long* q = tq + ty * kNTX + tx;
-    atomicAdd(q, w.q00);
-    atomicAdd(q + 1, w.q10);
-    atomicAdd(q + kNTX, w.q01);
-    atomicAdd(q + kNTX + 1, w.q11);
-    if (energy) {
-        unsigned long long* e = te + ty * kNTX + tx;
-        atomicAdd(e, w.e00);
-        atomicAdd(e + 1, w.e10);
-        atomicAdd(e + kNTX, w.e01);
-        atomicAdd(e + kNTX + 1, w.e11);
-    }
+// Global 64-bit integer reductions (fire-and-forget RED) into the node
+// accumulators.
+__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
+    if (v) atomicAdd(p, v);
 }
 
-__device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w) {
+__device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w,
+                                           bool energy) {
     const int64_t n = (int64_t)gy * A.GX + gx;
-    atomicAdd(A.acc_q + n, w.q00);
-    atomicAdd(A.acc_q + n + 1, w.q10);
-    atomicAdd(A.acc_q + n + A.GX, w.q01);
-    atomicAdd(A.acc_q + n + A.GX + 1, w.q11);
-    if (A.energy) {
-        atomicAdd(A.acc_e + n, w.e00);
-        atomicAdd(A.acc_e + n + 1, w.e10);
-        atomicAdd(A.acc_e + n + A.GX, w.e01);
-        atomicAdd(A.acc_e + n + A.GX + 1, w.e11);
+    red_add(A.acc_q + n, w.q00);
+    red_add(A.acc_q + n + 1, w.q10);
+    red_add(A.acc_q + n + A.GX, w.q01);
+    red_add(A.acc_q + n + A.GX + 1, w.q11);
+    if (energy) {
+        red_add(A.acc_e + n, w.e00);
+        red_add(A.acc_e + n + 1, w.e10);
+        red_add(A.acc_e + n + A.GX, w.e01);
+        red_add(A.acc_e + n + A.GX + 1, w.e11);
     }
 }
 
@@ -234,6 +223,64 @@ __device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, con
     }
 }
 
+// Per-lane fixed-point sums of the stayers of the current cell, kept as
+// 32-bit limbs so that the per-cell warp reduction is a handful of
+// redux.sync: charge weights (< 2^40) as 2 x 20-bit limbs, energy weights
+// (< 2^44) as 3 x 15-bit limbs.  A lane adds one particle per chunk and the
+// sums are flushed at least every kFlushChunks chunks, so each limb sum over
+// the warp stays below 2^32.
+constexpr int kFlushChunks = 64;
+
+struct StayAcc {
+    uint32_t q[4][2];
+    uint32_t e[4][3];
+};
+
+__device__ __forceinline__ void acc_zero(StayAcc& s) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        s.q[k][0] = s.q[k][1] = 0u;
+        s.e[k][0] = s.e[k][1] = s.e[k][2] = 0u;
+    }
+}
+
+template <bool ENERGY>
+__device__ __forceinline__ void acc_add(StayAcc& s, const Weights& w) {
+    const unsigned long long q[4] = {w.q00, w.q10, w.q01, w.q11};
+    const unsigned long long e[4] = {w.e00, w.e10, w.e01, w.e11};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        s.q[k][0] += (uint32_t)(q[k] & 0xFFFFFull);
+        s.q[k][1] += (uint32_t)(q[k] >> 20);
+        if (ENERGY) {
+            s.e[k][0] += (uint32_t)(e[k] & 0x7FFFull);
+            s.e[k][1] += (uint32_t)((e[k] >> 15) & 0x7FFFull);
+            s.e[k][2] += (uint32_t)(e[k] >> 30);
+        }
+    }
+}
+
+// Warp-reduce the limbs and add the cell's four node sums (lane 0).
+template <bool ENERGY>
+__device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane) {
+    unsigned long long q[4], e[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        q[k] = (unsigned long long)__reduce_add_sync(kFull, s.q[k][0]) +
+               ((unsigned long long)__reduce_add_sync(kFull, s.q[k][1]) << 20);
+        e[k] = 0ull;
+        if (ENERGY)
+            e[k] = (unsigned long long)__reduce_add_sync(kFull, s.e[k][0]) +
+                   ((unsigned long long)__reduce_add_sync(kFull, s.e[k][1]) << 15) +
+                   ((unsigned long long)__reduce_add_sync(kFull, s.e[k][2]) << 30);
+    }
+    if (lane == 0) {
+        Weights w{q[0], q[1], q[2], q[3], e[0], e[1], e[2], e[3]};
+        global_add(A, gx, gy, w, ENERGY);
+    }
+    acc_zero(s);
+}
+
 // One kernel body for the three uses:
 //   kCount   -- push, count leavers per direction (plain stores), far movers
 //               per target (atomics);
@@ -241,184 +288,173 @@ __device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, con
 //               (sub-segment of its target cell for its direction + rank by
 //               ballot), deposit the new positions;
 //   kDeposit -- deposit the current positions (no push).
+// A block owns a kTileX x kTileY tile of cells.  Its prologue stages in
+// shared memory the segment table of the tile, the node fields of the tile
+// and (scatter) the destination sub-segment starts of the tile and its
+// one-cell halo.  Each warp then walks whole cells of the tile, 32 particles
+// per chunk, with the next chunk's loads (possibly of the next cell) issued
+// before the current chunk is processed.
+constexpr int kHX = kTileX + 2, kHY = kTileY + 2;  // halo region of cells
+
 template <int MODE, bool ENERGY>
 __global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
     constexpr bool kDep = (MODE != kCount);
-    __shared__ unsigned long long tile_q[kDep ? kNTX * kNTY : 1];
-    __shared__ unsigned long long tile_e[(kDep && ENERGY) ? kNTX * kNTY : 1];
-    __shared__ uint32_t base_s[kWarps][kDirs];
+    __shared__ uint32_t off_s[kTileY][kTileX + 1];
+    __shared__ float4 fld_s[MODE != kDeposit ? (kTileY + 1) * (kTileX + 1) : 1];
+    __shared__ uint32_t sub_s[MODE == kScatter ? kDirs * kHX * kHY : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
-    const int ox = tgx0 - kHalo, oy = tgy0 - kHalo;  // node tile origin
-    if (kDep) {
-        for (int i = threadIdx.x; i < kNTX * kNTY; i += kThreads) {
-            tile_q[i] = 0ull;
-            if (ENERGY) tile_e[i] = 0ull;
-        }
-        __syncthreads();
+    const int tw = min(kTileX, A.nx - tgx0), th = min(kTileY, A.ny - tgy0);
+
+    // ---- prologue: stage the tile's tables in shared memory ----
+    for (int i = threadIdx.x; i < kTileY * (kTileX + 1); i += kThreads) {
+        const int r = i / (kTileX + 1), x = i % (kTileX + 1);
+        if (r < th && x <= tw) off_s[r][x] = A.off[(int64_t)(tgy0 + r) * A.nx + tgx0 + x];
     }
+    if (MODE != kDeposit) {
+        for (int i = threadIdx.x; i < (kTileY + 1) * (kTileX + 1); i += kThreads) {
+            const int r = i / (kTileX + 1), x = i % (kTileX + 1);
+            if (r <= th && x <= tw) fld_s[i] = __ldg(A.fld + (int64_t)(tgy0 + r) * A.GX + tgx0 + x);
+        }
+    }
+    if (MODE == kScatter) {
+        for (int i = threadIdx.x; i < kDirs * kHX * kHY; i += kThreads) {
+            const int d = i / (kHX * kHY), rem = i % (kHX * kHY);
+            const int tx = tgx0 - 1 + rem % kHX, ty = tgy0 - 1 + rem / kHX;
+            sub_s[i] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
+                           ? A.sub[(int64_t)d * A.ncells + (int64_t)ty * A.nx + tx]
+                           : 0u;
+        }
+    }
+    __syncthreads();
+
     const unsigned lt = lanemask_lt();
     unsigned long long left_exits = 0;
+    const int ncell_tile = kTileX * kTileY;
 
-    for (int lc = warp; lc < kTileX * kTileY; lc += kWarps) {
-        const int gx = tgx0 + (lc % kTileX), gy = tgy0 + (lc / kTileX);
-        if (gx >= A.nx || gy >= A.ny) continue;  // warp-uniform
-        const int64_t c = (int64_t)gy * A.nx + gx;
-        const uint32_t beg = A.off[c], end = A.off[c + 1];
-        if (beg == end) {
-            if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = 0u;
-            continue;
+    // next cell slot (of this warp) holding particles; empty cells met on the
+    // way get their zero direction counts in the count pass
+    auto next_cell = [&](int from) -> int {
+        for (int l = from; l < ncell_tile; l += kWarps) {
+            const int x = l % kTileX, r = l / kTileX;
+            if (x >= tw || r >= th) continue;
+            if (off_s[r][x + 1] > off_s[r][x]) return l;
+            if (MODE == kCount && lane < kDirs)
+                A.dcount[(int64_t)lane * A.ncells + (int64_t)(tgy0 + r) * A.nx + tgx0 + x] = 0u;
         }
-        const int64_t n0 = (int64_t)gy * A.GX + gx;
-        float4 f00 = make_float4(0, 0, 0, 0), f10 = f00, f01 = f00, f11 = f00;
-        if (MODE != kDeposit) {
-            f00 = __ldg(A.fld + n0);
-            f10 = __ldg(A.fld + n0 + 1);
-            f01 = __ldg(A.fld + n0 + A.GX);
-            f11 = __ldg(A.fld + n0 + A.GX + 1);
-        }
-        // running count per direction (registers: the loops below unroll)
-        uint32_t run[kDirs];
-#pragma unroll
-        for (int d = 0; d < kDirs; ++d) run[d] = 0u;
-        // destination base per direction: start of the target cell's
-        // sub-segment fed from this direction (per warp, in shared memory)
-        if (MODE == kScatter) {
-            __syncwarp();
-            if (lane < kDirs) {
-                const int tx = gx + lane % 3 - 1, ty = gy + lane / 3 - 1;
-                base_s[warp][lane] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
-                                         ? __ldg(A.sub + (int64_t)lane * A.ncells + (int64_t)ty * A.nx + tx)
-                                         : 0u;
-            }
-            __syncwarp();
-        }
-        unsigned long long sq00 = 0, sq10 = 0, sq01 = 0, sq11 = 0;
-        unsigned long long se00 = 0, se10 = 0, se01 = 0, se11 = 0;
+        return ncell_tile;
+    };
 
-        // software pipeline: the next chunk's loads are issued before the
-        // current chunk is processed
-        uint32_t i = beg + lane;
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-        float vz = 0.f;
-        if (i < end) {
-            a = __ldcs(A.src_a + i);
-            if (MODE != kCount) vz = __ldcs(A.src_vz + i);
+    int plc = next_cell(warp);
+    uint32_t pi0 = plc < ncell_tile ? off_s[plc / kTileX][plc % kTileX] : 0u;
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f);
+    float pvz = 0.f;
+    if (plc < ncell_tile) {
+        const uint32_t pe = off_s[plc / kTileX][plc % kTileX + 1];
+        if (pi0 + lane < pe) {
+            pa = __ldcs(A.src_a + pi0 + lane);
+            if (MODE != kCount) pvz = __ldcs(A.src_vz + pi0 + lane);
         }
-        for (uint32_t i0 = beg; i0 < end; i0 += 32) {
-            const bool valid = i < end;
-            const uint32_t inext = i + 32;
-            float4 an = make_float4(0.f, 0.f, 0.f, 0.f);
-            float vzn = 0.f;
-            if (inext < end) {
-                an = __ldcs(A.src_a + inext);
-                if (MODE != kCount) vzn = __ldcs(A.src_vz + inext);
-            }
-            Pushed p;
-            if (MODE == kDeposit) {
-                p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
-                p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
-            } else {
-                p = push_one(a, f00, f10, f01, f11, A.k, gx, gy, A.nx, A.ny);
-            }
-            const int dir = valid ? p.dir : -1;
-            if (MODE == kScatter) {
-                const unsigned lm = __ballot_sync(kFull, dir < 0 && valid && p.left);
-                left_exits += __popc(lm);
-            }
-            // rank among this cell's particles leaving in the same direction
-            uint32_t rank = 0;
+    }
+
+    uint32_t run[kDirs];
 #pragma unroll
-            for (int d = 0; d < kDirs; ++d) {
-                const unsigned m = __ballot_sync(kFull, dir == d);
-                if (dir == d) rank = run[d] + __popc(m & lt);
-                run[d] += __popc(m);
-            }
-            float en = 0.f;
-            if (kDep && ENERGY && dir >= 0) en = energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm);
-            if (dir == kStay) {
-                if (MODE == kScatter) store_particle(A, base_s[warp][kStay] + rank, p, vz);
-                if (kDep) {
-                    const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
-                    sq00 += w.q00; sq10 += w.q10; sq01 += w.q01; sq11 += w.q11;
-                    if (ENERGY) {
-                        se00 += w.e00; se10 += w.e10; se01 += w.e01; se11 += w.e11;
-                    }
-                }
-            } else if (dir >= 0) {
-                const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
-                if (dir == kFar) {
-                    if (MODE == kCount) atomicAdd(A.farin + nc, 1u);
-                    if (MODE == kScatter)
-                        store_particle(A, __ldg(A.sub + (int64_t)kFar * A.ncells + nc) +
-                                              atomicAdd(A.farcur + nc, 1u), p, vz);
-                } else if (MODE == kScatter) {
-                    store_particle(A, base_s[warp][dir] + rank, p, vz);
-                }
-                if (MODE == kScatter) {
-                    const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
-                    const int tx = p.gx - ox, ty = p.gy - oy;
-                    if (tx >= 0 && tx < kNTX - 1 && ty >= 0 && ty < kNTY - 1)
-                        tile_add(tile_q, tile_e, tx, ty, w, ENERGY);
-                    else
-                        global_add(A, p.gx, p.gy, w);
-                }
-            }
-            i = inext;
-            a = an;
-            vz = vzn;
+    for (int d = 0; d < kDirs; ++d) run[d] = 0u;
+    StayAcc acc;
+    acc_zero(acc);
+    int chunks = 0;
+
+    while (plc < ncell_tile) {
+        // the prefetched chunk becomes current
+        const int clc = plc;
+        const uint32_t ci0 = pi0;
+        const int cx = clc % kTileX, cr = clc / kTileX;
+        const uint32_t cend = off_s[cr][cx + 1];
+        const float4 a = pa;
+        const float vz = pvz;
+        const int gx = tgx0 + cx, gy = tgy0 + cr;
+        // advance the prefetch pointer and issue the next chunk's loads
+        pi0 += 32;
+        if (pi0 >= cend) {
+            plc = next_cell(clc + kWarps);
+            if (plc < ncell_tile) pi0 = off_s[plc / kTileX][plc % kTileX];
         }
-        if (MODE == kCount) {
-            if (lane == 0) {
-#pragma unroll
-                for (int d = 0; d < kDirs; ++d) A.dcount[(int64_t)d * A.ncells + c] = run[d];
+        pa = make_float4(0.f, 0.f, 0.f, 0.f);
+        pvz = 0.f;
+        if (plc < ncell_tile) {
+            const uint32_t pe = off_s[plc / kTileX][plc % kTileX + 1];
+            if (pi0 + lane < pe) {
+                pa = __ldcs(A.src_a + pi0 + lane);
+                if (MODE != kCount) pvz = __ldcs(A.src_vz + pi0 + lane);
             }
+        }
+
+        const bool valid = ci0 + lane < cend;
+        Pushed p;
+        if (MODE == kDeposit) {
+            p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
+            p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
         } else {
+            const int b = cr * (kTileX + 1) + cx;
+            p = push_one(a, fld_s[b], fld_s[b + 1], fld_s[b + kTileX + 1], fld_s[b + kTileX + 2],
+                         A.k, gx, gy, A.nx, A.ny);
+        }
+        const int dir = valid ? p.dir : -1;
+        if (MODE == kScatter) left_exits += __popc(__ballot_sync(kFull, valid && dir < 0 && p.left));
+        // rank among this cell's particles leaving in the same direction
+        uint32_t rank = 0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                sq00 += __shfl_xor_sync(kFull, sq00, o);
-                sq10 += __shfl_xor_sync(kFull, sq10, o);
-                sq01 += __shfl_xor_sync(kFull, sq01, o);
-                sq11 += __shfl_xor_sync(kFull, sq11, o);
-                if (ENERGY) {
-                    se00 += __shfl_xor_sync(kFull, se00, o);
-                    se10 += __shfl_xor_sync(kFull, se10, o);
-                    se01 += __shfl_xor_sync(kFull, se01, o);
-                    se11 += __shfl_xor_sync(kFull, se11, o);
-                }
+        for (int d = 0; d < kDirs; ++d) {
+            const unsigned m = __ballot_sync(kFull, dir == d);
+            if (dir == d) rank = run[d] + __popc(m & lt);
+            run[d] += __popc(m);
+        }
+        if (kDep) {
+            Weights w{0, 0, 0, 0, 0, 0, 0, 0};
+            if (dir >= 0) {
+                const float en = ENERGY ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
+                w = fixed_weights<ENERGY>(p.fx, p.fy, en);
             }
-            if (lane == 0 && run[kStay]) {
-                const int tx = gx - ox, ty = gy - oy;
-                unsigned long long* q = tile_q + ty * kNTX + tx;
-                atomicAdd(q, sq00);
-                atomicAdd(q + 1, sq10);
-                atomicAdd(q + kNTX, sq01);
-                atomicAdd(q + kNTX + 1, sq11);
-                if (ENERGY) {
-                    unsigned long long* e = tile_e + ty * kNTX + tx;
-                    atomicAdd(e, se00);
-                    atomicAdd(e + 1, se10);
-                    atomicAdd(e + kNTX, se01);
-                    atomicAdd(e + kNTX + 1, se11);
-                }
+            if (dir == kStay) {
+                acc_add<ENERGY>(acc, w);
+            } else if (MODE == kScatter && dir >= 0) {
+                global_add(A, p.gx, p.gy, w, ENERGY);
             }
+        }
+        if (MODE == kScatter && dir >= 0) {
+            uint32_t dst;
+            if (dir == kFar) {
+                const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
+                dst = __ldg(A.sub + (int64_t)kFar * A.ncells + nc) + atomicAdd(A.farcur + nc, 1u);
+            } else {
+                const int tx = cx + dir % 3, ty = cr + dir / 3;  // halo coordinates
+                dst = sub_s[dir * kHX * kHY + ty * kHX + tx] + rank;
+            }
+            store_particle(A, dst, p, vz);
+        }
+        if (MODE == kCount && dir == kFar)
+            atomicAdd(A.farin + (int64_t)p.gy * A.nx + p.gx, 1u);
+
+        ++chunks;
+        const bool cell_done = ci0 + 32 >= cend;
+        if (kDep && (cell_done || chunks >= kFlushChunks)) {
+            acc_flush<ENERGY>(acc, A, gx, gy, lane);
+            chunks = 0;
+        }
+        if (cell_done) {
+            if (MODE == kCount) {
+                uint32_t v = 0;
+#pragma unroll
+                for (int d = 0; d < kDirs; ++d)
+                    if (lane == d) v = run[d];
+                if (lane < kDirs) A.dcount[(int64_t)lane * A.ncells + (int64_t)gy * A.nx + gx] = v;
+            }
+#pragma unroll
+            for (int d = 0; d < kDirs; ++d) run[d] = 0u;
+            chunks = 0;
         }
     }
     if (MODE == kScatter && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
-    if (kDep) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < kNTX * kNTY; i += kThreads) {
-            const int nxn = ox + i % kNTX, nyn = oy + i / kNTX;
-            if (nxn < 0 || nyn < 0 || nxn >= A.GX || nyn > A.ny) continue;
-            const int64_t n = (int64_t)nyn * A.GX + nxn;
-            const unsigned long long q = tile_q[i];
-            if (q) atomicAdd(A.acc_q + n, q);
-            if (ENERGY) {
-                const unsigned long long e = tile_e[i];
-                if (e) atomicAdd(A.acc_e + n, e);
-            }
-        }
-    }
 }
 
 // ---- exclusive scan of the new per-cell counts ------------------------------
