@@ -113,25 +113,43 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     const float t = __fmul_rn(k.h, bz);
     const float vxp = __fmaf_rn(vym, t, vxm);
     const float vyp = __fmaf_rn(-vxm, t, vym);
-    const float s = __fdiv_rn(__fmul_rn(2.0f, t), __fmaf_rn(t, t, 1.0f));
+    // s = 2t/(1+t^2) with the approximate reciprocal: both passes compute the
+    // same bits, and its error (~1 ulp) is far below the FP32 state's
+    const float s = __fdividef(__fmul_rn(2.0f, t), __fmaf_rn(t, t, 1.0f));
     Pushed o;
     o.vx = __fadd_rn(__fmaf_rn(vyp, s, vxm), ax);
     o.vy = __fadd_rn(__fmaf_rn(-vxp, s, vym), ay);
     // Position update in cell units (src/mover.cpp:164-165), then re-cell.
     const float px = __fmaf_rn(o.vx, k.dtdx, fx);
     const float py = __fmaf_rn(o.vy, k.dtdy, fy);
-    const float sx = floorf(px), sy = floorf(py);
-    const float ngx = __fadd_rn((float)gx, sx), ngy = __fadd_rn((float)gy, sy);
-    // Absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H).  Written so
-    // that NaN lands outside.
-    const bool alive = (ngx >= 0.0f) && (ngx < (float)nx) && (ngy >= 0.0f) && (ngy < (float)ny);
-    o.left = !(ngx >= 0.0f);
-    o.gx = alive ? (int)ngx : gx;
-    o.gy = alive ? (int)ngy : gy;
-    const int ix = o.gx - gx, iy = o.gy - gy;
-    o.dir = !alive ? -1 : ((ix < -1 || ix > 1 || iy < -1 || iy > 1) ? kFar : (iy + 1) * 3 + (ix + 1));
-    o.fx = fminf(__fsub_rn(px, sx), kOneBelow);
-    o.fy = fminf(__fsub_rn(py, sy), kOneBelow);
+    if (px >= -1.0f && px < 2.0f && py >= -1.0f && py < 2.0f) {
+        // moved at most one cell per axis: floor(p) in {-1, 0, 1}
+        const int sx = (px >= 1.0f) - (px < 0.0f);
+        const int sy = (py >= 1.0f) - (py < 0.0f);
+        const int ngx = gx + sx, ngy = gy + sy;
+        // absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H)
+        const bool alive = ngx >= 0 && ngx < nx && ngy >= 0 && ngy < ny;
+        o.left = ngx < 0;
+        o.gx = ngx;
+        o.gy = ngy;
+        o.dir = alive ? (sy + 1) * 3 + (sx + 1) : -1;
+        const float fsx = (px >= 1.0f) ? 1.0f : ((px < 0.0f) ? -1.0f : 0.0f);
+        const float fsy = (py >= 1.0f) ? 1.0f : ((py < 0.0f) ? -1.0f : 0.0f);
+        o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
+        o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
+    } else {
+        // far jump, or NaN (which lands outside)
+        const float fsx = floorf(px), fsy = floorf(py);
+        const float ngx = __fadd_rn((float)gx, fsx), ngy = __fadd_rn((float)gy, fsy);
+        const bool alive = (ngx >= 0.0f) && (ngx < (float)nx) && (ngy >= 0.0f) && (ngy < (float)ny);
+        o.left = !(ngx >= 0.0f);
+        o.gx = alive ? (int)ngx : gx;
+        o.gy = alive ? (int)ngy : gy;
+        const int ix = o.gx - gx, iy = o.gy - gy;
+        o.dir = !alive ? -1 : ((ix < -1 || ix > 1 || iy < -1 || iy > 1) ? kFar : (iy + 1) * 3 + (ix + 1));
+        o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
+        o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
+    }
     return o;
 }
 
@@ -223,59 +241,39 @@ __device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, con
     }
 }
 
-// Per-lane fixed-point sums of the stayers of the current cell, kept as
-// 32-bit limbs so that the per-cell warp reduction is a handful of
-// redux.sync: charge weights (< 2^40) as 2 x 20-bit limbs, energy weights
-// (< 2^44) as 3 x 15-bit limbs.  A lane adds one particle per chunk and the
-// sums are flushed at least every kFlushChunks chunks, so each limb sum over
-// the warp stays below 2^32.
-constexpr int kFlushChunks = 64;
-
+// Per-lane fixed-point sums of the stayers of the current cell (64-bit; a
+// cell holds at most kMaxPerCell particles, so sums stay below 2^60).
 struct StayAcc {
-    uint32_t q[4][2];
-    uint32_t e[4][3];
+    unsigned long long q[4];
+    unsigned long long e[4];
 };
 
 __device__ __forceinline__ void acc_zero(StayAcc& s) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        s.q[k][0] = s.q[k][1] = 0u;
-        s.e[k][0] = s.e[k][1] = s.e[k][2] = 0u;
-    }
+    for (int k = 0; k < 4; ++k) s.q[k] = s.e[k] = 0ull;
 }
 
 template <bool ENERGY>
 __device__ __forceinline__ void acc_add(StayAcc& s, const Weights& w) {
-    const unsigned long long q[4] = {w.q00, w.q10, w.q01, w.q11};
-    const unsigned long long e[4] = {w.e00, w.e10, w.e01, w.e11};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        s.q[k][0] += (uint32_t)(q[k] & 0xFFFFFull);
-        s.q[k][1] += (uint32_t)(q[k] >> 20);
-        if (ENERGY) {
-            s.e[k][0] += (uint32_t)(e[k] & 0x7FFFull);
-            s.e[k][1] += (uint32_t)((e[k] >> 15) & 0x7FFFull);
-            s.e[k][2] += (uint32_t)(e[k] >> 30);
-        }
+    s.q[0] += w.q00; s.q[1] += w.q10; s.q[2] += w.q01; s.q[3] += w.q11;
+    if (ENERGY) {
+        s.e[0] += w.e00; s.e[1] += w.e10; s.e[2] += w.e01; s.e[3] += w.e11;
     }
 }
 
-// Warp-reduce the limbs and add the cell's four node sums (lane 0).
+// Warp-reduce (butterfly) and add the cell's four node sums (lane 0).
 template <bool ENERGY>
 __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane) {
-    unsigned long long q[4], e[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        q[k] = (unsigned long long)__reduce_add_sync(kFull, s.q[k][0]) +
-               ((unsigned long long)__reduce_add_sync(kFull, s.q[k][1]) << 20);
-        e[k] = 0ull;
-        if (ENERGY)
-            e[k] = (unsigned long long)__reduce_add_sync(kFull, s.e[k][0]) +
-                   ((unsigned long long)__reduce_add_sync(kFull, s.e[k][1]) << 15) +
-                   ((unsigned long long)__reduce_add_sync(kFull, s.e[k][2]) << 30);
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            s.q[k] += __shfl_xor_sync(kFull, s.q[k], o);
+            if (ENERGY) s.e[k] += __shfl_xor_sync(kFull, s.e[k], o);
+        }
     }
     if (lane == 0) {
-        Weights w{q[0], q[1], q[2], q[3], e[0], e[1], e[2], e[3]};
+        Weights w{s.q[0], s.q[1], s.q[2], s.q[3], s.e[0], s.e[1], s.e[2], s.e[3]};
         global_add(A, gx, gy, w, ENERGY);
     }
     acc_zero(s);
@@ -297,11 +295,12 @@ __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, in
 constexpr int kHX = kTileX + 2, kHY = kTileY + 2;  // halo region of cells
 
 template <int MODE, bool ENERGY>
-__global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
+__global__ void __launch_bounds__(kThreads, 4) k_particles(KArgs A) {
     constexpr bool kDep = (MODE != kCount);
     __shared__ uint32_t off_s[kTileY][kTileX + 1];
     __shared__ float4 fld_s[MODE != kDeposit ? (kTileY + 1) * (kTileX + 1) : 1];
     __shared__ uint32_t sub_s[MODE == kScatter ? kDirs * kHX * kHY : 1];
+    __shared__ uint32_t run_s[kWarps][kDirs + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
     const int tw = min(kTileX, A.nx - tgx0), th = min(kTileY, A.ny - tgy0);
@@ -357,12 +356,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
         }
     }
 
-    uint32_t run[kDirs];
-#pragma unroll
-    for (int d = 0; d < kDirs; ++d) run[d] = 0u;
+    if (lane < kDirs) run_s[warp][lane] = 0u;
+    __syncwarp();
     StayAcc acc;
     acc_zero(acc);
-    int chunks = 0;
 
     while (plc < ncell_tile) {
         // the prefetched chunk becomes current
@@ -402,12 +399,22 @@ __global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
         const int dir = valid ? p.dir : -1;
         if (MODE == kScatter) left_exits += __popc(__ballot_sync(kFull, valid && dir < 0 && p.left));
         // rank among this cell's particles leaving in the same direction
+        // (warp multi-split: lanes with equal direction bits form a group)
         uint32_t rank = 0;
+        {
+            const bool ranked = dir >= 0 && dir < kDirs;
+            unsigned same = __ballot_sync(kFull, ranked);
 #pragma unroll
-        for (int d = 0; d < kDirs; ++d) {
-            const unsigned m = __ballot_sync(kFull, dir == d);
-            if (dir == d) rank = run[d] + __popc(m & lt);
-            run[d] += __popc(m);
+            for (int bit = 0; bit < 4; ++bit) {
+                const unsigned b = __ballot_sync(kFull, (dir >> bit) & 1);
+                same &= ((dir >> bit) & 1) ? b : ~b;
+            }
+            const uint32_t before = __popc(same & lt);
+            const uint32_t r0 = ranked ? run_s[warp][dir] : 0u;
+            rank = r0 + before;
+            __syncwarp();
+            if (ranked && before == 0) run_s[warp][dir] = r0 + __popc(same);
+            __syncwarp();
         }
         if (kDep) {
             Weights w{0, 0, 0, 0, 0, 0, 0, 0};
@@ -435,23 +442,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_particles(KArgs A) {
         if (MODE == kCount && dir == kFar)
             atomicAdd(A.farin + (int64_t)p.gy * A.nx + p.gx, 1u);
 
-        ++chunks;
-        const bool cell_done = ci0 + 32 >= cend;
-        if (kDep && (cell_done || chunks >= kFlushChunks)) {
-            acc_flush<ENERGY>(acc, A, gx, gy, lane);
-            chunks = 0;
-        }
-        if (cell_done) {
-            if (MODE == kCount) {
-                uint32_t v = 0;
-#pragma unroll
-                for (int d = 0; d < kDirs; ++d)
-                    if (lane == d) v = run[d];
-                if (lane < kDirs) A.dcount[(int64_t)lane * A.ncells + (int64_t)gy * A.nx + gx] = v;
+        if (ci0 + 32 >= cend) {  // cell done
+            if (kDep) acc_flush<ENERGY>(acc, A, gx, gy, lane);
+            if (lane < kDirs) {
+                if (MODE == kCount)
+                    A.dcount[(int64_t)lane * A.ncells + (int64_t)gy * A.nx + gx] = run_s[warp][lane];
+                run_s[warp][lane] = 0u;
             }
-#pragma unroll
-            for (int d = 0; d < kDirs; ++d) run[d] = 0u;
-            chunks = 0;
+            __syncwarp();
         }
     }
     if (MODE == kScatter && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
