@@ -181,14 +181,15 @@ __device__ __forceinline__ Weights fixed_weights(float fx, float fy, float en) {
         // energy in units of 2^-22 eV (32 bits, clamped below 1024 eV) times
         // 16-bit axis weights: e = E * wx16 * wy16 / 2^32 < 2^32
         const uint32_t E = __float2uint_rn(__fmul_rn(en, 4194304.0f));
-        const uint32_t ax16 = ax >> 4, ay16 = ay >> 4;
+        const uint32_t ax16 = (ax + 8u) >> 4, ay16 = (ay + 8u) >> 4;
         const uint32_t bx16 = 65536u - ax16, by16 = 65536u - ay16;
         const unsigned long long ea = (unsigned long long)E * ax16;
         const unsigned long long eb = (unsigned long long)E * bx16;
-        w.e00 = (eb * by16) >> 32;
-        w.e10 = (ea * by16) >> 32;
-        w.e01 = (eb * ay16) >> 32;
-        w.e11 = (ea * ay16) >> 32;
+        // round to nearest: the products stay below 2^64 - 2^32
+        w.e00 = (eb * by16 + 0x80000000ull) >> 32;
+        w.e10 = (ea * by16 + 0x80000000ull) >> 32;
+        w.e01 = (eb * ay16 + 0x80000000ull) >> 32;
+        w.e11 = (ea * ay16 + 0x80000000ull) >> 32;
     } else {
         w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
     }
@@ -204,7 +205,7 @@ __device__ __forceinline__ float energy_ev(float vx, float vy, float vz, float h
 // Global 64-bit integer reductions (fire-and-forget RED) into the node
 // accumulators.
 __device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
-    if (v) atomicAdd(p, v);
+    atomicAdd(p, v);
 }
 
 __device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w,
@@ -286,174 +287,124 @@ __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, in
 //   kCount   -- push, count leavers per direction (plain stores), far movers
 //               per target (atomics);
 //   kScatter -- push again, place every particle at its deterministic slot
-//               (sub-segment of its target cell for its direction + rank by
-//               ballot), deposit the new positions;
+//               (sub-segment of its target cell for its direction + rank
+//               within the direction), deposit the new positions;
 //   kDeposit -- deposit the current positions (no push).
-// A block owns a kTileX x kTileY tile of cells.  Its prologue stages in
-// shared memory the segment table of the tile, the node fields of the tile
-// and (scatter) the destination sub-segment starts of the tile and its
-// one-cell halo.  Each warp then walks whole cells of the tile, 32 particles
-// per chunk, with the next chunk's loads (possibly of the next cell) issued
-// before the current chunk is processed.
-constexpr int kHX = kTileX + 2, kHY = kTileY + 2;  // halo region of cells
-
+// A block owns a kTileX x kTileY tile of cells and each warp walks whole
+// cells of it: the cell's segment bounds, its four node fields and (scatter)
+// the nine destination sub-segment starts are warp-uniform loads; particles
+// stream through in chunks of 32 with the next chunk's loads issued before
+// the current chunk is processed.
 template <int MODE, bool ENERGY>
-__global__ void __launch_bounds__(kThreads, 4) k_particles(KArgs A) {
+__global__ void __launch_bounds__(kThreads, (MODE == kScatter && ENERGY) ? 3 : 4) k_particles(KArgs A) {
     constexpr bool kDep = (MODE != kCount);
-    __shared__ uint32_t off_s[kTileY][kTileX + 1];
-    __shared__ float4 fld_s[MODE != kDeposit ? (kTileY + 1) * (kTileX + 1) : 1];
-    __shared__ uint32_t sub_s[MODE == kScatter ? kDirs * kHX * kHY : 1];
     __shared__ uint32_t run_s[kWarps][kDirs + 1];
+    __shared__ uint32_t base_s[MODE == kScatter ? kWarps : 1][kDirs + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
-    const int tw = min(kTileX, A.nx - tgx0), th = min(kTileY, A.ny - tgy0);
-
-    // ---- prologue: stage the tile's tables in shared memory ----
-    for (int i = threadIdx.x; i < kTileY * (kTileX + 1); i += kThreads) {
-        const int r = i / (kTileX + 1), x = i % (kTileX + 1);
-        if (r < th && x <= tw) off_s[r][x] = A.off[(int64_t)(tgy0 + r) * A.nx + tgx0 + x];
-    }
-    if (MODE != kDeposit) {
-        for (int i = threadIdx.x; i < (kTileY + 1) * (kTileX + 1); i += kThreads) {
-            const int r = i / (kTileX + 1), x = i % (kTileX + 1);
-            if (r <= th && x <= tw) fld_s[i] = __ldg(A.fld + (int64_t)(tgy0 + r) * A.GX + tgx0 + x);
-        }
-    }
-    if (MODE == kScatter) {
-        for (int i = threadIdx.x; i < kDirs * kHX * kHY; i += kThreads) {
-            const int d = i / (kHX * kHY), rem = i % (kHX * kHY);
-            const int tx = tgx0 - 1 + rem % kHX, ty = tgy0 - 1 + rem / kHX;
-            sub_s[i] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
-                           ? A.sub[(int64_t)d * A.ncells + (int64_t)ty * A.nx + tx]
-                           : 0u;
-        }
-    }
-    __syncthreads();
-
     const unsigned lt = lanemask_lt();
     unsigned long long left_exits = 0;
-    const int ncell_tile = kTileX * kTileY;
 
-    // next cell slot (of this warp) holding particles; empty cells met on the
-    // way get their zero direction counts in the count pass
-    auto next_cell = [&](int from) -> int {
-        for (int l = from; l < ncell_tile; l += kWarps) {
-            const int x = l % kTileX, r = l / kTileX;
-            if (x >= tw || r >= th) continue;
-            if (off_s[r][x + 1] > off_s[r][x]) return l;
-            if (MODE == kCount && lane < kDirs)
-                A.dcount[(int64_t)lane * A.ncells + (int64_t)(tgy0 + r) * A.nx + tgx0 + x] = 0u;
+    for (int lc = warp; lc < kTileX * kTileY; lc += kWarps) {
+        const int gx = tgx0 + (lc % kTileX), gy = tgy0 + (lc / kTileX);
+        if (gx >= A.nx || gy >= A.ny) continue;  // warp-uniform
+        const int64_t c = (int64_t)gy * A.nx + gx;
+        const uint32_t beg = A.off[c], end = A.off[c + 1];
+        if (beg == end) {
+            if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = 0u;
+            continue;
         }
-        return ncell_tile;
-    };
-
-    int plc = next_cell(warp);
-    uint32_t pi0 = plc < ncell_tile ? off_s[plc / kTileX][plc % kTileX] : 0u;
-    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f);
-    float pvz = 0.f;
-    if (plc < ncell_tile) {
-        const uint32_t pe = off_s[plc / kTileX][plc % kTileX + 1];
-        if (pi0 + lane < pe) {
-            pa = __ldcs(A.src_a + pi0 + lane);
-            if (MODE != kCount) pvz = __ldcs(A.src_vz + pi0 + lane);
+        // first chunk's loads go out before the per-cell tables
+        uint32_t i = beg + lane;
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        float vz = 0.f;
+        if (i < end) {
+            a = __ldcs(A.src_a + i);
+            if (MODE != kCount) vz = __ldcs(A.src_vz + i);
         }
-    }
-
-    if (lane < kDirs) run_s[warp][lane] = 0u;
-    __syncwarp();
-    StayAcc acc;
-    acc_zero(acc);
-
-    while (plc < ncell_tile) {
-        // the prefetched chunk becomes current
-        const int clc = plc;
-        const uint32_t ci0 = pi0;
-        const int cx = clc % kTileX, cr = clc / kTileX;
-        const uint32_t cend = off_s[cr][cx + 1];
-        const float4 a = pa;
-        const float vz = pvz;
-        const int gx = tgx0 + cx, gy = tgy0 + cr;
-        // advance the prefetch pointer and issue the next chunk's loads
-        pi0 += 32;
-        if (pi0 >= cend) {
-            plc = next_cell(clc + kWarps);
-            if (plc < ncell_tile) pi0 = off_s[plc / kTileX][plc % kTileX];
+        float4 f00 = make_float4(0, 0, 0, 0), f10 = f00, f01 = f00, f11 = f00;
+        if (MODE != kDeposit) {
+            const int64_t n0 = (int64_t)gy * A.GX + gx;
+            f00 = __ldg(A.fld + n0);
+            f10 = __ldg(A.fld + n0 + 1);
+            f01 = __ldg(A.fld + n0 + A.GX);
+            f11 = __ldg(A.fld + n0 + A.GX + 1);
         }
-        pa = make_float4(0.f, 0.f, 0.f, 0.f);
-        pvz = 0.f;
-        if (plc < ncell_tile) {
-            const uint32_t pe = off_s[plc / kTileX][plc % kTileX + 1];
-            if (pi0 + lane < pe) {
-                pa = __ldcs(A.src_a + pi0 + lane);
-                if (MODE != kCount) pvz = __ldcs(A.src_vz + pi0 + lane);
+        if (lane < kDirs) {
+            run_s[warp][lane] = 0u;
+            if (MODE == kScatter) {
+                const int tx = gx + lane % 3 - 1, ty = gy + lane / 3 - 1;
+                base_s[warp][lane] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
+                                         ? __ldg(A.sub + (int64_t)lane * A.ncells + (int64_t)ty * A.nx + tx)
+                                         : 0u;
             }
         }
+        __syncwarp();
+        StayAcc acc;
+        acc_zero(acc);
 
-        const bool valid = ci0 + lane < cend;
-        Pushed p;
-        if (MODE == kDeposit) {
-            p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
-            p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
-        } else {
-            const int b = cr * (kTileX + 1) + cx;
-            p = push_one(a, fld_s[b], fld_s[b + 1], fld_s[b + kTileX + 1], fld_s[b + kTileX + 2],
-                         A.k, gx, gy, A.nx, A.ny);
-        }
-        const int dir = valid ? p.dir : -1;
-        if (MODE == kScatter) left_exits += __popc(__ballot_sync(kFull, valid && dir < 0 && p.left));
-        // rank among this cell's particles leaving in the same direction
-        // (warp multi-split: lanes with equal direction bits form a group)
-        uint32_t rank = 0;
-        {
-            const bool ranked = dir >= 0 && dir < kDirs;
-            unsigned same = __ballot_sync(kFull, ranked);
-#pragma unroll
-            for (int bit = 0; bit < 4; ++bit) {
-                const unsigned b = __ballot_sync(kFull, (dir >> bit) & 1);
-                same &= ((dir >> bit) & 1) ? b : ~b;
+        for (uint32_t i0 = beg; i0 < end; i0 += 32) {
+            const bool valid = i < end;
+            const uint32_t inext = i + 32;
+            float4 an = make_float4(0.f, 0.f, 0.f, 0.f);
+            float vzn = 0.f;
+            if (inext < end) {
+                an = __ldcs(A.src_a + inext);
+                if (MODE != kCount) vzn = __ldcs(A.src_vz + inext);
             }
-            const uint32_t before = __popc(same & lt);
-            const uint32_t r0 = ranked ? run_s[warp][dir] : 0u;
-            rank = r0 + before;
-            __syncwarp();
-            if (ranked && before == 0) run_s[warp][dir] = r0 + __popc(same);
-            __syncwarp();
-        }
-        if (kDep) {
-            Weights w{0, 0, 0, 0, 0, 0, 0, 0};
-            if (dir >= 0) {
-                const float en = ENERGY ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
-                w = fixed_weights<ENERGY>(p.fx, p.fy, en);
-            }
-            if (dir == kStay) {
-                acc_add<ENERGY>(acc, w);
-            } else if (MODE == kScatter && dir >= 0) {
-                global_add(A, p.gx, p.gy, w, ENERGY);
-            }
-        }
-        if (MODE == kScatter && dir >= 0) {
-            uint32_t dst;
-            if (dir == kFar) {
-                const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
-                dst = __ldg(A.sub + (int64_t)kFar * A.ncells + nc) + atomicAdd(A.farcur + nc, 1u);
+            Pushed p;
+            if (MODE == kDeposit) {
+                p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
+                p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
             } else {
-                const int tx = cx + dir % 3, ty = cr + dir / 3;  // halo coordinates
-                dst = sub_s[dir * kHX * kHY + ty * kHX + tx] + rank;
+                p = push_one(a, f00, f10, f01, f11, A.k, gx, gy, A.nx, A.ny);
             }
-            store_particle(A, dst, p, vz);
-        }
-        if (MODE == kCount && dir == kFar)
-            atomicAdd(A.farin + (int64_t)p.gy * A.nx + p.gx, 1u);
-
-        if (ci0 + 32 >= cend) {  // cell done
-            if (kDep) acc_flush<ENERGY>(acc, A, gx, gy, lane);
-            if (lane < kDirs) {
-                if (MODE == kCount)
-                    A.dcount[(int64_t)lane * A.ncells + (int64_t)gy * A.nx + gx] = run_s[warp][lane];
-                run_s[warp][lane] = 0u;
+            const int dir = valid ? p.dir : -1;
+            if (MODE == kScatter) left_exits += __popc(__ballot_sync(kFull, valid && dir < 0 && p.left));
+            // rank among this cell's particles leaving in the same direction
+            // (warp multi-split: lanes with equal direction bits form a group)
+            uint32_t rank = 0;
+            {
+                const bool ranked = dir >= 0 && dir < kDirs;
+                unsigned same = __ballot_sync(kFull, ranked);
+#pragma unroll
+                for (int bit = 0; bit < 4; ++bit) {
+                    const unsigned b = __ballot_sync(kFull, (dir >> bit) & 1);
+                    same &= ((dir >> bit) & 1) ? b : ~b;
+                }
+                const uint32_t before = __popc(same & lt);
+                const uint32_t r0 = ranked ? run_s[warp][dir] : 0u;
+                rank = r0 + before;
+                __syncwarp();
+                if (ranked && before == 0) run_s[warp][dir] = r0 + __popc(same);
+                __syncwarp();
             }
-            __syncwarp();
+            if (kDep) {
+                const bool live = dir >= 0;
+                const float en = (ENERGY && live) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
+                const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
+                if (dir == kStay) acc_add<ENERGY>(acc, w);
+                if (MODE == kScatter && live && dir != kStay) global_add(A, p.gx, p.gy, w, ENERGY);
+            }
+            if (MODE == kScatter && dir >= 0) {
+                uint32_t dst;
+                if (dir == kFar) {
+                    const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
+                    dst = __ldg(A.sub + (int64_t)kFar * A.ncells + nc) + atomicAdd(A.farcur + nc, 1u);
+                } else {
+                    dst = base_s[warp][dir] + rank;
+                }
+                store_particle(A, dst, p, vz);
+            }
+            if (MODE == kCount && dir == kFar)
+                atomicAdd(A.farin + (int64_t)p.gy * A.nx + p.gx, 1u);
+            i = inext;
+            a = an;
+            vz = vzn;
         }
+        if (kDep) acc_flush<ENERGY>(acc, A, gx, gy, lane);
+        if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = run_s[warp][lane];
+        __syncwarp();
     }
     if (MODE == kScatter && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
 }
