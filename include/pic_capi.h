@@ -213,6 +213,33 @@ int pic_profile_read(pic_ctx* ctx, double* ms, int64_t* calls, int reset);
 /* Kernel launches issued by this context since creation. */
 int pic_launch_count(pic_ctx* ctx, int64_t* n);
 
+/* ---- allocation-free deposit ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they deposit -- a host framework that owns a fixed device
+ * memory budget and only hands out buffers it has already sized, or a
+ * time-critical loop where cudaMalloc/cudaFree (which may synchronise the
+ * device) are not allowed.  Deposits n reference Points (device memory,
+ * 56-byte records; pointer == -1 and out-of-domain points are skipped) of
+ * one species on an nx x ny cell grid: dev_final_mesh[(nx+1)*(ny+1)] is
+ * overwritten with the species' final_mesh and, when dev_rho is not NULL,
+ * final_mesh * (-charge/epsilon) is added to dev_rho.  Same arithmetic as
+ * pic_import_points + pic_charge_deposition (bit-identical final_mesh); no
+ * energy mesh.  Enqueued on cuda_stream (NULL: the default stream); calls no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *   - Scratch: one file-scope device array of 2^19 64-bit accumulators
+ *     (4 MiB; grids up to 524,288 nodes, larger ones are rejected with
+ *     PIC_ERR_CAPACITY), held by every GPU that loads the library until the
+ *     process exits, cleared at the start of every call.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and must be serialised by the caller. */
+int pic_deposit_points_noalloc(const pic_point* dev_points, int64_t n, int32_t nx, int32_t ny,
+                               double xmax, double ymax, const pic_species_desc* species,
+                               double surf_area, double epsilon, double* dev_final_mesh,
+                               double* dev_rho, void* cuda_stream);
+
 /* ---- Poisson controls -------------------------------------------------- */
 int pic_set_poisson(pic_ctx* ctx, int solver, int warm_start, double tol, int maxit);
 /* Iterations, achieved relative residual and device milliseconds of the most
