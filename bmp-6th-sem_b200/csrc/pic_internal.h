@@ -125,6 +125,15 @@ struct PoissonState {
     double last_relres = 0, last_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float* net_guess = nullptr;  // learned warm start output (nodes), optional
+    // levels >= fused_first run in one thread block (k_mg_fused)
+    int fused_first = 0;
+    size_t fused_smem = 0;
+    alignas(16) unsigned char fused_desc[1024] = {};
+    // the PCG loop as a graph with a device-side while node, per solver
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int body_nodes[2] = {0, 0};
+    bool graph_failed = false;
 };
 
 }  // namespace picb200

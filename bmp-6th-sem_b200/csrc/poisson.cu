@@ -28,11 +28,21 @@
 // spacing 2^l*dx; restriction is full weighting, prolongation bilinear, the
 // smoother red-black Gauss-Seidel with the colour order reversed after the
 // coarse correction, so the V-cycle is a symmetric preconditioner.  The
-// coarsest level (min(nx,ny) <= 4) gets symmetric RB-GS sweeps in one block.
+// coarsest level (min(nx,ny) <= 4) gets symmetric RB-GS sweeps.  All levels
+// from the first one whose hierarchy fits in shared memory down to the
+// coarsest run inside one thread block (k_mg_fused).
+//
+// The PCG loop is one CUDA graph: a while-conditional node whose body is one
+// iteration (V-cycle, z.r, p update, A p, x/r update, convergence test); the
+// test kernel sets the condition on the device, so a solve costs one graph
+// launch and one host synchronisation.  Without conditional-node support the
+// same kernels run from a host loop.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <string>
 
 #include "pic_internal.h"
 
@@ -53,7 +63,11 @@ enum {
     S_PQ = 3,   // p.Ap
     S_RZ_OLD = 4,
     S_TRUE_RR = 5,
-    S_COUNT = 6  // [6] is the arrival counter (as double bits)
+    S_COUNT = 6,  // [6] is the arrival counter (as double bits)
+    S_IT = 7,     // iterations done
+    S_TOL2 = 8,   // tol^2
+    S_MAXIT = 9,  // iteration limit
+    S_STATUS = 10 // 0 running/converged, 1 iteration limit, 2 not finite
 };
 
 struct Grid64 {
@@ -167,10 +181,14 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_setup(Grid64 g, const uint8
     // slots: S_RR = r.r, S_RR+1 = S_RZ holds bb temporarily; moved by k_fix_bb
 }
 
-__global__ void k_fix_bb(double* scal) {
+__global__ void k_fix_bb(double* scal, double tol2, int maxit, int restart) {
     scal[S_BB] = scal[S_RZ];
     scal[S_RZ] = 0.0;
     scal[S_RZ_OLD] = 0.0;
+    scal[S_TOL2] = tol2;
+    scal[S_MAXIT] = (double)maxit;
+    scal[S_STATUS] = 0.0;
+    if (!restart) scal[S_IT] = 0.0;
 }
 
 // z = M^-1 r (from the MG output or the diagonal); partial r.z
@@ -190,27 +208,31 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t nodes, const uin
     reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_RZ);
 }
 
-// p = z + beta p_old (beta = rz/rz_old, 0 on the first iteration);
+// p = z + beta p (beta = rz/rz_old; 0 on the first iteration after a
+// (re)start, marked by rz_old == 0)
+__global__ void k_pcg_p(int64_t nodes, const uint8_t* mask, const double* z, double* p,
+                        const double* scal) {
+    const double ro = scal[S_RZ_OLD];
+    const double beta = ro == 0.0 ? 0.0 : scal[S_RZ] / ro;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = mask[i] ? 0.0 : z[i] + beta * p[i];
+}
+
 // q = A p; partial p.q
-__global__ void __launch_bounds__(kRedThreads) k_pcg_p_ap(Grid64 g, const uint8_t* mask,
-                                                          const double* z, const double* p_old,
-                                                          double* p_new, double* q, int first,
-                                                          double* partials, int nblocks,
-                                                          unsigned* arrive, double* scal) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_ap(Grid64 g, const uint8_t* mask,
+                                                        const double* p, double* q,
+                                                        double* partials, int nblocks,
+                                                        unsigned* arrive, double* scal) {
     const int64_t nodes = (int64_t)g.GX * g.GY;
-    const double beta = first ? 0.0 : scal[S_RZ] / scal[S_RZ_OLD];
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
-        double pi = 0.0, qi = 0.0;
-        if (!mask[i]) {
-            auto P = [&](int64_t k) { return mask[k] ? 0.0 : z[k] + beta * p_old[k]; };
-            pi = z[i] + beta * p_old[i];
-            qi = g.cd * pi - g.cx * (P(i - 1) + P(i + 1)) - g.cy * (P(i - g.GX) + P(i + g.GX));
-        }
-        p_new[i] = pi;
+        double qi = 0.0;
+        if (!mask[i])
+            qi = g.cd * p[i] - g.cx * (p[i - 1] + p[i + 1]) - g.cy * (p[i - g.GX] + p[i + g.GX]);
         q[i] = qi;
-        acc[0] += pi * qi;
+        acc[0] += p[i] * qi;
     }
     reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_PQ);
 }
@@ -237,7 +259,22 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int64_t nodes, const
     reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_RR);
 }
 
-__global__ void k_shift_rz(double* scal) { scal[S_RZ_OLD] = scal[S_RZ]; }
+// End of an iteration: count it, keep rz for the next beta, decide whether
+// to go on (and tell the graph's while node when there is one).
+__global__ void k_pcg_cond(double* scal, cudaGraphConditionalHandle handle, int use_handle) {
+    const double it = scal[S_IT] + 1.0;
+    scal[S_IT] = it;
+    scal[S_RZ_OLD] = scal[S_RZ];
+    const double rr = scal[S_RR];
+    const bool finite = isfinite(rr);
+    bool go = finite && rr > scal[S_TOL2] * scal[S_BB];
+    if (go && it >= scal[S_MAXIT]) {
+        go = false;
+        scal[S_STATUS] = 1.0;
+    }
+    if (!finite) scal[S_STATUS] = 2.0;
+    if (use_handle) cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
 
 // true residual of the final iterate (reported relres)
 __global__ void __launch_bounds__(kRedThreads) k_true_residual(Grid64 g, const uint8_t* mask,
@@ -358,6 +395,127 @@ __global__ void k_mg_coarse(LevelDev L, int sweeps) {
     }
 }
 
+// All levels from `first` down to the coarsest in one thread block, in
+// shared memory: the same operations as the per-level kernels (zero-start red
+// sweep, black, (red, black) x (kNu-1), restrict; coarsest: symmetric sweeps;
+// then prolong + (black, red) x kNu), with block barriers between them.
+constexpr int kMaxFused = 12;
+constexpr int kFusedThreads = 1024;
+
+struct FusedLevels {
+    int n;  // fused levels
+    int GX[kMaxFused], GY[kMaxFused];
+    float cx[kMaxFused], cy[kMaxFused], cd[kMaxFused];
+    int ox[kMaxFused], ob[kMaxFused], om[kMaxFused];  // byte offsets in shared memory
+    const uint8_t* gmask[kMaxFused];
+    const float* gb;  // right-hand side of the first fused level
+    float* gx;        // its solution (output)
+    int sweeps;
+};
+
+__global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    auto X = [&](int l) { return reinterpret_cast<float*>(smem + F.ox[l]); };
+    auto B = [&](int l) { return reinterpret_cast<float*>(smem + F.ob[l]); };
+    auto M = [&](int l) { return reinterpret_cast<uint8_t*>(smem + F.om[l]); };
+    const int tid = threadIdx.x;
+    for (int l = 0; l < F.n; ++l) {
+        const int n = F.GX[l] * F.GY[l];
+        for (int k = tid; k < n; k += kFusedThreads) M(l)[k] = F.gmask[l][k];
+    }
+    {
+        const int n = F.GX[0] * F.GY[0];
+        for (int k = tid; k < n; k += kFusedThreads) B(0)[k] = F.gb[k];
+    }
+    __syncthreads();
+    auto sweep = [&](int l, int color) {
+        const int GX = F.GX[l], n = GX * F.GY[l];
+        float* x = X(l);
+        const float* b = B(l);
+        const uint8_t* m = M(l);
+        for (int k = tid; k < n; k += kFusedThreads) {
+            const int i = k % GX, j = k / GX;
+            if (((i + j) & 1) != color || m[k]) continue;
+            x[k] = __fmaf_rn(F.cx[l], x[k - 1] + x[k + 1], __fmaf_rn(F.cy[l], x[k - GX] + x[k + GX], b[k])) / F.cd[l];
+        }
+        __syncthreads();
+    };
+    auto residual = [&](int l, int i, int j) -> float {
+        const int GX = F.GX[l];
+        if (i < 0 || j < 0 || i >= GX || j >= F.GY[l]) return 0.0f;
+        const int k = j * GX + i;
+        if (M(l)[k]) return 0.0f;
+        const float* x = X(l);
+        const float ax = F.cd[l] * x[k] - F.cx[l] * (x[k - 1] + x[k + 1]) - F.cy[l] * (x[k - GX] + x[k + GX]);
+        return B(l)[k] - ax;
+    };
+    for (int l = 0; l < F.n - 1; ++l) {
+        const int GX = F.GX[l], n = GX * F.GY[l];
+        for (int k = tid; k < n; k += kFusedThreads) {
+            const int i = k % GX, j = k / GX;
+            X(l)[k] = (((i + j) & 1) == 0 && !M(l)[k]) ? B(l)[k] / F.cd[l] : 0.0f;
+        }
+        __syncthreads();
+        sweep(l, 1);
+        for (int s = 1; s < kNu; ++s) {
+            sweep(l, 0);
+            sweep(l, 1);
+        }
+        const int CGX = F.GX[l + 1], cn = CGX * F.GY[l + 1];
+        for (int kc = tid; kc < cn; kc += kFusedThreads) {
+            if (M(l + 1)[kc]) {
+                B(l + 1)[kc] = 0.0f;
+                continue;
+            }
+            const int i = 2 * (kc % CGX), j = 2 * (kc / CGX);
+            float s = 4.0f * residual(l, i, j);
+            s += 2.0f * (residual(l, i - 1, j) + residual(l, i + 1, j) + residual(l, i, j - 1) +
+                         residual(l, i, j + 1));
+            s += residual(l, i - 1, j - 1) + residual(l, i + 1, j - 1) + residual(l, i - 1, j + 1) +
+                 residual(l, i + 1, j + 1);
+            B(l + 1)[kc] = s * 0.0625f;
+        }
+        __syncthreads();
+    }
+    {
+        const int l = F.n - 1, n = F.GX[l] * F.GY[l];
+        for (int k = tid; k < n; k += kFusedThreads) X(l)[k] = 0.0f;
+        __syncthreads();
+        for (int s = 0; s < F.sweeps; ++s) {
+            sweep(l, 0);
+            sweep(l, 1);
+        }
+        for (int s = 0; s < F.sweeps; ++s) {
+            sweep(l, 1);
+            sweep(l, 0);
+        }
+    }
+    for (int l = F.n - 2; l >= 0; --l) {
+        const int GX = F.GX[l], n = GX * F.GY[l], CGX = F.GX[l + 1];
+        const float* xc = X(l + 1);
+        for (int k = tid; k < n; k += kFusedThreads) {
+            if (M(l)[k]) continue;
+            const int i = k % GX, j = k / GX, I = i >> 1, J = j >> 1;
+            const bool ox = i & 1, oy = j & 1;
+            float v;
+            if (!ox && !oy) v = xc[J * CGX + I];
+            else if (ox && !oy) v = 0.5f * (xc[J * CGX + I] + xc[J * CGX + I + 1]);
+            else if (!ox && oy) v = 0.5f * (xc[J * CGX + I] + xc[(J + 1) * CGX + I]);
+            else v = 0.25f * (xc[J * CGX + I] + xc[J * CGX + I + 1] + xc[(J + 1) * CGX + I] + xc[(J + 1) * CGX + I + 1]);
+            X(l)[k] += v;
+        }
+        __syncthreads();
+        for (int s = 0; s < kNu; ++s) {
+            sweep(l, 1);
+            sweep(l, 0);
+        }
+    }
+    {
+        const int n = F.GX[0] * F.GY[0];
+        for (int k = tid; k < n; k += kFusedThreads) F.gx[k] = X(0)[k];
+    }
+}
+
 // injected Dirichlet mask of a coarse level
 __global__ void k_mg_coarse_mask(const uint8_t* fmask, int fGX, int fGY, uint8_t* cmask, int cGX,
                                  int cGY) {
@@ -429,36 +587,105 @@ Grid64 fine_grid(pic_ctx* c) {
 
 unsigned* arrive_ptr(PoissonState& ps) { return reinterpret_cast<unsigned*>(ps.scal + S_COUNT); }
 
-int vcycle(pic_ctx* c) {
+// V-cycle on level 0 (b = r32 -> x = z32) enqueued on stream st; returns
+// the number of kernels launched.
+int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
     PoissonState& ps = c->ps;
-    const int L = (int)ps.levels.size();
+    const int kf = ps.fused_first;
     const dim3 b2(32, 8);
-    for (int l = 0; l < L - 1; ++l) {
+    int launches = 0;
+    for (int l = 0; l < kf; ++l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const dim3 gn = grid2d(F.GX, F.GY, b2);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        k_mg_init<<<gn, b2, 0, c->stream>>>(F);
-        k_mg_rbgs<<<gh, b2, 0, c->stream>>>(F, 1);
+        k_mg_init<<<gn, b2, 0, st>>>(F);
+        k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
         for (int s = 1; s < kNu; ++s) {
-            k_mg_rbgs<<<gh, b2, 0, c->stream>>>(F, 0);
-            k_mg_rbgs<<<gh, b2, 0, c->stream>>>(F, 1);
+            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 0);
+            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
         }
-        k_mg_restrict<<<grid2d(C.GX, C.GY, b2), b2, 0, c->stream>>>(F, C);
+        k_mg_restrict<<<grid2d(C.GX, C.GY, b2), b2, 0, st>>>(F, C);
+        launches += 3 + 2 * kNu - 1;
     }
-    k_mg_coarse<<<1, 256, 0, c->stream>>>(as_dev(ps.levels[L - 1]), kCoarseSweeps);
-    c->launches += 1 + (int64_t)(L - 1) * (2 + 2 * kNu + 2 * kNu);
-    for (int l = L - 2; l >= 0; --l) {
+    k_mg_fused<<<1, kFusedThreads, ps.fused_smem, st>>>(*reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    launches += 1;
+    for (int l = kf - 1; l >= 0; --l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        k_mg_prolong<<<grid2d(F.GX, F.GY, b2), b2, 0, c->stream>>>(F, C);
+        k_mg_prolong<<<grid2d(F.GX, F.GY, b2), b2, 0, st>>>(F, C);
         for (int s = 0; s < kNu; ++s) {
-            k_mg_rbgs<<<gh, b2, 0, c->stream>>>(F, 1);
-            k_mg_rbgs<<<gh, b2, 0, c->stream>>>(F, 0);
+            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
+            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 0);
         }
+        launches += 1 + 2 * kNu;
     }
-    PIC_CUDA(cudaGetLastError());
+    return launches;
+}
+
+// One PCG iteration enqueued on st; returns the number of kernels.
+int enqueue_iteration(pic_ctx* c, cudaStream_t st, bool jacobi,
+                      cudaGraphConditionalHandle handle, int use_handle) {
+    PoissonState& ps = c->ps;
+    const Grid64 g = fine_grid(c);
+    const int nb = ps.nblocks;
+    unsigned* arrive = arrive_ptr(ps);
+    int launches = 0;
+    if (!jacobi) launches += enqueue_vcycle(c, st);
+    k_pcg_rz<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
+                                         jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
+    k_pcg_p<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.z, ps.p[0], ps.scal);
+    k_pcg_ap<<<nb, kRedThreads, 0, st>>>(g, c->mask, ps.p[0], ps.q, ps.partials, nb, arrive, ps.scal);
+    k_pcg_update<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.p[0], ps.q, c->phi, ps.r,
+                                             ps.levels[0].b, ps.partials, nb, arrive, ps.scal);
+    k_pcg_cond<<<1, 1, 0, st>>>(ps.scal, handle, use_handle);
+    return launches + 5;
+}
+
+__global__ void k_cond_init(const double* scal, cudaGraphConditionalHandle handle) {
+    const double rr = scal[S_RR], bb = scal[S_BB];
+    cudaGraphSetConditional(handle, (bb > 0.0 && rr > scal[S_TOL2] * bb) ? 1u : 0u);
+}
+
+// Graph: k_cond_init -> while (condition) { one PCG iteration }.
+int build_graph(pic_ctx* c, bool jacobi) {
+    PoissonState& ps = c->ps;
+    const int slot = jacobi ? 1 : 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphConditionalHandle handle;
+    PIC_CUDA(cudaGraphCreate(&graph, 0));
+    auto fail_graph = [&](cudaError_t e) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return fail(PIC_ERR_CUDA, std::string("PCG graph: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return fail_graph(e);
+    cudaGraphNode_t n0;
+    double* scal = ps.scal;
+    void* args[] = {&scal, &handle};
+    cudaKernelNodeParams kp{};
+    kp.func = (void*)k_cond_init;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    if ((e = cudaGraphAddKernelNode(&n0, graph, nullptr, 0, &kp)) != cudaSuccess) return fail_graph(e);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    if ((e = cudaGraphAddNode(&wnode, graph, &n0, 1, &cp)) != cudaSuccess) return fail_graph(e);
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(ps.cap_stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeRelaxed)) != cudaSuccess)
+        return fail_graph(e);
+    ps.body_nodes[slot] = enqueue_iteration(c, ps.cap_stream, jacobi, handle, 1);
+    if ((e = cudaStreamEndCapture(ps.cap_stream, &body)) != cudaSuccess) return fail_graph(e);
+    if ((e = cudaGraphInstantiate(&ps.gexec[slot], graph, 0)) != cudaSuccess) return fail_graph(e);
+    cudaGraphDestroy(graph);
     return PIC_OK;
 }
 
@@ -525,6 +752,50 @@ int poisson_setup(pic_ctx* c) {
         hx *= 2;
         hy *= 2;
     }
+    // fuse every level from the first whose hierarchy fits in shared memory
+    const int L = (int)ps.levels.size();
+    auto level_bytes = [&](int l) {
+        const size_t n = (size_t)ps.levels[l].nodes;
+        return ((n * 4 + 15) & ~(size_t)15) * 2 + ((n + 15) & ~(size_t)15);
+    };
+    const size_t kSmemBudget = 220 * 1024;
+    size_t total = 0;
+    int kf = L;
+    for (int l = L - 1; l >= 0; --l) {
+        if (total + level_bytes(l) > kSmemBudget || L - l > kMaxFused) break;
+        total += level_bytes(l);
+        kf = l;
+    }
+    if (kf == L) return fail(PIC_ERR_CONFIG, "coarsest multigrid level does not fit in shared memory");
+    ps.fused_first = kf;
+    FusedLevels F{};
+    F.n = L - kf;
+    size_t off = 0;
+    for (int l = kf; l < L; ++l) {
+        const MGLevel& M = ps.levels[l];
+        const int i = l - kf;
+        const size_t n = (size_t)M.nodes;
+        F.GX[i] = M.GX;
+        F.GY[i] = M.GY;
+        F.cx[i] = M.cx;
+        F.cy[i] = M.cy;
+        F.cd[i] = M.cd;
+        F.ox[i] = (int)off;
+        off += (n * 4 + 15) & ~(size_t)15;
+        F.ob[i] = (int)off;
+        off += (n * 4 + 15) & ~(size_t)15;
+        F.om[i] = (int)off;
+        off += (n + 15) & ~(size_t)15;
+        F.gmask[i] = M.mask;
+    }
+    F.gb = ps.levels[kf].b;
+    F.gx = ps.levels[kf].x;
+    F.sweeps = kCoarseSweeps;
+    static_assert(sizeof(FusedLevels) <= sizeof(ps.fused_desc), "fused level table");
+    std::memcpy(ps.fused_desc, &F, sizeof(F));
+    ps.fused_smem = off;
+    PIC_CUDA(cudaFuncSetAttribute(k_mg_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
+    PIC_CUDA(cudaStreamCreateWithFlags(&ps.cap_stream, cudaStreamNonBlocking));
     return PIC_OK;
 }
 
@@ -547,6 +818,9 @@ void poisson_free(pic_ctx* c) {
     if (ps.host_scal) cudaFreeHost(ps.host_scal);
     if (ps.ev0) cudaEventDestroy(ps.ev0);
     if (ps.ev1) cudaEventDestroy(ps.ev1);
+    for (int i = 0; i < 2; ++i)
+        if (ps.gexec[i]) cudaGraphExecDestroy(ps.gexec[i]);
+    if (ps.cap_stream) cudaStreamDestroy(ps.cap_stream);
     ps = PoissonState{};
 }
 
@@ -556,88 +830,74 @@ int poisson_solve(pic_ctx* c) {
     const Grid64 g = fine_grid(c);
     const int nb = ps.nblocks;
     unsigned* arrive = arrive_ptr(ps);
+    const bool jacobi = ps.solver == PIC_SOLVER_JACOBI_PCG;
+    const int slot = jacobi ? 1 : 0;
     PIC_CUDA(cudaEventRecord(ps.ev0, c->stream));
     prof_begin(c, PIC_PHASE_POISSON);
     const bool zero_start = (ps.warm == PIC_WARM_ZERO) || !ps.have_prev;
     k_overwrite_rho<<<(unsigned)((nodes + 255) / 256), 256, 0, c->stream>>>(
         nodes, c->mask, c->dir_val, c->rho, c->phi, zero_start ? 1 : 0);
+    c->launches += 1;
     if (ps.warm == PIC_WARM_LEARNED && ps.have_prev && ps.net_guess) {
         // the network's guess replaces phi on non-electrode nodes
         k_apply_guess<<<(unsigned)((nodes + 255) / 256), 256, 0, c->stream>>>(nodes, c->mask,
                                                                               ps.net_guess, c->phi);
+        c->launches += 1;
     }
-    float* r32 = ps.levels[0].b;
-    float* z32 = ps.levels[0].x;
-    // r = b - A x, ||r||^2 and ||b_red||^2 into the device scalars
-    auto setup = [&]() -> int {
+    if (!ps.gexec[slot] && !ps.graph_failed) {
+        if (build_graph(c, jacobi) != PIC_OK) ps.graph_failed = true;  // host loop below
+    }
+    const double tol2 = ps.tol * ps.tol;
+    int restarts = 0;
+    double bb = 0, true_rr = 0;
+    int status = PIC_OK;
+    for (;;) {
         k_pcg_setup<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->dir_val, c->rho, c->phi,
-                                                       ps.r, r32, ps.partials, nb, arrive, ps.scal);
-        k_fix_bb<<<1, 1, 0, c->stream>>>(ps.scal);
+                                                       ps.r, ps.levels[0].b, ps.partials, nb,
+                                                       arrive, ps.scal);
+        k_fix_bb<<<1, 1, 0, c->stream>>>(ps.scal, tol2, ps.maxit, restarts > 0 ? 1 : 0);
         c->launches += 2;
         PIC_CUDA(cudaGetLastError());
-        PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost,
-                                 c->stream));
-        PIC_CUDA(cudaStreamSynchronize(c->stream));
-        return PIC_OK;
-    };
-    PIC_TRY(setup());
-    c->launches += 1;  // overwrite
-    const double bb = ps.host_scal[S_BB];
-    double rr = ps.host_scal[S_RR];
-    const double target = ps.tol * ps.tol * bb;
-    int it = 0, restarts = 0;
-    int status = PIC_OK;
-    const bool jacobi = ps.solver == PIC_SOLVER_JACOBI_PCG;
-    double true_rr = rr;
-    for (;;) {
-        bool first = true;
-        while (rr > target && bb > 0) {
-            if (it >= ps.maxit) {
-                status = PIC_ERR_NOT_CONVERGED;
-                break;
-            }
-            if (!jacobi) PIC_TRY(vcycle(c));
-            k_pcg_rz<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, ps.r, z32, 1.0 / g.cd,
-                                                        jacobi ? 1 : 0, ps.z, ps.partials, nb,
-                                                        arrive, ps.scal);
-            double* p_old = ps.p[ps.pcur];
-            double* p_new = ps.p[ps.pcur ^ 1];
-            k_pcg_p_ap<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, ps.z, p_old, p_new, ps.q,
-                                                          first ? 1 : 0, ps.partials, nb, arrive,
-                                                          ps.scal);
-            ps.pcur ^= 1;
-            k_pcg_update<<<nb, kRedThreads, 0, c->stream>>>(nodes, c->mask, p_new, ps.q, c->phi,
-                                                            ps.r, r32, ps.partials, nb, arrive,
-                                                            ps.scal);
-            k_shift_rz<<<1, 1, 0, c->stream>>>(ps.scal);
-            c->launches += 4;
-            PIC_CUDA(cudaGetLastError());
-            PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_RR, ps.scal + S_RR, sizeof(double),
+        if (ps.gexec[slot]) {
+            PIC_CUDA(cudaGraphLaunch(ps.gexec[slot], c->stream));
+        } else {
+            // host-driven loop: one synchronisation per iteration
+            PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 16 * sizeof(double),
                                      cudaMemcpyDeviceToHost, c->stream));
             PIC_CUDA(cudaStreamSynchronize(c->stream));
-            rr = ps.host_scal[S_RR];
-            first = false;
-            ++it;
-            if (!std::isfinite(rr)) {
-                status = PIC_ERR_NOT_CONVERGED;
-                break;
+            double rr = ps.host_scal[S_RR];
+            const double b0 = ps.host_scal[S_BB];
+            double it = ps.host_scal[S_IT];
+            while (b0 > 0 && rr > tol2 * b0 && std::isfinite(rr) && it < ps.maxit) {
+                c->launches += enqueue_iteration(c, c->stream, jacobi, 0, 0);
+                PIC_CUDA(cudaGetLastError());
+                PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 16 * sizeof(double),
+                                         cudaMemcpyDeviceToHost, c->stream));
+                PIC_CUDA(cudaStreamSynchronize(c->stream));
+                rr = ps.host_scal[S_RR];
+                it = ps.host_scal[S_IT];
             }
         }
         // the recursively updated residual can drift from b - A x: check the
-        // true residual and restart from the current iterate if it is above
-        // the target
+        // true residual and restart from the current iterate if needed
         k_true_residual<<<nb, kRedThreads, 0, c->stream>>>(g, c->mask, c->rho, c->phi, ps.partials,
                                                            nb, arrive, ps.scal);
         c->launches += 1;
-        PIC_CUDA(cudaMemcpyAsync(ps.host_scal + S_TRUE_RR, ps.scal + S_TRUE_RR, sizeof(double),
-                                 cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaMemcpyAsync(ps.host_scal, ps.scal, 16 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
         PIC_CUDA(cudaStreamSynchronize(c->stream));
+        bb = ps.host_scal[S_BB];
         true_rr = ps.host_scal[S_TRUE_RR];
-        if (status != PIC_OK || bb <= 0 || true_rr <= target || restarts >= 3) break;
+        const double st = ps.host_scal[S_STATUS];
+        if (st != 0.0) {
+            status = PIC_ERR_NOT_CONVERGED;
+            break;
+        }
+        if (bb <= 0 || true_rr <= tol2 * bb || restarts >= 3) break;
         ++restarts;
-        PIC_TRY(setup());
-        rr = ps.host_scal[S_RR];
     }
+    const int it = (int)ps.host_scal[S_IT];
+    if (ps.gexec[slot]) c->launches += (int64_t)it * ps.body_nodes[slot] + 1;
     PIC_TRY(fields_from_phi(c));
     prof_end(c, PIC_PHASE_POISSON);
     PIC_CUDA(cudaEventRecord(ps.ev1, c->stream));
