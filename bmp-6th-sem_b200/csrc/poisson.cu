@@ -28,7 +28,8 @@
 // spacing 2^l*dx; restriction is full weighting, prolongation bilinear, the
 // smoother red-black Gauss-Seidel with the colour order reversed after the
 // coarse correction, so the V-cycle is a symmetric preconditioner.  The
-// coarsest level (min(nx,ny) <= 4) gets symmetric RB-GS sweeps.  All levels
+// coarsest level (min(nx,ny) <= 2: one unknown per row or column) gets
+// symmetric RB-GS sweeps.  All levels
 // from the first one whose hierarchy fits in shared memory down to the
 // coarsest run inside one thread block (k_mg_fused).
 //
@@ -53,7 +54,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kRedThreads = 256;
 constexpr int kNu = 2;            // RB-GS sweeps before and after the coarse correction
-constexpr int kCoarseSweeps = 40; // symmetric sweep pairs on the coarsest level
+constexpr int kCoarseSweeps = 8;  // symmetric sweep pairs on the coarsest level (<= 2 cells)
 
 // device scalar slots
 enum {
@@ -407,6 +408,7 @@ struct FusedLevels {
     int GX[kMaxFused], GY[kMaxFused];
     float cx[kMaxFused], cy[kMaxFused], cd[kMaxFused];
     int ox[kMaxFused], ob[kMaxFused], om[kMaxFused];  // byte offsets in shared memory
+    uint32_t rcp_hw[kMaxFused];  // ceil(2^32 / ceil(GX/2))
     const uint8_t* gmask[kMaxFused];
     const float* gb;  // right-hand side of the first fused level
     float* gx;        // its solution (output)
@@ -428,15 +430,22 @@ __global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
         for (int k = tid; k < n; k += kFusedThreads) B(0)[k] = F.gb[k];
     }
     __syncthreads();
+    // one colour: h enumerates (row, half-column); hw = ceil(GX/2), and
+    // h / hw comes from a 32-bit reciprocal (exact for these sizes)
     auto sweep = [&](int l, int color) {
-        const int GX = F.GX[l], n = GX * F.GY[l];
+        const int GX = F.GX[l], GY = F.GY[l], hw = (GX + 1) >> 1;
+        const uint32_t rcp = F.rcp_hw[l];
         float* x = X(l);
         const float* b = B(l);
         const uint8_t* m = M(l);
-        for (int k = tid; k < n; k += kFusedThreads) {
-            const int i = k % GX, j = k / GX;
-            if (((i + j) & 1) != color || m[k]) continue;
-            x[k] = __fmaf_rn(F.cx[l], x[k - 1] + x[k + 1], __fmaf_rn(F.cy[l], x[k - GX] + x[k + GX], b[k])) / F.cd[l];
+        const float cx = F.cx[l], cy = F.cy[l], icd = 1.0f / F.cd[l];
+        for (int h = tid; h < hw * GY; h += kFusedThreads) {
+            const int j = (int)__umulhi((uint32_t)h, rcp);
+            const int i = 2 * (h - j * hw) + ((j + color) & 1);
+            if (i >= GX) continue;
+            const int k = j * GX + i;
+            if (m[k]) continue;
+            x[k] = __fmaf_rn(cx, x[k - 1] + x[k + 1], __fmaf_rn(cy, x[k - GX] + x[k + GX], b[k])) * icd;
         }
         __syncthreads();
     };
@@ -743,7 +752,7 @@ int poisson_setup(pic_ctx* c) {
             PIC_CUDA(cudaGetLastError());
         }
         ps.levels.push_back(L);
-        if (std::min(nx, ny) <= 4) break;
+        if (std::min(nx, ny) <= 2) break;
         prev_mask = L.mask;
         pGX = L.GX;
         pGY = L.GY;
@@ -758,7 +767,7 @@ int poisson_setup(pic_ctx* c) {
         const size_t n = (size_t)ps.levels[l].nodes;
         return ((n * 4 + 15) & ~(size_t)15) * 2 + ((n + 15) & ~(size_t)15);
     };
-    const size_t kSmemBudget = 220 * 1024;
+    const size_t kSmemBudget = 64 * 1024;  // small levels only: one SM does them
     size_t total = 0;
     int kf = L;
     for (int l = L - 1; l >= 0; --l) {
@@ -787,6 +796,8 @@ int poisson_setup(pic_ctx* c) {
         F.om[i] = (int)off;
         off += (n + 15) & ~(size_t)15;
         F.gmask[i] = M.mask;
+        const uint32_t hw = (uint32_t)((M.GX + 1) / 2);
+        F.rcp_hw[i] = (uint32_t)((0x100000000ull + hw - 1) / hw);
     }
     F.gb = ps.levels[kf].b;
     F.gx = ps.levels[kf].x;
