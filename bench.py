@@ -41,9 +41,9 @@ METRIC = "particle-steps/s (bin+deposit+push)"
 UNIT = "particle-steps/s"
 # Algorithmic HBM bytes per particle for each launch of the push (FP32 state,
 # 20 B per particle: float4 {fx, fy, vx, vy} + float vz).
-BYTES_COUNT_PASS = 20     # read the state
+BYTES_COUNT_PASS = 16     # read {fx, fy, vx, vy} (vz is not needed to classify)
 BYTES_SCATTER_PASS = 40   # read the state, write it to the new position
-BYTES_STEP = 60           # whole particle phase of one step
+BYTES_STEP = 56           # whole particle phase of one step
 BYTES_SURVEY_FP32 = 112   # the blueprint's per-particle-step figure (push 48 + deposit 12 + bin 52)
 
 
@@ -234,12 +234,18 @@ def measured_peaks():
 
 def ncu_traffic_per_particle():
     """Per-particle DRAM bytes of the scatter pass from the committed ncu
-    summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get("scatter_dram_bytes_per_particle"), d.get("source")
-    return None, None
+    summary (profiles/traffic.txt), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None, None
+    kv = {}
+    for line in open(p):
+        if line.startswith("#") or not line.strip():
+            continue
+        k, _, v = line.strip().partition(" ")
+        kv[k] = v
+    v = kv.get("scatter_dram_bytes_per_particle")
+    return (float(v) if v else None), kv.get("source")
 
 
 def run_ours(args, rank, world, local_rank):
