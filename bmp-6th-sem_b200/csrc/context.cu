@@ -83,6 +83,7 @@ void prof_end(pic_ctx* c, int phase) {
 }
 
 static void free_ctx(pic_ctx* c) {
+    ws_free(c);
     for (auto& p : c->prof_pending) {
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);

@@ -138,6 +138,8 @@ struct PoissonState {
 
 }  // namespace picb200
 
+struct pic_ws;  // learned warm start (warmstart.cu)
+
 struct pic_ctx {
     pic_config cfg{};
     int nx = 0, ny = 0, GX = 0, GY = 0;
@@ -175,6 +177,9 @@ struct pic_ctx {
     double prof_ms[PIC_NUM_PHASES] = {};
     int64_t prof_calls[PIC_NUM_PHASES] = {};
     int64_t launches = 0;
+    // learned warm start
+    pic_ws* ws = nullptr;
+    bool ws_record = false;
 };
 
 namespace picb200 {
@@ -200,6 +205,11 @@ int particles_flush_rho(pic_ctx* c, int s);     // acc -> final/energy mesh, rho
 int particles_push(pic_ctx* c, int s);          // pass1 + scan + pass2 (+deposit)
 int particles_count(pic_ctx* c, int s, int64_t* n);
 int particles_bin_counts(pic_ctx* c, int s, int32_t* dev_counts);
+
+// warmstart.cu
+void ws_free(pic_ctx* c);
+int ws_before_solve(pic_ctx* c, bool want_guess);  // 1 when a guess is in ps.net_guess
+int ws_after_solve(pic_ctx* c, bool record);
 
 // poisson.cu
 int poisson_setup(pic_ctx* c);

@@ -376,26 +376,6 @@ __global__ void k_mg_prolong(LevelDev F, LevelDev C) {
     F.x[k] += v;
 }
 
-// coarsest level: zero start, then symmetric RB-GS sweeps in one block
-__global__ void k_mg_coarse(LevelDev L, int sweeps) {
-    const int n = L.GX * L.GY;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) L.x[k] = 0.0f;
-    __syncthreads();
-    for (int s = 0; s < 2 * sweeps; ++s) {
-        for (int half = 0; half < 2; ++half) {
-            // forward sweeps: red then black; backward sweeps: black then red
-            const int color = (s < sweeps) ? half : 1 - half;
-            for (int k = threadIdx.x; k < n; k += blockDim.x) {
-                const int i = k % L.GX, j = k / L.GX;
-                if (((i + j) & 1) != color || L.mask[k]) continue;
-                const float t = L.b[k] + L.cx * (L.x[k - 1] + L.x[k + 1]) + L.cy * (L.x[k - L.GX] + L.x[k + L.GX]);
-                L.x[k] = t / L.cd;
-            }
-            __syncthreads();
-        }
-    }
-}
-
 // All levels from `first` down to the coarsest in one thread block, in
 // shared memory: the same operations as the per-level kernels (zero-start red
 // sweep, black, (red, black) x (kNu-1), restrict; coarsest: symmetric sweeps;
@@ -849,11 +829,17 @@ int poisson_solve(pic_ctx* c) {
     k_overwrite_rho<<<(unsigned)((nodes + 255) / 256), 256, 0, c->stream>>>(
         nodes, c->mask, c->dir_val, c->rho, c->phi, zero_start ? 1 : 0);
     c->launches += 1;
-    if (ps.warm == PIC_WARM_LEARNED && ps.have_prev && ps.net_guess) {
-        // the network's guess replaces phi on non-electrode nodes
-        k_apply_guess<<<(unsigned)((nodes + 255) / 256), 256, 0, c->stream>>>(nodes, c->mask,
-                                                                              ps.net_guess, c->phi);
-        c->launches += 1;
+    const bool learned = ps.warm == PIC_WARM_LEARNED;
+    const bool ws_active = learned || c->ws_record;
+    if (ws_active) {
+        const int guess = ws_before_solve(c, learned && ps.have_prev);
+        if (guess < 0) return guess;
+        if (guess == 1) {
+            // the network's guess replaces phi on non-electrode nodes
+            k_apply_guess<<<(unsigned)((nodes + 255) / 256), 256, 0, c->stream>>>(
+                nodes, c->mask, ps.net_guess, c->phi);
+            c->launches += 1;
+        }
     }
     if (!ps.gexec[slot] && !ps.graph_failed) {
         if (build_graph(c, jacobi) != PIC_OK) ps.graph_failed = true;  // host loop below
@@ -909,6 +895,7 @@ int poisson_solve(pic_ctx* c) {
     }
     const int it = (int)ps.host_scal[S_IT];
     if (ps.gexec[slot]) c->launches += (int64_t)it * ps.body_nodes[slot] + 1;
+    if (ws_active && status == PIC_OK) PIC_TRY(ws_after_solve(c, c->ws_record));
     PIC_TRY(fields_from_phi(c));
     prof_end(c, PIC_PHASE_POISSON);
     PIC_CUDA(cudaEventRecord(ps.ev1, c->stream));

@@ -1,0 +1,1065 @@
+// warmstart.cu -- learned initial guess for the Poisson PCG solve.
+//
+// Takes the place of the reference's ML Poisson surrogate
+// (SYCL-PIC-poissonsolver/src/poisson_ml_bridge.py:55-106,
+// src/predict_poisson_ml.py:194-221), which replaced the solve.  Here the
+// network only proposes phi_n as the starting point of PCG, which always runs
+// to the same tolerance afterwards: the converged answer does not depend on
+// the network.
+//
+// Network (the 3-level / 32-channel / 3x3 / two-convs-per-level encoder-
+// decoder), on the node grid zero-padded to P x P (P a multiple of 4):
+//   x0  = [phi_{n-1}/s0, db*dx^2/s1, mask]                  (3 channels)
+//   a1  = relu(conv3x3_3->32(x0)),  a2 = relu(conv(a1))        level 0
+//   p1  = avgpool2(a2); a3 = relu(conv(p1)), a4 = relu(conv(a3))   level 1
+//   p2  = avgpool2(a4); a5 = relu(conv(p2)), a6 = relu(conv(a5))   level 2
+//   u1  = up2(a6) + a4; a7 = relu(conv(u1)), a8 = relu(conv(a7))   level 1
+//   u0  = up2(a8) + a2; a9 = relu(conv(u0)), a10 = relu(conv(a9))  level 0
+//   out = conv3x3_32->1(a10)                   predicted (phi_n-phi_{n-1})/s2
+// db is the change of the solve's right-hand side between the two steps, so
+// by linearity the target is A_red^-1 db.
+//
+// Storage: activations and their gradients NHWC bf16 (32 channels), weights
+// bf16 with FP32 master copies and Adam moments.  The 32->32 convolutions
+// (forward, data gradient, weight gradient) are implicit GEMMs on the tensor
+// cores with mma.sync.m16n8k16 bf16 x bf16 -> fp32 (K = 9 taps x 32
+// channels); the 3->32 input and 32->1 output convolutions are small and run
+// on the FP32 cores.  Weight gradients are reduced through per-block
+// partials in a fixed order, so training is deterministic.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pic_internal.h"
+
+namespace picb200 {
+namespace {
+
+constexpr int C = 32;        // channels of the inner layers
+constexpr int TH = 8, TW = 32;  // output tile (pixels) of the tensor-core kernels
+constexpr int CP = 40;       // padded channel stride in shared memory (bank-conflict free)
+constexpr int kWgradBlocks = 296;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                        uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                          uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Load a (TH+2) x (TW+2) x 32 halo tile of an NHWC bf16 image into shared
+// memory ([row][col][CP]); pixels outside the image read as zero.
+__device__ __forceinline__ void load_halo(__nv_bfloat16* dst, const __nv_bfloat16* src, int P,
+                                          int y0, int x0) {
+    constexpr int kChunks = (TH + 2) * (TW + 2) * (C / 8);  // 16-byte chunks
+    for (int i = threadIdx.x; i < kChunks; i += blockDim.x) {
+        const int q = i & 3, pix = i >> 2;
+        const int r = pix / (TW + 2), col = pix % (TW + 2);
+        const int y = y0 + r - 1, x = x0 + col - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (y >= 0 && x >= 0 && y < P && x < P)
+            v = *reinterpret_cast<const uint4*>(src + ((int64_t)y * P + x) * C + q * 8);
+        *reinterpret_cast<uint4*>(dst + (r * (TW + 2) + col) * CP + q * 8) = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 32 -> 32 3x3 convolution (forward, or data gradient with transformed
+// weights).  Weights in global memory as [tap][n][k] bf16 (n = output
+// channel, k = input channel).  Epilogue: out = act(acc + bias), where act is
+// relu (forward) or a gate (out *= gate[p] > 0, data gradient); an optional
+// bf16 image is added before the gate.
+// ---------------------------------------------------------------------------
+struct ConvArgs {
+    const __nv_bfloat16* in;
+    const __nv_bfloat16* w;   // [9][32][32]
+    const float* bias;        // [32] or null
+    const __nv_bfloat16* gate;  // [P][P][32] or null: multiply by (gate > 0)
+    __nv_bfloat16* out;
+    int P;
+    int relu;
+};
+
+constexpr int kConvSmem = ((TH + 2) * (TW + 2) * CP + 9 * C * CP) * 2;
+
+__global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* in_s = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* w_s = in_s + (TH + 2) * (TW + 2) * CP;
+    const int y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
+    load_halo(in_s, A.in, A.P, y0, x0);
+    for (int i = threadIdx.x; i < 9 * C * (C / 8); i += blockDim.x) {
+        const int q = i & 3, row = i >> 2;  // row = tap*32 + n
+        *reinterpret_cast<uint4*>(w_s + row * CP + q * 8) =
+            *reinterpret_cast<const uint4*>(A.w + row * C + q * 8);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // warp = output row in the tile
+    float acc[2][4][4];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+            uint32_t a[2][4];
+#pragma unroll
+            for (int m = 0; m < 2; ++m) {
+                const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
+                const int koff = (lane >> 4) * 8;
+                const __nv_bfloat16* pa = in_s + ((warp + dy) * (TW + 2) + m * 16 + r + dx) * CP + kc * 16 + koff;
+                ldsm_x4(smem_u32(pa), a[m][0], a[m][1], a[m][2], a[m][3]);
+            }
+            uint32_t b[4][2];
+#pragma unroll
+            for (int nh = 0; nh < 2; ++nh) {
+                const int n = nh * 16 + (lane & 7) + (lane >> 4) * 8;
+                const int koff = ((lane >> 3) & 1) * 8;
+                const __nv_bfloat16* pb = w_s + (tap * C + n) * CP + kc * 16 + koff;
+                ldsm_x4(smem_u32(pb), b[nh * 2][0], b[nh * 2][1], b[nh * 2 + 1][0], b[nh * 2 + 1][1]);
+            }
+#pragma unroll
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int n = 0; n < 4; ++n)
+                    mma_bf16(acc[m][n], a[m][0], a[m][1], a[m][2], a[m][3], b[n][0], b[n][1]);
+        }
+    }
+    // epilogue: stage the tile in shared memory, then write 16-byte chunks
+    __syncthreads();
+    __nv_bfloat16* o_s = in_s;  // [TH*TW][CP]
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int px = m * 16 + g + h * 8;
+                const int ch = n * 8 + t * 2;
+                float v0 = acc[m][n][h * 2], v1 = acc[m][n][h * 2 + 1];
+                if (A.bias) {
+                    v0 += A.bias[ch];
+                    v1 += A.bias[ch + 1];
+                }
+                if (A.relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                *reinterpret_cast<__nv_bfloat162*>(o_s + (warp * TW + px) * CP + ch) =
+                    __floats2bfloat162_rn(v0, v1);
+            }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
+        const int q = i & 3, pix = i >> 2;
+        const int y = y0 + pix / TW, x = x0 + pix % TW;
+        if (y >= A.P || x >= A.P) continue;
+        const int64_t go = ((int64_t)y * A.P + x) * C + q * 8;
+        uint4 v = *reinterpret_cast<const uint4*>(o_s + pix * CP + q * 8);
+        if (A.gate) {
+            const uint4 gv = *reinterpret_cast<const uint4*>(A.gate + go);
+            __nv_bfloat162* pv = reinterpret_cast<__nv_bfloat162*>(&v);
+            const __nv_bfloat162* pg = reinterpret_cast<const __nv_bfloat162*>(&gv);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float2 f = __bfloat1622float2(pv[e]);
+                const float2 gg = __bfloat1622float2(pg[e]);
+                pv[e] = __floats2bfloat162_rn(gg.x > 0.f ? f.x : 0.f, gg.y > 0.f ? f.y : 0.f);
+            }
+        }
+        *reinterpret_cast<uint4*>(A.out + go) = v;
+    }
+}
+
+// Data-gradient weights: Wt[tap'][n = ci][k = co] = W[8 - tap][co][ci].
+__global__ void k_transpose_w(const __nv_bfloat16* w, __nv_bfloat16* wt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * C * C) return;
+    const int tap = i / (C * C), n = (i / C) % C, k = i % C;
+    wt[i] = w[((8 - tap) * C + k) * C + n];
+}
+
+// ---------------------------------------------------------------------------
+// 32 -> 32 weight gradient: dW[tap][co][ci] = sum_p dY[p][co] * X[p+tap][ci],
+// db[co] = sum_p dY[p][co].  Persistent blocks over output tiles; warp w
+// owns tap w (warp 0 also tap 8); per-block partials are summed afterwards.
+// ---------------------------------------------------------------------------
+constexpr int kWgradSmem = ((TH + 2) * (TW + 2) * CP + TH * TW * CP) * 2;
+
+__global__ void __launch_bounds__(256) k_wgrad32(const __nv_bfloat16* X, const __nv_bfloat16* dY,
+                                                 int P, float* partial) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* x_s = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* d_s = x_s + (TH + 2) * (TW + 2) * CP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tiles_x = (P + TW - 1) / TW, tiles_y = (P + TH - 1) / TH;
+    float acc[2][2][4][4];  // [tap slot][m][n][e]
+    float bsum = 0.f;       // bias gradient: thread t < 32 owns channel t
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[s][m][n][e] = 0.f;
+    for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
+        const int y0 = (tile / tiles_x) * TH, x0 = (tile % tiles_x) * TW;
+        __syncthreads();
+        load_halo(x_s, X, P, y0, x0);
+        for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
+            const int q = i & 3, pix = i >> 2;
+            const int y = y0 + pix / TW, x = x0 + pix % TW;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (y < P && x < P) v = *reinterpret_cast<const uint4*>(dY + ((int64_t)y * P + x) * C + q * 8);
+            *reinterpret_cast<uint4*>(d_s + pix * CP + q * 8) = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < C) {
+            float s = 0.f;
+            for (int pix = 0; pix < TH * TW; ++pix) s += __bfloat162float(d_s[pix * CP + threadIdx.x]);
+            bsum += s;
+        }
+#pragma unroll
+        for (int slot = 0; slot < 2; ++slot) {
+            const int tap = slot == 0 ? warp : 8;
+            if (slot == 1 && warp != 0) break;
+            const int dy = tap / 3, dx = tap % 3;
+#pragma unroll 1
+            for (int kp = 0; kp < TH * TW; kp += 16) {  // 16 pixels of one tile row
+                const int prow = kp / TW, pcol = kp % TW;
+                uint32_t a[2][4];
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    // A = dY^T: rows co, cols pixels; stored [pixel][co] -> transposed load
+                    const int p = kp + (lane & 7) + (lane >> 4) * 8;
+                    const int co = m * 16 + ((lane >> 3) & 1) * 8;
+                    ldsm_x4_t(smem_u32(d_s + p * CP + co), a[m][0], a[m][1], a[m][2], a[m][3]);
+                }
+                uint32_t b[4][2];
+#pragma unroll
+                for (int nh = 0; nh < 2; ++nh) {
+                    const int pl = (lane & 7) + ((lane >> 3) & 1) * 8;  // pixel within the 16
+                    const int ci = nh * 16 + (lane >> 4) * 8;
+                    const __nv_bfloat16* pb = x_s + ((prow + dy) * (TW + 2) + pcol + pl + dx) * CP + ci;
+                    ldsm_x4_t(smem_u32(pb), b[nh * 2][0], b[nh * 2][1], b[nh * 2 + 1][0], b[nh * 2 + 1][1]);
+                }
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+#pragma unroll
+                    for (int n = 0; n < 4; ++n)
+                        mma_bf16(acc[slot][m][n], a[m][0], a[m][1], a[m][2], a[m][3], b[n][0], b[n][1]);
+            }
+        }
+    }
+    // partial[block][tap][co][ci] and partial[block][9*32*32 + co]
+    float* out = partial + (int64_t)blockIdx.x * (9 * C * C + C);
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int slot = 0; slot < 2; ++slot) {
+        const int tap = slot == 0 ? warp : 8;
+        if (slot == 1 && warp != 0) break;
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int co = m * 16 + g + h * 8, ci = n * 8 + t * 2;
+                    out[(tap * C + co) * C + ci] = acc[slot][m][n][h * 2];
+                    out[(tap * C + co) * C + ci + 1] = acc[slot][m][n][h * 2 + 1];
+                }
+    }
+    if (threadIdx.x < C) out[9 * C * C + threadIdx.x] = bsum;
+}
+
+// Sums per-block partials (fixed order) into grad[n] (n values per block).
+__global__ void k_sum_partials(const float* partial, int nblocks, int n, float* grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.f;
+    for (int b = 0; b < nblocks; ++b) s += partial[(int64_t)b * n + i];
+    grad[i] = s;
+}
+
+// ---------------------------------------------------------------------------
+// FP32-core layers: input conv 3->32, output conv 32->1
+// ---------------------------------------------------------------------------
+// x0 layout: [P][P][4] bf16 (channel 3 unused).  w_in: [tap][ci(3)][co(32)] fp32.
+__global__ void k_conv_in(const __nv_bfloat16* x0, const float* w, const float* bias, int P,
+                          __nv_bfloat16* out) {
+    __shared__ float ws[9 * 3 * C + C];
+    for (int i = threadIdx.x; i < 9 * 3 * C; i += blockDim.x) ws[i] = w[i];
+    if (threadIdx.x < C) ws[9 * 3 * C + threadIdx.x] = bias[threadIdx.x];
+    __syncthreads();
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)P * P) return;
+    const int y = (int)(p / P), x = (int)(p % P);
+    float acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = ws[9 * 3 * C + c];
+    for (int tap = 0; tap < 9; ++tap) {
+        const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
+        const __nv_bfloat16* src = x0 + ((int64_t)yy * P + xx) * 4;
+#pragma unroll
+        for (int ci = 0; ci < 3; ++ci) {
+            const float v = __bfloat162float(src[ci]);
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] = fmaf(ws[(tap * 3 + ci) * C + c], v, acc[c]);
+        }
+    }
+    __nv_bfloat16* dst = out + p * C;
+#pragma unroll
+    for (int c = 0; c < C; c += 2)
+        *reinterpret_cast<__nv_bfloat162*>(dst + c) = __floats2bfloat162_rn(fmaxf(acc[c], 0.f), fmaxf(acc[c + 1], 0.f));
+}
+
+// out[p] = b + sum_tap sum_ci w[tap][ci] a[p+tap][ci]   (w_out: [tap][ci] fp32)
+__global__ void k_conv_out(const __nv_bfloat16* a, const float* w, const float* bias, int P,
+                           float* out) {
+    __shared__ float ws[9 * C];
+    for (int i = threadIdx.x; i < 9 * C; i += blockDim.x) ws[i] = w[i];
+    __syncthreads();
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)P * P) return;
+    const int y = (int)(p / P), x = (int)(p % P);
+    float s = bias[0];
+    for (int tap = 0; tap < 9; ++tap) {
+        const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
+        const __nv_bfloat162* src = reinterpret_cast<const __nv_bfloat162*>(a + ((int64_t)yy * P + xx) * C);
+#pragma unroll
+        for (int c = 0; c < C / 2; ++c) {
+            const float2 v = __bfloat1622float2(src[c]);
+            s = fmaf(ws[tap * C + 2 * c], v.x, s);
+            s = fmaf(ws[tap * C + 2 * c + 1], v.y, s);
+        }
+    }
+    out[p] = s;
+}
+
+// dA[p][ci] = (sum_tap w[tap][ci] dout[p - tap]) gated by (a[p][ci] > 0)
+__global__ void k_conv_out_dx(const float* dout, const float* w, const __nv_bfloat16* a, int P,
+                              __nv_bfloat16* da) {
+    __shared__ float ws[9 * C];
+    for (int i = threadIdx.x; i < 9 * C; i += blockDim.x) ws[i] = w[i];
+    __syncthreads();
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)P * P) return;
+    const int y = (int)(p / P), x = (int)(p % P);
+    float acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.f;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int yy = y - (tap / 3 - 1), xx = x - (tap % 3 - 1);
+        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
+        const float d = dout[(int64_t)yy * P + xx];
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = fmaf(ws[tap * C + c], d, acc[c]);
+    }
+    const __nv_bfloat16* ap = a + p * C;
+    __nv_bfloat16* dst = da + p * C;
+#pragma unroll
+    for (int c = 0; c < C; ++c) dst[c] = __float2bfloat16_rn(__bfloat162float(ap[c]) > 0.f ? acc[c] : 0.f);
+}
+
+// Small weight gradients on FP32 cores:
+//   input conv:  g[(tap*3+ci)*32+co] = sum_p x0[p+tap][ci] * dY[p][co], g[864+co] = sum_p dY[p][co]
+//   output conv: g[tap*32+ci] = sum_p a[p+tap][ci] * dout[p],           g[288] = sum_p dout[p]
+// One block per pixel chunk, each thread owns output entries; partials per block.
+__global__ void k_wgrad_in(const __nv_bfloat16* x0, const __nv_bfloat16* dY, int P, int chunk,
+                           float* partial) {
+    const int n = 9 * 3 * C + C;
+    const int64_t p0 = (int64_t)blockIdx.x * chunk;
+    const int64_t p1 = min((int64_t)P * P, p0 + chunk);
+    for (int o = threadIdx.x; o < n; o += blockDim.x) {
+        float s = 0.f;
+        if (o < 9 * 3 * C) {
+            const int tap = o / (3 * C), ci = (o / C) % 3, co = o % C;
+            const int dyy = tap / 3 - 1, dxx = tap % 3 - 1;
+            for (int64_t p = p0; p < p1; ++p) {
+                const int y = (int)(p / P) + dyy, x = (int)(p % P) + dxx;
+                if (y < 0 || x < 0 || y >= P || x >= P) continue;
+                s += __bfloat162float(x0[((int64_t)y * P + x) * 4 + ci]) * __bfloat162float(dY[p * C + co]);
+            }
+        } else {
+            const int co = o - 9 * 3 * C;
+            for (int64_t p = p0; p < p1; ++p) s += __bfloat162float(dY[p * C + co]);
+        }
+        partial[(int64_t)blockIdx.x * n + o] = s;
+    }
+}
+
+__global__ void k_wgrad_out(const __nv_bfloat16* a, const float* dout, int P, int chunk,
+                            float* partial) {
+    const int n = 9 * C + 1;
+    const int64_t p0 = (int64_t)blockIdx.x * chunk;
+    const int64_t p1 = min((int64_t)P * P, p0 + chunk);
+    for (int o = threadIdx.x; o < n; o += blockDim.x) {
+        float s = 0.f;
+        if (o < 9 * C) {
+            const int tap = o / C, ci = o % C;
+            const int dyy = tap / 3 - 1, dxx = tap % 3 - 1;
+            for (int64_t p = p0; p < p1; ++p) {
+                const int y = (int)(p / P) + dyy, x = (int)(p % P) + dxx;
+                if (y < 0 || x < 0 || y >= P || x >= P) continue;
+                s += __bfloat162float(a[((int64_t)y * P + x) * C + ci]) * dout[p];
+            }
+        } else {
+            for (int64_t p = p0; p < p1; ++p) s += dout[p];
+        }
+        partial[(int64_t)blockIdx.x * n + o] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pooling, upsampling, gates
+// ---------------------------------------------------------------------------
+__global__ void k_pool(const __nv_bfloat16* in, int P, __nv_bfloat16* out) {  // P = input size
+    const int Q = P / 2;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)Q * Q * C) return;
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int Y = (int)(q / Q), X = (int)(q % Q);
+    auto at = [&](int y, int x) { return __bfloat162float(in[((int64_t)y * P + x) * C + c]); };
+    out[i] = __float2bfloat16_rn(0.25f * (at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1) + at(2 * Y + 1, 2 * X) + at(2 * Y + 1, 2 * X + 1)));
+}
+
+// u = up2(coarse) + skip   (P = fine size)
+__global__ void k_up_add(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, int P,
+                         __nv_bfloat16* out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)P * P * C) return;
+    const int c = (int)(i % C);
+    const int64_t p = i / C;
+    const int y = (int)(p / P), x = (int)(p % P), Q = P / 2;
+    const float v = __bfloat162float(coarse[((int64_t)(y / 2) * Q + x / 2) * C + c]) + __bfloat162float(skip[i]);
+    out[i] = __float2bfloat16_rn(v);
+}
+
+// dcoarse[Y][X] = sum of the 2x2 fine gradients, gated by (act > 0)
+__global__ void k_down_sum_gate(const __nv_bfloat16* dfine, const __nv_bfloat16* act, int P,
+                                __nv_bfloat16* dcoarse) {
+    const int Q = P / 2;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)Q * Q * C) return;
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int Y = (int)(q / Q), X = (int)(q % Q);
+    auto at = [&](int y, int x) { return __bfloat162float(dfine[((int64_t)y * P + x) * C + c]); };
+    const float s = at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1) + at(2 * Y + 1, 2 * X) + at(2 * Y + 1, 2 * X + 1);
+    dcoarse[i] = __float2bfloat16_rn(__bfloat162float(act[i]) > 0.f ? s : 0.f);
+}
+
+// d = (dskip + 0.25 * dpooled[y/2][x/2]) gated by (act > 0)   (P = fine size)
+__global__ void k_skip_pool_gate(const __nv_bfloat16* dskip, const __nv_bfloat16* dpooled,
+                                 const __nv_bfloat16* act, int P, __nv_bfloat16* d) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)P * P * C) return;
+    const int c = (int)(i % C);
+    const int64_t p = i / C;
+    const int y = (int)(p / P), x = (int)(p % P), Q = P / 2;
+    const float v = __bfloat162float(dskip[i]) +
+                    0.25f * __bfloat162float(dpooled[((int64_t)(y / 2) * Q + x / 2) * C + c]);
+    d[i] = __float2bfloat16_rn(__bfloat162float(act[i]) > 0.f ? v : 0.f);
+}
+
+// ---------------------------------------------------------------------------
+// Inputs, loss, output, optimiser
+// ---------------------------------------------------------------------------
+// x0 = [phi/s0, db*dx^2/s1, mask] on the padded grid (zero outside)
+__global__ void k_make_input(const double* phi, const double* db, const uint8_t* mask, int GX,
+                             int GY, int P, float inv_s0, float s1f, __nv_bfloat16* x0) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)P * P) return;
+    const int y = (int)(p / P), x = (int)(p % P);
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    if (y < GY && x < GX) {
+        const int64_t k = (int64_t)y * GX + x;
+        c0 = (float)phi[k] * inv_s0;
+        c1 = mask[k] ? 0.f : (float)db[k] * s1f;
+        c2 = mask[k] ? 1.f : 0.f;
+    }
+    __nv_bfloat16* d = x0 + p * 4;
+    d[0] = __float2bfloat16_rn(c0);
+    d[1] = __float2bfloat16_rn(c1);
+    d[2] = __float2bfloat16_rn(c2);
+    d[3] = __float2bfloat16_rn(0.f);
+}
+
+// loss = mean over non-electrode nodes of (out - target)^2; dout = dloss/dout
+__global__ void k_mse(const float* out, const float* target, const uint8_t* mask, int GX, int GY,
+                      int P, float inv_count, float* dout, float* loss_partial) {
+    __shared__ float red[8];
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (p < (int64_t)P * P) {
+        const int y = (int)(p / P), x = (int)(p % P);
+        float d = 0.f;
+        if (y < GY && x < GX && !mask[(int64_t)y * GX + x]) {
+            const float e = out[p] - target[(int64_t)y * GX + x];
+            l = e * e * inv_count;
+            d = 2.f * e * inv_count;
+        }
+        dout[p] = d;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(kFull, l, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[w];
+        loss_partial[blockIdx.x] = s;
+    }
+}
+
+// guess = phi_prev + out * s2 on non-electrode nodes
+__global__ void k_make_guess(const double* phi_prev, const float* out, const uint8_t* mask, int GX,
+                             int GY, int P, float s2, float* guess) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)GX * GY) return;
+    const int y = (int)(k / GX), x = (int)(k % GX);
+    guess[k] = mask[k] ? 0.f : (float)phi_prev[k] + out[(int64_t)y * P + x] * s2;
+}
+
+// Adam on the FP32 master weights; refreshes the bf16 or fp32 working copy.
+__global__ void k_adam(float* w, float* m, float* v, const float* g, int n, float lr, float b1,
+                       float b2, float eps, float c1, float c2, float gscale,
+                       __nv_bfloat16* w_bf16, float* w_f32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i] * gscale;
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    w[i] = wi;
+    if (w_bf16) w_bf16[i] = __float2bfloat16_rn(wi);
+    if (w_f32) w_f32[i] = wi;
+}
+
+// Records a training pair: db = b_n - b_prev (RHS change), target = (phi_n -
+// phi_prev)/s2 -- both on the node grid -- plus the input image.
+__global__ void k_diff(const double* a, const double* b, int64_t n, double* out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] - b[i];
+}
+
+__global__ void k_target(const double* phi, const double* phi_prev, int64_t n, float inv_s2,
+                         float* t) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) t[i] = (float)((phi[i] - phi_prev[i]) * inv_s2);
+}
+
+inline unsigned g1(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Network state
+// ---------------------------------------------------------------------------
+
+// parameter blocks: 0 = input conv, 1..9 = 32->32 convs, 10 = output conv
+constexpr int kNumConv32 = 9;
+constexpr int kInW = 9 * 3 * C, kInB = C;
+constexpr int kW32 = 9 * C * C, kB32 = C;
+constexpr int kOutW = 9 * C, kOutB = 1;
+constexpr int kParams = kInW + kInB + kNumConv32 * (kW32 + kB32) + kOutW + kOutB;
+
+struct Net {
+    int P = 0, GX = 0, GY = 0;
+    float s0 = 1, s1 = 1, s2 = 1;  // input / target scales
+    // parameters (fp32 master, Adam moments, gradient)
+    float* w = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    float* g = nullptr;
+    int64_t adam_t = 0;
+    // bf16 working copies of the 32->32 weights, [layer][tap][n][k], and
+    // their data-gradient transposes
+    __nv_bfloat16* w16 = nullptr;
+    __nv_bfloat16* w16t = nullptr;
+    // activations (P = fine, Q = P/2, R = P/4)
+    __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
+    float* out = nullptr;
+    // gradients
+    __nv_bfloat16 *d_big[3] = {}, *d_mid[3] = {}, *d_small[2] = {};
+    float* dout = nullptr;
+    float* partial = nullptr;
+    size_t partial_floats = 0;
+    float* gsum = nullptr;  // summed 32->32 weight gradient before re-layout
+    float* loss_partial = nullptr;
+    // dataset of recorded pairs: x0 image (bf16, P*P*4) and target (f32, GX*GY)
+    int64_t cap_pairs = 0, n_pairs = 0, next_pair = 0;
+    __nv_bfloat16* ds_x = nullptr;
+    float* ds_t = nullptr;
+    // recording scratch
+    double* phi_prev = nullptr;
+    double* b_prev = nullptr;
+    double* db = nullptr;
+    bool have_prev = false;
+    bool trained = false;
+};
+
+static int64_t param_off(int block) {
+    if (block == 0) return 0;
+    if (block <= kNumConv32) return kInW + kInB + (int64_t)(block - 1) * (kW32 + kB32);
+    return kInW + kInB + (int64_t)kNumConv32 * (kW32 + kB32);
+}
+
+static void net_free(Net& N) {
+    cudaFree(N.w); cudaFree(N.m); cudaFree(N.v); cudaFree(N.g);
+    cudaFree(N.w16); cudaFree(N.w16t);
+    cudaFree(N.x0);
+    for (auto* p : N.a) cudaFree(p);
+    cudaFree(N.p1); cudaFree(N.p2); cudaFree(N.u0); cudaFree(N.u1); cudaFree(N.out);
+    for (auto* p : N.d_big) cudaFree(p);
+    for (auto* p : N.d_mid) cudaFree(p);
+    for (auto* p : N.d_small) cudaFree(p);
+    cudaFree(N.dout); cudaFree(N.partial); cudaFree(N.loss_partial); cudaFree(N.gsum);
+    cudaFree(N.ds_x); cudaFree(N.ds_t);
+    cudaFree(N.phi_prev); cudaFree(N.b_prev); cudaFree(N.db);
+    N = Net{};
+}
+
+// Deterministic initialisation (He-style uniform from a hashed index).
+static void init_params(std::vector<float>& w) {
+    auto u = [](uint64_t i) {
+        uint64_t z = i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E5Full;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    w.assign(kParams, 0.f);
+    for (int blk = 0; blk <= kNumConv32 + 1; ++blk) {
+        const int64_t off = param_off(blk);
+        const int fan_in = blk == 0 ? 27 : 9 * C;
+        const int nw = blk == 0 ? kInW : (blk <= kNumConv32 ? kW32 : kOutW);
+        const double bound = std::sqrt(6.0 / fan_in) * (blk == kNumConv32 + 1 ? 0.1 : 1.0);
+        for (int i = 0; i < nw; ++i) w[off + i] = (float)(bound * u(off + i));
+    }
+}
+
+}  // namespace picb200
+
+using namespace picb200;
+
+struct pic_ws {
+    Net net;
+};
+
+namespace picb200 {
+
+static int ws_alloc(pic_ctx* c) {
+    if (c->ws) return PIC_OK;
+    auto* W = new pic_ws();
+    c->ws = W;
+    Net& N = W->net;
+    N.GX = c->GX;
+    N.GY = c->GY;
+    N.P = ((std::max(c->GX, c->GY) + 3) / 4) * 4;
+    const int64_t P = N.P, Q = P / 2, R = P / 4;
+    auto balloc = [&](__nv_bfloat16** p, int64_t n) {
+        return cudaMalloc(p, (size_t)n * sizeof(__nv_bfloat16));
+    };
+    if (cudaMalloc(&N.w, kParams * 4) || cudaMalloc(&N.m, kParams * 4) ||
+        cudaMalloc(&N.v, kParams * 4) || cudaMalloc(&N.g, kParams * 4) ||
+        balloc(&N.w16, (int64_t)kNumConv32 * kW32) || balloc(&N.w16t, (int64_t)kNumConv32 * kW32) ||
+        balloc(&N.x0, P * P * 4))
+        return fail(PIC_ERR_CUDA, "warm start: parameter allocation failed");
+    const int64_t sizes[11] = {P, P, Q, Q, R, R, Q, Q, P, P, 0};  // a1..a10 at index 1..10
+    for (int i = 1; i <= 10; ++i)
+        if (balloc(&N.a[i], sizes[i - 1] * sizes[i - 1] * C))
+            return fail(PIC_ERR_CUDA, "warm start: activation allocation failed");
+    if (balloc(&N.p1, Q * Q * C) || balloc(&N.p2, R * R * C) || balloc(&N.u0, P * P * C) ||
+        balloc(&N.u1, Q * Q * C) || cudaMalloc(&N.out, P * P * 4) || cudaMalloc(&N.dout, P * P * 4))
+        return fail(PIC_ERR_CUDA, "warm start: activation allocation failed");
+    for (auto*& p : N.d_big)
+        if (balloc(&p, P * P * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
+    for (auto*& p : N.d_mid)
+        if (balloc(&p, Q * Q * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
+    for (auto*& p : N.d_small)
+        if (balloc(&p, R * R * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
+    N.partial_floats = (size_t)kWgradBlocks * (9 * C * C + C);
+    const size_t small_partials = (size_t)g1(P * P, 4096) * (9 * 3 * C + C);
+    N.partial_floats = std::max(N.partial_floats, small_partials);
+    if (cudaMalloc(&N.partial, N.partial_floats * 4) || cudaMalloc(&N.loss_partial, g1(P * P) * 4) ||
+        cudaMalloc(&N.gsum, (9 * C * C + C) * 4))
+        return fail(PIC_ERR_CUDA, "warm start: scratch allocation failed");
+    const size_t nodes = (size_t)c->nodes;
+    if (cudaMalloc(&N.phi_prev, nodes * 8) || cudaMalloc(&N.b_prev, nodes * 8) ||
+        cudaMalloc(&N.db, nodes * 8))
+        return fail(PIC_ERR_CUDA, "warm start: scratch allocation failed");
+    std::vector<float> w;
+    init_params(w);
+    PIC_CUDA(cudaMemcpy(N.w, w.data(), kParams * 4, cudaMemcpyHostToDevice));
+    PIC_CUDA(cudaMemset(N.m, 0, kParams * 4));
+    PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
+    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+    PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
+    return PIC_OK;
+}
+
+__global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16) {
+    // w: 10 blocks of [tap][ci][co] fp32 -> w16: [layer][tap][n=co][k=ci] bf16
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)kNumConv32 * kW32) return;
+    const int l = (int)(i / kW32), r = (int)(i % kW32);
+    const int tap = r / (C * C), n = (r / C) % C, k = r % C;
+    w16[i] = __float2bfloat16_rn(w[l * stride + (tap * C + k) * C + n]);
+}
+
+// refresh the bf16 working weights and their transposes from the masters
+static int ws_pack(pic_ctx* c) {
+    Net& N = c->ws->net;
+    k_pack_w16<<<g1((int64_t)kNumConv32 * kW32), 256, 0, c->stream>>>(N.w + param_off(1), kW32 + kB32, N.w16);
+    for (int l = 0; l < kNumConv32; ++l)
+        k_transpose_w<<<g1(kW32), 256, 0, c->stream>>>(N.w16 + (int64_t)l * kW32, N.w16t + (int64_t)l * kW32);
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
+                   bool transposed, const __nv_bfloat16* gate) {
+    Net& N = c->ws->net;
+    ConvArgs A;
+    A.in = in;
+    A.w = (transposed ? N.w16t : N.w16) + (int64_t)layer * kW32;
+    A.bias = transposed ? nullptr : N.w + param_off(layer + 1) + kW32;
+    A.gate = gate;
+    A.out = out;
+    A.P = P;
+    A.relu = transposed ? 0 : 1;
+    const dim3 grid((P + TW - 1) / TW, (P + TH - 1) / TH);
+    k_conv32<<<grid, 256, kConvSmem, c->stream>>>(A);
+}
+
+// [tap][co][ci] (+ bias) -> the parameter layout [tap][ci][co] (+ bias)
+__global__ void k_scatter_wgrad(const float* src, float* g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * C * C + C) return;
+    if (i < 9 * C * C) {
+        const int tap = i / (C * C), co = (i / C) % C, ci = i % C;
+        g[(tap * C + ci) * C + co] = src[i];
+    } else {
+        g[i] = src[i];
+    }
+}
+
+static void wgrad32(pic_ctx* c, int layer, const __nv_bfloat16* X, const __nv_bfloat16* dY, int P) {
+    Net& N = c->ws->net;
+    k_wgrad32<<<kWgradBlocks, 256, kWgradSmem, c->stream>>>(X, dY, P, N.partial);
+    k_sum_partials<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.partial, kWgradBlocks, 9 * C * C + C,
+                                                             N.gsum);
+    k_scatter_wgrad<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.gsum, N.g + param_off(layer + 1));
+}
+
+// Forward pass on the image in N.x0; result in N.out.
+static void forward(pic_ctx* c) {
+    Net& N = c->ws->net;
+    const int P = N.P, Q = P / 2, R = P / 4;
+    k_conv_in<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.x0, N.w, N.w + kInW, P, N.a[1]);
+    conv32(c, 0, N.a[1], N.a[2], P, false, nullptr);
+    k_pool<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(N.a[2], P, N.p1);
+    conv32(c, 1, N.p1, N.a[3], Q, false, nullptr);
+    conv32(c, 2, N.a[3], N.a[4], Q, false, nullptr);
+    k_pool<<<g1((int64_t)R * R * C), 256, 0, c->stream>>>(N.a[4], Q, N.p2);
+    conv32(c, 3, N.p2, N.a[5], R, false, nullptr);
+    conv32(c, 4, N.a[5], N.a[6], R, false, nullptr);
+    k_up_add<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(N.a[6], N.a[4], Q, N.u1);
+    conv32(c, 5, N.u1, N.a[7], Q, false, nullptr);
+    conv32(c, 6, N.a[7], N.a[8], Q, false, nullptr);
+    k_up_add<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(N.a[8], N.a[2], P, N.u0);
+    conv32(c, 7, N.u0, N.a[9], P, false, nullptr);
+    conv32(c, 8, N.a[9], N.a[10], P, false, nullptr);
+    const int64_t ob = param_off(kNumConv32 + 1);
+    k_conv_out<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.a[10], N.w + ob, N.w + ob + kOutW, P, N.out);
+    c->launches += 18;
+}
+
+// Backward pass from N.dout (dloss/dout) into N.g (overwrites the gradient).
+static void backward(pic_ctx* c) {
+    Net& N = c->ws->net;
+    const int P = N.P, Q = P / 2, R = P / 4;
+    const int64_t ob = param_off(kNumConv32 + 1);
+    __nv_bfloat16 *B0 = N.d_big[0], *B1 = N.d_big[1], *B2 = N.d_big[2];
+    __nv_bfloat16 *M0 = N.d_mid[0], *M1 = N.d_mid[1], *M2 = N.d_mid[2];
+    __nv_bfloat16 *S0 = N.d_small[0], *S1 = N.d_small[1];
+    // output conv
+    {
+        const int chunk = 4096;
+        const int nb = (int)g1((int64_t)P * P, chunk);
+        k_wgrad_out<<<nb, 256, 0, c->stream>>>(N.a[10], N.dout, P, chunk, N.partial);
+        k_sum_partials<<<g1(9 * C + 1), 256, 0, c->stream>>>(N.partial, nb, 9 * C + 1, N.g + ob);
+        k_conv_out_dx<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.dout, N.w + ob, N.a[10], P, B0);
+    }
+    // B0 = dPre10
+    wgrad32(c, 8, N.a[9], B0, P);
+    conv32(c, 8, B0, B1, P, true, N.a[9]);        // B1 = dPre9
+    wgrad32(c, 7, N.u0, B1, P);
+    conv32(c, 7, B1, B2, P, true, nullptr);       // B2 = dU0
+    k_down_sum_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(B2, N.a[8], P, M0);  // M0 = dPre8
+    wgrad32(c, 6, N.a[7], M0, Q);
+    conv32(c, 6, M0, M1, Q, true, N.a[7]);        // M1 = dPre7
+    wgrad32(c, 5, N.u1, M1, Q);
+    conv32(c, 5, M1, M2, Q, true, nullptr);       // M2 = dU1
+    k_down_sum_gate<<<g1((int64_t)R * R * C), 256, 0, c->stream>>>(M2, N.a[6], Q, S0);  // S0 = dPre6
+    wgrad32(c, 4, N.a[5], S0, R);
+    conv32(c, 4, S0, S1, R, true, N.a[5]);        // S1 = dPre5
+    wgrad32(c, 3, N.p2, S1, R);
+    conv32(c, 3, S1, S0, R, true, nullptr);       // S0 = dP2
+    k_skip_pool_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(M2, S0, N.a[4], Q, M0);  // M0 = dPre4
+    wgrad32(c, 2, N.a[3], M0, Q);
+    conv32(c, 2, M0, M1, Q, true, N.a[3]);        // M1 = dPre3
+    wgrad32(c, 1, N.p1, M1, Q);
+    conv32(c, 1, M1, M0, Q, true, nullptr);       // M0 = dP1
+    k_skip_pool_gate<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(B2, M0, N.a[2], P, B0);  // B0 = dPre2
+    wgrad32(c, 0, N.a[1], B0, P);
+    conv32(c, 0, B0, B1, P, true, N.a[1]);        // B1 = dPre1
+    {
+        const int chunk = 4096;
+        const int nb = (int)g1((int64_t)P * P, chunk);
+        k_wgrad_in<<<nb, 256, 0, c->stream>>>(N.x0, B1, P, chunk, N.partial);
+        k_sum_partials<<<g1(9 * 3 * C + C), 256, 0, c->stream>>>(N.partial, nb, 9 * 3 * C + C, N.g);
+    }
+    c->launches += 2 + 1 + 10 * 3 + 4 + 2;
+}
+
+}  // namespace picb200
+
+// ---------------------------------------------------------------------------
+// Hooks used by the Poisson solve and the C ABI
+// ---------------------------------------------------------------------------
+namespace picb200 {
+
+void ws_free(pic_ctx* c) {
+    if (!c->ws) return;
+    net_free(c->ws->net);
+    delete c->ws;
+    c->ws = nullptr;
+}
+
+// Before the solve: remember phi_{n-1} and b_{n-1} (after overwriteRho the
+// device rho holds b).  Called with the new b already in place.
+int ws_before_solve(pic_ctx* c, bool want_guess) {
+    if (!c->ws) PIC_TRY(ws_alloc(c));
+    Net& N = c->ws->net;
+    const int64_t n = c->nodes;
+    if (N.have_prev) k_diff<<<g1(n), 256, 0, c->stream>>>(c->rho, N.b_prev, n, N.db);
+    PIC_CUDA(cudaMemcpyAsync(N.phi_prev, c->phi, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if (want_guess && N.have_prev && N.trained) {
+        PIC_TRY(ws_pack(c));
+        k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
+            N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1, N.x0);
+        forward(c);
+        if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)n * 4));
+        k_make_guess<<<g1(n), 256, 0, c->stream>>>(N.phi_prev, N.out, c->mask, N.GX, N.GY, N.P, N.s2,
+                                                   c->ps.net_guess);
+        c->launches += 3;
+        PIC_CUDA(cudaGetLastError());
+        return 1;  // guess available
+    }
+    return 0;
+}
+
+// After the solve: record (input, target) when recording, keep b for the
+// next step.
+int ws_after_solve(pic_ctx* c, bool record) {
+    Net& N = c->ws->net;
+    const int64_t n = c->nodes;
+    if (record && N.have_prev && N.cap_pairs > 0) {
+        const int64_t slot = N.next_pair;
+        k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
+            N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1,
+            N.ds_x + slot * (int64_t)N.P * N.P * 4);
+        k_target<<<g1(n), 256, 0, c->stream>>>(c->phi, N.phi_prev, n, 1.f / N.s2, N.ds_t + slot * n);
+        N.next_pair = (N.next_pair + 1) % N.cap_pairs;
+        N.n_pairs = std::min(N.n_pairs + 1, N.cap_pairs);
+    }
+    PIC_CUDA(cudaMemcpyAsync(N.b_prev, c->rho, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+    N.have_prev = true;
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+}  // namespace picb200
+
+extern "C" {
+
+int pic_ws_record(pic_ctx* c, int64_t max_pairs, double phi_scale, double db_scale,
+                  double target_scale) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (max_pairs < 0 || !(phi_scale > 0) || !(db_scale > 0) || !(target_scale > 0))
+        return fail(PIC_ERR_ARG, "warm start: bad recording parameters");
+    PIC_TRY(ws_alloc(c));
+    Net& N = c->ws->net;
+    cudaFree(N.ds_x);
+    cudaFree(N.ds_t);
+    N.ds_x = nullptr;
+    N.ds_t = nullptr;
+    N.cap_pairs = N.n_pairs = N.next_pair = 0;
+    N.s0 = (float)phi_scale;
+    N.s1 = (float)db_scale;
+    N.s2 = (float)target_scale;
+    if (max_pairs > 0) {
+        if (cudaMalloc(&N.ds_x, (size_t)max_pairs * N.P * N.P * 4 * 2) ||
+            cudaMalloc(&N.ds_t, (size_t)max_pairs * c->nodes * 4))
+            return fail(PIC_ERR_CAPACITY, "warm start: dataset does not fit in device memory");
+        N.cap_pairs = max_pairs;
+    }
+    c->ws_record = max_pairs > 0;
+    return PIC_OK;
+}
+
+int pic_ws_pairs(pic_ctx* c, int64_t* n) {
+    if (!c || !n) return fail(PIC_ERR_ARG, "null argument");
+    *n = c->ws ? c->ws->net.n_pairs : 0;
+    return PIC_OK;
+}
+
+int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
+    if (!c || epochs < 0 || !(lr > 0)) return fail(PIC_ERR_ARG, "warm start: bad training arguments");
+    if (!c->ws || c->ws->net.n_pairs == 0) return fail(PIC_ERR_STATE, "warm start: no recorded pairs");
+    Net& N = c->ws->net;
+    const int P = N.P;
+    const float inv_count = 1.f / (float)c->nodes;
+    std::vector<float> lp(g1((int64_t)P * P));
+    double last = 0;
+    for (int e = 0; e < epochs; ++e) {
+        double ep = 0;
+        for (int64_t s = 0; s < N.n_pairs; ++s) {
+            PIC_TRY(ws_pack(c));
+            PIC_CUDA(cudaMemcpyAsync(N.x0, N.ds_x + s * (int64_t)P * P * 4, (size_t)P * P * 4 * 2,
+                                     cudaMemcpyDeviceToDevice, c->stream));
+            forward(c);
+            k_mse<<<g1((int64_t)P * P), 256, 0, c->stream>>>(N.out, N.ds_t + s * c->nodes, c->mask,
+                                                            N.GX, N.GY, P, inv_count, N.dout,
+                                                            N.loss_partial);
+            PIC_CUDA(cudaMemcpyAsync(lp.data(), N.loss_partial, lp.size() * 4, cudaMemcpyDeviceToHost,
+                                     c->stream));
+            backward(c);
+            N.adam_t += 1;
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float c1 = 1.f / (1.f - std::pow(b1, (float)N.adam_t));
+            const float c2 = 1.f / (1.f - std::pow(b2, (float)N.adam_t));
+            k_adam<<<g1(kParams), 256, 0, c->stream>>>(N.w, N.m, N.v, N.g, kParams, (float)lr, b1, b2,
+                                                       1e-8f, c1, c2, 1.f, nullptr, nullptr);
+            PIC_CUDA(cudaStreamSynchronize(c->stream));
+            double l = 0;
+            for (float v : lp) l += v;
+            ep += l;
+            c->launches += 4;
+        }
+        last = ep / (double)N.n_pairs;
+    }
+    N.trained = true;
+    if (loss_out) *loss_out = last;
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+int pic_ws_get_params(pic_ctx* c, float* host, int64_t n) {
+    if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
+    if (n < kParams) return fail(PIC_ERR_CAPACITY, "warm start: parameter buffer too small");
+    PIC_TRY(ws_alloc(c));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    PIC_CUDA(cudaMemcpy(host, c->ws->net.w, kParams * 4, cudaMemcpyDeviceToHost));
+    return PIC_OK;
+}
+
+int pic_ws_set_params(pic_ctx* c, const float* host, int64_t n, double phi_scale, double db_scale,
+                      double target_scale) {
+    if (!c || !host || n != kParams) return fail(PIC_ERR_ARG, "warm start: parameter count mismatch");
+    PIC_TRY(ws_alloc(c));
+    Net& N = c->ws->net;
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    PIC_CUDA(cudaMemcpy(N.w, host, kParams * 4, cudaMemcpyHostToDevice));
+    N.s0 = (float)phi_scale;
+    N.s1 = (float)db_scale;
+    N.s2 = (float)target_scale;
+    N.trained = true;
+    return PIC_OK;
+}
+
+int64_t pic_ws_num_params(void) { return kParams; }
+
+// One forward + backward on a caller-given input image and target, for
+// gradient checks: x0 host [P*P*3] (channels phi, db, mask already scaled),
+// target host [GX*GY]; returns out [P*P], gradient [kParams], loss.
+int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* target_host, float* out_host,
+                      float* grad_host, double* loss) {
+    if (!c || !x0_host || !target_host) return fail(PIC_ERR_ARG, "null argument");
+    PIC_TRY(ws_alloc(c));
+    Net& N = c->ws->net;
+    const int P = N.P;
+    std::vector<__nv_bfloat16> x((size_t)P * P * 4);
+    for (int64_t p = 0; p < (int64_t)P * P; ++p) {
+        for (int ch = 0; ch < 3; ++ch) x[p * 4 + ch] = __float2bfloat16(x0_host[p * 3 + ch]);
+        x[p * 4 + 3] = __float2bfloat16(0.f);
+    }
+    float* t = nullptr;
+    PIC_CUDA(cudaMalloc(&t, (size_t)c->nodes * 4));
+    PIC_CUDA(cudaMemcpy(N.x0, x.data(), x.size() * 2, cudaMemcpyHostToDevice));
+    PIC_CUDA(cudaMemcpy(t, target_host, (size_t)c->nodes * 4, cudaMemcpyHostToDevice));
+    PIC_TRY(ws_pack(c));
+    forward(c);
+    k_mse<<<g1((int64_t)P * P), 256, 0, c->stream>>>(N.out, t, c->mask, N.GX, N.GY, P,
+                                                    1.f / (float)c->nodes, N.dout, N.loss_partial);
+    std::vector<float> lp(g1((int64_t)P * P));
+    PIC_CUDA(cudaMemcpyAsync(lp.data(), N.loss_partial, lp.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    backward(c);
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(t);
+    if (out_host) PIC_CUDA(cudaMemcpy(out_host, N.out, (size_t)P * P * 4, cudaMemcpyDeviceToHost));
+    if (grad_host) PIC_CUDA(cudaMemcpy(grad_host, N.g, kParams * 4, cudaMemcpyDeviceToHost));
+    if (loss) {
+        double l = 0;
+        for (float v : lp) l += v;
+        *loss = l;
+    }
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+int pic_ws_grid(pic_ctx* c, int* P) {
+    if (!c || !P) return fail(PIC_ERR_ARG, "null argument");
+    *P = ((std::max(c->GX, c->GY) + 3) / 4) * 4;
+    return PIC_OK;
+}
+
+}  // extern "C"

@@ -131,6 +131,15 @@ def lib():
         "pic_set_profiling": (cint, [vp, cint]),
         "pic_profile_read": (cint, [vp, vp, vp, cint]),
         "pic_launch_count": (cint, [vp, P(i64)]),
+        "pic_ws_record": (cint, [vp, i64, dbl, dbl, dbl]),
+        "pic_ws_pairs": (cint, [vp, P(i64)]),
+        "pic_ws_train": (cint, [vp, cint, dbl, P(dbl)]),
+        "pic_ws_num_params": (i64, []),
+        "pic_ws_get_params": (cint, [vp, vp, i64]),
+        "pic_ws_set_params": (cint, [vp, vp, i64, dbl, dbl, dbl]),
+        "pic_ws_grid": (cint, [vp, P(cint)]),
+        "pic_ws_debug_step": (cint, [vp, vp, vp, vp, vp, P(dbl)]),
+        "pic_deposit_points_noalloc": (cint, [vp, i64, i32, i32, dbl, dbl, vp, dbl, dbl, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -316,6 +325,46 @@ class Pic:
 
     def set_poisson(self, solver=SOLVER_MG_PCG, warm=WARM_PREVIOUS, tol=1e-8, maxit=500):
         _check(lib().pic_set_poisson(self.h, solver, warm, tol, maxit))
+
+    # ---- learned warm start ----
+    def ws_record(self, max_pairs: int, phi_scale: float, db_scale: float, target_scale: float):
+        _check(lib().pic_ws_record(self.h, max_pairs, phi_scale, db_scale, target_scale))
+
+    def ws_pairs(self) -> int:
+        n = ctypes.c_int64(0)
+        _check(lib().pic_ws_pairs(self.h, ctypes.byref(n)))
+        return n.value
+
+    def ws_train(self, epochs: int, lr: float) -> float:
+        loss = ctypes.c_double(0)
+        _check(lib().pic_ws_train(self.h, epochs, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def ws_params(self) -> np.ndarray:
+        n = lib().pic_ws_num_params()
+        out = np.zeros(n, np.float32)
+        _check(lib().pic_ws_get_params(self.h, _p(out), n))
+        return out
+
+    def ws_set_params(self, theta, phi_scale, db_scale, target_scale):
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        _check(lib().pic_ws_set_params(self.h, _p(theta), len(theta), phi_scale, db_scale, target_scale))
+
+    def ws_grid(self) -> int:
+        P = ctypes.c_int(0)
+        _check(lib().pic_ws_grid(self.h, ctypes.byref(P)))
+        return P.value
+
+    def ws_debug_step(self, x0: np.ndarray, target: np.ndarray):
+        P = self.ws_grid()
+        x0 = np.ascontiguousarray(x0, dtype=np.float32)
+        target = np.ascontiguousarray(target, dtype=np.float32)
+        assert x0.shape == (P, P, 3) and target.size == self.nodes
+        out = np.zeros((P, P), np.float32)
+        grad = np.zeros(lib().pic_ws_num_params(), np.float32)
+        loss = ctypes.c_double(0)
+        _check(lib().pic_ws_debug_step(self.h, _p(x0), _p(target), _p(out), _p(grad), ctypes.byref(loss)))
+        return out, grad, loss.value
 
     def poisson_stats(self):
         it, rr, ms = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)

@@ -240,6 +240,34 @@ int pic_deposit_points_noalloc(const pic_point* dev_points, int64_t n, int32_t n
                                double surf_area, double epsilon, double* dev_final_mesh,
                                double* dev_rho, void* cuda_stream);
 
+/* ---- learned warm start ------------------------------------------------
+ * Replaces the reference's ML surrogate slot (src/poisson_ml_bridge.py:55-106)
+ * with a PCG initial guess: a 3-level conv encoder-decoder (32 channels, 3x3,
+ * BF16 tensor-core kernels with FP32 accumulation) predicting phi_n from
+ * phi_{n-1}, the change of the right-hand side and the electrode mask.  PCG
+ * then runs to the same tolerance, so the answer never depends on it. */
+/* Start (max_pairs > 0) or stop (0) recording (input, target) pairs at each
+ * Poisson solve; the scales normalise phi (V), the RHS change times dx^2 (V)
+ * and the target phi_n - phi_{n-1} (V). */
+int pic_ws_record(pic_ctx* ctx, int64_t max_pairs, double phi_scale, double db_scale,
+                  double target_scale);
+int pic_ws_pairs(pic_ctx* ctx, int64_t* n);
+/* Adam epochs over the recorded pairs (one pair per step); *loss = mean
+ * normalised squared error of the last epoch. */
+int pic_ws_train(pic_ctx* ctx, int epochs, double lr, double* loss);
+int64_t pic_ws_num_params(void);
+int pic_ws_get_params(pic_ctx* ctx, float* host, int64_t n);
+int pic_ws_set_params(pic_ctx* ctx, const float* host, int64_t n, double phi_scale,
+                      double db_scale, double target_scale);
+/* Side length P of the network's padded square grid. */
+int pic_ws_grid(pic_ctx* ctx, int* P);
+/* One forward + backward pass on a given scaled input image x0[P*P*3]
+ * (channels phi, RHS change, mask) and target[GRID_X*GRID_Y]: returns the
+ * output image out[P*P], the parameter gradient grad[pic_ws_num_params()]
+ * and the loss.  For gradient checks. */
+int pic_ws_debug_step(pic_ctx* ctx, const float* x0, const float* target, float* out,
+                      float* grad, double* loss);
+
 /* ---- Poisson controls -------------------------------------------------- */
 int pic_set_poisson(pic_ctx* ctx, int solver, int warm_start, double tol, int maxit);
 /* Iterations, achieved relative residual and device milliseconds of the most
