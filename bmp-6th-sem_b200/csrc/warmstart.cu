@@ -395,52 +395,104 @@ __global__ void k_conv_out_dx(const float* dout, const float* w, const __nv_bflo
     for (int c = 0; c < C; ++c) dst[c] = __float2bfloat16_rn(__bfloat162float(ap[c]) > 0.f ? acc[c] : 0.f);
 }
 
-// Small weight gradients on FP32 cores:
+// Small weight gradients on FP32 cores, persistent blocks over TH x TW tiles
+// staged in shared memory; each thread owns fixed output entries and keeps
+// their sums in registers; one partial per block, summed afterwards.
 //   input conv:  g[(tap*3+ci)*32+co] = sum_p x0[p+tap][ci] * dY[p][co], g[864+co] = sum_p dY[p][co]
 //   output conv: g[tap*32+ci] = sum_p a[p+tap][ci] * dout[p],           g[288] = sum_p dout[p]
-// One block per pixel chunk, each thread owns output entries; partials per block.
-__global__ void k_wgrad_in(const __nv_bfloat16* x0, const __nv_bfloat16* dY, int P, int chunk,
-                           float* partial) {
-    const int n = 9 * 3 * C + C;
-    const int64_t p0 = (int64_t)blockIdx.x * chunk;
-    const int64_t p1 = min((int64_t)P * P, p0 + chunk);
-    for (int o = threadIdx.x; o < n; o += blockDim.x) {
-        float s = 0.f;
-        if (o < 9 * 3 * C) {
-            const int tap = o / (3 * C), ci = (o / C) % 3, co = o % C;
-            const int dyy = tap / 3 - 1, dxx = tap % 3 - 1;
-            for (int64_t p = p0; p < p1; ++p) {
-                const int y = (int)(p / P) + dyy, x = (int)(p % P) + dxx;
-                if (y < 0 || x < 0 || y >= P || x >= P) continue;
-                s += __bfloat162float(x0[((int64_t)y * P + x) * 4 + ci]) * __bfloat162float(dY[p * C + co]);
-            }
-        } else {
-            const int co = o - 9 * 3 * C;
-            for (int64_t p = p0; p < p1; ++p) s += __bfloat162float(dY[p * C + co]);
+constexpr int kSmallWgradBlocks = 296;
+constexpr int kInOut = 9 * 3 * C + C;   // 896 input-conv gradient entries
+constexpr int kOutOut = 9 * C + 1;      // 289 output-conv gradient entries
+
+__global__ void __launch_bounds__(256) k_wgrad_in(const __nv_bfloat16* x0, const __nv_bfloat16* dY,
+                                                  int P, float* partial) {
+    __shared__ float xs[TH + 2][TW + 2][3];
+    __shared__ float ds[TH * TW][C + 1];
+    const int tiles_x = (P + TW - 1) / TW, tiles_y = (P + TH - 1) / TH;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};  // outputs threadIdx.x + 256*j
+    for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
+        const int y0 = (tile / tiles_x) * TH, x0p = (tile % tiles_x) * TW;
+        __syncthreads();
+        for (int i = threadIdx.x; i < (TH + 2) * (TW + 2); i += blockDim.x) {
+            const int r = i / (TW + 2), col = i % (TW + 2);
+            const int y = y0 + r - 1, x = x0p + col - 1;
+            const bool in = y >= 0 && x >= 0 && y < P && x < P;
+            for (int ci = 0; ci < 3; ++ci)
+                xs[r][col][ci] = in ? __bfloat162float(x0[((int64_t)y * P + x) * 4 + ci]) : 0.f;
         }
-        partial[(int64_t)blockIdx.x * n + o] = s;
+        for (int i = threadIdx.x; i < TH * TW * C; i += blockDim.x) {
+            const int pix = i / C, co = i % C;
+            const int y = y0 + pix / TW, x = x0p + pix % TW;
+            ds[pix][co] = (y < P && x < P) ? __bfloat162float(dY[((int64_t)y * P + x) * C + co]) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int o = threadIdx.x + 256 * j;
+            if (o >= kInOut) break;
+            float s = 0.f;
+            if (o < 9 * 3 * C) {
+                const int tap = o / (3 * C), ci = (o / C) % 3, co = o % C;
+                const int dy = tap / 3, dx = tap % 3;
+                for (int r = 0; r < TH; ++r)
+                    for (int col = 0; col < TW; ++col)
+                        s = fmaf(xs[r + dy][col + dx][ci], ds[r * TW + col][co], s);
+            } else {
+                const int co = o - 9 * 3 * C;
+                for (int pix = 0; pix < TH * TW; ++pix) s += ds[pix][co];
+            }
+            acc[j] += s;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int o = threadIdx.x + 256 * j;
+        if (o < kInOut) partial[(int64_t)blockIdx.x * kInOut + o] = acc[j];
     }
 }
 
-__global__ void k_wgrad_out(const __nv_bfloat16* a, const float* dout, int P, int chunk,
-                            float* partial) {
-    const int n = 9 * C + 1;
-    const int64_t p0 = (int64_t)blockIdx.x * chunk;
-    const int64_t p1 = min((int64_t)P * P, p0 + chunk);
-    for (int o = threadIdx.x; o < n; o += blockDim.x) {
-        float s = 0.f;
-        if (o < 9 * C) {
-            const int tap = o / C, ci = o % C;
-            const int dyy = tap / 3 - 1, dxx = tap % 3 - 1;
-            for (int64_t p = p0; p < p1; ++p) {
-                const int y = (int)(p / P) + dyy, x = (int)(p % P) + dxx;
-                if (y < 0 || x < 0 || y >= P || x >= P) continue;
-                s += __bfloat162float(a[((int64_t)y * P + x) * C + ci]) * dout[p];
-            }
-        } else {
-            for (int64_t p = p0; p < p1; ++p) s += dout[p];
+__global__ void __launch_bounds__(256) k_wgrad_out(const __nv_bfloat16* a, const float* dout, int P,
+                                                   float* partial) {
+    __shared__ float as[TH + 2][TW + 2][C + 1];
+    __shared__ float ds[TH * TW];
+    const int tiles_x = (P + TW - 1) / TW, tiles_y = (P + TH - 1) / TH;
+    float acc[2] = {0.f, 0.f};
+    for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
+        const int y0 = (tile / tiles_x) * TH, x0p = (tile % tiles_x) * TW;
+        __syncthreads();
+        for (int i = threadIdx.x; i < (TH + 2) * (TW + 2) * C; i += blockDim.x) {
+            const int pix = i / C, ci = i % C;
+            const int r = pix / (TW + 2), col = pix % (TW + 2);
+            const int y = y0 + r - 1, x = x0p + col - 1;
+            as[r][col][ci] = (y >= 0 && x >= 0 && y < P && x < P)
+                                 ? __bfloat162float(a[((int64_t)y * P + x) * C + ci])
+                                 : 0.f;
         }
-        partial[(int64_t)blockIdx.x * n + o] = s;
+        for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
+            const int y = y0 + i / TW, x = x0p + i % TW;
+            ds[i] = (y < P && x < P) ? dout[(int64_t)y * P + x] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int o = threadIdx.x + 256 * j;
+            if (o >= kOutOut) break;
+            float s = 0.f;
+            if (o < 9 * C) {
+                const int tap = o / C, ci = o % C, dy = tap / 3, dx = tap % 3;
+                for (int r = 0; r < TH; ++r)
+                    for (int col = 0; col < TW; ++col)
+                        s = fmaf(as[r + dy][col + dx][ci], ds[r * TW + col], s);
+            } else {
+                for (int pix = 0; pix < TH * TW; ++pix) s += ds[pix];
+            }
+            acc[j] += s;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int o = threadIdx.x + 256 * j;
+        if (o < kOutOut) partial[(int64_t)blockIdx.x * kOutOut + o] = acc[j];
     }
 }
 
@@ -622,6 +674,7 @@ struct Net {
     float* partial = nullptr;
     size_t partial_floats = 0;
     float* gsum = nullptr;  // summed 32->32 weight gradient before re-layout
+    float* loss_acc = nullptr;  // per-pair loss of the current epoch
     float* loss_partial = nullptr;
     // dataset of recorded pairs: x0 image (bf16, P*P*4) and target (f32, GX*GY)
     int64_t cap_pairs = 0, n_pairs = 0, next_pair = 0;
@@ -650,7 +703,7 @@ static void net_free(Net& N) {
     for (auto* p : N.d_big) cudaFree(p);
     for (auto* p : N.d_mid) cudaFree(p);
     for (auto* p : N.d_small) cudaFree(p);
-    cudaFree(N.dout); cudaFree(N.partial); cudaFree(N.loss_partial); cudaFree(N.gsum);
+    cudaFree(N.dout); cudaFree(N.partial); cudaFree(N.loss_partial); cudaFree(N.gsum); cudaFree(N.loss_acc);
     cudaFree(N.ds_x); cudaFree(N.ds_t);
     cudaFree(N.phi_prev); cudaFree(N.b_prev); cudaFree(N.db);
     N = Net{};
@@ -715,9 +768,7 @@ static int ws_alloc(pic_ctx* c) {
         if (balloc(&p, Q * Q * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
     for (auto*& p : N.d_small)
         if (balloc(&p, R * R * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
-    N.partial_floats = (size_t)kWgradBlocks * (9 * C * C + C);
-    const size_t small_partials = (size_t)g1(P * P, 4096) * (9 * 3 * C + C);
-    N.partial_floats = std::max(N.partial_floats, small_partials);
+    N.partial_floats = (size_t)std::max(kWgradBlocks, kSmallWgradBlocks) * (9 * C * C + C);
     if (cudaMalloc(&N.partial, N.partial_floats * 4) || cudaMalloc(&N.loss_partial, g1(P * P) * 4) ||
         cudaMalloc(&N.gsum, (9 * C * C + C) * 4))
         return fail(PIC_ERR_CUDA, "warm start: scratch allocation failed");
@@ -821,13 +872,9 @@ static void backward(pic_ctx* c) {
     __nv_bfloat16 *M0 = N.d_mid[0], *M1 = N.d_mid[1], *M2 = N.d_mid[2];
     __nv_bfloat16 *S0 = N.d_small[0], *S1 = N.d_small[1];
     // output conv
-    {
-        const int chunk = 4096;
-        const int nb = (int)g1((int64_t)P * P, chunk);
-        k_wgrad_out<<<nb, 256, 0, c->stream>>>(N.a[10], N.dout, P, chunk, N.partial);
-        k_sum_partials<<<g1(9 * C + 1), 256, 0, c->stream>>>(N.partial, nb, 9 * C + 1, N.g + ob);
-        k_conv_out_dx<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.dout, N.w + ob, N.a[10], P, B0);
-    }
+    k_wgrad_out<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.a[10], N.dout, P, N.partial);
+    k_sum_partials<<<g1(kOutOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kOutOut, N.g + ob);
+    k_conv_out_dx<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.dout, N.w + ob, N.a[10], P, B0);
     // B0 = dPre10
     wgrad32(c, 8, N.a[9], B0, P);
     conv32(c, 8, B0, B1, P, true, N.a[9]);        // B1 = dPre9
@@ -851,12 +898,8 @@ static void backward(pic_ctx* c) {
     k_skip_pool_gate<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(B2, M0, N.a[2], P, B0);  // B0 = dPre2
     wgrad32(c, 0, N.a[1], B0, P);
     conv32(c, 0, B0, B1, P, true, N.a[1]);        // B1 = dPre1
-    {
-        const int chunk = 4096;
-        const int nb = (int)g1((int64_t)P * P, chunk);
-        k_wgrad_in<<<nb, 256, 0, c->stream>>>(N.x0, B1, P, chunk, N.partial);
-        k_sum_partials<<<g1(9 * 3 * C + C), 256, 0, c->stream>>>(N.partial, nb, 9 * 3 * C + C, N.g);
-    }
+    k_wgrad_in<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.x0, B1, P, N.partial);
+    k_sum_partials<<<g1(kInOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kInOut, N.g);
     c->launches += 2 + 1 + 10 * 3 + 4 + 2;
 }
 
@@ -937,8 +980,11 @@ int pic_ws_record(pic_ctx* c, int64_t max_pairs, double phi_scale, double db_sca
     N.s1 = (float)db_scale;
     N.s2 = (float)target_scale;
     if (max_pairs > 0) {
+        cudaFree(N.loss_acc);
+        N.loss_acc = nullptr;
         if (cudaMalloc(&N.ds_x, (size_t)max_pairs * N.P * N.P * 4 * 2) ||
-            cudaMalloc(&N.ds_t, (size_t)max_pairs * c->nodes * 4))
+            cudaMalloc(&N.ds_t, (size_t)max_pairs * c->nodes * 4) ||
+            cudaMalloc(&N.loss_acc, (size_t)max_pairs * 4))
             return fail(PIC_ERR_CAPACITY, "warm start: dataset does not fit in device memory");
         N.cap_pairs = max_pairs;
     }
@@ -970,8 +1016,7 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
             k_mse<<<g1((int64_t)P * P), 256, 0, c->stream>>>(N.out, N.ds_t + s * c->nodes, c->mask,
                                                             N.GX, N.GY, P, inv_count, N.dout,
                                                             N.loss_partial);
-            PIC_CUDA(cudaMemcpyAsync(lp.data(), N.loss_partial, lp.size() * 4, cudaMemcpyDeviceToHost,
-                                     c->stream));
+            k_sum_partials<<<1, 32, 0, c->stream>>>(N.loss_partial, (int)lp.size(), 1, N.loss_acc + s);
             backward(c);
             N.adam_t += 1;
             const float b1 = 0.9f, b2 = 0.999f;
@@ -979,12 +1024,12 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
             const float c2 = 1.f / (1.f - std::pow(b2, (float)N.adam_t));
             k_adam<<<g1(kParams), 256, 0, c->stream>>>(N.w, N.m, N.v, N.g, kParams, (float)lr, b1, b2,
                                                        1e-8f, c1, c2, 1.f, nullptr, nullptr);
-            PIC_CUDA(cudaStreamSynchronize(c->stream));
-            double l = 0;
-            for (float v : lp) l += v;
-            ep += l;
-            c->launches += 4;
+            c->launches += 5;
         }
+        std::vector<float> ls((size_t)N.n_pairs);
+        PIC_CUDA(cudaMemcpyAsync(ls.data(), N.loss_acc, ls.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        for (float v : ls) ep += v;
         last = ep / (double)N.n_pairs;
     }
     N.trained = true;
