@@ -208,6 +208,7 @@ int particles_bin_counts(pic_ctx* c, int s, int32_t* dev_counts);
 
 // warmstart.cu
 void ws_free(pic_ctx* c);
+bool ws_tracking(const pic_ctx* c);  // hooks must run at every solve
 int ws_before_solve(pic_ctx* c, bool want_guess);  // 1 when a guess is in ps.net_guess
 int ws_after_solve(pic_ctx* c, bool record);
 

@@ -830,7 +830,7 @@ int poisson_solve(pic_ctx* c) {
         nodes, c->mask, c->dir_val, c->rho, c->phi, zero_start ? 1 : 0);
     c->launches += 1;
     const bool learned = ps.warm == PIC_WARM_LEARNED;
-    const bool ws_active = learned || c->ws_record;
+    const bool ws_active = learned || ws_tracking(c);
     if (ws_active) {
         const int guess = ws_before_solve(c, learned && ps.have_prev);
         if (guess < 0) return guess;

@@ -202,14 +202,6 @@ __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
     }
 }
 
-// Data-gradient weights: Wt[tap'][n = ci][k = co] = W[8 - tap][co][ci].
-__global__ void k_transpose_w(const __nv_bfloat16* w, __nv_bfloat16* wt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 9 * C * C) return;
-    const int tap = i / (C * C), n = (i / C) % C, k = i % C;
-    wt[i] = w[((8 - tap) * C + k) * C + n];
-}
-
 // ---------------------------------------------------------------------------
 // 32 -> 32 weight gradient: dW[tap][co][ci] = sum_p dY[p][co] * X[p+tap][ci],
 // db[co] = sum_p dY[p][co].  Persistent blocks over output tiles; warp w
@@ -572,21 +564,37 @@ __global__ void k_make_input(const double* phi, const double* db, const uint8_t*
     d[3] = __float2bfloat16_rn(0.f);
 }
 
-// loss = mean over non-electrode nodes of (out - target)^2; dout = dloss/dout
-__global__ void k_mse(const float* out, const float* target, const uint8_t* mask, int GX, int GY,
-                      int P, float inv_count, float* dout, float* loss_partial) {
+// The loss is the starting residual of PCG from the network's guess, in
+// scaled units.  With the guess phi_prev + s2*out on non-electrode nodes, the
+// residual of the reduced system is (s1/dx^2) * r with
+//   r = rhs - kappa * L(u),  rhs = (b_n - b_{n-1}) dx^2 / s1,  kappa = s2/s1,
+//   L(u) = (2 + 2 beta) u - (u_w + u_e) - beta (u_s + u_n),  beta = dx^2/dy^2,
+// u = out on non-electrode nodes and 0 on electrodes (every wall node is an
+// electrode, so a free node's four neighbours are inside the grid).
+// loss = sum over free nodes of r^2 / nodes.
+__device__ __forceinline__ bool free_node(const uint8_t* mask, int GX, int GY, int y, int x) {
+    return y > 0 && x > 0 && y < GY - 1 && x < GX - 1 && !mask[(int64_t)y * GX + x];
+}
+
+__global__ void k_resid(const float* out, const float* rhs, const uint8_t* mask, int GX, int GY,
+                        int P, float kappa, float beta, float inv_count, float* resid,
+                        float* loss_partial) {
     __shared__ float red[8];
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.f;
-    if (p < (int64_t)P * P) {
-        const int y = (int)(p / P), x = (int)(p % P);
-        float d = 0.f;
-        if (y < GY && x < GX && !mask[(int64_t)y * GX + x]) {
-            const float e = out[p] - target[(int64_t)y * GX + x];
-            l = e * e * inv_count;
-            d = 2.f * e * inv_count;
+    if (k < (int64_t)GX * GY) {
+        const int y = (int)(k / GX), x = (int)(k % GX);
+        float r = 0.f;
+        if (free_node(mask, GX, GY, y, x)) {
+            auto u = [&](int yy, int xx) {
+                return mask[(int64_t)yy * GX + xx] ? 0.f : out[(int64_t)yy * P + xx];
+            };
+            const float Lu = (2.f + 2.f * beta) * u(y, x) - (u(y, x - 1) + u(y, x + 1)) -
+                             beta * (u(y - 1, x) + u(y + 1, x));
+            r = rhs[k] - kappa * Lu;
         }
-        dout[p] = d;
+        resid[k] = r;
+        l = r * r * inv_count;
     }
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(kFull, l, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
@@ -596,6 +604,23 @@ __global__ void k_mse(const float* out, const float* target, const uint8_t* mask
         for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[w];
         loss_partial[blockIdx.x] = s;
     }
+}
+
+// dloss/dout = -(2 kappa / nodes) L(r) on free nodes, 0 elsewhere (L is
+// symmetric on the free nodes; r is 0 on electrodes).
+__global__ void k_resid_grad(const float* resid, const uint8_t* mask, int GX, int GY, int P,
+                             float kappa, float beta, float inv_count, float* dout) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)P * P) return;
+    const int y = (int)(p / P), x = (int)(p % P);
+    float d = 0.f;
+    if (y < GY && x < GX && free_node(mask, GX, GY, y, x)) {
+        auto r = [&](int yy, int xx) { return resid[(int64_t)yy * GX + xx]; };
+        const float Lr = (2.f + 2.f * beta) * r(y, x) - (r(y, x - 1) + r(y, x + 1)) -
+                         beta * (r(y - 1, x) + r(y + 1, x));
+        d = -2.f * kappa * inv_count * Lr;
+    }
+    dout[p] = d;
 }
 
 // guess = phi_prev + out * s2 on non-electrode nodes
@@ -624,17 +649,47 @@ __global__ void k_adam(float* w, float* m, float* v, const float* g, int n, floa
     if (w_f32) w_f32[i] = wi;
 }
 
-// Records a training pair: db = b_n - b_prev (RHS change), target = (phi_n -
-// phi_prev)/s2 -- both on the node grid -- plus the input image.
+// Records a training pair: db = b_n - b_prev (RHS change) on the node grid
+// and the input image.
 __global__ void k_diff(const double* a, const double* b, int64_t n, double* out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = a[i] - b[i];
 }
 
-__global__ void k_target(const double* phi, const double* phi_prev, int64_t n, float inv_s2,
-                         float* t) {
+// rhs = (b_n - b_{n-1}) dx^2 / s1 on free nodes, 0 on electrodes
+__global__ void k_rhs(const double* db, const uint8_t* mask, int64_t n, double dx2_over_s1, float* t) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) t[i] = (float)((phi[i] - phi_prev[i]) * inv_s2);
+    if (i < n) t[i] = mask[i] ? 0.f : (float)(db[i] * dx2_over_s1);
+}
+
+// Sums of squares over non-electrode nodes of phi_prev, db*dx^2 and
+// phi - phi_prev, and the number of those nodes: one partial quadruple per
+// block (summed on the host in block order).
+__global__ void k_sumsq4(const double* phi_prev, const double* db, const double* phi,
+                         const uint8_t* mask, int64_t n, double dx2, double* partial) {
+    __shared__ double red[4][8];
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (mask[i]) continue;
+        const double a = phi_prev[i], b = db[i] * dx2, d = phi[i] - phi_prev[i];
+        s[0] += a * a;
+        s[1] += b * b;
+        s[2] += d * d;
+        s[3] += 1.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double v = s[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += red[threadIdx.x][w];
+        partial[blockIdx.x * 4 + threadIdx.x] = v;
+    }
 }
 
 inline unsigned g1(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
@@ -668,9 +723,11 @@ struct Net {
     // activations (P = fine, Q = P/2, R = P/4)
     __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
     float* out = nullptr;
+    const __nv_bfloat16* xin = nullptr;  // input image of the current pass (x0 or a recorded pair)
     // gradients
     __nv_bfloat16 *d_big[3] = {}, *d_mid[3] = {}, *d_small[2] = {};
     float* dout = nullptr;
+    float* resid = nullptr;  // scaled starting residual on the node grid
     float* partial = nullptr;
     size_t partial_floats = 0;
     float* gsum = nullptr;  // summed 32->32 weight gradient before re-layout
@@ -686,6 +743,8 @@ struct Net {
     double* db = nullptr;
     bool have_prev = false;
     bool trained = false;
+    bool packed = false;      // w16/w16t match the masters
+    bool auto_scale = false;  // take s0, s1, s2 from the first recorded pair
 };
 
 static int64_t param_off(int block) {
@@ -703,7 +762,7 @@ static void net_free(Net& N) {
     for (auto* p : N.d_big) cudaFree(p);
     for (auto* p : N.d_mid) cudaFree(p);
     for (auto* p : N.d_small) cudaFree(p);
-    cudaFree(N.dout); cudaFree(N.partial); cudaFree(N.loss_partial); cudaFree(N.gsum); cudaFree(N.loss_acc);
+    cudaFree(N.dout); cudaFree(N.resid); cudaFree(N.partial); cudaFree(N.loss_partial); cudaFree(N.gsum); cudaFree(N.loss_acc);
     cudaFree(N.ds_x); cudaFree(N.ds_t);
     cudaFree(N.phi_prev); cudaFree(N.b_prev); cudaFree(N.db);
     N = Net{};
@@ -760,7 +819,8 @@ static int ws_alloc(pic_ctx* c) {
         if (balloc(&N.a[i], sizes[i - 1] * sizes[i - 1] * C))
             return fail(PIC_ERR_CUDA, "warm start: activation allocation failed");
     if (balloc(&N.p1, Q * Q * C) || balloc(&N.p2, R * R * C) || balloc(&N.u0, P * P * C) ||
-        balloc(&N.u1, Q * Q * C) || cudaMalloc(&N.out, P * P * 4) || cudaMalloc(&N.dout, P * P * 4))
+        balloc(&N.u1, Q * Q * C) || cudaMalloc(&N.out, P * P * 4) || cudaMalloc(&N.dout, P * P * 4) ||
+        cudaMalloc(&N.resid, (size_t)c->nodes * 4))
         return fail(PIC_ERR_CUDA, "warm start: activation allocation failed");
     for (auto*& p : N.d_big)
         if (balloc(&p, P * P * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
@@ -769,7 +829,7 @@ static int ws_alloc(pic_ctx* c) {
     for (auto*& p : N.d_small)
         if (balloc(&p, R * R * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
     N.partial_floats = (size_t)std::max(kWgradBlocks, kSmallWgradBlocks) * (9 * C * C + C);
-    if (cudaMalloc(&N.partial, N.partial_floats * 4) || cudaMalloc(&N.loss_partial, g1(P * P) * 4) ||
+    if (cudaMalloc(&N.partial, N.partial_floats * 4) || cudaMalloc(&N.loss_partial, g1(std::max<int64_t>(P * P, c->nodes)) * 4) ||
         cudaMalloc(&N.gsum, (9 * C * C + C) * 4))
         return fail(PIC_ERR_CUDA, "warm start: scratch allocation failed");
     const size_t nodes = (size_t)c->nodes;
@@ -786,22 +846,27 @@ static int ws_alloc(pic_ctx* c) {
     return PIC_OK;
 }
 
-__global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16) {
-    // w: 10 blocks of [tap][ci][co] fp32 -> w16: [layer][tap][n=co][k=ci] bf16
+// w: 9 blocks of [tap][ci][co] fp32 (stride apart) -> w16: [layer][tap][n=co][k=ci]
+// bf16 and its data-gradient form w16t[layer][tap][n=ci][k=co] = w16[layer][8-tap][co][ci].
+__global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16, __nv_bfloat16* w16t) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)kNumConv32 * kW32) return;
     const int l = (int)(i / kW32), r = (int)(i % kW32);
     const int tap = r / (C * C), n = (r / C) % C, k = r % C;
     w16[i] = __float2bfloat16_rn(w[l * stride + (tap * C + k) * C + n]);
+    w16t[i] = __float2bfloat16_rn(w[l * stride + ((8 - tap) * C + n) * C + k]);
 }
 
-// refresh the bf16 working weights and their transposes from the masters
+// Refresh the bf16 working weights and their transposes from the masters
+// (only after the masters changed).
 static int ws_pack(pic_ctx* c) {
     Net& N = c->ws->net;
-    k_pack_w16<<<g1((int64_t)kNumConv32 * kW32), 256, 0, c->stream>>>(N.w + param_off(1), kW32 + kB32, N.w16);
-    for (int l = 0; l < kNumConv32; ++l)
-        k_transpose_w<<<g1(kW32), 256, 0, c->stream>>>(N.w16 + (int64_t)l * kW32, N.w16t + (int64_t)l * kW32);
+    if (N.packed) return PIC_OK;
+    k_pack_w16<<<g1((int64_t)kNumConv32 * kW32), 256, 0, c->stream>>>(N.w + param_off(1), kW32 + kB32,
+                                                                       N.w16, N.w16t);
+    c->launches += 1;
     PIC_CUDA(cudaGetLastError());
+    N.packed = true;
     return PIC_OK;
 }
 
@@ -840,11 +905,11 @@ static void wgrad32(pic_ctx* c, int layer, const __nv_bfloat16* X, const __nv_bf
     k_scatter_wgrad<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.gsum, N.g + param_off(layer + 1));
 }
 
-// Forward pass on the image in N.x0; result in N.out.
+// Forward pass on the image N.xin; result in N.out.
 static void forward(pic_ctx* c) {
     Net& N = c->ws->net;
     const int P = N.P, Q = P / 2, R = P / 4;
-    k_conv_in<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.x0, N.w, N.w + kInW, P, N.a[1]);
+    k_conv_in<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.xin, N.w, N.w + kInW, P, N.a[1]);
     conv32(c, 0, N.a[1], N.a[2], P, false, nullptr);
     k_pool<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(N.a[2], P, N.p1);
     conv32(c, 1, N.p1, N.a[3], Q, false, nullptr);
@@ -861,6 +926,23 @@ static void forward(pic_ctx* c) {
     const int64_t ob = param_off(kNumConv32 + 1);
     k_conv_out<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.a[10], N.w + ob, N.w + ob + kOutW, P, N.out);
     c->launches += 18;
+}
+
+// Loss of the guess N.out against the scaled right-hand-side change rhs
+// (free nodes of the node grid): residual, its sum into *loss_slot, and
+// dloss/dout into N.dout.
+static void enqueue_loss(pic_ctx* c, const float* rhs, float* loss_slot) {
+    Net& N = c->ws->net;
+    const int64_t nodes = c->nodes;
+    const float kappa = N.s2 / N.s1;
+    const float beta = (float)((c->dx * c->dx) / (c->dy * c->dy));
+    const float inv_count = 1.f / (float)nodes;
+    k_resid<<<g1(nodes), 256, 0, c->stream>>>(N.out, rhs, c->mask, N.GX, N.GY, N.P, kappa, beta,
+                                              inv_count, N.resid, N.loss_partial);
+    k_sum_partials<<<1, 32, 0, c->stream>>>(N.loss_partial, (int)g1(nodes), 1, loss_slot);
+    k_resid_grad<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(N.resid, c->mask, N.GX, N.GY, N.P,
+                                                                kappa, beta, inv_count, N.dout);
+    c->launches += 3;
 }
 
 // Backward pass from N.dout (dloss/dout) into N.g (overwrites the gradient).
@@ -898,7 +980,7 @@ static void backward(pic_ctx* c) {
     k_skip_pool_gate<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(B2, M0, N.a[2], P, B0);  // B0 = dPre2
     wgrad32(c, 0, N.a[1], B0, P);
     conv32(c, 0, B0, B1, P, true, N.a[1]);        // B1 = dPre1
-    k_wgrad_in<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.x0, B1, P, N.partial);
+    k_wgrad_in<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.xin, B1, P, N.partial);
     k_sum_partials<<<g1(kInOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kInOut, N.g);
     c->launches += 2 + 1 + 10 * 3 + 4 + 2;
 }
@@ -909,6 +991,10 @@ static void backward(pic_ctx* c) {
 // Hooks used by the Poisson solve and the C ABI
 // ---------------------------------------------------------------------------
 namespace picb200 {
+
+// A trained network (or a recording in progress) needs phi_{n-1} and b_{n-1}
+// at every solve, whichever warm start the solve itself uses.
+bool ws_tracking(const pic_ctx* c) { return c->ws && (c->ws_record || c->ws->net.trained); }
 
 void ws_free(pic_ctx* c) {
     if (!c->ws) return;
@@ -929,6 +1015,7 @@ int ws_before_solve(pic_ctx* c, bool want_guess) {
         PIC_TRY(ws_pack(c));
         k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
             N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1, N.x0);
+        N.xin = N.x0;
         forward(c);
         if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)n * 4));
         k_make_guess<<<g1(n), 256, 0, c->stream>>>(N.phi_prev, N.out, c->mask, N.GX, N.GY, N.P, N.s2,
@@ -946,11 +1033,33 @@ int ws_after_solve(pic_ctx* c, bool record) {
     Net& N = c->ws->net;
     const int64_t n = c->nodes;
     if (record && N.have_prev && N.cap_pairs > 0) {
+        if (N.auto_scale) {
+            // root-mean-square of each quantity over the non-electrode nodes
+            constexpr int kB = 148;
+            double* part = reinterpret_cast<double*>(N.partial);
+            k_sumsq4<<<kB, 256, 0, c->stream>>>(N.phi_prev, N.db, c->phi, c->mask, n, c->dx * c->dx, part);
+            c->launches += 1;
+            double h[kB * 4];
+            PIC_CUDA(cudaMemcpyAsync(h, part, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+            PIC_CUDA(cudaStreamSynchronize(c->stream));
+            double t[4] = {0, 0, 0, 0};
+            for (int b = 0; b < kB; ++b)
+                for (int k = 0; k < 4; ++k) t[k] += h[b * 4 + k];
+            float sc[3];
+            for (int k = 0; k < 3; ++k) {
+                const double rms = std::sqrt(t[k] / std::max(t[3], 1.0));
+                sc[k] = (rms > 0 && std::isfinite(rms)) ? (float)rms : 1.f;
+            }
+            N.s0 = sc[0];
+            N.s1 = sc[1];
+            N.s2 = sc[2];
+            N.auto_scale = false;
+        }
         const int64_t slot = N.next_pair;
         k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
             N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1,
             N.ds_x + slot * (int64_t)N.P * N.P * 4);
-        k_target<<<g1(n), 256, 0, c->stream>>>(c->phi, N.phi_prev, n, 1.f / N.s2, N.ds_t + slot * n);
+        k_rhs<<<g1(n), 256, 0, c->stream>>>(N.db, c->mask, n, c->dx * c->dx / N.s1, N.ds_t + slot * n);
         N.next_pair = (N.next_pair + 1) % N.cap_pairs;
         N.n_pairs = std::min(N.n_pairs + 1, N.cap_pairs);
     }
@@ -967,28 +1076,52 @@ extern "C" {
 int pic_ws_record(pic_ctx* c, int64_t max_pairs, double phi_scale, double db_scale,
                   double target_scale) {
     if (!c) return fail(PIC_ERR_ARG, "null context");
-    if (max_pairs < 0 || !(phi_scale > 0) || !(db_scale > 0) || !(target_scale > 0))
-        return fail(PIC_ERR_ARG, "warm start: bad recording parameters");
+    if (max_pairs == 0) {  // stop recording, keep the dataset and the scales
+        c->ws_record = false;
+        return PIC_OK;
+    }
     PIC_TRY(ws_alloc(c));
     Net& N = c->ws->net;
+    if (max_pairs < 0) {  // stop and release the dataset
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(N.ds_x);
+        cudaFree(N.ds_t);
+        N.ds_x = nullptr;
+        N.ds_t = nullptr;
+        N.cap_pairs = N.n_pairs = N.next_pair = 0;
+        c->ws_record = false;
+        return PIC_OK;
+    }
+    const bool autos = phi_scale == 0 && db_scale == 0 && target_scale == 0;
+    if (!autos && (!(phi_scale > 0) || !(db_scale > 0) || !(target_scale > 0)))
+        return fail(PIC_ERR_ARG, "warm start: scales must all be positive, or all 0 (automatic)");
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
     cudaFree(N.ds_x);
     cudaFree(N.ds_t);
+    cudaFree(N.loss_acc);
     N.ds_x = nullptr;
     N.ds_t = nullptr;
+    N.loss_acc = nullptr;
     N.cap_pairs = N.n_pairs = N.next_pair = 0;
+    c->ws_record = false;
+    if (cudaMalloc(&N.ds_x, (size_t)max_pairs * N.P * N.P * 4 * 2) ||
+        cudaMalloc(&N.ds_t, (size_t)max_pairs * c->nodes * 4) ||
+        cudaMalloc(&N.loss_acc, (size_t)max_pairs * 4)) {
+        cudaGetLastError();
+        cudaFree(N.ds_x);
+        cudaFree(N.ds_t);
+        cudaFree(N.loss_acc);
+        N.ds_x = nullptr;
+        N.ds_t = nullptr;
+        N.loss_acc = nullptr;
+        return fail(PIC_ERR_CAPACITY, "warm start: dataset does not fit in device memory");
+    }
     N.s0 = (float)phi_scale;
     N.s1 = (float)db_scale;
     N.s2 = (float)target_scale;
-    if (max_pairs > 0) {
-        cudaFree(N.loss_acc);
-        N.loss_acc = nullptr;
-        if (cudaMalloc(&N.ds_x, (size_t)max_pairs * N.P * N.P * 4 * 2) ||
-            cudaMalloc(&N.ds_t, (size_t)max_pairs * c->nodes * 4) ||
-            cudaMalloc(&N.loss_acc, (size_t)max_pairs * 4))
-            return fail(PIC_ERR_CAPACITY, "warm start: dataset does not fit in device memory");
-        N.cap_pairs = max_pairs;
-    }
-    c->ws_record = max_pairs > 0;
+    N.auto_scale = autos;
+    N.cap_pairs = max_pairs;
+    c->ws_record = true;
     return PIC_OK;
 }
 
@@ -1003,20 +1136,14 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
     if (!c->ws || c->ws->net.n_pairs == 0) return fail(PIC_ERR_STATE, "warm start: no recorded pairs");
     Net& N = c->ws->net;
     const int P = N.P;
-    const float inv_count = 1.f / (float)c->nodes;
-    std::vector<float> lp(g1((int64_t)P * P));
     double last = 0;
     for (int e = 0; e < epochs; ++e) {
         double ep = 0;
         for (int64_t s = 0; s < N.n_pairs; ++s) {
             PIC_TRY(ws_pack(c));
-            PIC_CUDA(cudaMemcpyAsync(N.x0, N.ds_x + s * (int64_t)P * P * 4, (size_t)P * P * 4 * 2,
-                                     cudaMemcpyDeviceToDevice, c->stream));
+            N.xin = N.ds_x + s * (int64_t)P * P * 4;
             forward(c);
-            k_mse<<<g1((int64_t)P * P), 256, 0, c->stream>>>(N.out, N.ds_t + s * c->nodes, c->mask,
-                                                            N.GX, N.GY, P, inv_count, N.dout,
-                                                            N.loss_partial);
-            k_sum_partials<<<1, 32, 0, c->stream>>>(N.loss_partial, (int)lp.size(), 1, N.loss_acc + s);
+            enqueue_loss(c, N.ds_t + s * c->nodes, N.loss_acc + s);
             backward(c);
             N.adam_t += 1;
             const float b1 = 0.9f, b2 = 0.999f;
@@ -1024,7 +1151,8 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
             const float c2 = 1.f / (1.f - std::pow(b2, (float)N.adam_t));
             k_adam<<<g1(kParams), 256, 0, c->stream>>>(N.w, N.m, N.v, N.g, kParams, (float)lr, b1, b2,
                                                        1e-8f, c1, c2, 1.f, nullptr, nullptr);
-            c->launches += 5;
+            N.packed = false;
+            c->launches += 1;
         }
         std::vector<float> ls((size_t)N.n_pairs);
         PIC_CUDA(cudaMemcpyAsync(ls.data(), N.loss_acc, ls.size() * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1054,6 +1182,7 @@ int pic_ws_set_params(pic_ctx* c, const float* host, int64_t n, double phi_scale
     Net& N = c->ws->net;
     PIC_CUDA(cudaStreamSynchronize(c->stream));
     PIC_CUDA(cudaMemcpy(N.w, host, kParams * 4, cudaMemcpyHostToDevice));
+    N.packed = false;
     N.s0 = (float)phi_scale;
     N.s1 = (float)db_scale;
     N.s2 = (float)target_scale;
@@ -1063,12 +1192,13 @@ int pic_ws_set_params(pic_ctx* c, const float* host, int64_t n, double phi_scale
 
 int64_t pic_ws_num_params(void) { return kParams; }
 
-// One forward + backward on a caller-given input image and target, for
-// gradient checks: x0 host [P*P*3] (channels phi, db, mask already scaled),
-// target host [GX*GY]; returns out [P*P], gradient [kParams], loss.
-int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* target_host, float* out_host,
+// One forward + backward on a caller-given input image and scaled
+// right-hand-side change, for gradient checks: x0 host [P*P*3] (channels phi,
+// RHS change, mask, already scaled), rhs host [GX*GY]; returns out [P*P],
+// gradient [kParams], loss.  Uses the network's current scales for kappa.
+int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* rhs_host, float* out_host,
                       float* grad_host, double* loss) {
-    if (!c || !x0_host || !target_host) return fail(PIC_ERR_ARG, "null argument");
+    if (!c || !x0_host || !rhs_host) return fail(PIC_ERR_ARG, "null argument");
     PIC_TRY(ws_alloc(c));
     Net& N = c->ws->net;
     const int P = N.P;
@@ -1078,26 +1208,35 @@ int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* target_host
         x[p * 4 + 3] = __float2bfloat16(0.f);
     }
     float* t = nullptr;
+    float* l = nullptr;
     PIC_CUDA(cudaMalloc(&t, (size_t)c->nodes * 4));
+    PIC_CUDA(cudaMalloc(&l, 4));
     PIC_CUDA(cudaMemcpy(N.x0, x.data(), x.size() * 2, cudaMemcpyHostToDevice));
-    PIC_CUDA(cudaMemcpy(t, target_host, (size_t)c->nodes * 4, cudaMemcpyHostToDevice));
+    PIC_CUDA(cudaMemcpy(t, rhs_host, (size_t)c->nodes * 4, cudaMemcpyHostToDevice));
     PIC_TRY(ws_pack(c));
+    N.xin = N.x0;
     forward(c);
-    k_mse<<<g1((int64_t)P * P), 256, 0, c->stream>>>(N.out, t, c->mask, N.GX, N.GY, P,
-                                                    1.f / (float)c->nodes, N.dout, N.loss_partial);
-    std::vector<float> lp(g1((int64_t)P * P));
-    PIC_CUDA(cudaMemcpyAsync(lp.data(), N.loss_partial, lp.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    enqueue_loss(c, t, l);
     backward(c);
+    float lh = 0.f;
+    PIC_CUDA(cudaMemcpyAsync(&lh, l, 4, cudaMemcpyDeviceToHost, c->stream));
     PIC_CUDA(cudaStreamSynchronize(c->stream));
     cudaFree(t);
+    cudaFree(l);
     if (out_host) PIC_CUDA(cudaMemcpy(out_host, N.out, (size_t)P * P * 4, cudaMemcpyDeviceToHost));
     if (grad_host) PIC_CUDA(cudaMemcpy(grad_host, N.g, kParams * 4, cudaMemcpyDeviceToHost));
-    if (loss) {
-        double l = 0;
-        for (float v : lp) l += v;
-        *loss = l;
-    }
+    if (loss) *loss = lh;
     PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+int pic_ws_scales(pic_ctx* c, double* scales) {
+    if (!c || !scales) return fail(PIC_ERR_ARG, "null argument");
+    if (!c->ws) return fail(PIC_ERR_STATE, "warm start: no network");
+    const Net& N = c->ws->net;
+    scales[0] = N.s0;
+    scales[1] = N.s1;
+    scales[2] = N.s2;
     return PIC_OK;
 }
 

@@ -138,6 +138,7 @@ def lib():
         "pic_ws_get_params": (cint, [vp, vp, i64]),
         "pic_ws_set_params": (cint, [vp, vp, i64, dbl, dbl, dbl]),
         "pic_ws_grid": (cint, [vp, P(cint)]),
+        "pic_ws_scales": (cint, [vp, P(dbl)]),
         "pic_ws_debug_step": (cint, [vp, vp, vp, vp, vp, P(dbl)]),
         "pic_deposit_points_noalloc": (cint, [vp, i64, i32, i32, dbl, dbl, vp, dbl, dbl, vp, vp, vp]),
     }
@@ -327,7 +328,8 @@ class Pic:
         _check(lib().pic_set_poisson(self.h, solver, warm, tol, maxit))
 
     # ---- learned warm start ----
-    def ws_record(self, max_pairs: int, phi_scale: float, db_scale: float, target_scale: float):
+    def ws_record(self, max_pairs: int, phi_scale: float = 0.0, db_scale: float = 0.0,
+                  target_scale: float = 0.0):
         _check(lib().pic_ws_record(self.h, max_pairs, phi_scale, db_scale, target_scale))
 
     def ws_pairs(self) -> int:
@@ -349,6 +351,11 @@ class Pic:
     def ws_set_params(self, theta, phi_scale, db_scale, target_scale):
         theta = np.ascontiguousarray(theta, dtype=np.float32)
         _check(lib().pic_ws_set_params(self.h, _p(theta), len(theta), phi_scale, db_scale, target_scale))
+
+    def ws_scales(self):
+        out = (ctypes.c_double * 3)()
+        _check(lib().pic_ws_scales(self.h, out))
+        return tuple(out)
 
     def ws_grid(self) -> int:
         P = ctypes.c_int(0)

@@ -246,11 +246,17 @@ int pic_deposit_points_noalloc(const pic_point* dev_points, int64_t n, int32_t n
  * BF16 tensor-core kernels with FP32 accumulation) predicting phi_n from
  * phi_{n-1}, the change of the right-hand side and the electrode mask.  PCG
  * then runs to the same tolerance, so the answer never depends on it. */
-/* Start (max_pairs > 0) or stop (0) recording (input, target) pairs at each
- * Poisson solve; the scales normalise phi (V), the RHS change times dx^2 (V)
- * and the target phi_n - phi_{n-1} (V). */
+/* max_pairs > 0: (re)start recording (input, target) pairs at each Poisson
+ * solve into a new dataset that keeps the newest max_pairs; the scales
+ * normalise phi (V), the RHS change times dx^2 (V) and the target
+ * phi_n - phi_{n-1} (V).  All three 0: each is set to its root-mean-square
+ * over the non-electrode nodes of the first recorded pair (read back with
+ * pic_ws_scales).  max_pairs == 0: stop recording, keep the dataset (training
+ * can continue).  max_pairs < 0: stop and release the dataset. */
 int pic_ws_record(pic_ctx* ctx, int64_t max_pairs, double phi_scale, double db_scale,
                   double target_scale);
+/* The three scales in use: phi, RHS change times dx^2, target. */
+int pic_ws_scales(pic_ctx* ctx, double* scales3);
 int pic_ws_pairs(pic_ctx* ctx, int64_t* n);
 /* Adam epochs over the recorded pairs (one pair per step); *loss = mean
  * normalised squared error of the last epoch. */
@@ -261,11 +267,16 @@ int pic_ws_set_params(pic_ctx* ctx, const float* host, int64_t n, double phi_sca
                       double db_scale, double target_scale);
 /* Side length P of the network's padded square grid. */
 int pic_ws_grid(pic_ctx* ctx, int* P);
-/* One forward + backward pass on a given scaled input image x0[P*P*3]
- * (channels phi, RHS change, mask) and target[GRID_X*GRID_Y]: returns the
- * output image out[P*P], the parameter gradient grad[pic_ws_num_params()]
- * and the loss.  For gradient checks. */
-int pic_ws_debug_step(pic_ctx* ctx, const float* x0, const float* target, float* out,
+/* Training loss: the starting residual of PCG from the network's guess, in
+ * scaled units, r = rhs - kappa L(out) on non-electrode nodes, where
+ * rhs = (b_n - b_{n-1}) dx^2 / s1, kappa = s2/s1, and
+ * L(u) = (2 + 2 dx^2/dy^2) u - (u_w + u_e) - (dx^2/dy^2)(u_s + u_n) with
+ * u = 0 on electrodes; loss = sum r^2 / (GX*GY).
+ * One forward + backward pass on a given scaled input image x0[P*P*3]
+ * (channels phi, RHS change, mask) and rhs[GX*GY]: returns the output image
+ * out[P*P], the parameter gradient grad[pic_ws_num_params()] and the loss.
+ * For gradient checks. */
+int pic_ws_debug_step(pic_ctx* ctx, const float* x0, const float* rhs, float* out,
                       float* grad, double* loss);
 
 /* ---- Poisson controls -------------------------------------------------- */

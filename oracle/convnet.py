@@ -80,26 +80,33 @@ def conv_dw(x, dy):
     return dw, dy.sum(axis=(0, 1))
 
 
-def pool(x):
-    return bf16(0.25 * (x[0::2, 0::2] + x[0::2, 1::2] + x[1::2, 0::2] + x[1::2, 1::2]))
+def pool(x, rnd=None):
+    rnd = bf16 if rnd is None else rnd
+    return rnd(0.25 * (x[0::2, 0::2] + x[0::2, 1::2] + x[1::2, 0::2] + x[1::2, 1::2]))
 
 
 def up(x):
     return np.repeat(np.repeat(x, 2, axis=0), 2, axis=1)
 
 
-def forward(theta, x0):
-    """x0: [P, P, 3].  Returns (out [P, P], cache)."""
+def _identity(x):
+    return np.asarray(x, dtype=np.float64)
+
+
+def forward(theta, x0, exact=False):
+    """x0: [P, P, 3].  Returns (out [P, P], cache).  exact=True skips every
+    bfloat16 rounding (plain FP64 network, for gradient checks)."""
+    bf16 = _identity if exact else globals()["bf16"]
     w_in, b_in, convs, w_out, b_out = unpack(theta)
     wb = [(bf16(w), b) for (w, b) in convs]
     x0 = bf16(x0)
     a = [None] * 11
     a[1] = bf16(np.maximum(conv(x0, w_in, b_in), 0))
     a[2] = bf16(np.maximum(conv(a[1], *wb[0]), 0))
-    p1 = pool(a[2])
+    p1 = pool(a[2], bf16)
     a[3] = bf16(np.maximum(conv(p1, *wb[1]), 0))
     a[4] = bf16(np.maximum(conv(a[3], *wb[2]), 0))
-    p2 = pool(a[4])
+    p2 = pool(a[4], bf16)
     a[5] = bf16(np.maximum(conv(p2, *wb[3]), 0))
     a[6] = bf16(np.maximum(conv(a[5], *wb[4]), 0))
     u1 = bf16(up(a[6]) + a[4])
@@ -112,19 +119,42 @@ def forward(theta, x0):
     return out, dict(x0=x0, a=a, p1=p1, p2=p2, u0=u0, u1=u1, wb=wb, w_out=w_out)
 
 
-def loss_grad(theta, x0, target, mask, GX, GY):
-    """MSE over non-electrode nodes of the GX x GY node grid (mean over all
-    GX*GY nodes, as the CUDA loss) and its gradient w.r.t. theta."""
-    out, K = forward(theta, x0)
+def stencil(v, beta):
+    """L(v) = (2 + 2 beta) v - (v_w + v_e) - beta (v_s + v_n), zero outside."""
+    return ((2 + 2 * beta) * v - _shift(v, 0, -1) - _shift(v, 0, 1)
+            - beta * (_shift(v, -1, 0) + _shift(v, 1, 0)))
+
+
+def free_nodes(mask, GX, GY):
+    """Non-electrode nodes off the outer ring (every wall node is an electrode)."""
+    free = mask.reshape(GY, GX) == 0
+    free[0, :] = free[-1, :] = free[:, 0] = free[:, -1] = False
+    return free
+
+
+def residual(out, rhs, mask, GX, GY, kappa, beta):
+    """Scaled starting residual of PCG from the guess: r = rhs - kappa L(u) on
+    free nodes, 0 elsewhere, with u = out on free nodes and 0 on electrodes."""
+    free = free_nodes(mask, GX, GY)
+    u = np.where(free, out[:GY, :GX], 0.0)
+    return np.where(free, rhs.reshape(GY, GX) - kappa * stencil(u, beta), 0.0)
+
+
+def loss_grad(theta, x0, rhs, mask, GX, GY, kappa, beta, exact=False):
+    """Residual loss sum(r^2)/(GX*GY) of the guess (warmstart.cu k_resid) and
+    its gradient w.r.t. theta.  Gradient images are rounded to bfloat16 where
+    the CUDA kernels store them, unless exact=True.  Weight gradients are taken
+    with respect to the bf16 working copies and applied to the FP32 masters
+    (straight-through)."""
+    bf16 = _identity if exact else globals()["bf16"]
+    out, K = forward(theta, x0, exact)
     P = out.shape[0]
-    valid = np.zeros((P, P), bool)
-    valid[:GY, :GX] = mask.reshape(GY, GX) == 0
-    t = np.zeros((P, P))
-    t[:GY, :GX] = target.reshape(GY, GX)
     n = GX * GY
-    e = np.where(valid, out - t, 0.0)
-    loss = float((e * e).sum() / n)
-    dout = 2.0 * e / n
+    r = residual(out, rhs, mask, GX, GY, kappa, beta)
+    loss = float((r * r).sum() / n)
+    free = free_nodes(mask, GX, GY)
+    dout = np.zeros((P, P))
+    dout[:GY, :GX] = np.where(free, -2.0 * kappa / n * stencil(r, beta), 0.0)
     g = np.zeros(N_PARAMS)
     offs = [IN_W + IN_B + i * (W32 + B32) for i in range(N_CONV32)]
     o_out = IN_W + IN_B + N_CONV32 * (W32 + B32)
