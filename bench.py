@@ -39,11 +39,11 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s (bin+deposit+push)"
 UNIT = "particle-steps/s"
-# Algorithmic HBM bytes per particle for each launch of the push (FP32 state,
-# 20 B per particle: float4 {fx, fy, vx, vy} + float vz).
-BYTES_COUNT_PASS = 16     # read {fx, fy, vx, vy} (vz is not needed to classify)
-BYTES_SCATTER_PASS = 40   # read the state, write it to the new position
-BYTES_STEP = 56           # whole particle phase of one step
+# Algorithmic HBM bytes per particle of the push pass (FP32 state, 20 B per
+# particle: float4 {fx, fy, vx, vy} + float vz): read the state, write it to
+# its slot in the other buffer.  Binning and the deposit ride on this pass.
+BYTES_PUSH_PASS = 40
+BYTES_STEP = 40           # whole particle phase of one step
 BYTES_SURVEY_FP32 = 112   # the blueprint's per-particle-step figure (push 48 + deposit 12 + bin 52)
 
 
@@ -59,6 +59,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-energy", action="store_true",
                     help="skip the energy-weighted mesh (deposit_energy = 0)")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned warm-start comparison")
+    ap.add_argument("--ws-pairs", type=int, default=64,
+                    help="pairs recorded for the learned warm start")
+    ap.add_argument("--ws-epochs", type=int, default=6)
+    ap.add_argument("--ws-eval", type=int, default=12,
+                    help="evaluation steps, each solved from both guesses")
     return ap.parse_args()
 
 
@@ -244,7 +251,7 @@ def ncu_traffic_per_particle():
             continue
         k, _, v = line.strip().partition(" ")
         kv[k] = v
-    v = kv.get("scatter_dram_bytes_per_particle")
+    v = kv.get("push_dram_bytes_per_particle")
     return (float(v) if v else None), kv.get("source")
 
 
@@ -331,18 +338,18 @@ def run_ours(args, rank, world, local_rank):
         it += 1
     L.pic_profile_read(pic.h, ctypes.cast(ms6, ctypes.c_void_p), ctypes.cast(calls6, ctypes.c_void_p), 1)
     L.pic_set_profiling(pic.h, 0)
-    phase_names = ["push_count", "scan", "push_scatter", "deposit", "flush", "poisson"]
+    phase_names = ["push", "fixup", "relayout", "deposit", "flush", "poisson"]
     phases = {phase_names[i]: {"ms_per_step": ms6[i] / prof_steps, "calls_per_step": calls6[i] / prof_steps}
               for i in range(P_PHASES)}
     peak, peak_kind = measured_peaks()
-    scatter_ms = ms6[2] / calls6[2] if calls6[2] else float("nan")
+    push_ms = ms6[0] / calls6[0] if calls6[0] else float("nan")
     avg_n = n_part / 2
-    achieved = BYTES_SCATTER_PASS * avg_n / (scatter_ms * 1e-3) / 1e9
+    achieved = BYTES_PUSH_PASS * avg_n / (push_ms * 1e-3) / 1e9
     traffic_pp, traffic_src = ncu_traffic_per_particle()
-    roofline = {"kernel": "k_particles<kScatter> (push + scatter + fused deposit)",
+    roofline = {"kernel": "k_cells<kPush> (gather + Boris + binning + fused deposit, one pass)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
-                "bytes_per_particle": BYTES_SCATTER_PASS,
+                "bytes_per_particle": BYTES_PUSH_PASS,
                 "traffic": (traffic_pp * avg_n) if traffic_pp else None,
                 "traffic_source": traffic_src}
     step_particle_ms = (ms6[0] + ms6[1] + ms6[2] + ms6[4]) / prof_steps
@@ -351,6 +358,9 @@ def run_ours(args, rank, world, local_rank):
                      "survey_112B_equivalent_GBs": BYTES_SURVEY_FP32 * n_part / (step_particle_ms * 1e-3) / 1e9}
     roofline_step["frac"] = roofline_step["achieved_GBs"] / peak
 
+    learned = None
+    if not args.no_learned:
+        learned, it = run_learned(pic, args, it)
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(pic, args.steps, n_part, it)
@@ -368,8 +378,9 @@ def run_ours(args, rank, world, local_rank):
                       "wall_s": t_wall},
         "poisson": {"solver": "MG-PCG (FP32 V-cycle, FP64 CG)", "warm_start": "previous phi",
                     "ms_per_step_plain": pois_sum / args.steps,
-                    "ms_per_step_learned": None, "iters_per_step": statistics.mean(iters),
-                    "relres": relres, "tol": 1e-8},
+                    "ms_per_step_learned": learned["ms_per_step_learned"] if learned else None,
+                    "iters_per_step": statistics.mean(iters),
+                    "relres": relres, "tol": 1e-8, "learned": learned},
         "roofline": roofline, "roofline_particle_phase": roofline_step,
         "phases": phases, "gpu_launches": gpu_launches, "clocks": clocks, "e2e": e2e,
     }
@@ -377,6 +388,56 @@ def run_ours(args, rank, world, local_rank):
 
 
 P_PHASES = 6
+
+
+def run_learned(pic, args, it):
+    """The learned warm start on this workload (a short form of the
+    train-then-evaluate protocol): record (input, RHS change) pairs from the
+    running simulation, train the network on the GPU, then solve every
+    evaluation step twice from the same state -- from the network's guess and
+    from phi_{n-1} -- both to the same 1e-8 relative residual.  Poisson device
+    milliseconds come from the library's own events around each solve."""
+    import pic_b200 as P
+    pic.ws_record(args.ws_pairs)
+    for _ in range(args.ws_pairs + 1):
+        pic.step(it)
+        it += 1
+    pic.ws_record(0)
+    t0 = time.perf_counter()
+    loss0 = pic.ws_train(1, 1e-3)
+    loss = pic.ws_train(max(args.ws_epochs - 1, 1), 1e-3)
+    train_s = time.perf_counter() - t0
+    ml, mp, il, ip, dphi = [], [], [], [], []
+    for _ in range(args.ws_eval):
+        pic.zero_rho()
+        for s in range(2):
+            pic.charge_deposition(s)
+        rho, phi_prev = pic.rho(), pic.phi()
+        pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_LEARNED, 1e-8, 500)
+        pic.poisson_solve(it)
+        n_l, r_l, ms_l = pic.poisson_stats()
+        phi_l = pic.phi()
+        pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_PREVIOUS, 1e-8, 500)
+        pic.set_phi(phi_prev)
+        pic.set_rho(rho)
+        pic.poisson_solve(it)
+        n_p, r_p, ms_p = pic.poisson_stats()
+        dphi.append(float(np.abs(phi_l - pic.phi()).max()))
+        for s in range(2):
+            pic.move_particles(s, it)
+        it += 1
+        ml.append(ms_l)
+        mp.append(ms_p)
+        il.append(n_l)
+        ip.append(n_p)
+    pic.ws_record(-1)
+    return {"ms_per_step_learned": statistics.mean(ml), "ms_per_step_plain_same_state": statistics.mean(mp),
+            "iters_learned": statistics.mean(il), "iters_plain_same_state": statistics.mean(ip),
+            "max_abs_dphi_V": max(dphi), "train_pairs": args.ws_pairs, "train_epochs": args.ws_epochs,
+            "train_s": train_s, "loss_first_epoch": loss0, "loss_last_epoch": loss,
+            "eval_steps": args.ws_eval, "scales": list(pic.ws_scales()),
+            "what": "residual loss |db - A guess|^2 (scaled); network: 3-level conv encoder-decoder, "
+                    "32 channels, bf16 mma.sync tensor cores, FP32 accumulation"}, it
 
 
 def run_e2e(pic, steps, n_part, it0):

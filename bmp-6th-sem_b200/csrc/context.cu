@@ -226,6 +226,8 @@ int pic_create(const pic_config* cfg_in, pic_ctx** out) {
         cudaMemcpy(c->phi, phi0.data(), n * 8, cudaMemcpyHostToDevice) ||
         cudaMemset(c->rho, 0, n * 8) || cudaMemset(c->fld, 0, n * sizeof(float4)))
         return bail(fail(PIC_ERR_CUDA, "grid initialisation copy failed"));
+    c->bz_uniform = true;
+    c->bz_value = cfg.b0;
     int st = fields_set_bz(c);
     if (st) return bail(st);
     for (int s = 0; s < cfg.num_species; ++s)
@@ -466,6 +468,13 @@ int pic_update_fields_from_phi(pic_ctx* c) {
 int pic_set_bz(pic_ctx* c, const double* host) {
     if (!c || !host) return fail(PIC_ERR_ARG, "null argument");
     PIC_TRY(copy_to_device(c, c->bz, host, (size_t)c->nodes * 8));
+    c->bz_uniform = true;
+    c->bz_value = host[0];
+    for (int64_t i = 1; i < c->nodes; ++i)
+        if (host[i] != host[0]) {
+            c->bz_uniform = false;
+            break;
+        }
     return fields_set_bz(c);
 }
 

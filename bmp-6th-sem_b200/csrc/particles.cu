@@ -8,36 +8,43 @@
 //   * interpolate() (src/interpolation.cpp:13-171);
 //   * deterministic_mover() + MoverKernel (src/mover.cpp:103-176, 304-366).
 //
-// Layout: particles of a species live cell-sorted in a double buffer.  The
-// cell of a particle is implied by its position in the buffer: off[c] ..
-// off[c+1] is cell c (c = gy*nx + gx).  Each particle is 20 bytes:
-//   float4 {fx, fy, vx, vy} (in-cell offsets in [0,1), velocities in m/s)
-//   float  vz
+// Layout: the particles of a species live in a double buffer of 20-byte
+// slots, float4 {fx, fy, vx, vy} (in-cell offsets in [0,1), velocities in
+// m/s) plus float vz.  Cell c (c = gy*nx + gx) owns the slots base[c] ..
+// base[c+1] of both buffers with slack: its particles are a front run (the
+// ones that stayed in the cell at the last push) and a back run (the ones
+// that moved in), with a free gap between them.
 //
-// One push step of a species is four launches:
-//   1. k_particles<COUNT>   -- gather + Boris for every particle, classify as
-//      stayer / mover / dead, count stayers per cell and movers per target
-//      cell.  Nothing per particle is written.
-//   2. k_scan_partials, k_scan_apply -- exclusive scan of the new per-cell
-//      counts into the new segment table.
-//   3. k_particles<SCATTER> -- the same push again (bit-identical: every
-//      float operation is an explicit round-to-nearest intrinsic, so the two
-//      passes cannot contract differently), scatter into the other buffer and
-//      deposit the NEW positions into the 64-bit fixed-point accumulators.
-// The deposit of positions x_{n+1} therefore rides on the push of step n; the
-// next charge_deposition only converts the accumulators.  Per particle-step
-// the traffic is 20 B (pass 1) + 40 B (pass 2) of HBM.
+// One push of a species is ONE pass over its particles (k_cells<kPush>): a
+// warp walks a cell, gathers E and Bz, pushes, and
+//   * writes a particle that stays in its cell to the front of the cell's
+//     slots in the other buffer, at its rank among the cell's stayers
+//     (ballot + popc: no atomics);
+//   * appends a particle that moves to a neighbouring cell to the back of
+//     that cell's slots: lanes moving the same way form a group
+//     (match.any), the group leader reserves the slots with one atomic on
+//     the target's back count.  The reservation is capped at the target's
+//     capacity minus its current count (the most stayers it can have), so
+//     front and back runs never meet;
+//   * deposits the new position: stayers accumulate per-lane integer
+//     moments reduced once per cell, movers add their four fixed-point
+//     corner weights with 64-bit RED.
+// A mover whose target is full, or which jumped more than one cell, goes to
+// a side list; a small kernel (k_fixup) then places it in the free space of
+// its target cell, or keeps it on the list (still part of the state: it is
+// pushed and deposited from there at the next step).  When the list grows,
+// the host rebuilds the layout from the per-cell counts (k_relayout_*).
+// Per particle-step the HBM traffic is 20 B read + 20 B written.
 //
-// Work decomposition: a block owns a kTileX x kTileY tile of cells; each warp
-// walks whole cells of the tile (field values of the cell's four nodes are
-// warp-uniform loads).  Stayers accumulate their deposit in registers and are
-// reduced once per cell; movers deposit with shared atomics into the block's
-// node tile (kHalo cells of margin) or global atomics beyond it.  The tile is
-// flushed once to HBM with 64-bit integer atomics.
+// Determinism: the charge and energy deposits are sums of integers, so they
+// do not depend on the order in which particles are processed or placed;
+// the set of particles in each cell is deterministic, their order within
+// the back run is not.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "pic_internal.h"
 
@@ -51,11 +58,27 @@ constexpr int kScanTile = 2048;               // cells per scan block
 constexpr uint32_t kAxisOne = 1u << kAxisBits;
 constexpr float kAxisScale = (float)(1u << kAxisBits);
 constexpr float kOneBelow = 0x1.fffffep-1f;   // largest float < 1
+constexpr float kEnergyScale = 4194304.0f;    // eV -> 2^-22 eV units
+constexpr int kFixupBlocks = 296;
 
-enum Mode { kCount = 0, kScatter = 1, kDeposit = 2 };
-constexpr int kDirs = 9;      // 3x3 neighbourhood, d = (sy+1)*3 + (sx+1)
-constexpr int kStay = 4;      // d of a particle that keeps its cell
+enum Mode { kPush = 0, kDeposit = 1 };
+constexpr int kStay = 4;      // d = (sy+1)*3 + (sx+1) of a particle that keeps its cell
 constexpr int kFar = 9;       // moved more than one cell in x or y
+
+// list_counts slots
+enum { kOvf = 0, kLoose0 = 1, kLoose1 = 2 };
+
+struct ListDev {
+    float4* a;
+    float* vz;
+    uint32_t* cell;
+    uint32_t* count;
+    uint32_t cap;
+};
+
+__host__ __forceinline__ ListDev list_dev(const LooseList& L) {
+    return ListDev{L.a, L.vz, L.cell, L.count, L.cap};
+}
 
 struct KArgs {
     int nx, ny, GX;
@@ -66,22 +89,46 @@ struct KArgs {
     const float* __restrict__ src_vz;
     float4* __restrict__ dst_a;
     float* __restrict__ dst_vz;
-    const uint32_t* __restrict__ off;
-    uint32_t* dcount;   // [9][ncells]
-    const uint32_t* __restrict__ sub;  // [10][ncells]
-    uint32_t* farin;
-    uint32_t* farcur;
+    const uint32_t* __restrict__ base;
+    const uint32_t* __restrict__ front_src;
+    const uint32_t* __restrict__ back_src;
+    uint32_t* front_dst;
+    uint32_t* back_dst;
+    ListDev ovf;
     unsigned long long* acc_q;
     unsigned long long* acc_e;
-    unsigned long long* counters;  // [0] left exits, [1] cell overflow, [2] scatter guard
-    uint32_t cap;                  // particles the destination buffer holds
-    int energy;
+    unsigned long long* counters;  // [0] left exits, [1] cell limit, [2] lost particles
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Asynchronous global -> shared copies (cp.async); a false predicate copies
+// nothing and fills the destination with zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool pred) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(pred ? 16 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool pred) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(pred ? 4 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Result of one gather + Boris + position update.
@@ -92,11 +139,11 @@ struct Pushed {
     bool left;
 };
 
-// Bilinear gather of E and Bz from the cell's four nodes plus the Boris push
-// of deterministic_mover (src/mover.cpp:123-174) in FP32.  Weights:
+// Bilinear gather of E (and Bz) from the cell's four nodes plus the Boris
+// push of deterministic_mover (src/mover.cpp:123-174) in FP32.  Weights:
 // (1-fx)(1-fy), fx(1-fy), (1-fx)fy, fx*fy == the reference's unnormalised
-// weights divided by dx*dy.  Every operation is an explicit _rn intrinsic so
-// the COUNT and SCATTER passes produce identical bits.
+// weights divided by dx*dy.  Every operation is an explicit _rn intrinsic:
+// the result does not depend on how the compiler contracts the code.
 __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, float4 n01,
                                            float4 n11, const SpeciesConsts& k, int gx, int gy,
                                            int nx, int ny) {
@@ -106,50 +153,41 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     const float w01 = __fmul_rn(ofx, fy), w11 = __fmul_rn(fx, fy);
     const float ex = __fmaf_rn(w11, n11.x, __fmaf_rn(w01, n01.x, __fmaf_rn(w10, n10.x, __fmul_rn(w00, n00.x))));
     const float ey = __fmaf_rn(w11, n11.y, __fmaf_rn(w01, n01.y, __fmaf_rn(w10, n10.y, __fmul_rn(w00, n00.y))));
-    const float bz = __fmaf_rn(w11, n11.z, __fmaf_rn(w01, n01.z, __fmaf_rn(w10, n10.z, __fmul_rn(w00, n00.z))));
-    // Boris rotation about z (src/mover.cpp:151-162).
+    // Boris rotation about z (src/mover.cpp:151-162): t = h Bz, s = 2t/(1+t^2)
+    float t, s;
+    if (k.bzu) {
+        t = k.bt;
+        s = k.bs;
+    } else {
+        const float bz = __fmaf_rn(w11, n11.z, __fmaf_rn(w01, n01.z, __fmaf_rn(w10, n10.z, __fmul_rn(w00, n00.z))));
+        t = __fmul_rn(k.h, bz);
+        // approximate reciprocal: ~1 ulp, far below the FP32 state's error
+        s = __fdividef(__fmul_rn(2.0f, t), __fmaf_rn(t, t, 1.0f));
+    }
     const float ax = __fmul_rn(k.h, ex), ay = __fmul_rn(k.h, ey);
     const float vxm = __fadd_rn(a.z, ax), vym = __fadd_rn(a.w, ay);
-    const float t = __fmul_rn(k.h, bz);
     const float vxp = __fmaf_rn(vym, t, vxm);
     const float vyp = __fmaf_rn(-vxm, t, vym);
-    // s = 2t/(1+t^2) with the approximate reciprocal: both passes compute the
-    // same bits, and its error (~1 ulp) is far below the FP32 state's
-    const float s = __fdividef(__fmul_rn(2.0f, t), __fmaf_rn(t, t, 1.0f));
     Pushed o;
     o.vx = __fadd_rn(__fmaf_rn(vyp, s, vxm), ax);
     o.vy = __fadd_rn(__fmaf_rn(-vxp, s, vym), ay);
-    // Position update in cell units (src/mover.cpp:164-165), then re-cell.
+    // Position update in cell units (src/mover.cpp:164-165), then re-cell:
+    // the integer part moves the cell, the remainder is the new offset.
     const float px = __fmaf_rn(o.vx, k.dtdx, fx);
     const float py = __fmaf_rn(o.vy, k.dtdy, fy);
-    if (px >= -1.0f && px < 2.0f && py >= -1.0f && py < 2.0f) {
-        // moved at most one cell per axis: floor(p) in {-1, 0, 1}
-        const int sx = (px >= 1.0f) - (px < 0.0f);
-        const int sy = (py >= 1.0f) - (py < 0.0f);
-        const int ngx = gx + sx, ngy = gy + sy;
-        // absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H)
-        const bool alive = ngx >= 0 && ngx < nx && ngy >= 0 && ngy < ny;
-        o.left = ngx < 0;
-        o.gx = ngx;
-        o.gy = ngy;
-        o.dir = alive ? (sy + 1) * 3 + (sx + 1) : -1;
-        const float fsx = (px >= 1.0f) ? 1.0f : ((px < 0.0f) ? -1.0f : 0.0f);
-        const float fsy = (py >= 1.0f) ? 1.0f : ((py < 0.0f) ? -1.0f : 0.0f);
-        o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
-        o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
-    } else {
-        // far jump, or NaN (which lands outside)
-        const float fsx = floorf(px), fsy = floorf(py);
-        const float ngx = __fadd_rn((float)gx, fsx), ngy = __fadd_rn((float)gy, fsy);
-        const bool alive = (ngx >= 0.0f) && (ngx < (float)nx) && (ngy >= 0.0f) && (ngy < (float)ny);
-        o.left = !(ngx >= 0.0f);
-        o.gx = alive ? (int)ngx : gx;
-        o.gy = alive ? (int)ngy : gy;
-        const int ix = o.gx - gx, iy = o.gy - gy;
-        o.dir = !alive ? -1 : ((ix < -1 || ix > 1 || iy < -1 || iy > 1) ? kFar : (iy + 1) * 3 + (ix + 1));
-        o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
-        o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
-    }
+    const float fsx = floorf(px), fsy = floorf(py);
+    o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
+    o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
+    // beyond 2^20 cells (or NaN) a particle is lost whatever the grid
+    const bool ok = fabsf(px) < 1048576.0f && fabsf(py) < 1048576.0f;
+    const int sx = ok ? (int)fsx : 0, sy = ok ? (int)fsy : 0;
+    o.gx = gx + sx;
+    o.gy = gy + sy;
+    // absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H)
+    const bool alive = ok && (unsigned)o.gx < (unsigned)nx && (unsigned)o.gy < (unsigned)ny;
+    o.left = ok ? (o.gx < 0) : (px < 0.0f);
+    const bool near = (unsigned)(sx + 1) < 3u && (unsigned)(sy + 1) < 3u;
+    o.dir = !alive ? -1 : (near ? (sy + 1) * 3 + (sx + 1) : kFar);
     return o;
 }
 
@@ -160,46 +198,29 @@ __device__ __forceinline__ uint32_t axis_fixed(float f) {
     return __float_as_uint(t) - 0x4B400000u;
 }
 
-// Fixed-point corner weights of a particle at offsets (fx, fy): exact 40-bit
-// products summing to exactly 2^40; e_* are the energy-weighted weights in
-// units of 2^-24 eV (en * q/2^40 * 2^24, rounded half up).
-struct Weights {
-    unsigned long long q00, q10, q01, q11;
-    unsigned long long e00, e10, e01, e11;
-};
-
-template <bool ENERGY>
-__device__ __forceinline__ Weights fixed_weights(float fx, float fy, float en) {
-    const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
-    const uint32_t bx = kAxisOne - ax, by = kAxisOne - ay;
-    Weights w;
-    w.q00 = (unsigned long long)bx * by;
-    w.q10 = (unsigned long long)ax * by;
-    w.q01 = (unsigned long long)bx * ay;
-    w.q11 = (unsigned long long)ax * ay;
-    if (ENERGY) {
-        // energy in units of 2^-22 eV (32 bits, clamped below 1024 eV) times
-        // 16-bit axis weights: e = E * wx16 * wy16 / 2^32 < 2^32
-        const uint32_t E = __float2uint_rn(__fmul_rn(en, 4194304.0f));
-        const uint32_t ax16 = (ax + 8u) >> 4, ay16 = (ay + 8u) >> 4;
-        const uint32_t bx16 = 65536u - ax16, by16 = 65536u - ay16;
-        const unsigned long long ea = (unsigned long long)E * ax16;
-        const unsigned long long eb = (unsigned long long)E * bx16;
-        // round to nearest: the products stay below 2^64 - 2^32
-        w.e00 = (eb * by16 + 0x80000000ull) >> 32;
-        w.e10 = (ea * by16 + 0x80000000ull) >> 32;
-        w.e01 = (eb * ay16 + 0x80000000ull) >> 32;
-        w.e11 = (ea * ay16 + 0x80000000ull) >> 32;
-    } else {
-        w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
-    }
-    return w;
-}
-
 // Kinetic energy in eV (0.5 v^2/|q/m|, src/interpolation.cpp:88-89), clamped.
 __device__ __forceinline__ float energy_ev(float vx, float vy, float vz, float half_inv_abs_qm) {
     const float v2 = __fmaf_rn(vz, vz, __fmaf_rn(vy, vy, __fmul_rn(vx, vx)));
     return fminf(__fmul_rn(v2, half_inv_abs_qm), kEnergyClampEv);
+}
+
+// Energy-weighted corner weights of one particle, rounded to integers of
+// 2^-22 eV (each below 2^32): e00 <-> (gx,gy), e10 <-> (gx+1,gy),
+// e01 <-> (gx,gy+1), e11 <-> (gx+1,gy+1).
+struct EWeights {
+    uint32_t e00, e10, e01, e11;
+};
+
+__device__ __forceinline__ EWeights energy_weights(float fx, float fy, float en) {
+    const float es = __fmul_rn(en, kEnergyScale);
+    const float a = __fmul_rn(es, __fsub_rn(1.0f, fx)), b = __fmul_rn(es, fx);
+    const float ofy = __fsub_rn(1.0f, fy);
+    EWeights w;
+    w.e00 = __float2uint_rn(__fmul_rn(a, ofy));
+    w.e10 = __float2uint_rn(__fmul_rn(b, ofy));
+    w.e01 = __float2uint_rn(__fmul_rn(a, fy));
+    w.e11 = __float2uint_rn(__fmul_rn(b, fy));
+    return w;
 }
 
 // Global 64-bit integer reductions (fire-and-forget RED) into the node
@@ -208,54 +229,64 @@ __device__ __forceinline__ void red_add(unsigned long long* p, unsigned long lon
     atomicAdd(p, v);
 }
 
-__device__ __forceinline__ void global_add(const KArgs& A, int gx, int gy, const Weights& w,
-                                           bool energy) {
-    const int64_t n = (int64_t)gy * A.GX + gx;
-    red_add(A.acc_q + n, w.q00);
-    red_add(A.acc_q + n + 1, w.q10);
-    red_add(A.acc_q + n + A.GX, w.q01);
-    red_add(A.acc_q + n + A.GX + 1, w.q11);
-    if (energy) {
-        red_add(A.acc_e + n, w.e00);
-        red_add(A.acc_e + n + 1, w.e10);
-        red_add(A.acc_e + n + A.GX, w.e01);
-        red_add(A.acc_e + n + A.GX + 1, w.e11);
+// Deposit of one particle straight into the node accumulators: its four
+// charge corner weights are the exact 40-bit products of the 20-bit axis
+// weights (they sum to exactly 2^40).
+template <bool ENERGY>
+__device__ __forceinline__ void deposit_one(unsigned long long* acc_q, unsigned long long* acc_e,
+                                            int GX, uint32_t n, float fx, float fy, float en) {
+    const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
+    const uint32_t bx = kAxisOne - ax, by = kAxisOne - ay;
+    red_add(acc_q + n, (unsigned long long)bx * by);
+    red_add(acc_q + n + 1, (unsigned long long)ax * by);
+    red_add(acc_q + n + GX, (unsigned long long)bx * ay);
+    red_add(acc_q + n + GX + 1, (unsigned long long)ax * ay);
+    if (ENERGY) {
+        const EWeights e = energy_weights(fx, fy, en);
+        red_add(acc_e + n, e.e00);
+        red_add(acc_e + n + 1, e.e10);
+        red_add(acc_e + n + GX, e.e01);
+        red_add(acc_e + n + GX + 1, e.e11);
     }
 }
 
-__device__ __forceinline__ void store_particle(const KArgs& A, uint32_t dst, const Pushed& p,
-                                               float vz) {
-    if (dst < A.cap) {
-        __stcs(A.dst_a + dst, make_float4(p.fx, p.fy, p.vx, p.vy));
-        __stcs(A.dst_vz + dst, vz);
-    } else {
-        atomicOr(A.counters + 2, 1ull);
-    }
-}
-
-// Per-lane fixed-point sums of the stayers of the current cell (64-bit).  A
-// cell holds at most kMaxPerCell = 2^16 particles, so a lane sums at most
-// 2^11 of them: charge sums stay below 2^51, energy sums below 2^43.  The
-// per-cell warp reduction runs on two 32-bit limbs per value with
-// redux.sync (26/22-bit low limbs keep every limb sum below 2^32).
+// Per-lane sums of the particles that stay in the warp's cell.  Charge as
+// moments of the 20-bit axis weights -- count, sum ax, sum ay, sum ax*ay --
+// from which the four corner sums follow exactly:
+//   Q00 = N 2^40 - (SX + SY) 2^20 + SXY,  Q10 = SX 2^20 - SXY,
+//   Q01 = SY 2^20 - SXY,                   Q11 = SXY.
+// A lane holds at most kMaxPerCell/32 = 2^11 particles: SX, SY < 2^31,
+// SXY < 2^51, energy sums < 2^43.
 struct StayAcc {
-    unsigned long long q[4];
+    uint32_t n, sx, sy;
+    unsigned long long sxy;
     unsigned long long e[4];
 };
 
 __device__ __forceinline__ void acc_zero(StayAcc& s) {
+    s.n = s.sx = s.sy = 0u;
+    s.sxy = 0ull;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) s.q[k] = s.e[k] = 0ull;
+    for (int k = 0; k < 4; ++k) s.e[k] = 0ull;
 }
 
 template <bool ENERGY>
-__device__ __forceinline__ void acc_add(StayAcc& s, const Weights& w) {
-    s.q[0] += w.q00; s.q[1] += w.q10; s.q[2] += w.q01; s.q[3] += w.q11;
+__device__ __forceinline__ void acc_add(StayAcc& s, float fx, float fy, float en) {
+    const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
+    s.n += 1u;
+    s.sx += ax;
+    s.sy += ay;
+    s.sxy += (unsigned long long)ax * ay;
     if (ENERGY) {
-        s.e[0] += w.e00; s.e[1] += w.e10; s.e[2] += w.e01; s.e[3] += w.e11;
+        const EWeights e = energy_weights(fx, fy, en);
+        s.e[0] += e.e00;
+        s.e[1] += e.e10;
+        s.e[2] += e.e01;
+        s.e[3] += e.e11;
     }
 }
 
+// Warp sum of a value below 2^(LO+27) as two 32-bit limbs (redux.sync).
 template <int LO>
 __device__ __forceinline__ unsigned long long warp_sum_limbs(unsigned long long v) {
     const uint32_t lo = (uint32_t)(v & ((1ull << LO) - 1ull));
@@ -264,191 +295,406 @@ __device__ __forceinline__ unsigned long long warp_sum_limbs(unsigned long long 
            ((unsigned long long)__reduce_add_sync(kFull, hi) << LO);
 }
 
-// Warp-reduce and add the cell's four node sums (lane 0).
+// Warp-reduce the cell's stayer sums and add them to its four nodes (lane 0).
 template <bool ENERGY>
 __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane) {
-    Weights w;
-    w.q00 = warp_sum_limbs<26>(s.q[0]);
-    w.q10 = warp_sum_limbs<26>(s.q[1]);
-    w.q01 = warp_sum_limbs<26>(s.q[2]);
-    w.q11 = warp_sum_limbs<26>(s.q[3]);
-    w.e00 = w.e10 = w.e01 = w.e11 = 0ull;
+    const unsigned long long N = __reduce_add_sync(kFull, s.n);
+    const unsigned long long SX = warp_sum_limbs<26>(s.sx);
+    const unsigned long long SY = warp_sum_limbs<26>(s.sy);
+    const unsigned long long SXY = warp_sum_limbs<26>(s.sxy);
+    unsigned long long E[4] = {0ull, 0ull, 0ull, 0ull};
     if (ENERGY) {
-        w.e00 = warp_sum_limbs<22>(s.e[0]);
-        w.e10 = warp_sum_limbs<22>(s.e[1]);
-        w.e01 = warp_sum_limbs<22>(s.e[2]);
-        w.e11 = warp_sum_limbs<22>(s.e[3]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) E[k] = warp_sum_limbs<22>(s.e[k]);
     }
-    if (lane == 0) global_add(A, gx, gy, w, ENERGY);
+    if (lane == 0 && N) {
+        const int64_t n = (int64_t)gy * A.GX + gx;
+        red_add(A.acc_q + n, (N << 40) - ((SX + SY) << 20) + SXY);
+        red_add(A.acc_q + n + 1, (SX << 20) - SXY);
+        red_add(A.acc_q + n + A.GX, (SY << 20) - SXY);
+        red_add(A.acc_q + n + A.GX + 1, SXY);
+        if (ENERGY) {
+            red_add(A.acc_e + n, E[0]);
+            red_add(A.acc_e + n + 1, E[1]);
+            red_add(A.acc_e + n + A.GX, E[2]);
+            red_add(A.acc_e + n + A.GX + 1, E[3]);
+        }
+    }
     acc_zero(s);
 }
 
-// One kernel body for the three uses:
-//   kCount   -- push, count leavers per direction (plain stores), far movers
-//               per target (atomics);
-//   kScatter -- push again, place every particle at its deterministic slot
-//               (sub-segment of its target cell for its direction + rank
-//               within the direction), deposit the new positions;
-//   kDeposit -- deposit the current positions (no push).
-// A block owns a kTileX x kTileY tile of cells and each warp walks whole
-// cells of it: the cell's segment bounds, its four node fields and (scatter)
-// the nine destination sub-segment starts are warp-uniform loads; particles
-// stream through in chunks of 32 with the next chunk's loads issued before
-// the current chunk is processed.
+__device__ __forceinline__ void store_slot(float4* dst_a, float* dst_vz, uint32_t slot,
+                                           const Pushed& p, float vz) {
+    __stcs(dst_a + slot, make_float4(p.fx, p.fy, p.vx, p.vy));
+    __stcs(dst_vz + slot, vz);
+}
+
+// Appends the lanes with `on` set to a side list (one atomic per warp).
+__device__ __forceinline__ void list_append(const ListDev& L, bool on, uint32_t cell,
+                                            const Pushed& p, float vz, unsigned lt, int lane,
+                                            unsigned long long* lost) {
+    const unsigned m = __ballot_sync(kFull, on);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    uint32_t b = 0;
+    if (lane == leader) b = atomicAdd(L.count, (uint32_t)__popc(m));
+    b = __shfl_sync(kFull, b, leader);
+    if (on) {
+        const uint32_t s = b + __popc(m & lt);
+        if (s < L.cap) {
+            L.a[s] = make_float4(p.fx, p.fy, p.vx, p.vy);
+            L.vz[s] = vz;
+            L.cell[s] = cell;
+        } else {
+            atomicOr(lost, 1ull);
+        }
+    }
+}
+
+// One kernel body for the two uses:
+//   kPush    -- push, place every particle in the other buffer, deposit the
+//               new positions;
+//   kDeposit -- deposit the current positions (no push, nothing moves).
+// A block owns a kTileX x kTileY tile of cells.  Its prologue stages the
+// tile's per-cell slot metadata and the node fields in shared memory; then
+// each warp streams through the particles of its cells (tile cells warp,
+// warp + kWarps, ...) in chunks of 32.  The chunks travel through a per-warp
+// ring of kDepth chunk buffers in shared memory filled by cp.async, kDepth-1
+// chunks ahead of the one being processed -- across cell boundaries, so the
+// load pipeline never drains.
+constexpr int kDepth = 4;
+constexpr int kTileCells = kTileX * kTileY;
+constexpr int kTileNodesX = kTileX + 1;
+constexpr int kTileNodes = (kTileX + 1) * (kTileY + 1);
+
+struct CellMeta {
+    uint32_t b0, b1, nf, nb;
+};
+
+// Movers wait in a per-warp queue in shared memory and are placed 32 at a
+// time (all lanes busy): deposit, grouping by target cell (match.any), one
+// slot reservation per group, store.
+constexpr int kQueue = 64;
+
+struct MoverQueue {
+    float4 a[kQueue];
+    float vz[kQueue];
+    uint2 tn[kQueue];  // target cell, its lower-left node
+};
+
+// Places `count` (<= 32) queued movers, entries 0..count-1.
+template <bool ENERGY>
+__device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q, int count, int lane,
+                                             unsigned lt) {
+    __syncwarp();
+    const bool on = lane < count;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+    float vz = 0.f;
+    uint2 tn = make_uint2(0u, 0u);
+    if (on) {
+        a = q.a[lane];
+        vz = q.vz[lane];
+        tn = q.tn[lane];
+    }
+    const uint32_t t = tn.x;
+    const float en = (ENERGY && on) ? energy_ev(a.z, a.w, vz, A.k.half_inv_abs_qm) : 0.f;
+    // movers bound for the same cell form a group; its leader reserves the
+    // group's slots at the back of the cell, capped at the cell's capacity
+    // minus its current count (the most stayers it can have)
+    const unsigned grp = __match_any_sync(kFull, on ? t : (0x80000000u | (uint32_t)lane));
+    const int leader = __ffs(grp) - 1;
+    uint32_t old = 0, lim = 0;
+    if (on && lane == leader) {
+        const uint32_t cnt = __popc(grp);
+        lim = (A.base[t + 1] - A.base[t]) - (A.front_src[t] + A.back_src[t]);
+        old = atomicAdd(A.back_dst + t, cnt);
+        // give back what does not fit (the count then ends at
+        // min(requested, lim) with slots 0.. taken)
+        if (old + cnt > lim) atomicSub(A.back_dst + t, old >= lim ? cnt : old + cnt - lim);
+    }
+    if (on) deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, tn.y, a.x, a.y, en);
+    old = __shfl_sync(kFull, old, leader);
+    lim = __shfl_sync(kFull, lim, leader);
+    bool spill = false;
+    Pushed p;
+    p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
+    if (on) {
+        const uint32_t k = old + __popc(grp & lt);
+        if (k < lim) store_slot(A.dst_a, A.dst_vz, A.base[t + 1] - 1u - k, p, vz);
+        else spill = true;
+    }
+    list_append(A.ovf, spill, t, p, vz, lt, lane, A.counters + 2);
+}
+
 template <int MODE, bool ENERGY>
-__global__ void __launch_bounds__(kThreads, (MODE == kScatter && ENERGY) ? 3 : 4) k_particles(KArgs A) {
-    constexpr bool kDep = (MODE != kCount);
-    __shared__ uint32_t run_s[kWarps][kDirs + 1];
-    __shared__ uint32_t base_s[MODE == kScatter ? kWarps : 1][kDirs + 1];
+__global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
+    __shared__ CellMeta s_meta[kTileCells];
+    __shared__ float4 s_fld[MODE == kPush ? kTileNodes : 1];
+    __shared__ MoverQueue s_q[MODE == kPush ? kWarps : 1];
+    __shared__ float4 s_ring_a[kWarps][kDepth][32];
+    __shared__ float s_ring_vz[kWarps][kDepth][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
     const unsigned lt = lanemask_lt();
-    unsigned long long left_exits = 0;
+    for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
+        const int gx = tgx0 + (i % kTileX), gy = tgy0 + (i / kTileX);
+        CellMeta m{0u, 0u, 0u, 0u};
+        if (gx < A.nx && gy < A.ny) {
+            const int64_t c = (int64_t)gy * A.nx + gx;
+            m.b0 = A.base[c];
+            m.b1 = A.base[c + 1];
+            m.nf = A.front_src[c];
+            m.nb = A.back_src[c];
+        }
+        s_meta[i] = m;
+    }
+    if (MODE == kPush) {
+        for (int i = threadIdx.x; i < kTileNodes; i += kThreads) {
+            const int x = tgx0 + (i % kTileNodesX), y = tgy0 + (i / kTileNodesX);
+            s_fld[i] = (x < A.GX && y < A.ny + 1) ? __ldg(A.fld + (int64_t)y * A.GX + x)
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    __syncthreads();
 
-    for (int lc = warp; lc < kTileX * kTileY; lc += kWarps) {
-        const int gx = tgx0 + (lc % kTileX), gy = tgy0 + (lc / kTileX);
-        if (gx >= A.nx || gy >= A.ny) continue;  // warp-uniform
-        const int64_t c = (int64_t)gy * A.nx + gx;
-        const uint32_t beg = A.off[c], end = A.off[c + 1];
-        if (beg == end) {
-            if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = 0u;
-            continue;
+    unsigned long long left_exits = 0;
+    // the warp's cells are lc = warp + kWarps*k; empty ones only get their
+    // front count written
+    auto next_cell = [&](int lc, bool mark_empty) {
+        for (; lc < kTileCells; lc += kWarps) {
+            const CellMeta m = s_meta[lc];
+            if (m.nf + m.nb) break;
+            const int gx = tgx0 + (lc % kTileX), gy = tgy0 + (lc / kTileX);
+            if (MODE == kPush && mark_empty && lane == 0 && gx < A.nx && gy < A.ny)
+                A.front_dst[(int64_t)gy * A.nx + gx] = 0u;
         }
-        // first chunk's loads go out before the per-cell tables
-        uint32_t i = beg + lane;
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-        float vz = 0.f;
-        if (i < end) {
-            a = __ldcs(A.src_a + i);
-            if (MODE != kCount) vz = __ldcs(A.src_vz + i);
-        }
-        float4 f00 = make_float4(0, 0, 0, 0), f10 = f00, f01 = f00, f11 = f00;
-        if (MODE != kDeposit) {
-            const int64_t n0 = (int64_t)gy * A.GX + gx;
-            f00 = __ldg(A.fld + n0);
-            f10 = __ldg(A.fld + n0 + 1);
-            f01 = __ldg(A.fld + n0 + A.GX);
-            f11 = __ldg(A.fld + n0 + A.GX + 1);
-        }
-        if (lane < kDirs) {
-            run_s[warp][lane] = 0u;
-            if (MODE == kScatter) {
-                const int tx = gx + lane % 3 - 1, ty = gy + lane / 3 - 1;
-                base_s[warp][lane] = (tx >= 0 && ty >= 0 && tx < A.nx && ty < A.ny)
-                                         ? __ldg(A.sub + (int64_t)lane * A.ncells + (int64_t)ty * A.nx + tx)
-                                         : 0u;
+        return lc;
+    };
+    // producer: issues the copies of the chunk (plc, pj0) into ring slot r
+    // and advances; every call commits one (possibly empty) copy group
+    int plc = next_cell(warp, false);
+    CellMeta pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
+    uint32_t pj0 = 0;
+    auto issue = [&](int r) {
+        if (plc < kTileCells) {
+            const uint32_t jj = pj0 + lane, np = pm.nf + pm.nb;
+            const bool v = jj < np;
+            const uint32_t i = !v ? 0u : (jj < pm.nf ? pm.b0 + jj : pm.b1 - pm.nb + (jj - pm.nf));
+            cp_async16(&s_ring_a[warp][r][lane], A.src_a + i, v);
+            cp_async4(&s_ring_vz[warp][r][lane], A.src_vz + i, v);
+            if (pj0 + 32 >= np) {
+                plc = next_cell(plc + kWarps, false);
+                pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
+                pj0 = 0;
+            } else {
+                pj0 += 32;
             }
         }
-        __syncwarp();
+        cp_async_commit();
+    };
+
+    MoverQueue& q = s_q[MODE == kPush ? warp : 0];
+    int queued = 0;  // warp-uniform
+    int lc = next_cell(warp, true);
+    if (lc < kTileCells) {
+#pragma unroll
+        for (int r = 0; r < kDepth - 1; ++r) issue(r);
+        CellMeta m = s_meta[lc];
+        uint32_t j0 = 0;
+        int r = 0;
         StayAcc acc;
         acc_zero(acc);
+        uint32_t stay_run = 0;
+        for (;;) {
+            const uint32_t n = m.nf + m.nb;
+            const bool last = j0 + 32 >= n;
+            // the next chunk: same cell, or the warp's next non-empty cell
+            const int lcn = last ? next_cell(lc + kWarps, true) : lc;
+            const uint32_t jn0 = last ? 0u : j0 + 32;
+            // refill the slot freed by the previous chunk, then wait for this one
+            issue(r == 0 ? kDepth - 1 : r - 1);
+            cp_async_wait<kDepth - 1>();
+            const float4 a = s_ring_a[warp][r][lane];
+            const float vz = s_ring_vz[warp][r][lane];
+            r = (r + 1 == kDepth) ? 0 : r + 1;
 
-        for (uint32_t i0 = beg; i0 < end; i0 += 32) {
-            const bool valid = i < end;
-            const uint32_t inext = i + 32;
-            float4 an = make_float4(0.f, 0.f, 0.f, 0.f);
-            float vzn = 0.f;
-            if (inext < end) {
-                an = __ldcs(A.src_a + inext);
-                if (MODE != kCount) vzn = __ldcs(A.src_vz + inext);
-            }
+            const int lx = lc % kTileX, ly = lc / kTileX;
+            const int gx = tgx0 + lx, gy = tgy0 + ly;
+            const bool valid = j0 + lane < n;
             Pushed p;
             if (MODE == kDeposit) {
                 p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
                 p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
             } else {
-                p = push_one(a, f00, f10, f01, f11, A.k, gx, gy, A.nx, A.ny);
+                const float4* f = s_fld + ly * kTileNodesX + lx;
+                p = push_one(a, f[0], f[1], f[kTileNodesX], f[kTileNodesX + 1], A.k, gx, gy, A.nx, A.ny);
             }
             const int dir = valid ? p.dir : -1;
-            if (MODE == kScatter) left_exits += __popc(__ballot_sync(kFull, valid && dir < 0 && p.left));
-            // rank among this cell's particles leaving in the same direction
-            // (warp multi-split: lanes with equal direction bits form a group)
-            uint32_t rank = 0;
-            {
-                const bool ranked = dir >= 0 && dir < kDirs;
-                unsigned same = __ballot_sync(kFull, ranked);
-#pragma unroll
-                for (int bit = 0; bit < 4; ++bit) {
-                    const unsigned b = __ballot_sync(kFull, (dir >> bit) & 1);
-                    same &= ((dir >> bit) & 1) ? b : ~b;
+            const bool stay = dir == kStay;
+            const bool live = dir >= 0;
+            const float en = (ENERGY && live) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
+            if (stay) acc_add<ENERGY>(acc, p.fx, p.fy, en);
+            if (MODE == kPush) {
+                left_exits += __popc(__ballot_sync(kFull, valid && !live && p.left));
+                const unsigned sm = __ballot_sync(kFull, stay);
+                if (stay) store_slot(A.dst_a, A.dst_vz, m.b0 + stay_run + __popc(sm & lt), p, vz);
+                stay_run += __popc(sm);
+                const bool mv = live && !stay;
+                const unsigned mm = __ballot_sync(kFull, mv);
+                if (mm) {  // warp-uniform: queue the movers
+                    if (mv) {
+                        const int e = queued + __popc(mm & lt);
+                        q.a[e] = make_float4(p.fx, p.fy, p.vx, p.vy);
+                        q.vz[e] = vz;
+                        q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
+                    }
+                    queued += __popc(mm);
+                    if (queued >= 32) {
+                        place_movers<ENERGY>(A, q, 32, lane, lt);
+                        // the rest (< 32) moves to the front of the queue
+                        queued -= 32;
+                        __syncwarp();
+                        if (lane < queued) {
+                            q.a[lane] = q.a[32 + lane];
+                            q.vz[lane] = q.vz[32 + lane];
+                            q.tn[lane] = q.tn[32 + lane];
+                        }
+                        __syncwarp();
+                    }
                 }
-                const uint32_t before = __popc(same & lt);
-                const uint32_t r0 = ranked ? run_s[warp][dir] : 0u;
-                rank = r0 + before;
-                __syncwarp();
-                if (ranked && before == 0) run_s[warp][dir] = r0 + __popc(same);
-                __syncwarp();
             }
-            if (kDep) {
-                const bool live = dir >= 0;
-                const float en = (ENERGY && live) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
-                const Weights w = fixed_weights<ENERGY>(p.fx, p.fy, en);
-                if (dir == kStay) acc_add<ENERGY>(acc, w);
-                if (MODE == kScatter && live && dir != kStay) global_add(A, p.gx, p.gy, w, ENERGY);
+            if (last) {
+                acc_flush<ENERGY>(acc, A, gx, gy, lane);
+                if (MODE == kPush && lane == 0) A.front_dst[(int64_t)gy * A.nx + gx] = stay_run;
+                stay_run = 0;
+                if (lcn >= kTileCells) break;
+                m = s_meta[lcn];
             }
-            if (MODE == kScatter && dir >= 0) {
-                uint32_t dst;
-                if (dir == kFar) {
-                    const int64_t nc = (int64_t)p.gy * A.nx + p.gx;
-                    dst = __ldg(A.sub + (int64_t)kFar * A.ncells + nc) + atomicAdd(A.farcur + nc, 1u);
-                } else {
-                    dst = base_s[warp][dir] + rank;
-                }
-                store_particle(A, dst, p, vz);
-            }
-            if (MODE == kCount && dir == kFar)
-                atomicAdd(A.farin + (int64_t)p.gy * A.nx + p.gx, 1u);
-            i = inext;
-            a = an;
-            vz = vzn;
+            lc = lcn;
+            j0 = jn0;
         }
-        if (kDep) acc_flush<ENERGY>(acc, A, gx, gy, lane);
-        if (MODE == kCount && lane < kDirs) A.dcount[(int64_t)lane * A.ncells + c] = run_s[warp][lane];
-        __syncwarp();
+        cp_async_wait<0>();
     }
-    if (MODE == kScatter && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
+    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, queued, lane, lt);
+    if (MODE == kPush && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
 }
 
-// ---- exclusive scan of the new per-cell counts ------------------------------
-//
-// Cell t receives, from each direction d, the particles that left cell
-// t - dir(d) in direction d, plus its far movers.  Its new segment is laid
-// out by direction (d = 0..8, then far), so every particle has a
-// deterministic slot except far movers (atomic cursor).
+// ---- side lists ---------------------------------------------------------------
 
-struct ScanArgs {
-    const uint32_t* dcount;
-    uint32_t* farin;
-    uint32_t* farcur;
-    uint32_t* sub;
-    uint32_t* off_next;
-    int nx, ny;
-    int64_t ncells;
+struct FixArgs {
+    int nx, ny, GX;
+    SpeciesConsts k;
+    const float4* __restrict__ fld;
+    float4* dst_a;
+    float* dst_vz;
+    const uint32_t* __restrict__ base;
+    const uint32_t* __restrict__ front;  // final front counts of the new buffer
+    uint32_t* back;                      // back counts of the new buffer
+    ListDev ovf;    // pushed this step, not yet placed
+    ListDev prev;   // part of the state before the push, not yet pushed
+    ListDev next;   // output: pushed, did not fit
+    unsigned long long* acc_q;
+    unsigned long long* acc_e;
+    unsigned long long* counters;
 };
 
-__device__ __forceinline__ void incoming(const ScanArgs& S, int64_t t, uint32_t (&in)[kDirs + 1]) {
-    const int tx = (int)(t % S.nx), ty = (int)(t / S.nx);
-#pragma unroll
-    for (int d = 0; d < kDirs; ++d) {
-        const int sx = tx - (d % 3 - 1), sy = ty - (d / 3 - 1);
-        in[d] = (sx >= 0 && sy >= 0 && sx < S.nx && sy < S.ny)
-                    ? S.dcount[(int64_t)d * S.ncells + (int64_t)sy * S.nx + sx]
-                    : 0u;
+// Pushes (and deposits) the particles of the previous side list, then tries
+// to place them and this push's spilled movers in the free gap of their
+// target cells; what does not fit goes to the next side list.
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_fixup(FixArgs F) {
+    const uint32_t n_prev = min(*F.prev.count, F.prev.cap);
+    const uint32_t n_ovf = min(*F.ovf.count, F.ovf.cap);
+    const uint32_t total = n_prev + n_ovf;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        Pushed p;
+        float vz;
+        uint32_t t;
+        if (i < n_prev) {
+            const uint32_t c = F.prev.cell[i];
+            const int gx = (int)(c % (uint32_t)F.nx), gy = (int)(c / (uint32_t)F.nx);
+            const int64_t n0 = (int64_t)gy * F.GX + gx;
+            vz = F.prev.vz[i];
+            p = push_one(F.prev.a[i], F.fld[n0], F.fld[n0 + 1], F.fld[n0 + F.GX], F.fld[n0 + F.GX + 1],
+                         F.k, gx, gy, F.nx, F.ny);
+            if (p.dir < 0) {
+                if (p.left) atomicAdd(F.counters, 1ull);
+                continue;
+            }
+            const float en = ENERGY ? energy_ev(p.vx, p.vy, vz, F.k.half_inv_abs_qm) : 0.f;
+            deposit_one<ENERGY>(F.acc_q, F.acc_e, F.GX, (uint32_t)(p.gy * F.GX + p.gx), p.fx, p.fy, en);
+            t = (uint32_t)(p.gy * F.nx + p.gx);
+        } else {
+            const uint32_t e = i - n_prev;
+            const float4 a = F.ovf.a[e];
+            p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
+            vz = F.ovf.vz[e];
+            t = F.ovf.cell[e];
+        }
+        const uint32_t lim = (F.base[t + 1] - F.base[t]) - F.front[t];
+        const uint32_t k = atomicAdd(F.back + t, 1u);
+        if (k < lim) {
+            store_slot(F.dst_a, F.dst_vz, F.base[t + 1] - 1u - k, p, vz);
+        } else {
+            atomicSub(F.back + t, 1u);
+            const uint32_t s = atomicAdd(F.next.count, 1u);
+            if (s < F.next.cap) {
+                F.next.a[s] = make_float4(p.fx, p.fy, p.vx, p.vy);
+                F.next.vz[s] = vz;
+                F.next.cell[s] = t;
+            } else {
+                atomicOr(F.counters + 2, 1ull);
+            }
+        }
     }
-    in[kDirs] = S.farin[t];
 }
 
-__global__ void __launch_bounds__(256) k_scan_partials(ScanArgs S, uint32_t* partials) {
+// Deposit of the particles on a side list (stand-alone deposit).
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_list_deposit(ListDev L, int nx, int GX, float half_inv_abs_qm,
+                                                      unsigned long long* acc_q, unsigned long long* acc_e) {
+    const uint32_t n = min(*L.count, L.cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = L.a[i];
+        const uint32_t c = L.cell[i];
+        const float en = ENERGY ? energy_ev(a.z, a.w, L.vz[i], half_inv_abs_qm) : 0.f;
+        deposit_one<ENERGY>(acc_q, acc_e, GX, c + c / (uint32_t)nx, a.x, a.y, en);  // node = c + gy
+    }
+}
+
+// ---- layouts: counts, exclusive scans ------------------------------------------
+//
+// Slot capacity of a cell holding n particles: n + n/2 + 16 (room for a
+// step's incoming movers and for the count to drift between re-layouts).
+__host__ __device__ __forceinline__ uint32_t cell_capacity(uint32_t n) { return n + n / 2u + 16u; }
+
+// cnt[c] = front[c] + back[c]
+__global__ void k_cell_counts(const uint32_t* front, const uint32_t* back, int64_t ncells, uint32_t* cnt) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncells) cnt[c] = front[c] + back[c];
+}
+
+// cnt[cell] += 1 for each side-list entry
+__global__ void k_list_counts(ListDev L, uint32_t* cnt) {
+    const uint32_t n = min(*L.count, L.cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(cnt + L.cell[i], 1u);
+}
+
+template <bool CAP>
+__device__ __forceinline__ uint32_t scan_value(const uint32_t* in, int64_t t) {
+    return CAP ? cell_capacity(in[t]) : in[t];
+}
+
+template <bool CAP>
+__global__ void __launch_bounds__(256) k_scan_partials(const uint32_t* in, int64_t n, uint32_t* partials) {
     __shared__ uint32_t red[8];
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     uint32_t s = 0;
     for (int j = threadIdx.x; j < kScanTile; j += 256) {
         const int64_t t = base + j;
-        if (t >= S.ncells) break;
-        uint32_t in[kDirs + 1];
-        incoming(S, t, in);
-#pragma unroll
-        for (int d = 0; d <= kDirs; ++d) s += in[d];
+        if (t >= n) break;
+        s += scan_value<CAP>(in, t);
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -460,10 +706,11 @@ __global__ void __launch_bounds__(256) k_scan_partials(ScanArgs S, uint32_t* par
     }
 }
 
-// off_next[t] = particles in cells before t; sub[d][t] = start of the part of
-// t's segment fed from direction d; off_next[ncells] = total.  Zeroes the far
-// counters for the next step and flags cells above kMaxPerCell.
-__global__ void __launch_bounds__(256) k_scan_apply(ScanArgs S, const uint32_t* partials,
+// out[t] = sum of values before t, out[n] = total.  With CAP the values are
+// cell capacities, and cells above kMaxPerCell raise counters[1].
+template <bool CAP>
+__global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* in, int64_t n,
+                                                    const uint32_t* partials, uint32_t* out,
                                                     unsigned long long* counters) {
     __shared__ uint32_t red[8];
     __shared__ uint32_t wsum[8];
@@ -475,21 +722,15 @@ __global__ void __launch_bounds__(256) k_scan_apply(ScanArgs S, const uint32_t* 
     __syncthreads();
     uint32_t block_pre = 0;
     for (int w = 0; w < 8; ++w) block_pre += red[w];
-    // each thread owns 8 consecutive cells
+    // each thread owns 8 consecutive entries
     const int64_t c0 = (int64_t)blockIdx.x * kScanTile + threadIdx.x * 8;
-    uint32_t tot[8];
+    uint32_t v[8];
     uint32_t tsum = 0, vmax = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        tot[j] = 0;
-        if (c0 + j < S.ncells) {
-            uint32_t in[kDirs + 1];
-            incoming(S, c0 + j, in);
-#pragma unroll
-            for (int d = 0; d <= kDirs; ++d) tot[j] += in[d];
-        }
-        tsum += tot[j];
-        vmax = max(vmax, tot[j]);
+        v[j] = (c0 + j < n) ? scan_value<CAP>(in, c0 + j) : 0u;
+        tsum += v[j];
+        vmax = max(vmax, v[j]);
     }
     uint32_t incl = tsum;
 #pragma unroll
@@ -505,23 +746,46 @@ __global__ void __launch_bounds__(256) k_scan_apply(ScanArgs S, const uint32_t* 
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int64_t t = c0 + j;
-        if (t < S.ncells) {
-            S.off_next[t] = run;
-            uint32_t in[kDirs + 1];
-            incoming(S, t, in);
-            uint32_t r = run;
-#pragma unroll
-            for (int d = 0; d <= kDirs; ++d) {
-                S.sub[(int64_t)d * S.ncells + t] = r;
-                r += in[d];
-            }
-            S.farin[t] = 0;
-            S.farcur[t] = 0;
-        }
-        run += tot[j];
-        if (t == S.ncells - 1) S.off_next[S.ncells] = run;
+        if (t < n) out[t] = run;
+        run += v[j];
+        if (t == n - 1) out[n] = run;
     }
-    if (vmax > kMaxPerCell) atomicOr(counters + 1, 1ull);
+    if (CAP && vmax > kMaxPerCell) atomicOr(counters + 1, 1ull);
+}
+
+// Copies every cell's particles (front run, then back run) from the old
+// layout to the front of its slots in the new one; new_front = count.
+__global__ void k_relayout_cells(const float4* __restrict__ src_a, const float* __restrict__ src_vz,
+                                 const uint32_t* __restrict__ base, const uint32_t* __restrict__ front,
+                                 const uint32_t* __restrict__ back, const uint32_t* __restrict__ nbase,
+                                 int64_t ncells, float4* dst_a, float* dst_vz, uint32_t* nfront,
+                                 uint32_t* nback) {
+    const int64_t c = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (c >= ncells) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nf = front[c], nb = back[c], b0 = base[c], back0 = base[c + 1] - nb;
+    const uint32_t d0 = nbase[c];
+    for (uint32_t j = lane; j < nf + nb; j += 32) {
+        const uint32_t i = j < nf ? b0 + j : back0 + (j - nf);
+        dst_a[d0 + j] = src_a[i];
+        dst_vz[d0 + j] = src_vz[i];
+    }
+    if (lane == 0) {
+        nfront[c] = nf + nb;
+        nback[c] = 0u;
+    }
+}
+
+// Side-list particles into the new layout, after the cell's own particles.
+__global__ void k_relayout_list(ListDev L, const uint32_t* __restrict__ nbase, uint32_t* nfront,
+                                float4* dst_a, float* dst_vz) {
+    const uint32_t n = min(*L.count, L.cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = L.cell[i];
+        const uint32_t s = nbase[c] + atomicAdd(nfront + c, 1u);
+        dst_a[s] = L.a[i];
+        dst_vz[s] = L.vz[i];
+    }
 }
 
 // ---- import / export ------------------------------------------------------
@@ -530,7 +794,7 @@ __global__ void __launch_bounds__(256) k_scan_apply(ScanArgs S, const uint32_t* 
 // gx = (int)(x * (1/dx)) in FP64 (src/particles.cpp:230-235).
 __global__ void k_import_convert(const pic_point* __restrict__ pts, int64_t n, int nx, int ny,
                                  double inv_dx, double inv_dy, float4* tmp_a, float* tmp_vz,
-                                 uint32_t* cell_of, uint32_t* farin) {
+                                 uint32_t* cell_of, uint32_t* cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const pic_point p = pts[i];
@@ -547,31 +811,35 @@ __global__ void k_import_convert(const pic_point* __restrict__ pts, int64_t n, i
         }
     }
     cell_of[i] = cell;
-    if (cell != 0xffffffffu) atomicAdd(farin + cell, 1u);
+    if (cell != 0xffffffffu) atomicAdd(cnt + cell, 1u);
 }
 
 __global__ void k_import_scatter(const float4* __restrict__ tmp_a, const float* __restrict__ tmp_vz,
                                  const uint32_t* __restrict__ cell_of, int64_t n,
-                                 const uint32_t* __restrict__ off, uint32_t* farcur,
+                                 const uint32_t* __restrict__ base, uint32_t* front,
                                  float4* dst_a, float* dst_vz) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t c = cell_of[i];
     if (c == 0xffffffffu) return;
-    const uint32_t d = off[c] + atomicAdd(farcur + c, 1u);
+    const uint32_t d = base[c] + atomicAdd(front + c, 1u);
     dst_a[d] = tmp_a[i];
     dst_vz[d] = tmp_vz[i];
 }
 
-// Sorted SoA -> reference Point AoS.  x = (gx + fx)*dx in FP64.
+// Layout -> reference Point AoS in cell order (dense[c] = particles before
+// cell c).  x = (gx + fx)*dx in FP64.
 __global__ void k_export(const float4* __restrict__ a, const float* __restrict__ vz,
-                         const uint32_t* __restrict__ off, int nx, int64_t ncells, double dx,
-                         double dy, pic_point* out) {
+                         const uint32_t* __restrict__ base, const uint32_t* __restrict__ front,
+                         const uint32_t* __restrict__ back, const uint32_t* __restrict__ dense,
+                         int nx, int64_t ncells, double dx, double dy, pic_point* out) {
     const int64_t c = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (c >= ncells) return;
     const int lane = threadIdx.x & 31;
     const int gx = (int)(c % nx), gy = (int)(c / nx);
-    for (uint32_t i = off[c] + lane; i < off[c + 1]; i += 32) {
+    const uint32_t nf = front[c], nb = back[c], b0 = base[c], back0 = base[c + 1] - nb, d0 = dense[c];
+    for (uint32_t j = lane; j < nf + nb; j += 32) {
+        const uint32_t i = j < nf ? b0 + j : back0 + (j - nf);
         const float4 v = a[i];
         pic_point p;
         p.x = ((double)gx + (double)v.x) * dx;
@@ -580,45 +848,42 @@ __global__ void k_export(const float4* __restrict__ a, const float* __restrict__
         p.vx = v.z;
         p.vy = v.w;
         p.vz = vz[i];
-        p.pointer = (int32_t)i;
+        p.pointer = (int32_t)(d0 + j);
         p.pad_ = 0;
-        out[i] = p;
+        out[d0 + j] = p;
     }
 }
 
-// Sorted state -> raw arrays (cell, fx, fy, vx, vy, vz), storage order.
+// Layout -> raw arrays (cell, fx, fy, vx, vy, vz) in cell order.
 __global__ void k_export_state(const float4* __restrict__ a, const float* __restrict__ vz,
-                               const uint32_t* __restrict__ off, int64_t ncells, int64_t n,
-                               int32_t* cell, float* fx, float* fy, float* vx, float* vy,
-                               float* vzo) {
+                               const uint32_t* __restrict__ base, const uint32_t* __restrict__ front,
+                               const uint32_t* __restrict__ back, const uint32_t* __restrict__ dense,
+                               int64_t ncells, int32_t* cell, float* fx, float* fy, float* vx,
+                               float* vy, float* vzo) {
     const int64_t c = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (c >= ncells) return;
     const int lane = threadIdx.x & 31;
-    for (uint32_t i = off[c] + lane; i < off[c + 1]; i += 32) {
+    const uint32_t nf = front[c], nb = back[c], b0 = base[c], back0 = base[c + 1] - nb, d0 = dense[c];
+    for (uint32_t j = lane; j < nf + nb; j += 32) {
+        const uint32_t i = j < nf ? b0 + j : back0 + (j - nf);
         const float4 v = a[i];
-        cell[i] = (int32_t)c;
-        fx[i] = v.x;
-        fy[i] = v.y;
-        vx[i] = v.z;
-        vy[i] = v.w;
-        vzo[i] = vz[i];
+        const uint32_t o = d0 + j;
+        cell[o] = (int32_t)c;
+        fx[o] = v.x;
+        fy[o] = v.y;
+        vx[o] = v.z;
+        vy[o] = v.w;
+        vzo[o] = vz[i];
     }
-    (void)n;
 }
 
 // Live particles per reference bucket key gy*GRID_X + gx.
-__global__ void k_bin_counts(const uint32_t* __restrict__ off, int nx, int ny, int GX,
-                             int32_t* counts) {
+__global__ void k_bin_counts(const uint32_t* __restrict__ cnt, int nx, int ny, int GX, int32_t* counts) {
     const int64_t nodes = (int64_t)GX * (ny + 1);
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nodes) return;
     const int gx = (int)(k % GX), gy = (int)(k / GX);
-    int32_t v = 0;
-    if (gx < nx && gy < ny) {
-        const int64_t c = (int64_t)gy * nx + gx;
-        v = (int32_t)(off[c + 1] - off[c]);
-    }
-    counts[k] = v;
+    counts[k] = (gx < nx && gy < ny) ? (int32_t)cnt[(int64_t)gy * nx + gx] : 0;
 }
 
 // ---- accumulators -> meshes -------------------------------------------------
@@ -677,19 +942,21 @@ __device__ __forceinline__ uint32_t blob_count(const PlasmaArgs& P, int64_t c) {
     return (uint32_t)floor(m + (double)u01(r.x));
 }
 
-// counts enter as the "stay" direction of each cell
-__global__ void k_plasma_counts(PlasmaArgs P, int64_t ncells, uint32_t* stay_count) {
+__global__ void k_plasma_counts(PlasmaArgs P, int64_t ncells, uint32_t* cnt) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
-    stay_count[c] = (uint32_t)P.ppc + blob_count(P, c);
+    cnt[c] = (uint32_t)P.ppc + blob_count(P, c);
 }
 
-__global__ void k_plasma_generate(PlasmaArgs P, const uint32_t* __restrict__ off, int64_t ncells,
-                                  float4* a, float* vz) {
+// Particle j of cell c gets the Philox counter dense[c] + j (its index in
+// cell order) and the slot base[c] + j.
+__global__ void k_plasma_generate(PlasmaArgs P, const uint32_t* __restrict__ dense,
+                                  const uint32_t* __restrict__ base, int64_t ncells, float4* a,
+                                  float* vz, uint32_t* front, uint32_t* back) {
     const int64_t c = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (c >= ncells) return;
     const int lane = threadIdx.x & 31;
-    const uint32_t beg = off[c], end = off[c + 1];
+    const uint32_t beg = dense[c], end = dense[c + 1], b0 = base[c];
     for (uint32_t i = beg + lane; i < end; i += 32) {
         const uint4 r0 = philox(make_uint4(i, P.species, 0u, 0x5EEDu), P.key);
         const uint4 r1 = philox(make_uint4(i, P.species, 1u, 0x5EEDu), P.key);
@@ -706,21 +973,43 @@ __global__ void k_plasma_generate(PlasmaArgs P, const uint32_t* __restrict__ off
             vx += P.drift_vx;
             vy += P.drift_vy;
         }
-        a[i] = make_float4(fx, fy, vx, vy);
-        vz[i] = vzz;
+        const uint32_t s = b0 + (i - beg);
+        a[s] = make_float4(fx, fy, vx, vy);
+        vz[s] = vzz;
+    }
+    if (lane == 0) {
+        front[c] = end - beg;
+        back[c] = 0u;
     }
 }
 
 inline unsigned grid1d(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-int scan_counts(pic_ctx* c, Species& sp) {
-    const int64_t ncells = c->ncells;
-    const int nparts = (int)((ncells + kScanTile - 1) / kScanTile);
-    ScanArgs S{sp.dcount, sp.farin, sp.farcur, sp.sub, sp.off_next, c->nx, c->ny, ncells};
-    k_scan_partials<<<nparts, 256, 0, c->stream>>>(S, c->scan_partials);
-    k_scan_apply<<<nparts, 256, 0, c->stream>>>(S, c->scan_partials, sp.counters);
+// out[0..n] = exclusive scan of in (CAP: of cell capacities); returns the
+// total through *total when not null (synchronises).
+template <bool CAP>
+int scan_cells(pic_ctx* c, Species& sp, const uint32_t* in, uint32_t* out, uint32_t* total) {
+    const int64_t n = c->ncells;
+    const int nparts = (int)((n + kScanTile - 1) / kScanTile);
+    k_scan_partials<CAP><<<nparts, 256, 0, c->stream>>>(in, n, c->scan_partials);
+    k_scan_apply<CAP><<<nparts, 256, 0, c->stream>>>(in, n, c->scan_partials, out, sp.counters);
+    c->launches += 2;
     PIC_CUDA(cudaGetLastError());
+    if (total) {
+        PIC_CUDA(cudaMemcpyAsync(total, out + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+    }
     return PIC_OK;
+}
+
+// Species constants for a push, with the Boris factors of a uniform Bz.
+SpeciesConsts push_consts(const pic_ctx* c, const Species& sp) {
+    SpeciesConsts k = sp.k;
+    k.bzu = c->bz_uniform ? 1 : 0;
+    const float t = k.h * (float)c->bz_value;
+    k.bt = t;
+    k.bs = (float)(2.0 * (double)t / (1.0 + (double)t * (double)t));
+    return k;
 }
 
 KArgs make_args(pic_ctx* c, Species& sp) {
@@ -729,22 +1018,21 @@ KArgs make_args(pic_ctx* c, Species& sp) {
     A.ny = c->ny;
     A.GX = c->GX;
     A.ncells = c->ncells;
-    A.k = sp.k;
+    A.k = push_consts(c, sp);
     A.fld = c->fld;
     A.src_a = sp.buf[sp.cur].a;
     A.src_vz = sp.buf[sp.cur].vz;
     A.dst_a = sp.buf[sp.cur ^ 1].a;
     A.dst_vz = sp.buf[sp.cur ^ 1].vz;
-    A.off = sp.off;
-    A.dcount = sp.dcount;
-    A.sub = sp.sub;
-    A.farin = sp.farin;
-    A.farcur = sp.farcur;
+    A.base = sp.base;
+    A.front_src = sp.front[sp.cur];
+    A.back_src = sp.back[sp.cur];
+    A.front_dst = sp.front[sp.cur ^ 1];
+    A.back_dst = sp.back[sp.cur ^ 1];
+    A.ovf = list_dev(sp.ovf);
     A.acc_q = sp.acc_q;
     A.acc_e = sp.acc_e;
     A.counters = sp.counters;
-    A.cap = (uint32_t)sp.capacity;
-    A.energy = c->cfg.deposit_energy ? 1 : 0;
     return A;
 }
 
@@ -752,16 +1040,41 @@ dim3 tile_grid(pic_ctx* c) {
     return dim3((unsigned)((c->nx + kTileX - 1) / kTileX), (unsigned)((c->ny + kTileY - 1) / kTileY));
 }
 
-void swap_buffers(Species& sp) {
-    sp.cur ^= 1;
-    std::swap(sp.off, sp.off_next);
-}
+int check_flags(pic_ctx* c, Species& sp, bool sync);
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// host entry points
+// host side
 // ---------------------------------------------------------------------------
+
+static int list_alloc(LooseList& L, uint32_t cap, uint32_t* count) {
+    cudaFree(L.a);
+    cudaFree(L.vz);
+    cudaFree(L.cell);
+    L = LooseList{};
+    PIC_CUDA(cudaMalloc(&L.a, (size_t)cap * sizeof(float4)));
+    PIC_CUDA(cudaMalloc(&L.vz, (size_t)cap * sizeof(float)));
+    PIC_CUDA(cudaMalloc(&L.cell, (size_t)cap * sizeof(uint32_t)));
+    L.cap = cap;
+    L.count = count;
+    return PIC_OK;
+}
+
+static void list_free(LooseList& L) {
+    cudaFree(L.a);
+    cudaFree(L.vz);
+    cudaFree(L.cell);
+    L = LooseList{};
+}
+
+static int grow_store(pic_ctx* c, int s, int64_t capacity);
+static int grow_lists(pic_ctx* c, int s);
+
+// Side lists hold up to 1/16 of the slots (at least 2^20 particles).
+static uint32_t list_capacity(int64_t slots) {
+    return (uint32_t)std::min<int64_t>(std::max<int64_t>(slots / 16, 1 << 20), 0x40000000ll);
+}
 
 int species_setup(pic_ctx* c, int s) {
     Species& sp = c->sp[s];
@@ -777,40 +1090,66 @@ int species_setup(pic_ctx* c, int s) {
     sp.k.dtdy = (float)(c->cfg.dt / c->dy);
     sp.k.half_inv_abs_qm = sp.ctom != 0 ? (float)(0.5 / std::fabs(sp.ctom)) : 0.f;
     const size_t nc = (size_t)c->ncells;
-    PIC_CUDA(cudaMalloc(&sp.off, (nc + 1) * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.off_next, (nc + 1) * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.dcount, 9 * nc * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.sub, 10 * nc * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.farin, nc * sizeof(uint32_t)));
-    PIC_CUDA(cudaMalloc(&sp.farcur, nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.base, (nc + 1) * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.base_next, (nc + 1) * sizeof(uint32_t)));
+    for (int b = 0; b < 2; ++b) {
+        PIC_CUDA(cudaMalloc(&sp.front[b], nc * sizeof(uint32_t)));
+        PIC_CUDA(cudaMalloc(&sp.back[b], nc * sizeof(uint32_t)));
+        PIC_CUDA(cudaMemsetAsync(sp.front[b], 0, nc * sizeof(uint32_t), c->stream));
+        PIC_CUDA(cudaMemsetAsync(sp.back[b], 0, nc * sizeof(uint32_t), c->stream));
+    }
+    PIC_CUDA(cudaMalloc(&sp.cnt, nc * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.dense, (nc + 1) * sizeof(uint32_t)));
+    PIC_CUDA(cudaMalloc(&sp.list_counts, 4 * sizeof(uint32_t)));
+    PIC_CUDA(cudaMemsetAsync(sp.list_counts, 0, 4 * sizeof(uint32_t), c->stream));
     PIC_CUDA(cudaMalloc(&sp.acc_q, (size_t)c->nodes * sizeof(unsigned long long)));
     PIC_CUDA(cudaMalloc(&sp.acc_e, (size_t)c->nodes * sizeof(unsigned long long)));
     PIC_CUDA(cudaMalloc(&sp.final_mesh, (size_t)c->nodes * sizeof(double)));
     PIC_CUDA(cudaMalloc(&sp.energy_mesh, (size_t)c->nodes * sizeof(double)));
     PIC_CUDA(cudaMalloc(&sp.counters, 4 * sizeof(unsigned long long)));
-    PIC_CUDA(cudaMemsetAsync(sp.off, 0, (nc + 1) * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.off_next, 0, (nc + 1) * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, 9 * nc * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.sub, 0, 10 * nc * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, nc * sizeof(uint32_t), c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.farcur, 0, nc * sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMallocHost(&sp.host_flags, 16 * sizeof(uint32_t)));
+    std::memset(sp.host_flags, 0, 16 * sizeof(uint32_t));
+    PIC_CUDA(cudaEventCreateWithFlags(&sp.flags_ev, cudaEventDisableTiming));
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.final_mesh, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.energy_mesh, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    // an empty layout: every cell owns cell_capacity(0) slots
+    PIC_CUDA(cudaMemsetAsync(sp.cnt, 0, nc * sizeof(uint32_t), c->stream));
+    uint32_t total = 0;
+    PIC_TRY(scan_cells<true>(c, sp, sp.cnt, sp.base, &total));
+    PIC_TRY(grow_store(c, s, total));
+    PIC_TRY(grow_lists(c, s));
+    // four blocks of the particle kernels per SM need 4 x 44 KB of shared memory
+    PIC_CUDA(cudaFuncSetAttribute(k_cells<kPush, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    PIC_CUDA(cudaFuncSetAttribute(k_cells<kPush, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    PIC_CUDA(cudaFuncSetAttribute(k_cells<kDeposit, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    PIC_CUDA(cudaFuncSetAttribute(k_cells<kDeposit, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
     sp.acc_fresh = true;  // zero particles: the zero accumulator is their deposit
     return PIC_OK;
 }
 
 void species_free(Species& sp) {
     cudaFree(sp.store);
-    cudaFree(sp.off);
-    cudaFree(sp.off_next);
-    cudaFree(sp.dcount);
-    cudaFree(sp.sub);
-    cudaFree(sp.farin);
-    cudaFree(sp.farcur);
+    cudaFree(sp.base);
+    cudaFree(sp.base_next);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(sp.front[b]);
+        cudaFree(sp.back[b]);
+    }
+    cudaFree(sp.cnt);
+    cudaFree(sp.dense);
+    cudaFree(sp.list_counts);
+    list_free(sp.ovf);
+    list_free(sp.loose[0]);
+    list_free(sp.loose[1]);
+    if (sp.host_flags) cudaFreeHost(sp.host_flags);
+    if (sp.flags_ev) cudaEventDestroy(sp.flags_ev);
     cudaFree(sp.acc_q);
     cudaFree(sp.acc_e);
     cudaFree(sp.final_mesh);
@@ -819,15 +1158,15 @@ void species_free(Species& sp) {
     sp = Species{};
 }
 
-int species_reserve(pic_ctx* c, int s, int64_t capacity) {
+// Grows the buffers to `capacity` slots each, keeping the current buffer's
+// contents (same layout).
+static int grow_store(pic_ctx* c, int s, int64_t capacity) {
     Species& sp = c->sp[s];
-    if (capacity <= sp.capacity) return PIC_OK;
-    // multiples of 64 particles keep both buffers' float4 arrays 256-byte aligned
+    if (capacity <= sp.capacity && sp.store) return PIC_OK;
+    // multiples of 64 slots keep both buffers' float4 arrays 256-byte aligned
     capacity = (capacity + 63) & ~(int64_t)63;
     if (capacity > (int64_t)0xF0000000ll)
-        return fail(PIC_ERR_CAPACITY, "a species holds at most 4.0e9 particles (32-bit offsets)");
-    int64_t live = 0;
-    if (sp.store) PIC_TRY(particles_count(c, s, &live));
+        return fail(PIC_ERR_CAPACITY, "a species holds at most 4.0e9 particle slots (32-bit indices)");
     float* store = nullptr;
     PIC_CUDA(cudaMalloc(&store, (size_t)capacity * 2 * 5 * sizeof(float)));
     ParticleSoA nb[2];
@@ -835,10 +1174,10 @@ int species_reserve(pic_ctx* c, int s, int64_t capacity) {
         nb[b].a = reinterpret_cast<float4*>(store + (size_t)b * capacity * 5);
         nb[b].vz = store + (size_t)b * capacity * 5 + (size_t)capacity * 4;
     }
-    if (sp.store && live > 0) {
-        PIC_CUDA(cudaMemcpyAsync(nb[0].a, sp.buf[sp.cur].a, (size_t)live * sizeof(float4),
+    if (sp.store && sp.capacity > 0) {
+        PIC_CUDA(cudaMemcpyAsync(nb[sp.cur].a, sp.buf[sp.cur].a, (size_t)sp.capacity * sizeof(float4),
                                  cudaMemcpyDeviceToDevice, c->stream));
-        PIC_CUDA(cudaMemcpyAsync(nb[0].vz, sp.buf[sp.cur].vz, (size_t)live * sizeof(float),
+        PIC_CUDA(cudaMemcpyAsync(nb[sp.cur].vz, sp.buf[sp.cur].vz, (size_t)sp.capacity * sizeof(float),
                                  cudaMemcpyDeviceToDevice, c->stream));
         PIC_CUDA(cudaStreamSynchronize(c->stream));
     }
@@ -846,8 +1185,116 @@ int species_reserve(pic_ctx* c, int s, int64_t capacity) {
     sp.store = store;
     sp.buf[0] = nb[0];
     sp.buf[1] = nb[1];
-    sp.cur = 0;
     sp.capacity = capacity;
+    return PIC_OK;
+}
+
+// Sizes the side lists for the current capacity; only called while they
+// are empty.
+static int grow_lists(pic_ctx* c, int s) {
+    Species& sp = c->sp[s];
+    const uint32_t lc = list_capacity(sp.capacity);
+    if (lc <= sp.ovf.cap) return PIC_OK;
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    PIC_TRY(list_alloc(sp.ovf, lc, sp.list_counts + kOvf));
+    PIC_TRY(list_alloc(sp.loose[0], lc, sp.list_counts + kLoose0));
+    PIC_TRY(list_alloc(sp.loose[1], lc, sp.list_counts + kLoose1));
+    return PIC_OK;
+}
+
+static int normalize(pic_ctx* c, int s);
+
+int species_reserve(pic_ctx* c, int s, int64_t capacity) {
+    Species& sp = c->sp[s];
+    if (sp.store) PIC_TRY(normalize(c, s));  // side lists empty before they are resized
+    PIC_TRY(grow_store(c, s, capacity));
+    return grow_lists(c, s);
+}
+
+namespace {
+
+// Reads the loose-list count and error flags recorded after the last push.
+// sync: wait for them; otherwise only look when they are already there.
+int check_flags(pic_ctx* c, Species& sp, bool sync) {
+    if (!sp.flags_pending) return PIC_OK;
+    if (sync) {
+        PIC_CUDA(cudaEventSynchronize(sp.flags_ev));
+    } else {
+        const cudaError_t e = cudaEventQuery(sp.flags_ev);
+        if (e == cudaErrorNotReady) return PIC_OK;
+        if (e != cudaSuccess) return fail(PIC_ERR_CUDA, std::string("flags event: ") + cudaGetErrorString(e));
+    }
+    sp.flags_pending = false;
+    const unsigned long long* fl = reinterpret_cast<const unsigned long long*>(sp.host_flags + 4);
+    if (fl[1]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
+    if (fl[2]) return fail(PIC_ERR_CAPACITY, "particle side list overflowed: particles were lost");
+    return PIC_OK;
+}
+
+}  // namespace
+
+// Rebuilds the layout from the current per-cell counts (cell runs plus the
+// side list): every cell gets cell_capacity(count) slots with its particles
+// at the front.  Synchronises.
+static int relayout(pic_ctx* c, int s) {
+    Species& sp = c->sp[s];
+    const int64_t nc = c->ncells;
+    const int src = sp.cur;
+    const ListDev L = list_dev(sp.loose[sp.lcur]);
+    k_cell_counts<<<grid1d(nc, 256), 256, 0, c->stream>>>(sp.front[src], sp.back[src], nc, sp.cnt);
+    k_list_counts<<<kFixupBlocks, 256, 0, c->stream>>>(L, sp.cnt);
+    c->launches += 2;
+    uint32_t total = 0;
+    PIC_TRY(scan_cells<true>(c, sp, sp.cnt, sp.base_next, &total));
+    const int dst = src ^ 1;
+    if ((int64_t)total > sp.capacity) {
+        // grow: a fresh store, the old current buffer copied into its buffer
+        // `src` first (same layout), then rebuilt into `dst` as usual
+        PIC_TRY(grow_store(c, s, (int64_t)total + total / 8));
+    }
+    k_relayout_cells<<<grid1d(nc, 8), 256, 0, c->stream>>>(
+        sp.buf[src].a, sp.buf[src].vz, sp.base, sp.front[src], sp.back[src], sp.base_next, nc,
+        sp.buf[dst].a, sp.buf[dst].vz, sp.front[dst], sp.back[dst]);
+    k_relayout_list<<<kFixupBlocks, 256, 0, c->stream>>>(L, sp.base_next, sp.front[dst], sp.buf[dst].a,
+                                                         sp.buf[dst].vz);
+    c->launches += 2;
+    PIC_CUDA(cudaGetLastError());
+    PIC_CUDA(cudaMemsetAsync(sp.list_counts, 0, 4 * sizeof(uint32_t), c->stream));
+    std::swap(sp.base, sp.base_next);
+    sp.cur = dst;
+    sp.lcur = 0;
+    sp.flags_pending = false;
+    sp.host_flags[0] = 0u;
+    unsigned long long flags[3] = {0, 0, 0};
+    PIC_CUDA(cudaMemcpyAsync(flags, sp.counters, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    if (flags[1]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
+    if (flags[2]) return fail(PIC_ERR_CAPACITY, "particle side list overflowed: particles were lost");
+    return grow_lists(c, s);
+}
+
+// Every particle in a cell run (side list empty).  Synchronises.
+static int normalize(pic_ctx* c, int s) {
+    Species& sp = c->sp[s];
+    PIC_TRY(check_flags(c, sp, true));
+    uint32_t n = 0;
+    PIC_CUDA(cudaMemcpyAsync(&n, sp.list_counts + kLoose0 + sp.lcur, sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    if (n > 0) PIC_TRY(relayout(c, s));
+    return PIC_OK;
+}
+
+// cnt = particles per cell, dense = its exclusive scan; *total = particles.
+static int count_cells(pic_ctx* c, int s, int64_t* total) {
+    Species& sp = c->sp[s];
+    PIC_TRY(normalize(c, s));
+    k_cell_counts<<<grid1d(c->ncells, 256), 256, 0, c->stream>>>(sp.front[sp.cur], sp.back[sp.cur],
+                                                                 c->ncells, sp.cnt);
+    c->launches += 1;
+    uint32_t t = 0;
+    PIC_TRY(scan_cells<false>(c, sp, sp.cnt, sp.dense, &t));
+    *total = t;
     return PIC_OK;
 }
 
@@ -871,85 +1318,111 @@ int particles_import_staging(pic_ctx* c, int64_t n, pic_point** dev_points) {
     return PIC_OK;
 }
 
+// Installs a fresh layout from sp.cnt (particles per cell): base from the
+// cell capacities, growing the buffers when needed.  The current buffer's
+// contents are dropped.
+static int fresh_layout(pic_ctx* c, int s) {
+    Species& sp = c->sp[s];
+    uint32_t total = 0;
+    PIC_TRY(scan_cells<true>(c, sp, sp.cnt, sp.base, &total));
+    PIC_CUDA(cudaMemsetAsync(sp.list_counts, 0, 4 * sizeof(uint32_t), c->stream));
+    sp.lcur = 0;
+    sp.flags_pending = false;
+    sp.host_flags[0] = 0u;
+    if ((int64_t)total > sp.capacity) {
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(sp.store);
+        sp.store = nullptr;
+        sp.capacity = 0;
+        PIC_TRY(grow_store(c, s, total));
+    }
+    PIC_TRY(grow_lists(c, s));
+    unsigned long long flags[2] = {0, 0};
+    PIC_CUDA(cudaMemcpyAsync(flags, sp.counters, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    if (flags[1]) {
+        PIC_CUDA(cudaMemsetAsync(sp.counters + 1, 0, 8, c->stream));
+        return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
+    }
+    return PIC_OK;
+}
+
 int particles_import(pic_ctx* c, int s, int64_t n) {
     Species& sp = c->sp[s];
-    PIC_TRY(species_reserve(c, s, std::max<int64_t>(n, 1)));
     if (aligned_points_bytes(n) + (size_t)n * 4 > c->staging_bytes)
         return fail(PIC_ERR_STATE, "import staging too small");
     const pic_point* dev_points = static_cast<const pic_point*>(c->staging);
     uint32_t* cell_of =
         reinterpret_cast<uint32_t*>(static_cast<char*>(c->staging) + aligned_points_bytes(n));
-    const ParticleSoA tmp = sp.buf[sp.cur ^ 1];
-    const ParticleSoA dst = sp.buf[sp.cur];
-    // every imported particle enters as a "far mover" of its cell
-    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, (size_t)c->ncells * 4, c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, (size_t)c->ncells * 4 * 9, c->stream));
+    // converted points wait in a temporary buffer of n slots
+    float4* tmp_a = nullptr;
+    float* tmp_vz = nullptr;
+    if (n > 0) {
+        PIC_CUDA(cudaMalloc(&tmp_a, (size_t)n * sizeof(float4)));
+        PIC_CUDA(cudaMalloc(&tmp_vz, (size_t)n * sizeof(float)));
+    }
+    PIC_CUDA(cudaMemsetAsync(sp.cnt, 0, (size_t)c->ncells * 4, c->stream));
     if (n > 0)
         k_import_convert<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, n, c->nx, c->ny,
-                                                                1.0 / c->dx, 1.0 / c->dy, tmp.a,
-                                                                tmp.vz, cell_of, sp.farin);
-    PIC_TRY(scan_counts(c, sp));
-    if (n > 0)
-        k_import_scatter<<<grid1d(n, 256), 256, 0, c->stream>>>(tmp.a, tmp.vz, cell_of, n,
-                                                                sp.sub + 9 * c->ncells,
-                                                                sp.farcur, dst.a,
-                                                                dst.vz);
-    PIC_CUDA(cudaGetLastError());
-    std::swap(sp.off, sp.off_next);
-    PIC_CUDA(cudaMemsetAsync(sp.farcur, 0, (size_t)c->ncells * 4, c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
-    unsigned long long flags[2] = {0, 0};
-    PIC_CUDA(cudaMemcpyAsync(flags, sp.counters, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));
-    if (flags[1]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
+                                                                1.0 / c->dx, 1.0 / c->dy, tmp_a,
+                                                                tmp_vz, cell_of, sp.cnt);
+    int st = fresh_layout(c, s);
+    if (st == PIC_OK) {
+        const int b = sp.cur;
+        cudaMemsetAsync(sp.front[b], 0, (size_t)c->ncells * 4, c->stream);
+        cudaMemsetAsync(sp.back[b], 0, (size_t)c->ncells * 4, c->stream);
+        if (n > 0)
+            k_import_scatter<<<grid1d(n, 256), 256, 0, c->stream>>>(tmp_a, tmp_vz, cell_of, n, sp.base,
+                                                                    sp.front[b], sp.buf[b].a, sp.buf[b].vz);
+        c->launches += 2;
+        PIC_CUDA(cudaGetLastError());
+        PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
+        PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    cudaFree(tmp_a);
+    cudaFree(tmp_vz);
     sp.acc_fresh = false;
-    return PIC_OK;
+    return st;
 }
 
 int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out) {
     Species& sp = c->sp[s];
     int64_t n = 0;
-    PIC_TRY(particles_count(c, s, &n));
+    PIC_TRY(count_cells(c, s, &n));
     *n_out = n;
-    if (n == 0 || !sp.store) return PIC_OK;
-    const int wpb = 8;
-    k_export<<<grid1d(c->ncells, wpb), wpb * 32, 0, c->stream>>>(
-        sp.buf[sp.cur].a, sp.buf[sp.cur].vz, sp.off, c->nx, c->ncells, c->dx, c->dy, dev_out);
+    if (n == 0) return PIC_OK;
+    const int b = sp.cur;
+    k_export<<<grid1d(c->ncells, 8), 256, 0, c->stream>>>(sp.buf[b].a, sp.buf[b].vz, sp.base,
+                                                          sp.front[b], sp.back[b], sp.dense, c->nx,
+                                                          c->ncells, c->dx, c->dy, dev_out);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
 
 int particles_export_state(pic_ctx* c, int s, void* dev, int64_t n) {
     Species& sp = c->sp[s];
-    if (n == 0 || !sp.store) return PIC_OK;
+    int64_t m = 0;
+    PIC_TRY(count_cells(c, s, &m));
+    if (m != n) return fail(PIC_ERR_STATE, "particle count changed during export");
+    if (n == 0) return PIC_OK;
     int32_t* cell = static_cast<int32_t*>(dev);
     float* f = reinterpret_cast<float*>(cell + n);
+    const int b = sp.cur;
     k_export_state<<<grid1d(c->ncells, 8), 256, 0, c->stream>>>(
-        sp.buf[sp.cur].a, sp.buf[sp.cur].vz, sp.off, c->ncells, n, cell, f, f + n, f + 2 * n,
-        f + 3 * n, f + 4 * n);
+        sp.buf[b].a, sp.buf[b].vz, sp.base, sp.front[b], sp.back[b], sp.dense, c->ncells, cell, f,
+        f + n, f + 2 * n, f + 3 * n, f + 4 * n);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
 
-int particles_count(pic_ctx* c, int s, int64_t* n) {
-    Species& sp = c->sp[s];
-    uint32_t v = 0;
-    unsigned long long flags[3] = {0, 0, 0};
-    PIC_CUDA(cudaMemcpyAsync(&v, sp.off + c->ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                             c->stream));
-    PIC_CUDA(cudaMemcpyAsync(flags, sp.counters, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));
-    *n = v;
-    if (flags[1]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
-    if (flags[2]) return fail(PIC_ERR_STATE, "push passes disagreed: a scatter write was refused");
-    return PIC_OK;
-}
+int particles_count(pic_ctx* c, int s, int64_t* n) { return count_cells(c, s, n); }
 
 int particles_bin_counts(pic_ctx* c, int s, int32_t* dev_counts) {
     Species& sp = c->sp[s];
-    k_bin_counts<<<grid1d(c->nodes, 256), 256, 0, c->stream>>>(sp.off, c->nx, c->ny, c->GX,
-                                                               dev_counts);
+    int64_t n = 0;
+    PIC_TRY(count_cells(c, s, &n));
+    k_bin_counts<<<grid1d(c->nodes, 256), 256, 0, c->stream>>>(sp.cnt, c->nx, c->ny, c->GX, dev_counts);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
@@ -971,28 +1444,15 @@ int particles_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d) {
     P.drift_vy = (float)d->drift_vy;
     P.key = make_uint2((uint32_t)d->seed, (uint32_t)(d->seed >> 32));
     P.species = (uint32_t)s;
-    PIC_CUDA(cudaMemsetAsync(sp.dcount, 0, (size_t)c->ncells * 4 * 9, c->stream));
-    PIC_CUDA(cudaMemsetAsync(sp.farin, 0, (size_t)c->ncells * 4, c->stream));
-    k_plasma_counts<<<grid1d(c->ncells, 256), 256, 0, c->stream>>>(P, c->ncells,
-                                                                   sp.dcount + 4 * c->ncells);
-    PIC_TRY(scan_counts(c, sp));
-    std::swap(sp.off, sp.off_next);
-    int64_t n = 0;
-    PIC_TRY(particles_count(c, s, &n));
-    unsigned long long flags[2] = {0, 0};
-    PIC_CUDA(cudaMemcpyAsync(flags, sp.counters, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));
-    if (flags[1]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
-    if (n > sp.capacity) {
-        // the old particles are replaced: drop them before growing
-        sp.capacity = 0;
-        cudaFree(sp.store);
-        sp.store = nullptr;
-        PIC_TRY(species_reserve(c, s, n));
-    }
-    k_plasma_generate<<<grid1d(c->ncells, 8), 256, 0, c->stream>>>(P, sp.off, c->ncells,
-                                                                    sp.buf[sp.cur].a,
-                                                                    sp.buf[sp.cur].vz);
+    k_plasma_counts<<<grid1d(c->ncells, 256), 256, 0, c->stream>>>(P, c->ncells, sp.cnt);
+    c->launches += 1;
+    PIC_TRY(scan_cells<false>(c, sp, sp.cnt, sp.dense, nullptr));
+    PIC_TRY(fresh_layout(c, s));
+    const int b = sp.cur;
+    k_plasma_generate<<<grid1d(c->ncells, 8), 256, 0, c->stream>>>(P, sp.dense, sp.base, c->ncells,
+                                                                    sp.buf[b].a, sp.buf[b].vz,
+                                                                    sp.front[b], sp.back[b]);
+    c->launches += 1;
     PIC_CUDA(cudaGetLastError());
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
@@ -1002,20 +1462,23 @@ int particles_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d) {
 
 int particles_deposit(pic_ctx* c, int s) {
     Species& sp = c->sp[s];
-    if (!sp.store) {
-        sp.acc_fresh = true;
-        return PIC_OK;
-    }
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     KArgs A = make_args(c, sp);
+    const bool energy = c->cfg.deposit_energy != 0;
+    const ListDev L = list_dev(sp.loose[sp.lcur]);
     prof_begin(c, PIC_PHASE_DEPOSIT);
-    if (A.energy)
-        k_particles<kDeposit, true><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
-    else
-        k_particles<kDeposit, false><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+    if (energy) {
+        k_cells<kDeposit, true><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+        k_list_deposit<true><<<kFixupBlocks, 256, 0, c->stream>>>(L, c->nx, c->GX, sp.k.half_inv_abs_qm,
+                                                                  sp.acc_q, sp.acc_e);
+    } else {
+        k_cells<kDeposit, false><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+        k_list_deposit<false><<<kFixupBlocks, 256, 0, c->stream>>>(L, c->nx, c->GX, sp.k.half_inv_abs_qm,
+                                                                   sp.acc_q, sp.acc_e);
+    }
     prof_end(c, PIC_PHASE_DEPOSIT);
-    c->launches += 1;
+    c->launches += 2;
     PIC_CUDA(cudaGetLastError());
     sp.acc_fresh = true;
     return PIC_OK;
@@ -1041,28 +1504,66 @@ int particles_flush_rho(pic_ctx* c, int s) {
 
 int particles_push(pic_ctx* c, int s) {
     Species& sp = c->sp[s];
-    if (!sp.store) return PIC_OK;
+    // a side list that keeps growing means the layout no longer fits the
+    // particle distribution: rebuild it (looked at without waiting)
+    PIC_TRY(check_flags(c, sp, false));
+    if (!sp.flags_pending && sp.host_flags[0] > sp.loose[0].cap / 8u) {
+        prof_begin(c, PIC_PHASE_RELAYOUT);
+        PIC_TRY(relayout(c, s));
+        prof_end(c, PIC_PHASE_RELAYOUT);
+    }
     KArgs A = make_args(c, sp);
     const dim3 g = tile_grid(c);
-    prof_begin(c, PIC_PHASE_PUSH_COUNT);
-    k_particles<kCount, false><<<g, kThreads, 0, c->stream>>>(A);
-    prof_end(c, PIC_PHASE_PUSH_COUNT);
-    PIC_CUDA(cudaGetLastError());
-    prof_begin(c, PIC_PHASE_SCAN);
-    PIC_TRY(scan_counts(c, sp));
-    prof_end(c, PIC_PHASE_SCAN);
+    const bool energy = c->cfg.deposit_energy != 0;
+    const int dst = sp.cur ^ 1;
+    PIC_CUDA(cudaMemsetAsync(sp.back[dst], 0, (size_t)c->ncells * 4, c->stream));
     // the accumulators collect the deposit of the new positions
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
-    prof_begin(c, PIC_PHASE_PUSH_SCATTER);
-    if (A.energy)
-        k_particles<kScatter, true><<<g, kThreads, 0, c->stream>>>(A);
+    prof_begin(c, PIC_PHASE_PUSH);
+    if (energy)
+        k_cells<kPush, true><<<g, kThreads, 0, c->stream>>>(A);
     else
-        k_particles<kScatter, false><<<g, kThreads, 0, c->stream>>>(A);
-    prof_end(c, PIC_PHASE_PUSH_SCATTER);
-    c->launches += 4;
+        k_cells<kPush, false><<<g, kThreads, 0, c->stream>>>(A);
+    prof_end(c, PIC_PHASE_PUSH);
     PIC_CUDA(cudaGetLastError());
-    swap_buffers(sp);
+    FixArgs F{};
+    F.nx = c->nx;
+    F.ny = c->ny;
+    F.GX = c->GX;
+    F.k = push_consts(c, sp);
+    F.fld = c->fld;
+    F.dst_a = sp.buf[dst].a;
+    F.dst_vz = sp.buf[dst].vz;
+    F.base = sp.base;
+    F.front = sp.front[dst];
+    F.back = sp.back[dst];
+    F.ovf = list_dev(sp.ovf);
+    F.prev = list_dev(sp.loose[sp.lcur]);
+    F.next = list_dev(sp.loose[sp.lcur ^ 1]);
+    F.acc_q = sp.acc_q;
+    F.acc_e = sp.acc_e;
+    F.counters = sp.counters;
+    prof_begin(c, PIC_PHASE_FIXUP);
+    if (energy)
+        k_fixup<true><<<kFixupBlocks, 256, 0, c->stream>>>(F);
+    else
+        k_fixup<false><<<kFixupBlocks, 256, 0, c->stream>>>(F);
+    prof_end(c, PIC_PHASE_FIXUP);
+    PIC_CUDA(cudaGetLastError());
+    c->launches += 2;
+    // the consumed lists start empty next time
+    PIC_CUDA(cudaMemsetAsync(sp.list_counts + kOvf, 0, sizeof(uint32_t), c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.list_counts + kLoose0 + sp.lcur, 0, sizeof(uint32_t), c->stream));
+    sp.lcur ^= 1;
+    sp.cur = dst;
+    // side-list size and error flags, read back without waiting
+    PIC_CUDA(cudaMemcpyAsync(sp.host_flags, sp.list_counts + kLoose0 + sp.lcur, sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaMemcpyAsync(sp.host_flags + 4, sp.counters, 3 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaEventRecord(sp.flags_ev, c->stream));
+    sp.flags_pending = true;
     sp.acc_fresh = true;
     return PIC_OK;
 }

@@ -42,12 +42,13 @@ int fail(int status, const std::string& msg);
 constexpr int kAxisBits = 20;
 constexpr double kChargeUnit = 1.0 / 1099511627776.0;  // 2^-40
 // The energy mesh (a diagnostic: printEnergy) uses each particle's kinetic
-// energy in units of 2^-22 eV as a 32-bit integer, clamped below 1024 eV,
-// times 16-bit axis weights: one contribution stays below 2^32.
+// energy, clamped below 1024 eV, times its FP32 corner weights, rounded to an
+// integer number of 2^-22 eV: one contribution stays below 2^32.
 constexpr double kEnergyUnit = 1.0 / 4194304.0;  // 2^-22
 constexpr float kEnergyClampEv = 1023.9375f;      // (2^32 - 2^18) * 2^-22
-// Particles per cell above which a node sum could overflow (4 cells touch a
-// node: 2^18 contributions of < 2^44 stay below 2^62).
+// Particle slots a cell may hold (the per-lane moment sums of the deposit
+// need at most 2^11 particles per lane).  A re-layout flags cells whose
+// capacity would exceed it.
 constexpr uint32_t kMaxPerCell = 1u << 16;
 
 // ---------------------------------------------------------------------------
@@ -55,13 +56,16 @@ constexpr uint32_t kMaxPerCell = 1u << 16;
 // ---------------------------------------------------------------------------
 constexpr int kTileX = 64;  // cells per block in x
 constexpr int kTileY = 4;   // cells per block in y
-constexpr int kHalo = 1;    // mover halo (cells) kept in the shared tile
 constexpr int kWarps = 8;   // 256 threads per block
 
 struct SpeciesConsts {
     float h;          // 0.5*(q/m)*dt
     float dtdx, dtdy; // dt/dx, dt/dy
     float half_inv_abs_qm;  // 0.5/|q/m| -> kinetic energy in eV
+    // uniform Bz (bzu != 0): the Boris rotation factors t = h*Bz and
+    // s = 2t/(1+t^2), the same for every particle
+    int bzu;
+    float bt, bs;
 };
 
 // Cell-sorted state of one species (one buffer of a double buffer):
@@ -71,27 +75,47 @@ struct ParticleSoA {
     float* vz;
 };
 
+// Particles held outside the cell layout (a mover that found its target
+// cell full, or one that jumped more than one cell): state plus target cell.
+struct LooseList {
+    float4* a = nullptr;
+    float* vz = nullptr;
+    uint32_t* cell = nullptr;
+    uint32_t* count = nullptr;  // device counter (entries may exceed cap: then lost)
+    uint32_t cap = 0;
+};
+
+// Slot layout.  Cell c owns slots base[c] .. base[c+1] of each buffer; its
+// particles are the front run base[c] .. base[c]+front[c] (those that stayed
+// in the cell at the last push, or all of them after a re-layout) and the
+// back run base[c+1]-back[c] .. base[c+1] (those that moved in).  The free
+// gap between the runs absorbs the next push's incoming movers.
 struct Species {
     pic_species_desc desc{};
     double ctom = 0, weighing = 0;
     SpeciesConsts k{};
-    int64_t capacity = 0;
+    int64_t capacity = 0;           // slots per buffer
     float* store = nullptr;         // 2 buffers x 5 arrays x capacity floats
     ParticleSoA buf[2]{};
     int cur = 0;
-    uint32_t* off = nullptr;        // [ncells+1] segment starts of buf[cur]
-    uint32_t* off_next = nullptr;   // [ncells+1] segment starts being built
-    uint32_t* dcount = nullptr;     // [9][ncells] particles leaving cell s in direction d
-                                    //   (d = (sy+1)*3 + (sx+1); d = 4 stays)
-    uint32_t* sub = nullptr;        // [10][ncells] start of cell t's sub-segment fed
-                                    //   from direction d (9: far movers)
-    uint32_t* farin = nullptr;      // [ncells] far movers (jump > 1 cell) entering a cell
-    uint32_t* farcur = nullptr;     // [ncells] far-mover slots handed out
+    uint32_t* base = nullptr;       // [ncells+1] slot layout (both buffers)
+    uint32_t* base_next = nullptr;  // [ncells+1] layout being built
+    uint32_t* front[2] = {nullptr, nullptr};  // [ncells] per buffer
+    uint32_t* back[2] = {nullptr, nullptr};   // [ncells] per buffer
+    uint32_t* cnt = nullptr;        // [ncells] scratch: particles per cell
+    uint32_t* dense = nullptr;      // [ncells+1] scratch: exclusive scan of cnt
+    uint32_t* list_counts = nullptr;  // [4] device counters of the lists below
+    LooseList ovf;                  // push output: not yet placed
+    LooseList loose[2];             // [lcur]: part of the state, not yet placed
+    int lcur = 0;
+    uint32_t* host_flags = nullptr; // pinned: loose count + counters after the last push
+    cudaEvent_t flags_ev = nullptr;
+    bool flags_pending = false;
     unsigned long long* acc_q = nullptr;  // [nodes] fixed-point charge weights
     unsigned long long* acc_e = nullptr;  // [nodes] fixed-point energy weights
     double* final_mesh = nullptr;   // [nodes]
     double* energy_mesh = nullptr;  // [nodes]
-    unsigned long long* counters = nullptr;  // [0] left exits, [1] max per cell flag
+    unsigned long long* counters = nullptr;  // [0] left exits, [1] cell limit, [2] lost particles
     bool acc_fresh = false;         // acc_* hold the deposit of the current positions
 };
 
@@ -165,6 +189,8 @@ struct pic_ctx {
     picb200::Species sp[PIC_MAX_SPECIES];
     picb200::PoissonState ps;
     bool fields_valid = false;
+    bool bz_uniform = true;        // every node has the same Bz (bz_value)
+    double bz_value = 0.0;
     // instrumentation
     bool profiling = false;
     struct ProfEvent {

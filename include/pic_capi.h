@@ -199,12 +199,12 @@ int pic_set_bz(pic_ctx* ctx, const double* host);
 
 /* ---- instrumentation (no reference counterpart; the reference returns
  * host wall seconds per operator, src/sycl_pic_ctypes.cpp:127-236) ------- */
-#define PIC_PHASE_PUSH_COUNT 0   /* pass 1: push + per-cell counts          */
-#define PIC_PHASE_SCAN 1         /* exclusive scan of the new cell counts    */
-#define PIC_PHASE_PUSH_SCATTER 2 /* pass 2: push + scatter + fused deposit   */
-#define PIC_PHASE_DEPOSIT 3      /* stand-alone deposit of current positions */
-#define PIC_PHASE_FLUSH 4        /* accumulators -> final/energy mesh, rho   */
-#define PIC_PHASE_POISSON 5      /* whole Poisson solve incl. E field        */
+#define PIC_PHASE_PUSH 0         /* the push pass: gather, Boris, binning, fused deposit */
+#define PIC_PHASE_FIXUP 1        /* side list: movers whose target cell was full      */
+#define PIC_PHASE_RELAYOUT 2     /* slot-layout rebuilds (rare)                        */
+#define PIC_PHASE_DEPOSIT 3      /* stand-alone deposit of current positions          */
+#define PIC_PHASE_FLUSH 4        /* accumulators -> final/energy mesh, rho             */
+#define PIC_PHASE_POISSON 5      /* whole Poisson solve incl. E field                  */
 #define PIC_NUM_PHASES 6
 /* When on, CUDA events bracket every phase on the context stream. */
 int pic_set_profiling(pic_ctx* ctx, int on);
