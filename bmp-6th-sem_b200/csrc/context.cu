@@ -5,8 +5,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pic_internal.h"
@@ -28,32 +31,152 @@ static int check_species(pic_ctx* c, int s) {
     return PIC_OK;
 }
 
-static int ensure_host_staging(pic_ctx* c, size_t bytes) {
-    if (bytes <= c->host_staging_bytes) return PIC_OK;
-    if (c->host_staging) cudaFreeHost(c->host_staging);
-    c->host_staging = nullptr;
-    c->host_staging_bytes = 0;
-    PIC_CUDA(cudaMallocHost(&c->host_staging, bytes));
-    c->host_staging_bytes = bytes;
+// ---------------------------------------------------------------------------
+// Host <-> device streaming of large arrays (particles, grids).  Caller memory
+// is ordinary pageable memory, so every copy passes through pinned staging:
+// two kPipeChunk buffers alternate, the host-side copy of one chunk (split
+// over a pool of threads) overlapping the DMA of the other.
+// ---------------------------------------------------------------------------
+namespace {
+
+class CopyPool {
+  public:
+    static CopyPool& get() {
+        static CopyPool pool;
+        return pool;
+    }
+
+    void copy(void* dst, const void* src, size_t bytes) {
+        if (bytes < (4u << 20) || workers_.empty()) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        std::lock_guard<std::mutex> one_at_a_time(call_mu_);
+        const int parts = (int)workers_.size() + 1;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = static_cast<char*>(dst);
+            src_ = static_cast<const char*>(src);
+            bytes_ = bytes;
+            parts_ = parts;
+            pending_ = parts - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        part(0);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+  private:
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int n = (int)std::min<unsigned>(hw ? hw : 1u, 16u) - 1;
+        for (int i = 0; i < n; ++i) workers_.emplace_back([this, i] { loop(i + 1); });
+    }
+
+    void part(int i) {
+        // 64-byte aligned part boundaries
+        const size_t per = ((bytes_ / parts_) + 63) & ~(size_t)63;
+        const size_t a = std::min(bytes_, per * (size_t)i), b = std::min(bytes_, per * (size_t)(i + 1));
+        if (b > a) std::memcpy(dst_ + a, src_ + a, b - a);
+    }
+
+    void loop(int i) {
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            lk.unlock();
+            part(i);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+
+    std::vector<std::thread> workers_;
+    std::mutex call_mu_, mu_;
+    std::condition_variable cv_, done_;
+    uint64_t gen_ = 0;
+    int pending_ = 0, parts_ = 1;
+    bool stop_ = false;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+constexpr size_t kPipeChunk = 32u << 20;
+
+}  // namespace
+
+static int ensure_pipe(pic_ctx* c) {
+    for (int b = 0; b < 2; ++b) {
+        if (!c->pipe_buf[b]) PIC_CUDA(cudaMallocHost(&c->pipe_buf[b], kPipeChunk));
+        if (!c->pipe_ev[b]) PIC_CUDA(cudaEventCreateWithFlags(&c->pipe_ev[b], cudaEventDisableTiming));
+    }
     return PIC_OK;
 }
 
-// Device -> host copy through pinned staging (pageable destinations would
-// serialise the stream anyway).
-static int copy_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes) {
-    PIC_TRY(ensure_host_staging(c, bytes));
-    PIC_CUDA(cudaMemcpyAsync(c->host_staging, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));
-    std::memcpy(host, c->host_staging, bytes);
+// host (pageable) -> device, enqueued on the context stream; returns when
+// the last chunk has been handed to the DMA engine.
+static int stream_to_device(pic_ctx* c, void* dev, const void* host, size_t bytes) {
+    PIC_TRY(ensure_pipe(c));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));  // staging may still feed an earlier copy
+    for (size_t off = 0, k = 0; off < bytes; off += kPipeChunk, ++k) {
+        const size_t m = std::min(kPipeChunk, bytes - off);
+        const int b = (int)(k & 1);
+        if (k >= 2) PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));  // its previous DMA is done
+        CopyPool::get().copy(c->pipe_buf[b], static_cast<const char*>(host) + off, m);
+        PIC_CUDA(cudaMemcpyAsync(static_cast<char*>(dev) + off, c->pipe_buf[b], m,
+                                 cudaMemcpyHostToDevice, c->stream));
+        PIC_CUDA(cudaEventRecord(c->pipe_ev[b], c->stream));
+    }
     return PIC_OK;
+}
+
+// device -> host (pageable), after the work queued on the stream; synchronous.
+static int stream_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes) {
+    PIC_TRY(ensure_pipe(c));
+    const size_t nchunks = (bytes + kPipeChunk - 1) / kPipeChunk;
+    auto issue = [&](size_t k) -> int {
+        const size_t off = k * kPipeChunk, m = std::min(kPipeChunk, bytes - off);
+        const int b = (int)(k & 1);
+        PIC_CUDA(cudaMemcpyAsync(c->pipe_buf[b], static_cast<const char*>(dev) + off, m,
+                                 cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaEventRecord(c->pipe_ev[b], c->stream));
+        return PIC_OK;
+    };
+    if (nchunks == 0) return PIC_OK;
+    PIC_TRY(issue(0));
+    for (size_t k = 0; k < nchunks; ++k) {
+        // the other buffer was emptied in the previous iteration
+        if (k + 1 < nchunks) PIC_TRY(issue(k + 1));
+        const int b = (int)(k & 1);
+        PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));
+        const size_t off = k * kPipeChunk, m = std::min(kPipeChunk, bytes - off);
+        CopyPool::get().copy(static_cast<char*>(host) + off, c->pipe_buf[b], m);
+    }
+    return PIC_OK;
+}
+
+// Device -> host copy (pageable destination), synchronous.
+static int copy_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes) {
+    return stream_to_host(c, host, dev, bytes);
 }
 
 static int copy_to_device(pic_ctx* c, void* dev, const void* host, size_t bytes) {
-    PIC_TRY(ensure_host_staging(c, bytes));
-    PIC_CUDA(cudaStreamSynchronize(c->stream));  // staging may still feed a copy
-    std::memcpy(c->host_staging, host, bytes);
-    PIC_CUDA(cudaMemcpyAsync(dev, c->host_staging, bytes, cudaMemcpyHostToDevice, c->stream));
-    return PIC_OK;
+    return stream_to_device(c, dev, host, bytes);
 }
 
 static cudaEvent_t pool_event(pic_ctx* c) {
@@ -101,6 +224,10 @@ static void free_ctx(pic_ctx* c) {
     cudaFree(c->scan_partials);
     cudaFree(c->staging);
     if (c->host_staging) cudaFreeHost(c->host_staging);
+    for (int b = 0; b < 2; ++b) {
+        if (c->pipe_buf[b]) cudaFreeHost(c->pipe_buf[b]);
+        if (c->pipe_ev[b]) cudaEventDestroy(c->pipe_ev[b]);
+    }
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -280,16 +407,7 @@ int pic_import_points(pic_ctx* c, int s, const pic_point* host, int64_t n) {
     if (n > (int64_t)0xF0000000ll) return fail(PIC_ERR_CAPACITY, "too many points");
     pic_point* dev = nullptr;
     PIC_TRY(particles_import_staging(c, n, &dev));
-    // chunked through pinned staging so arbitrary host memory works
-    const int64_t chunk = 1 << 20;
-    PIC_TRY(ensure_host_staging(c, (size_t)std::min<int64_t>(n, chunk) * sizeof(pic_point) + 64));
-    for (int64_t i0 = 0; i0 < n; i0 += chunk) {
-        const int64_t m = std::min<int64_t>(chunk, n - i0);
-        PIC_CUDA(cudaStreamSynchronize(c->stream));
-        std::memcpy(c->host_staging, host + i0, (size_t)m * sizeof(pic_point));
-        PIC_CUDA(cudaMemcpyAsync(dev + i0, c->host_staging, (size_t)m * sizeof(pic_point),
-                                 cudaMemcpyHostToDevice, c->stream));
-    }
+    PIC_TRY(stream_to_device(c, dev, host, (size_t)n * sizeof(pic_point)));
     return particles_import(c, s, n);
 }
 
@@ -305,16 +423,7 @@ int pic_export_points(pic_ctx* c, int s, pic_point* host, int64_t capacity, int6
     pic_point* dev = static_cast<pic_point*>(c->staging);
     int64_t n2 = 0;
     PIC_TRY(particles_export(c, s, dev, &n2));
-    const int64_t chunk = 1 << 20;
-    PIC_TRY(ensure_host_staging(c, (size_t)std::min<int64_t>(n, chunk) * sizeof(pic_point) + 64));
-    for (int64_t i0 = 0; i0 < n; i0 += chunk) {
-        const int64_t m = std::min<int64_t>(chunk, n - i0);
-        PIC_CUDA(cudaMemcpyAsync(c->host_staging, dev + i0, (size_t)m * sizeof(pic_point),
-                                 cudaMemcpyDeviceToHost, c->stream));
-        PIC_CUDA(cudaStreamSynchronize(c->stream));
-        std::memcpy(host + i0, c->host_staging, (size_t)m * sizeof(pic_point));
-    }
-    return PIC_OK;
+    return stream_to_host(c, host, dev, (size_t)n * sizeof(pic_point));
 }
 
 int pic_export_state(pic_ctx* c, int s, int32_t* cell, float* fx, float* fy, float* vx,

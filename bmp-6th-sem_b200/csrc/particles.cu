@@ -790,41 +790,46 @@ __global__ void k_relayout_list(ListDev L, const uint32_t* __restrict__ nbase, u
 
 // ---- import / export ------------------------------------------------------
 
-// Reference Point -> cell + FP32 offsets.  The cell follows InsertKernel:
-// gx = (int)(x * (1/dx)) in FP64 (src/particles.cpp:230-235).
-__global__ void k_import_convert(const pic_point* __restrict__ pts, int64_t n, int nx, int ny,
-                                 double inv_dx, double inv_dy, float4* tmp_a, float* tmp_vz,
-                                 uint32_t* cell_of, uint32_t* cnt) {
+// Reference Point -> cell.  The cell follows InsertKernel: gx = (int)(x *
+// (1/dx)) in FP64 (src/particles.cpp:230-235); dead (pointer == -1) and
+// out-of-domain points get no cell.
+__device__ __forceinline__ uint32_t point_cell(const pic_point& p, int nx, int ny, double inv_dx,
+                                               double inv_dy, double& sx, double& sy) {
+    if (p.pointer == -1) return 0xffffffffu;
+    sx = p.x * inv_dx;
+    sy = p.y * inv_dy;
+    if (!(sx >= 0.0 && sy >= 0.0 && sx < (double)nx && sy < (double)ny)) return 0xffffffffu;
+    return (uint32_t)(int)sy * (uint32_t)nx + (uint32_t)(int)sx;
+}
+
+__global__ void k_import_count(const pic_point* __restrict__ pts, int64_t n, int nx, int ny,
+                               double inv_dx, double inv_dy, uint32_t* cell_of, uint32_t* cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const pic_point p = pts[i];
-    uint32_t cell = 0xffffffffu;
-    if (p.pointer != -1) {
-        const double sx = p.x * inv_dx, sy = p.y * inv_dy;
-        if (sx >= 0.0 && sy >= 0.0 && sx < (double)nx && sy < (double)ny) {
-            const int gx = (int)sx, gy = (int)sy;
-            cell = (uint32_t)gy * (uint32_t)nx + (uint32_t)gx;
-            const float fx = fminf((float)(sx - gx), kOneBelow);
-            const float fy = fminf((float)(sy - gy), kOneBelow);
-            tmp_a[i] = make_float4(fx, fy, (float)p.vx, (float)p.vy);
-            tmp_vz[i] = (float)p.vz;
-        }
-    }
+    double sx, sy;
+    const uint32_t cell = point_cell(pts[i], nx, ny, inv_dx, inv_dy, sx, sy);
     cell_of[i] = cell;
     if (cell != 0xffffffffu) atomicAdd(cnt + cell, 1u);
 }
 
-__global__ void k_import_scatter(const float4* __restrict__ tmp_a, const float* __restrict__ tmp_vz,
-                                 const uint32_t* __restrict__ cell_of, int64_t n,
-                                 const uint32_t* __restrict__ base, uint32_t* front,
-                                 float4* dst_a, float* dst_vz) {
+// The FP32 in-cell offset is the FP64 remainder (clamped below 1).
+__global__ void k_import_place(const pic_point* __restrict__ pts, const uint32_t* __restrict__ cell_of,
+                               int64_t n, int nx, int ny, double inv_dx, double inv_dy,
+                               const uint32_t* __restrict__ base, uint32_t* front, float4* dst_a,
+                               float* dst_vz) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t c = cell_of[i];
     if (c == 0xffffffffu) return;
+    const pic_point p = pts[i];
+    const double sx = p.x * inv_dx, sy = p.y * inv_dy;
+    const int gx = (int)sx, gy = (int)sy;
     const uint32_t d = base[c] + atomicAdd(front + c, 1u);
-    dst_a[d] = tmp_a[i];
-    dst_vz[d] = tmp_vz[i];
+    dst_a[d] = make_float4(fminf((float)(sx - gx), kOneBelow), fminf((float)(sy - gy), kOneBelow),
+                           (float)p.vx, (float)p.vy);
+    dst_vz[d] = (float)p.vz;
+    (void)nx;
+    (void)ny;
 }
 
 // Layout -> reference Point AoS in cell order (dense[c] = particles before
@@ -1354,36 +1359,24 @@ int particles_import(pic_ctx* c, int s, int64_t n) {
     const pic_point* dev_points = static_cast<const pic_point*>(c->staging);
     uint32_t* cell_of =
         reinterpret_cast<uint32_t*>(static_cast<char*>(c->staging) + aligned_points_bytes(n));
-    // converted points wait in a temporary buffer of n slots
-    float4* tmp_a = nullptr;
-    float* tmp_vz = nullptr;
-    if (n > 0) {
-        PIC_CUDA(cudaMalloc(&tmp_a, (size_t)n * sizeof(float4)));
-        PIC_CUDA(cudaMalloc(&tmp_vz, (size_t)n * sizeof(float)));
-    }
     PIC_CUDA(cudaMemsetAsync(sp.cnt, 0, (size_t)c->ncells * 4, c->stream));
     if (n > 0)
-        k_import_convert<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, n, c->nx, c->ny,
-                                                                1.0 / c->dx, 1.0 / c->dy, tmp_a,
-                                                                tmp_vz, cell_of, sp.cnt);
-    int st = fresh_layout(c, s);
-    if (st == PIC_OK) {
-        const int b = sp.cur;
-        cudaMemsetAsync(sp.front[b], 0, (size_t)c->ncells * 4, c->stream);
-        cudaMemsetAsync(sp.back[b], 0, (size_t)c->ncells * 4, c->stream);
-        if (n > 0)
-            k_import_scatter<<<grid1d(n, 256), 256, 0, c->stream>>>(tmp_a, tmp_vz, cell_of, n, sp.base,
-                                                                    sp.front[b], sp.buf[b].a, sp.buf[b].vz);
-        c->launches += 2;
-        PIC_CUDA(cudaGetLastError());
-        PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
-        PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
-        PIC_CUDA(cudaStreamSynchronize(c->stream));
-    }
-    cudaFree(tmp_a);
-    cudaFree(tmp_vz);
+        k_import_count<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, n, c->nx, c->ny, 1.0 / c->dx,
+                                                              1.0 / c->dy, cell_of, sp.cnt);
+    PIC_TRY(fresh_layout(c, s));
+    const int b = sp.cur;
+    PIC_CUDA(cudaMemsetAsync(sp.front[b], 0, (size_t)c->ncells * 4, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.back[b], 0, (size_t)c->ncells * 4, c->stream));
+    if (n > 0)
+        k_import_place<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, cell_of, n, c->nx, c->ny,
+                                                              1.0 / c->dx, 1.0 / c->dy, sp.base,
+                                                              sp.front[b], sp.buf[b].a, sp.buf[b].vz);
+    c->launches += 2;
+    PIC_CUDA(cudaGetLastError());
+    PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
+    PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     sp.acc_fresh = false;
-    return st;
+    return PIC_OK;
 }
 
 int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out) {

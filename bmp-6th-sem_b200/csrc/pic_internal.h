@@ -186,6 +186,8 @@ struct pic_ctx {
     size_t staging_bytes = 0;
     void* host_staging = nullptr;  // pinned host staging
     size_t host_staging_bytes = 0;
+    void* pipe_buf[2] = {nullptr, nullptr};  // pinned chunks of the host<->device pipeline
+    cudaEvent_t pipe_ev[2] = {nullptr, nullptr};
     picb200::Species sp[PIC_MAX_SPECIES];
     picb200::PoissonState ps;
     bool fields_valid = false;

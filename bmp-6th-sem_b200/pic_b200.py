@@ -238,13 +238,17 @@ class Pic:
         pts = np.ascontiguousarray(pts)
         _check(lib().pic_import_points(self.h, s, _p(pts) if len(pts) else None, len(pts)))
 
-    def export_points(self, s: int) -> np.ndarray:
+    def export_points(self, s: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Points of species s; into `out` (a POINT_DTYPE array at least as
+        long as the particle count) when given, returning the filled view."""
         n = ctypes.c_int64(0)
         _check(lib().pic_export_points(self.h, s, None, 0, ctypes.byref(n)))
-        out = np.zeros(n.value, POINT_DTYPE)
+        if out is None:
+            out = np.zeros(n.value, POINT_DTYPE)
+        assert out.dtype == POINT_DTYPE and out.flags["C_CONTIGUOUS"] and len(out) >= n.value
         if n.value:
-            _check(lib().pic_export_points(self.h, s, _p(out), n.value, ctypes.byref(n)))
-        return out
+            _check(lib().pic_export_points(self.h, s, _p(out), len(out), ctypes.byref(n)))
+        return out[:n.value]
 
     def load_plasma(self, s: int, ppc: int, temperature_ev: float, seed: int, blob_peak_ppc=0.0,
                     blob_cx=0.0, blob_cy=0.0, blob_sigma=0.0, drift_vx=0.0, drift_vy=0.0):
