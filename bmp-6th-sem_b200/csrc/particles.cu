@@ -110,18 +110,17 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Asynchronous global -> shared copies (cp.async); a false predicate copies
-// nothing and fills the destination with zeros.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool pred) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-                 "r"(pred ? 16 : 0)
-                 : "memory");
+// Asynchronous global -> shared copies (cp.async) to a shared-space address;
+// a false predicate copies nothing and fills the destination with zeros.
+// Only the wait orders them against the shared-memory reads of the data.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool pred) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(pred ? 16 : 0));
 }
 
-__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool pred) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-                 "r"(pred ? 4 : 0)
-                 : "memory");
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, bool pred) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(pred ? 4 : 0));
 }
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -475,13 +474,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
     int plc = next_cell(warp, false);
     CellMeta pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
     uint32_t pj0 = 0;
+    const uint32_t ring_a0 = smem_u32(&s_ring_a[warp][0][lane]);
+    const uint32_t ring_vz0 = smem_u32(&s_ring_vz[warp][0][lane]);
     auto issue = [&](int r) {
         if (plc < kTileCells) {
             const uint32_t jj = pj0 + lane, np = pm.nf + pm.nb;
             const bool v = jj < np;
             const uint32_t i = !v ? 0u : (jj < pm.nf ? pm.b0 + jj : pm.b1 - pm.nb + (jj - pm.nf));
-            cp_async16(&s_ring_a[warp][r][lane], A.src_a + i, v);
-            cp_async4(&s_ring_vz[warp][r][lane], A.src_vz + i, v);
+            cp_async16(ring_a0 + (uint32_t)r * (32u * 16u), A.src_a + i, v);
+            cp_async4(ring_vz0 + (uint32_t)r * (32u * 4u), A.src_vz + i, v);
             if (pj0 + 32 >= np) {
                 plc = next_cell(plc + kWarps, false);
                 pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
