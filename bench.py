@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--ws-epochs", type=int, default=6)
     ap.add_argument("--ws-eval", type=int, default=12,
                     help="evaluation steps, each solved from both guesses")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 64-instance batched ensemble measurement")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -440,6 +443,51 @@ def run_learned(pic, args, it):
                     "32 channels, bf16 mma.sync tensor cores, FP32 accumulation"}, it
 
 
+def run_ensemble(args, rank):
+    """The 64-instance ensemble (grids 128^2..384^2, left electrode 50-300 V,
+    Bz 0-0.02 T, 32 particles/cell/species, 5e14-2e15 m^-3, seeded per
+    instance): one launch per phase over all instances, the Poisson solves
+    in one persistent launch, the step replayed as a CUDA graph, tile shape
+    autotuned.  Times from the ensemble's own CUDA events."""
+    import pic_b200 as P
+    import pic_configs as C
+    ws = C.cfg5_instances()
+    t0 = time.perf_counter()
+    E = P.Ensemble([C.library_config(w) for w in ws])
+    for k, w in enumerate(ws):
+        C.load_plasma(E[k], w, seed=5000 + 97 * k + 7919 * rank)
+    setup_s = time.perf_counter() - t0
+    n_part = sum(E[k].count(s) for k in range(len(ws)) for s in range(2))
+    shape, ms_shapes = E.autotune()
+    for it in range(args.warmup):
+        E.step(it)
+    dep, pois, push, iters = [], [], [], []
+    for it in range(args.warmup, args.warmup + args.ensemble_steps):
+        E.step(it)
+        d, p, q = E.timing()
+        dep.append(d)
+        pois.append(p)
+        push.append(q)
+        iters.append(statistics.mean(E[k].poisson_stats()[0] for k in range(len(ws))))
+    info = E.info()
+    worst_rel = max(E[k].poisson_stats()[1] for k in range(len(ws)))
+    E.close()
+    part_ms = statistics.mean(d + q for d, q in zip(dep, push))
+    peak, peak_kind = measured_peaks()
+    push_ms = statistics.mean(push)
+    return {"workload": f"{len(ws)} instances, grids {min(w.nx for w in ws)}^2..{max(w.nx for w in ws)}^2, "
+                        "left electrode 50-300 V, Bz 0-0.02 T, 32 ppc/species, 5e14-2e15 m^-3",
+            "instances": len(ws), "particles": n_part,
+            "particle_steps_per_s": n_part / (part_ms * 1e-3),
+            "ms_per_step_particles": part_ms, "ms_per_step_poisson_all": statistics.mean(pois),
+            "ms_per_step_total": statistics.mean(a + b + c for a, b, c in zip(dep, pois, push)),
+            "poisson_iters_mean": statistics.mean(iters), "worst_relres": worst_rel,
+            "push_roofline_frac": BYTES_PUSH_PASS * n_part / (push_ms * 1e-3) / 1e9 / peak,
+            "tile_shape": ["64x4", "32x8", "128x2", "16x16"][shape], "ms_per_shape": ms_shapes,
+            "graph": info["graph"], "solver_blocks": info["solver_blocks"], "steps": args.ensemble_steps,
+            "setup_s": setup_s}
+
+
 def run_e2e(pic, steps, n_part, it0):
     """Same metric through the public C ABI with host buffers: import both
     species from host Points, K x (zero rho, deposit, read rho to host, push),
@@ -517,6 +565,8 @@ def main():
                                              device_id=torch.device(f"cuda:{local_rank}"))
     line, pic, w = run_ours(args, rank, world, local_rank)
     pic.close()
+    if not args.no_ensemble and args.config == "cfg3":
+        line["ensemble"] = run_ensemble(args, rank)
     if rank == 0 and not args.no_cpu_baseline:
         scale = 4 if w.nx >= 512 else 1
         value, pois_ms, sample, threads, _, _ = cpu_reference_run(w, scale, args.cpu_seconds)

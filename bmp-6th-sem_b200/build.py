@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpicb200.so")
-SOURCES = ["context.cu", "particles.cu", "poisson.cu", "compat.cu", "picdat.cu", "noalloc.cu", "warmstart.cu"]
+SOURCES = ["context.cu", "particles.cu", "poisson.cu", "compat.cu", "picdat.cu", "noalloc.cu", "warmstart.cu", "ensemble.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -611,6 +613,72 @@ int pic_profile_read(pic_ctx* c, double* ms, int64_t* calls, int reset) {
         if (reset) {
             c->prof_ms[i] = 0;
             c->prof_calls[i] = 0;
+        }
+    }
+    return PIC_OK;
+}
+
+int pic_set_tile_shape(pic_ctx* c, int shape) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    if (shape < 0 || shape >= particles_num_tile_shapes()) return fail(PIC_ERR_ARG, "unknown tile shape");
+    c->tile_shape = shape;
+    return PIC_OK;
+}
+
+int pic_autotune(pic_ctx* c, int* shape_out, double* ms_per_shape) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    // cache key: device, grid, particles (two significant digits), species
+    int64_t n = 0;
+    for (int s = 0; s < c->cfg.num_species; ++s) {
+        int64_t m = 0;
+        PIC_TRY(particles_count(c, s, &m));
+        n += m;
+    }
+    cudaDeviceProp prop{};
+    PIC_CUDA(cudaGetDeviceProperties(&prop, c->device));
+    int64_t rounded = n;
+    int64_t scale = 1;
+    while (rounded >= 100) {
+        rounded /= 10;
+        scale *= 10;
+    }
+    std::string dev(prop.name);
+    for (char& ch : dev)
+        if (ch == ' ') ch = '_';
+    char key[256];
+    std::snprintf(key, sizeof(key), "%s %d %d %lld %d", dev.c_str(), c->nx, c->ny,
+                  (long long)(rounded * scale), c->cfg.num_species);
+    const char* path = std::getenv("PIC_TUNE_CACHE");
+    const int nshapes = particles_num_tile_shapes();
+    if (path && !ms_per_shape) {
+        if (FILE* f = std::fopen(path, "r")) {
+            char line[512];
+            int found = -1;
+            while (std::fgets(line, sizeof(line), f)) {
+                const size_t kl = std::strlen(key);
+                if (std::strncmp(line, key, kl) == 0 && line[kl] == ' ') found = std::atoi(line + kl + 1);
+            }
+            std::fclose(f);
+            if (found >= 0 && found < nshapes) {
+                c->tile_shape = found;
+                if (shape_out) *shape_out = found;
+                return PIC_OK;
+            }
+        }
+    }
+    std::vector<double> ms((size_t)nshapes, 0.0);
+    PIC_TRY(particles_time_shapes(c, 3, ms.data()));
+    int best = 0;
+    for (int k = 1; k < nshapes; ++k)
+        if (ms[k] < ms[best]) best = k;
+    c->tile_shape = best;
+    if (shape_out) *shape_out = best;
+    if (ms_per_shape)
+        for (int k = 0; k < nshapes; ++k) ms_per_shape[k] = ms[k];
+    if (path) {
+        if (FILE* f = std::fopen(path, "a")) {
+            std::fprintf(f, "%s %d\n", key, best);
+            std::fclose(f);
         }
     }
     return PIC_OK;

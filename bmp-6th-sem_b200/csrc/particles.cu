@@ -362,9 +362,6 @@ __device__ __forceinline__ void list_append(const ListDev& L, bool on, uint32_t 
 // chunks ahead of the one being processed -- across cell boundaries, so the
 // load pipeline never drains.
 constexpr int kDepth = 4;
-constexpr int kTileCells = kTileX * kTileY;
-constexpr int kTileNodesX = kTileX + 1;
-constexpr int kTileNodes = (kTileX + 1) * (kTileY + 1);
 
 struct CellMeta {
     uint32_t b0, b1, nf, nb;
@@ -425,15 +422,19 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q, int 
     list_append(A.ovf, spill, t, p, vz, lt, lane, A.counters + 2);
 }
 
-template <int MODE, bool ENERGY>
-__global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
+template <int MODE, bool ENERGY, int TX, int TY>
+__device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_y) {
+    constexpr int kTileX = TX, kTileY = TY;
+    constexpr int kTileCells = kTileX * kTileY;
+    constexpr int kTileNodesX = kTileX + 1;
+    constexpr int kTileNodes = (kTileX + 1) * (kTileY + 1);
     __shared__ CellMeta s_meta[kTileCells];
     __shared__ float4 s_fld[MODE == kPush ? kTileNodes : 1];
     __shared__ MoverQueue s_q[MODE == kPush ? kWarps : 1];
     __shared__ float4 s_ring_a[kWarps][kDepth][32];
     __shared__ float s_ring_vz[kWarps][kDepth][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tgx0 = blockIdx.x * kTileX, tgy0 = blockIdx.y * kTileY;
+    const int tgx0 = tile_x * kTileX, tgy0 = tile_y * kTileY;
     const unsigned lt = lanemask_lt();
     for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
         const int gx = tgx0 + (i % kTileX), gy = tgy0 + (i / kTileX);
@@ -578,6 +579,33 @@ __global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
     }
     if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, queued, lane, lt);
     if (MODE == kPush && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
+}
+
+// Tile shapes the kernels are built for (cells per block in x, y); every
+// shape has 256 cells.
+#define PIC_TILE_SHAPES(X) X(64, 4) X(32, 8) X(128, 2) X(16, 16)
+constexpr int kNumTileShapes = 4;
+constexpr int kTileShapeX[kNumTileShapes] = {64, 32, 128, 16};
+constexpr int kTileShapeY[kNumTileShapes] = {4, 8, 2, 16};
+
+template <int MODE, bool ENERGY, int TX, int TY>
+__global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
+    cells_body<MODE, ENERGY, TX, TY>(A, blockIdx.x, blockIdx.y);
+}
+
+// One launch over many instances: block b works on tile (work[b].y & 0xffff,
+// work[b].y >> 16) of instance work[b].x, whose arguments are args[work[b].x].
+template <int MODE, bool ENERGY, int TX, int TY>
+__global__ void __launch_bounds__(kThreads, 4) k_cells_batch(const KArgs* __restrict__ args,
+                                                             const uint2* __restrict__ work) {
+    __shared__ KArgs s_args;
+    const uint2 w = work[blockIdx.x];
+    static_assert(sizeof(KArgs) % 8 == 0, "KArgs copy");
+    for (int i = threadIdx.x; i < (int)(sizeof(KArgs) / 8); i += kThreads)
+        reinterpret_cast<unsigned long long*>(&s_args)[i] =
+            reinterpret_cast<const unsigned long long*>(args + w.x)[i];
+    __syncthreads();
+    cells_body<MODE, ENERGY, TX, TY>(s_args, (int)(w.y & 0xffffu), (int)(w.y >> 16));
 }
 
 // ---- side lists ---------------------------------------------------------------
@@ -1042,8 +1070,49 @@ KArgs make_args(pic_ctx* c, Species& sp) {
     return A;
 }
 
-dim3 tile_grid(pic_ctx* c) {
-    return dim3((unsigned)((c->nx + kTileX - 1) / kTileX), (unsigned)((c->ny + kTileY - 1) / kTileY));
+dim3 tile_grid(const pic_ctx* c, int shape) {
+    return dim3((unsigned)((c->nx + kTileShapeX[shape] - 1) / kTileShapeX[shape]),
+                (unsigned)((c->ny + kTileShapeY[shape] - 1) / kTileShapeY[shape]));
+}
+
+// Launch of k_cells with the tile shape `shape` (index into kTileShape*).
+template <int MODE, bool ENERGY>
+void launch_cells(int shape, dim3 grid, cudaStream_t st, const KArgs& A) {
+    switch (shape) {
+        case 1: k_cells<MODE, ENERGY, 32, 8><<<grid, kThreads, 0, st>>>(A); break;
+        case 2: k_cells<MODE, ENERGY, 128, 2><<<grid, kThreads, 0, st>>>(A); break;
+        case 3: k_cells<MODE, ENERGY, 16, 16><<<grid, kThreads, 0, st>>>(A); break;
+        default: k_cells<MODE, ENERGY, 64, 4><<<grid, kThreads, 0, st>>>(A); break;
+    }
+}
+
+template <int MODE, bool ENERGY>
+void launch_cells_batch(int shape, unsigned nblocks, cudaStream_t st, const KArgs* args,
+                        const uint2* work) {
+    switch (shape) {
+        case 1: k_cells_batch<MODE, ENERGY, 32, 8><<<nblocks, kThreads, 0, st>>>(args, work); break;
+        case 2: k_cells_batch<MODE, ENERGY, 128, 2><<<nblocks, kThreads, 0, st>>>(args, work); break;
+        case 3: k_cells_batch<MODE, ENERGY, 16, 16><<<nblocks, kThreads, 0, st>>>(args, work); break;
+        default: k_cells_batch<MODE, ENERGY, 64, 4><<<nblocks, kThreads, 0, st>>>(args, work); break;
+    }
+}
+
+template <typename K>
+cudaError_t max_shared(K k) {
+    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+}
+
+// Four blocks of the particle kernels per SM need ~4 x 44 KB of shared memory.
+template <int MODE, bool ENERGY>
+cudaError_t carveouts() {
+    cudaError_t e = cudaSuccess;
+#define PIC_CARVE(TX, TY)                                                           \
+    if (e == cudaSuccess) e = max_shared(k_cells<MODE, ENERGY, TX, TY>);           \
+    if (e == cudaSuccess) e = max_shared(k_cells_batch<MODE, ENERGY, TX, TY>);
+    PIC_TILE_SHAPES(PIC_CARVE)
+#undef PIC_CARVE
+    return e;
 }
 
 int check_flags(pic_ctx* c, Species& sp, bool sync);
@@ -1127,15 +1196,10 @@ int species_setup(pic_ctx* c, int s) {
     PIC_TRY(scan_cells<true>(c, sp, sp.cnt, sp.base, &total));
     PIC_TRY(grow_store(c, s, total));
     PIC_TRY(grow_lists(c, s));
-    // four blocks of the particle kernels per SM need 4 x 44 KB of shared memory
-    PIC_CUDA(cudaFuncSetAttribute(k_cells<kPush, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    PIC_CUDA(cudaFuncSetAttribute(k_cells<kPush, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    PIC_CUDA(cudaFuncSetAttribute(k_cells<kDeposit, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    PIC_CUDA(cudaFuncSetAttribute(k_cells<kDeposit, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
+    PIC_CUDA((carveouts<kPush, true>()));
+    PIC_CUDA((carveouts<kPush, false>()));
+    PIC_CUDA((carveouts<kDeposit, true>()));
+    PIC_CUDA((carveouts<kDeposit, false>()));
     sp.acc_fresh = true;  // zero particles: the zero accumulator is their deposit
     return PIC_OK;
 }
@@ -1462,12 +1526,13 @@ int particles_deposit(pic_ctx* c, int s) {
     const bool energy = c->cfg.deposit_energy != 0;
     const ListDev L = list_dev(sp.loose[sp.lcur]);
     prof_begin(c, PIC_PHASE_DEPOSIT);
+    const int sh = c->tile_shape;
     if (energy) {
-        k_cells<kDeposit, true><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+        launch_cells<kDeposit, true>(sh, tile_grid(c, sh), c->stream, A);
         k_list_deposit<true><<<kFixupBlocks, 256, 0, c->stream>>>(L, c->nx, c->GX, sp.k.half_inv_abs_qm,
                                                                   sp.acc_q, sp.acc_e);
     } else {
-        k_cells<kDeposit, false><<<tile_grid(c), kThreads, 0, c->stream>>>(A);
+        launch_cells<kDeposit, false>(sh, tile_grid(c, sh), c->stream, A);
         k_list_deposit<false><<<kFixupBlocks, 256, 0, c->stream>>>(L, c->nx, c->GX, sp.k.half_inv_abs_qm,
                                                                    sp.acc_q, sp.acc_e);
     }
@@ -1507,7 +1572,8 @@ int particles_push(pic_ctx* c, int s) {
         prof_end(c, PIC_PHASE_RELAYOUT);
     }
     KArgs A = make_args(c, sp);
-    const dim3 g = tile_grid(c);
+    const int sh = c->tile_shape;
+    const dim3 g = tile_grid(c, sh);
     const bool energy = c->cfg.deposit_energy != 0;
     const int dst = sp.cur ^ 1;
     PIC_CUDA(cudaMemsetAsync(sp.back[dst], 0, (size_t)c->ncells * 4, c->stream));
@@ -1516,9 +1582,9 @@ int particles_push(pic_ctx* c, int s) {
     PIC_CUDA(cudaMemsetAsync(sp.acc_e, 0, (size_t)c->nodes * 8, c->stream));
     prof_begin(c, PIC_PHASE_PUSH);
     if (energy)
-        k_cells<kPush, true><<<g, kThreads, 0, c->stream>>>(A);
+        launch_cells<kPush, true>(sh, g, c->stream, A);
     else
-        k_cells<kPush, false><<<g, kThreads, 0, c->stream>>>(A);
+        launch_cells<kPush, false>(sh, g, c->stream, A);
     prof_end(c, PIC_PHASE_PUSH);
     PIC_CUDA(cudaGetLastError());
     FixArgs F{};
@@ -1560,6 +1626,445 @@ int particles_push(pic_ctx* c, int s) {
     sp.flags_pending = true;
     sp.acc_fresh = true;
     return PIC_OK;
+}
+
+}  // namespace picb200
+
+// ---------------------------------------------------------------------------
+// Tile-shape autotuning
+// ---------------------------------------------------------------------------
+namespace picb200 {
+
+int particles_num_tile_shapes() { return kNumTileShapes; }
+
+// Times `reps` push passes of every species with each tile shape on the
+// current particles, without committing them (no buffer swap, no side-list
+// placement), then restores what the passes touched: the side-list count,
+// the counters, and the accumulators (marked stale, so the next
+// charge_deposition redeposits).  ms[k] = mean milliseconds of one pass over
+// all species with shape k.
+int particles_time_shapes(pic_ctx* c, int reps, double* ms) {
+    if (!c->fields_valid) PIC_TRY(fields_from_phi(c));
+    const int ns = c->cfg.num_species;
+    unsigned long long* saved = nullptr;
+    PIC_CUDA(cudaMalloc(&saved, (size_t)ns * 4 * sizeof(unsigned long long)));
+    for (int s = 0; s < ns; ++s)
+        PIC_CUDA(cudaMemcpyAsync(saved + 4 * s, c->sp[s].counters, 4 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PIC_CUDA(cudaEventCreate(&e0));
+    PIC_CUDA(cudaEventCreate(&e1));
+    int status = PIC_OK;
+    const bool energy = c->cfg.deposit_energy != 0;
+    for (int sh = 0; sh < kNumTileShapes && status == PIC_OK; ++sh) {
+        float total = 0.f;
+        for (int r = -1; r < reps; ++r) {  // r = -1: warm-up
+            cudaEventRecord(e0, c->stream);
+            for (int s = 0; s < ns; ++s) {
+                Species& sp = c->sp[s];
+                KArgs A = make_args(c, sp);
+                cudaMemsetAsync(sp.back[sp.cur ^ 1], 0, (size_t)c->ncells * 4, c->stream);
+                cudaMemsetAsync(sp.list_counts + kOvf, 0, sizeof(uint32_t), c->stream);
+                if (energy)
+                    launch_cells<kPush, true>(sh, tile_grid(c, sh), c->stream, A);
+                else
+                    launch_cells<kPush, false>(sh, tile_grid(c, sh), c->stream, A);
+            }
+            cudaEventRecord(e1, c->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+                status = fail(PIC_ERR_CUDA, "autotune: push launch failed");
+                break;
+            }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r >= 0) total += t;
+        }
+        if (ms) ms[sh] = total / (float)std::max(reps, 1);
+    }
+    for (int s = 0; s < ns; ++s) {
+        Species& sp = c->sp[s];
+        cudaMemcpyAsync(sp.counters, saved + 4 * s, 4 * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToDevice, c->stream);
+        cudaMemsetAsync(sp.list_counts + kOvf, 0, sizeof(uint32_t), c->stream);
+        sp.acc_fresh = false;
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(saved);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PIC_CUDA(cudaGetLastError());
+    return status;
+}
+
+}  // namespace picb200
+
+// ---------------------------------------------------------------------------
+// Batched particle phases: one launch per phase over the contexts of an
+// ensemble (same device, same stream).  Per-instance arguments live in
+// device tables rebuilt by the host before each step; the kernels only read
+// them, so a captured step replays with the tables of the next step.
+// ---------------------------------------------------------------------------
+namespace picb200 {
+namespace {
+
+struct ZeroEntry {
+    uint32_t* ptr;
+    uint64_t words;  // 4-byte words
+};
+
+__global__ void k_batch_zero(const ZeroEntry* __restrict__ e, int n) {
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
+    for (int i = 0; i < n; ++i) {
+        const ZeroEntry z = e[i];
+        for (int64_t w = gtid; w < (int64_t)z.words; w += gsize) z.ptr[w] = 0u;
+    }
+}
+
+struct FlushEntry {
+    int64_t nodes;
+    unsigned long long* acc_q;
+    unsigned long long* acc_e;
+    double qscale, escale, chrg;
+    double* final_mesh;
+    double* energy_mesh;
+    double* rho;
+    int energy;
+};
+
+__global__ void k_batch_flush(const FlushEntry* __restrict__ e, int n) {
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
+    for (int i = 0; i < n; ++i) {
+        const FlushEntry F = e[i];
+        for (int64_t k = gtid; k < F.nodes; k += gsize) {
+            const double f = (double)F.acc_q[k] * F.qscale;
+            F.acc_q[k] = 0ull;
+            F.final_mesh[k] = f;
+            if (F.energy) {
+                F.energy_mesh[k] = (double)F.acc_e[k] * F.escale;
+                F.acc_e[k] = 0ull;
+            } else {
+                F.energy_mesh[k] = 0.0;
+            }
+            F.rho[k] += f * F.chrg;
+        }
+    }
+}
+
+constexpr int kFixupBlocksPerInstance = 4;
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_fixup_batch(const FixArgs* __restrict__ args) {
+    // the single-instance body reads blockIdx.x / gridDim.x: emulate them
+    const int inst = blockIdx.x / kFixupBlocksPerInstance;
+    const FixArgs F = args[inst];
+    const uint32_t n_prev = min(*F.prev.count, F.prev.cap);
+    const uint32_t n_ovf = min(*F.ovf.count, F.ovf.cap);
+    const uint32_t total = n_prev + n_ovf;
+    const uint32_t b = blockIdx.x % kFixupBlocksPerInstance;
+    for (uint32_t i = b * blockDim.x + threadIdx.x; i < total; i += kFixupBlocksPerInstance * blockDim.x) {
+        Pushed p;
+        float vz;
+        uint32_t t;
+        if (i < n_prev) {
+            const uint32_t c = F.prev.cell[i];
+            const int gx = (int)(c % (uint32_t)F.nx), gy = (int)(c / (uint32_t)F.nx);
+            const int64_t n0 = (int64_t)gy * F.GX + gx;
+            vz = F.prev.vz[i];
+            p = push_one(F.prev.a[i], F.fld[n0], F.fld[n0 + 1], F.fld[n0 + F.GX], F.fld[n0 + F.GX + 1],
+                         F.k, gx, gy, F.nx, F.ny);
+            if (p.dir < 0) {
+                if (p.left) atomicAdd(F.counters, 1ull);
+                continue;
+            }
+            const float en = ENERGY ? energy_ev(p.vx, p.vy, vz, F.k.half_inv_abs_qm) : 0.f;
+            deposit_one<ENERGY>(F.acc_q, F.acc_e, F.GX, (uint32_t)(p.gy * F.GX + p.gx), p.fx, p.fy, en);
+            t = (uint32_t)(p.gy * F.nx + p.gx);
+        } else {
+            const uint32_t e = i - n_prev;
+            const float4 a = F.ovf.a[e];
+            p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
+            vz = F.ovf.vz[e];
+            t = F.ovf.cell[e];
+        }
+        const uint32_t lim = (F.base[t + 1] - F.base[t]) - F.front[t];
+        const uint32_t k = atomicAdd(F.back + t, 1u);
+        if (k < lim) {
+            store_slot(F.dst_a, F.dst_vz, F.base[t + 1] - 1u - k, p, vz);
+        } else {
+            atomicSub(F.back + t, 1u);
+            const uint32_t s = atomicAdd(F.next.count, 1u);
+            if (s < F.next.cap) {
+                F.next.a[s] = make_float4(p.fx, p.fy, p.vx, p.vy);
+                F.next.vz[s] = vz;
+                F.next.cell[s] = t;
+            } else {
+                atomicOr(F.counters + 2, 1ull);
+            }
+        }
+    }
+}
+
+// flags[i] = {loose count (new current list), left exits lo/hi, cell-limit, lost}
+struct FlagEntry {
+    const uint32_t* loose_count;
+    const unsigned long long* counters;
+};
+
+__global__ void k_batch_flags(const FlagEntry* __restrict__ e, int n, unsigned long long* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[4 * i] = *e[i].loose_count;
+    out[4 * i + 1] = e[i].counters[0];
+    out[4 * i + 2] = e[i].counters[1];
+    out[4 * i + 3] = e[i].counters[2];
+}
+
+}  // namespace
+
+struct ParticleBatchImpl {
+    int n = 0, ns = 0;
+    uint2* work[kNumTileShapes] = {};
+    unsigned nblocks[kNumTileShapes] = {};
+    KArgs* d_args = nullptr;      // [ns][n]
+    FixArgs* d_fix = nullptr;     // [ns][n]
+    FlushEntry* d_flush = nullptr;  // [ns][n]
+    ZeroEntry* d_zero = nullptr;  // [ns][3n] before each push, [ns][2n] after, [n] rho
+    FlagEntry* d_flagsrc = nullptr;  // [ns][n]
+    unsigned long long* d_flags = nullptr;  // [ns][n][4]
+    // pinned host mirrors (one upload per step)
+    char* h_tables = nullptr;
+    char* d_tables = nullptr;
+    size_t table_bytes = 0;
+    unsigned long long* h_flags = nullptr;
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int batch_create(pic_ctx** cs, int n, ParticleBatchImpl** out) {
+    auto* B = new ParticleBatchImpl();
+    *out = B;
+    B->n = n;
+    B->ns = cs[0]->cfg.num_species;
+    for (int sh = 0; sh < kNumTileShapes; ++sh) {
+        std::vector<uint2> w;
+        for (int i = 0; i < n; ++i) {
+            const dim3 g = tile_grid(cs[i], sh);
+            for (unsigned y = 0; y < g.y; ++y)
+                for (unsigned x = 0; x < g.x; ++x) w.push_back(make_uint2((uint32_t)i, x | (y << 16)));
+        }
+        B->nblocks[sh] = (unsigned)w.size();
+        PIC_CUDA(cudaMalloc(&B->work[sh], w.size() * sizeof(uint2)));
+        PIC_CUDA(cudaMemcpy(B->work[sh], w.data(), w.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    const int ns = B->ns;
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(bytes);
+        return o;
+    };
+    const size_t o_args = carve(sizeof(KArgs) * ns * n), o_fix = carve(sizeof(FixArgs) * ns * n);
+    const size_t o_flush = carve(sizeof(FlushEntry) * ns * n), o_zero = carve(sizeof(ZeroEntry) * (ns * 5 * n + n));
+    const size_t o_flag = carve(sizeof(FlagEntry) * ns * n);
+    B->table_bytes = off;
+    PIC_CUDA(cudaMalloc(&B->d_tables, off));
+    PIC_CUDA(cudaMallocHost(&B->h_tables, off));
+    std::memset(B->h_tables, 0, off);
+    B->d_args = reinterpret_cast<KArgs*>(B->d_tables + o_args);
+    B->d_fix = reinterpret_cast<FixArgs*>(B->d_tables + o_fix);
+    B->d_flush = reinterpret_cast<FlushEntry*>(B->d_tables + o_flush);
+    B->d_zero = reinterpret_cast<ZeroEntry*>(B->d_tables + o_zero);
+    B->d_flagsrc = reinterpret_cast<FlagEntry*>(B->d_tables + o_flag);
+    PIC_CUDA(cudaMalloc(&B->d_flags, sizeof(unsigned long long) * 4 * ns * n));
+    PIC_CUDA(cudaMallocHost(&B->h_flags, sizeof(unsigned long long) * 4 * ns * n));
+    std::memset(B->h_flags, 0, sizeof(unsigned long long) * 4 * ns * n);
+    return PIC_OK;
+}
+
+void batch_destroy(ParticleBatchImpl* B) {
+    if (!B) return;
+    for (auto* w : B->work) cudaFree(w);
+    cudaFree(B->d_tables);
+    cudaFree(B->d_flags);
+    if (B->h_tables) cudaFreeHost(B->h_tables);
+    if (B->h_flags) cudaFreeHost(B->h_flags);
+    delete B;
+}
+
+// Host part before a step: side-list checks (and rare re-layouts) per
+// instance, then the tables of this step, uploaded on `st`.
+int batch_prepare(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st) {
+    const int n = B->n, ns = B->ns;
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < ns; ++s) {
+            Species& sp = cs[i]->sp[s];
+            const unsigned long long* f = B->h_flags + 4 * ((size_t)s * n + i);
+            if (f[2]) return fail(PIC_ERR_CAPACITY, "a cell exceeds the per-cell particle limit");
+            if (f[3]) return fail(PIC_ERR_CAPACITY, "particle side list overflowed: particles were lost");
+            if (f[0] > sp.loose[0].cap / 8u) {
+                PIC_TRY(relayout(cs[i], s));
+                B->h_flags[4 * ((size_t)s * n + i)] = 0;
+            }
+        }
+    const size_t o_args = 0, o_fix = align256(sizeof(KArgs) * ns * n);
+    const size_t o_flush = o_fix + align256(sizeof(FixArgs) * ns * n);
+    const size_t o_zero = o_flush + align256(sizeof(FlushEntry) * ns * n);
+    const size_t o_flag = o_zero + align256(sizeof(ZeroEntry) * (ns * 5 * n + n));
+    KArgs* ha = reinterpret_cast<KArgs*>(B->h_tables + o_args);
+    FixArgs* hf = reinterpret_cast<FixArgs*>(B->h_tables + o_fix);
+    FlushEntry* hl = reinterpret_cast<FlushEntry*>(B->h_tables + o_flush);
+    ZeroEntry* hz = reinterpret_cast<ZeroEntry*>(B->h_tables + o_zero);
+    FlagEntry* hg = reinterpret_cast<FlagEntry*>(B->h_tables + o_flag);
+    for (int i = 0; i < n; ++i) {
+        pic_ctx* c = cs[i];
+        hz[(size_t)ns * 5 * n + i] = ZeroEntry{reinterpret_cast<uint32_t*>(c->rho), (uint64_t)c->nodes * 2};
+        for (int s = 0; s < ns; ++s) {
+            Species& sp = c->sp[s];
+            const size_t k = (size_t)s * n + i;
+            const int dst = sp.cur ^ 1;
+            ha[k] = make_args(c, sp);
+            FixArgs& F = hf[k];
+            F = FixArgs{};
+            F.nx = c->nx;
+            F.ny = c->ny;
+            F.GX = c->GX;
+            F.k = push_consts(c, sp);
+            F.fld = c->fld;
+            F.dst_a = sp.buf[dst].a;
+            F.dst_vz = sp.buf[dst].vz;
+            F.base = sp.base;
+            F.front = sp.front[dst];
+            F.back = sp.back[dst];
+            F.ovf = list_dev(sp.ovf);
+            F.prev = list_dev(sp.loose[sp.lcur]);
+            F.next = list_dev(sp.loose[sp.lcur ^ 1]);
+            F.acc_q = sp.acc_q;
+            F.acc_e = sp.acc_e;
+            F.counters = sp.counters;
+            const double area = c->dx * c->dy;
+            hl[k] = FlushEntry{c->nodes, sp.acc_q, sp.acc_e, kChargeUnit * area * sp.weighing,
+                               kEnergyUnit * area * sp.weighing, -sp.desc.charge / c->cfg.epsilon,
+                               sp.final_mesh, sp.energy_mesh, c->rho, c->cfg.deposit_energy ? 1 : 0};
+            // before the push: back counts of the new buffer, the accumulators
+            ZeroEntry* zb = hz + (size_t)s * 5 * n;
+            zb[i] = ZeroEntry{sp.back[dst], (uint64_t)c->ncells};
+            zb[n + i] = ZeroEntry{reinterpret_cast<uint32_t*>(sp.acc_q), (uint64_t)c->nodes * 2};
+            zb[2 * n + i] = ZeroEntry{reinterpret_cast<uint32_t*>(sp.acc_e), (uint64_t)c->nodes * 2};
+            // after the fix-up: the consumed side lists
+            zb[3 * n + i] = ZeroEntry{sp.list_counts + kOvf, 1};
+            zb[4 * n + i] = ZeroEntry{sp.list_counts + kLoose0 + sp.lcur, 1};
+            hg[k] = FlagEntry{sp.list_counts + kLoose0 + (sp.lcur ^ 1), sp.counters};
+        }
+    }
+    PIC_CUDA(cudaMemcpyAsync(B->d_tables, B->h_tables, B->table_bytes, cudaMemcpyHostToDevice, st));
+    return PIC_OK;
+}
+
+// zero rho of every instance; flush the accumulators of every species into
+// final/energy mesh and rho (charge_deposition).
+int batch_deposit(ParticleBatchImpl* B, cudaStream_t st) {
+    const int n = B->n, ns = B->ns;
+    k_batch_zero<<<296, 256, 0, st>>>(B->d_zero + (size_t)ns * 5 * n, n);
+    k_batch_flush<<<296, 256, 0, st>>>(B->d_flush, ns * n);
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+// push every species of every instance, then gather the side-list counts and
+// flags for the host (copied into B->h_flags on `st`).
+int batch_push(ParticleBatchImpl* B, int shape, bool energy, cudaStream_t st) {
+    const int n = B->n, ns = B->ns;
+    for (int s = 0; s < ns; ++s) {
+        k_batch_zero<<<296, 256, 0, st>>>(B->d_zero + (size_t)s * 5 * n, 3 * n);
+        if (energy)
+            launch_cells_batch<kPush, true>(shape, B->nblocks[shape], st, B->d_args + (size_t)s * n, B->work[shape]);
+        else
+            launch_cells_batch<kPush, false>(shape, B->nblocks[shape], st, B->d_args + (size_t)s * n, B->work[shape]);
+        if (energy)
+            k_fixup_batch<true><<<n * kFixupBlocksPerInstance, 256, 0, st>>>(B->d_fix + (size_t)s * n);
+        else
+            k_fixup_batch<false><<<n * kFixupBlocksPerInstance, 256, 0, st>>>(B->d_fix + (size_t)s * n);
+        k_batch_zero<<<1, 256, 0, st>>>(B->d_zero + (size_t)s * 5 * n + 3 * n, 2 * n);
+    }
+    k_batch_flags<<<(ns * n + 127) / 128, 128, 0, st>>>(B->d_flagsrc, ns * n, B->d_flags);
+    PIC_CUDA(cudaMemcpyAsync(B->h_flags, B->d_flags, sizeof(unsigned long long) * 4 * ns * n,
+                             cudaMemcpyDeviceToHost, st));
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+// Host bookkeeping after a step (the buffers and lists every push flips).
+void batch_commit(pic_ctx** cs, int n) {
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < cs[i]->cfg.num_species; ++s) {
+            Species& sp = cs[i]->sp[s];
+            sp.cur ^= 1;
+            sp.lcur ^= 1;
+            sp.acc_fresh = true;
+            sp.flags_pending = false;
+        }
+}
+
+}  // namespace picb200
+
+namespace picb200 {
+
+// Times `reps` batched push passes of all species with each tile shape on the
+// current particles of every instance, without committing them; restores
+// the counters and side-list counts the passes touched and marks the
+// accumulators stale.  Tables must be prepared (batch_prepare).
+int batch_time_shapes(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st, int reps, bool energy,
+                      double* ms) {
+    const int n = B->n, ns = B->ns;
+    unsigned long long* saved = nullptr;
+    PIC_CUDA(cudaMalloc(&saved, (size_t)n * ns * 4 * sizeof(unsigned long long)));
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < ns; ++s)
+            PIC_CUDA(cudaMemcpyAsync(saved + 4 * ((size_t)i * ns + s), cs[i]->sp[s].counters,
+                                     4 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PIC_CUDA(cudaEventCreate(&e0));
+    PIC_CUDA(cudaEventCreate(&e1));
+    int status = PIC_OK;
+    for (int sh = 0; sh < kNumTileShapes && status == PIC_OK; ++sh) {
+        float total = 0.f;
+        for (int r = -1; r < reps; ++r) {
+            cudaEventRecord(e0, st);
+            for (int s = 0; s < ns; ++s) {
+                k_batch_zero<<<296, 256, 0, st>>>(B->d_zero + (size_t)s * 5 * n, 3 * n);
+                k_batch_zero<<<1, 256, 0, st>>>(B->d_zero + (size_t)s * 5 * n + 3 * n, n);  // ovf counts
+                if (energy)
+                    launch_cells_batch<kPush, true>(sh, B->nblocks[sh], st, B->d_args + (size_t)s * n, B->work[sh]);
+                else
+                    launch_cells_batch<kPush, false>(sh, B->nblocks[sh], st, B->d_args + (size_t)s * n, B->work[sh]);
+            }
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+                status = fail(PIC_ERR_CUDA, "autotune: batched push launch failed");
+                break;
+            }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r >= 0) total += t;
+        }
+        if (ms) ms[sh] = total / (float)std::max(reps, 1);
+    }
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < ns; ++s) {
+            Species& sp = cs[i]->sp[s];
+            cudaMemcpyAsync(sp.counters, saved + 4 * ((size_t)i * ns + s), 4 * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToDevice, st);
+            cudaMemsetAsync(sp.list_counts + kOvf, 0, sizeof(uint32_t), st);
+            sp.acc_fresh = false;
+        }
+    cudaStreamSynchronize(st);
+    cudaFree(saved);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PIC_CUDA(cudaGetLastError());
+    return status;
 }
 
 }  // namespace picb200

@@ -54,9 +54,7 @@ constexpr uint32_t kMaxPerCell = 1u << 16;
 // ---------------------------------------------------------------------------
 // Particle kernel tiling
 // ---------------------------------------------------------------------------
-constexpr int kTileX = 64;  // cells per block in x
-constexpr int kTileY = 4;   // cells per block in y
-constexpr int kWarps = 8;   // 256 threads per block
+constexpr int kWarps = 8;   // 256 threads per block (a tile of 256 cells)
 
 struct SpeciesConsts {
     float h;          // 0.5*(q/m)*dt
@@ -191,6 +189,7 @@ struct pic_ctx {
     picb200::Species sp[PIC_MAX_SPECIES];
     picb200::PoissonState ps;
     bool fields_valid = false;
+    int tile_shape = 0;            // particle-kernel tile shape (see particles.cu)
     bool bz_uniform = true;        // every node has the same Bz (bz_value)
     double bz_value = 0.0;
     // instrumentation
@@ -233,6 +232,18 @@ int particles_flush_rho(pic_ctx* c, int s);     // acc -> final/energy mesh, rho
 int particles_push(pic_ctx* c, int s);          // pass1 + scan + pass2 (+deposit)
 int particles_count(pic_ctx* c, int s, int64_t* n);
 int particles_bin_counts(pic_ctx* c, int s, int32_t* dev_counts);
+// batched particle phases over an ensemble's contexts (particles.cu)
+struct ParticleBatchImpl;
+int batch_create(pic_ctx** cs, int n, ParticleBatchImpl** out);
+void batch_destroy(ParticleBatchImpl* B);
+int batch_prepare(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st);
+int batch_deposit(ParticleBatchImpl* B, cudaStream_t st);
+int batch_push(ParticleBatchImpl* B, int shape, bool energy, cudaStream_t st);
+void batch_commit(pic_ctx** cs, int n);
+int batch_time_shapes(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st, int reps, bool energy,
+                      double* ms);
+int particles_num_tile_shapes();
+int particles_time_shapes(pic_ctx* c, int reps, double* ms);  // ms[particles_num_tile_shapes()]
 
 // warmstart.cu
 void ws_free(pic_ctx* c);
@@ -247,5 +258,15 @@ int poisson_solve(pic_ctx* c);
 int fields_from_phi(pic_ctx* c);
 int efield_export(pic_ctx* c);
 int fields_set_bz(pic_ctx* c);
+// batched solve of many contexts (poisson.cu)
+size_t poisson_batch_desc_bytes();
+size_t poisson_batch_max_fused_smem();
+int poisson_batch_describe(pic_ctx* c, void* host_desc, const void* dev_fused, int blk0, int nblk);
+const void* poisson_fused_table(pic_ctx* c, size_t* bytes);
+size_t poisson_fused_smem(pic_ctx* c);
+int poisson_batch_blocks(size_t smem, int* blocks);
+int poisson_batch_launch(const void* dev_insts, int n, const int* inst_of, double* partials,
+                         unsigned* barriers, int* err, size_t smem, int blocks, cudaStream_t st);
+int poisson_batch_finish(pic_ctx* c, const double* scal, float ms);
 
 }  // namespace picb200

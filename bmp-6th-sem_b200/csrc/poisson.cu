@@ -38,6 +38,7 @@
 // test kernel sets the condition on the device, so a solve costs one graph
 // launch and one host synchronisation.  Without conditional-node support the
 // same kernels run from a host loop.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -395,8 +396,7 @@ struct FusedLevels {
     int sweeps;
 };
 
-__global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* smem) {
     auto X = [&](int l) { return reinterpret_cast<float*>(smem + F.ox[l]); };
     auto B = [&](int l) { return reinterpret_cast<float*>(smem + F.ob[l]); };
     auto M = [&](int l) { return reinterpret_cast<uint8_t*>(smem + F.om[l]); };
@@ -503,6 +503,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
         const int n = F.GX[0] * F.GY[0];
         for (int k = tid; k < n; k += kFusedThreads) F.gx[k] = X(0)[k];
     }
+}
+
+__global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    fused_body(F, smem);
 }
 
 // injected Dirichlet mask of a coarse level
@@ -933,6 +938,492 @@ int fields_set_bz(pic_ctx* c) {
     k_set_bz_field<<<(unsigned)((c->nodes + 255) / 256), 256, 0, c->stream>>>(c->bz, c->nodes,
                                                                               c->fld);
     PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
+}  // namespace picb200
+
+// ---------------------------------------------------------------------------
+// Batched solve: the Poisson solves of many instances (an ensemble) in ONE
+// persistent cooperative launch.  Every phase of the PCG iteration and of the
+// V-cycle loops over the instances that are still iterating, each instance's
+// nodes spread over the whole grid, with grid-wide barriers between phases;
+// an instance's fused coarse levels run in one block (block i for instance
+// i).  Dot products are reduced per warp into a per-instance table and
+// summed by one block per instance in fixed order: deterministic.  The solve
+// ends with the true residual and the E field of every instance.
+// ---------------------------------------------------------------------------
+namespace picb200 {
+namespace {
+
+constexpr int kMaxBatchLevels = 10;
+
+struct BatchInst {
+    int GX, GY;
+    double cx, cy, cd;
+    double dx, dy;
+    int64_t nodes;
+    const uint8_t* mask;
+    const double* dv;
+    double* rho;  // becomes the right-hand side b
+    double* phi;
+    double* r;
+    double* z;
+    double* p;
+    double* q;
+    const double* bz;
+    float4* fld;
+    int kf;  // multigrid levels before the fused ones
+    LevelDev lev[kMaxBatchLevels];  // levels 0 .. kf
+    const FusedLevels* fused;
+    double* scal;
+    double tol2;
+    int maxit;
+    int zero_start;
+    int blk0, nblk;  // the blocks of the launch that work on this instance
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Barrier of the nblk blocks working on one instance: a monotonic arrival
+// counter (zeroed before the launch); the blocks are co-resident (cooperative
+// launch).  The wait is bounded: past kSpinLimit polls the barrier sets
+// *err and lets the block go on, so a fault can never hang the GPU (the
+// host then reports PIC_ERR_TIMEOUT).
+constexpr unsigned kSpinLimit = 1u << 26;
+
+struct GroupBarrier {
+    unsigned* ctr;
+    unsigned target;
+    int nblk;
+    int* err;
+    __device__ __forceinline__ void sync() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            target += (unsigned)nblk;
+            __threadfence();
+            atomicAdd(ctr, 1u);
+            unsigned polls = 0;
+            while (ld_acquire(ctr) < target) {
+                if (++polls > kSpinLimit) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+};
+
+// Blocks blk0 .. blk0+nblk of the launch work on instance inst_of[block] and
+// meet at the instance's own barriers between phases; each instance iterates
+// until its own convergence.
+__global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst* __restrict__ insts,
+                                                                  int n, const int* __restrict__ inst_of,
+                                                                  double* partials, unsigned* barriers,
+                                                                  int* err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_red[2][kFusedThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int me = inst_of[blockIdx.x];  // -1: a spare block
+    if (me < 0) return;
+    const BatchInst* I = insts + me;
+    GroupBarrier grid{barriers + me, 0u, I->nblk, err};
+    const int64_t ltid = (int64_t)(blockIdx.x - I->blk0) * blockDim.x + threadIdx.x;
+    const int64_t lsize = (int64_t)I->nblk * blockDim.x;
+    const bool first = blockIdx.x == I->blk0;
+
+    // block sums of two values -> partials[block][0..1]
+    auto put2 = [&](double a, double b) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(kFull, a, o);
+            b += __shfl_xor_sync(kFull, b, o);
+        }
+        if (lane == 0) {
+            s_red[0][warp] = a;
+            s_red[1][warp] = b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double ta = 0.0, tb = 0.0;
+            for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+                ta += s_red[0][w];
+                tb += s_red[1][w];
+            }
+            partials[2 * blockIdx.x] = ta;
+            partials[2 * blockIdx.x + 1] = tb;
+        }
+    };
+    // the instance's first block: sum of its blocks' partials, fixed order
+    auto total = [&](int v) {
+        double t = 0.0;
+        for (int b = I->blk0; b < I->blk0 + I->nblk; ++b) t += partials[2 * b + v];
+        return t;
+    };
+    auto stencil64 = [&](const double* x, int64_t k) {
+        return I->cd * x[k] - I->cx * (x[k - 1] + x[k + 1]) - I->cy * (x[k - I->GX] + x[k + I->GX]);
+    };
+
+    // overwriteRho and the electrode potentials (zero start: phi = 0 elsewhere)
+    if (I) {
+        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+            if (I->mask[k]) {
+                I->rho[k] = -I->dv[k];
+                I->phi[k] = I->dv[k];
+            } else {
+                I->rho[k] = -I->rho[k];
+                if (I->zero_start) I->phi[k] = 0.0;
+            }
+        }
+    }
+    grid.sync();
+    // r = b - A x, MG input r32; |r|^2 and |b_red|^2
+    if (I) {
+        double rr = 0.0, bb = 0.0;
+        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+            double ri = 0.0;
+            if (!I->mask[k]) {
+                ri = I->rho[k] - stencil64(I->phi, k);
+                const double br = I->rho[k] + I->cx * (dirv(I->mask, I->dv, k - 1) + dirv(I->mask, I->dv, k + 1)) +
+                                  I->cy * (dirv(I->mask, I->dv, k - I->GX) + dirv(I->mask, I->dv, k + I->GX));
+                bb += br * br;
+            }
+            I->r[k] = ri;
+            I->lev[0].b[k] = (float)ri;
+            rr += ri * ri;
+        }
+        put2(rr, bb);
+    }
+    grid.sync();
+    if (first && threadIdx.x == 0) {
+        const double rr = total(0), bb = total(1);
+        I->scal[S_RR] = rr;
+        I->scal[S_BB] = bb;
+        I->scal[S_RZ_OLD] = 0.0;
+        I->scal[S_IT] = 0.0;
+        I->scal[S_STATUS] = 0.0;
+        I->scal[S_COUNT] = (bb > 0.0 && rr > I->tol2 * bb) ? 1.0 : 0.0;  // go on
+    }
+    grid.sync();
+    const int maxkf = I->kf;
+    for (int it = 0; it < I->maxit; ++it) {
+        if (I->scal[S_COUNT] == 0.0) break;  // the same value for all the instance's blocks
+        const bool on = true;
+        // ---- V-cycle: levels above the fused ones ----
+        // one colour of a Gauss-Seidel sweep; four nodes per thread and
+        // round, their loads issued before their stores (memory-level
+        // parallelism: one block per SM)
+        auto half_sweep = [&](int l, int color) {
+            if (on && l < I->kf) {
+                const LevelDev& L = I->lev[l];
+                const int hw = (L.GX + 1) >> 1, n = hw * L.GY, ls = (int)lsize;
+                for (int h0 = (int)ltid; h0 < n; h0 += 4 * ls) {
+                    int k[4];
+                    bool ok[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int h = h0 + u * ls;
+                        const int j = h / hw;
+                        const int x = 2 * (h - j * hw) + ((j + color) & 1);
+                        k[u] = j * L.GX + x;
+                        ok[u] = h < n && x < L.GX;
+                        ok[u] = ok[u] && !L.mask[k[u]];
+                    }
+                    float v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        v[u] = ok[u] ? __fmaf_rn(L.cx, L.x[k[u] - 1] + L.x[k[u] + 1],
+                                                 __fmaf_rn(L.cy, L.x[k[u] - L.GX] + L.x[k[u] + L.GX], L.b[k[u]]))
+                                     : 0.0f;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (ok[u]) L.x[k[u]] = v[u] / L.cd;
+                }
+            }
+            grid.sync();
+        };
+        for (int l = 0; l < maxkf; ++l) {
+            if (on && l < I->kf) {
+                const LevelDev& L = I->lev[l];
+                float* __restrict__ lx = L.x;
+                const float* __restrict__ lb = L.b;
+                const uint8_t* __restrict__ lm = L.mask;
+                const int nn = L.GX * L.GY;
+#pragma unroll 4
+                for (int k = (int)ltid; k < nn; k += (int)lsize) {
+                    const int j = k / L.GX, x = k - j * L.GX;
+                    lx[k] = (((x + j) & 1) == 0 && !lm[k]) ? lb[k] / L.cd : 0.0f;
+                }
+            }
+            grid.sync();
+            half_sweep(l, 1);
+            for (int s = 1; s < kNu; ++s) {
+                half_sweep(l, 0);
+                half_sweep(l, 1);
+            }
+            if (on && l < I->kf) {
+                const LevelDev& F = I->lev[l];
+                const LevelDev& C = I->lev[l + 1];
+                const int nc = C.GX * C.GY;
+#pragma unroll 4
+                for (int kc = (int)ltid; kc < nc; kc += (int)lsize) {
+                    if (C.mask[kc]) {
+                        C.b[kc] = 0.0f;
+                        continue;
+                    }
+                    const int jc = kc / C.GX;
+                    const int x = 2 * (kc - jc * C.GX), j = 2 * jc;
+                    float s = 4.0f * fine_residual(F, x, j);
+                    s += 2.0f * (fine_residual(F, x - 1, j) + fine_residual(F, x + 1, j) +
+                                 fine_residual(F, x, j - 1) + fine_residual(F, x, j + 1));
+                    s += fine_residual(F, x - 1, j - 1) + fine_residual(F, x + 1, j - 1) +
+                         fine_residual(F, x - 1, j + 1) + fine_residual(F, x + 1, j + 1);
+                    C.b[kc] = s * 0.0625f;
+                }
+            }
+            grid.sync();
+        }
+        if (on && first) fused_body(*I->fused, smem);
+        grid.sync();
+        for (int l = maxkf - 1; l >= 0; --l) {
+            if (on && l < I->kf) {
+                const LevelDev& F = I->lev[l];
+                const LevelDev& C = I->lev[l + 1];
+                const int nf = F.GX * F.GY;
+                float* __restrict__ fx = F.x;
+                const float* __restrict__ cxv = C.x;
+#pragma unroll 4
+                for (int k = (int)ltid; k < nf; k += (int)lsize) {
+                    if (F.mask[k]) continue;
+                    const int j = k / F.GX, x = k - j * F.GX;
+                    const int cI = x >> 1, cJ = j >> 1;
+                    const bool ox = x & 1, oy = j & 1;
+                    auto X = [&](int a, int b) { return cxv[b * C.GX + a]; };
+                    float v;
+                    if (!ox && !oy) v = X(cI, cJ);
+                    else if (ox && !oy) v = 0.5f * (X(cI, cJ) + X(cI + 1, cJ));
+                    else if (!ox && oy) v = 0.5f * (X(cI, cJ) + X(cI, cJ + 1));
+                    else v = 0.25f * (X(cI, cJ) + X(cI + 1, cJ) + X(cI, cJ + 1) + X(cI + 1, cJ + 1));
+                    fx[k] += v;
+                }
+            }
+            grid.sync();
+            for (int s = 0; s < kNu; ++s) {
+                half_sweep(l, 1);
+                half_sweep(l, 0);
+            }
+        }
+        // ---- PCG update ----
+        if (on) {
+            double rz = 0.0;
+            const float* __restrict__ x0 = I->lev[0].x;
+            const double* __restrict__ rv = I->r;
+            double* __restrict__ zv = I->z;
+            const uint8_t* __restrict__ mk = I->mask;
+            const int nn = (int)I->nodes;
+#pragma unroll 4
+            for (int k = (int)ltid; k < nn; k += (int)lsize) {
+                const double zi = mk[k] ? 0.0 : (double)x0[k];
+                zv[k] = zi;
+                rz += rv[k] * zi;
+            }
+            put2(rz, 0.0);
+        }
+        grid.sync();
+        if (on && first && threadIdx.x == 0) I->scal[S_RZ] = total(0);
+        grid.sync();
+        if (on) {
+            const double ro = I->scal[S_RZ_OLD];
+            const double beta = ro == 0.0 ? 0.0 : I->scal[S_RZ] / ro;
+            const double* __restrict__ zv = I->z;
+            double* __restrict__ pv = I->p;
+            const uint8_t* __restrict__ mk = I->mask;
+            const int nn = (int)I->nodes;
+#pragma unroll 4
+            for (int k = (int)ltid; k < nn; k += (int)lsize) pv[k] = mk[k] ? 0.0 : zv[k] + beta * pv[k];
+        }
+        grid.sync();
+        if (on) {
+            double pq = 0.0;
+            const double* __restrict__ pv = I->p;
+            double* __restrict__ qv = I->q;
+            const uint8_t* __restrict__ mk = I->mask;
+            const int nn = (int)I->nodes, GX = I->GX;
+            const double cd = I->cd, cx = I->cx, cy = I->cy;
+#pragma unroll 4
+            for (int k = (int)ltid; k < nn; k += (int)lsize) {
+                const double qi = mk[k] ? 0.0 : cd * pv[k] - cx * (pv[k - 1] + pv[k + 1]) - cy * (pv[k - GX] + pv[k + GX]);
+                qv[k] = qi;
+                pq += pv[k] * qi;
+            }
+            put2(pq, 0.0);
+        }
+        grid.sync();
+        if (on && first && threadIdx.x == 0) I->scal[S_PQ] = total(0);
+        grid.sync();
+        if (on) {
+            const double alpha = I->scal[S_RZ] / I->scal[S_PQ];
+            double rr = 0.0;
+            const double* __restrict__ pv = I->p;
+            const double* __restrict__ qv = I->q;
+            double* __restrict__ xv = I->phi;
+            double* __restrict__ rv = I->r;
+            float* __restrict__ b0 = I->lev[0].b;
+            const uint8_t* __restrict__ mk = I->mask;
+            const int nn = (int)I->nodes;
+#pragma unroll 4
+            for (int k = (int)ltid; k < nn; k += (int)lsize) {
+                double ri = 0.0;
+                if (!mk[k]) {
+                    xv[k] += alpha * pv[k];
+                    ri = rv[k] - alpha * qv[k];
+                }
+                rv[k] = ri;
+                b0[k] = (float)ri;
+                rr += ri * ri;
+            }
+            put2(rr, 0.0);
+        }
+        grid.sync();
+        if (on && first && threadIdx.x == 0) {
+            const double rr = total(0);
+            const double its = I->scal[S_IT] + 1.0;
+            I->scal[S_IT] = its;
+            I->scal[S_RZ_OLD] = I->scal[S_RZ];
+            I->scal[S_RR] = rr;
+            const bool finite = isfinite(rr);
+            bool go = finite && rr > I->tol2 * I->scal[S_BB];
+            if (go && its >= (double)I->maxit) {
+                go = false;
+                I->scal[S_STATUS] = 1.0;
+            }
+            if (!finite) I->scal[S_STATUS] = 2.0;
+            I->scal[S_COUNT] = go ? 1.0 : 0.0;
+        }
+        grid.sync();
+    }
+    // true residual of every instance, then its E field
+    if (I) {
+        double rr = 0.0;
+        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+            if (I->mask[k]) continue;
+            const double ri = I->rho[k] - stencil64(I->phi, k);
+            rr += ri * ri;
+        }
+        put2(rr, 0.0);
+    }
+    grid.sync();
+    if (first && threadIdx.x == 0) {
+        I->scal[S_TRUE_RR] = total(0);
+        if (*err) I->scal[S_STATUS] = 3.0;
+    }
+    if (I) {
+        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+            const int x = (int)(k % I->GX), j = (int)(k / I->GX);
+            double ex, ey;
+            efield_at(I->phi, I->GX, I->GY, I->dx, I->dy, x, j, ex, ey);
+            I->fld[k] = make_float4((float)ex, (float)ey, (float)I->bz[k], 0.0f);
+        }
+    }
+}
+
+}  // namespace
+
+// Host side of the batched solve: descriptors live in device memory owned by
+// the caller (`dev_insts`, `partials`, `active`); built once per ensemble.
+size_t poisson_batch_desc_bytes() { return sizeof(BatchInst); }
+size_t poisson_batch_max_fused_smem() { return 64 * 1024 + 1024; }
+
+int poisson_batch_describe(pic_ctx* c, void* host_desc, const void* dev_fused, int blk0, int nblk) {
+    PoissonState& ps = c->ps;
+    if (ps.fused_first + 1 > kMaxBatchLevels) return fail(PIC_ERR_CONFIG, "too many multigrid levels for the batched solve");
+    if (ps.warm == PIC_WARM_LEARNED) return fail(PIC_ERR_CONFIG, "the batched solve has no learned warm start");
+    if (ps.solver != PIC_SOLVER_MG_PCG) return fail(PIC_ERR_CONFIG, "the batched solve is MG-PCG only");
+    BatchInst I{};
+    const Grid64 g = fine_grid(c);
+    I.GX = g.GX;
+    I.GY = g.GY;
+    I.cx = g.cx;
+    I.cy = g.cy;
+    I.cd = g.cd;
+    I.dx = c->dx;
+    I.dy = c->dy;
+    I.nodes = c->nodes;
+    I.mask = c->mask;
+    I.dv = c->dir_val;
+    I.rho = c->rho;
+    I.phi = c->phi;
+    I.r = ps.r;
+    I.z = ps.z;
+    I.p = ps.p[0];
+    I.q = ps.q;
+    I.bz = c->bz;
+    I.fld = c->fld;
+    I.kf = ps.fused_first;
+    for (int l = 0; l <= ps.fused_first; ++l) I.lev[l] = as_dev(ps.levels[l]);
+    I.fused = static_cast<const FusedLevels*>(dev_fused);
+    I.scal = ps.scal;
+    I.tol2 = ps.tol * ps.tol;
+    I.maxit = ps.maxit;
+    I.zero_start = (ps.warm == PIC_WARM_ZERO || !ps.have_prev) ? 1 : 0;
+    I.blk0 = blk0;
+    I.nblk = nblk;
+    std::memcpy(host_desc, &I, sizeof(I));
+    return PIC_OK;
+}
+
+// The instance's fused-level table, for a device copy.
+const void* poisson_fused_table(pic_ctx* c, size_t* bytes) {
+    *bytes = sizeof(FusedLevels);
+    return c->ps.fused_desc;
+}
+
+size_t poisson_fused_smem(pic_ctx* c) { return c->ps.fused_smem; }
+
+int poisson_batch_launch(const void* dev_insts, int n, const int* inst_of, double* partials,
+                         unsigned* barriers, int* err, size_t smem, int blocks, cudaStream_t st) {
+    // the barriers' arrival counters start at zero
+    PIC_CUDA(cudaMemsetAsync(barriers, 0, (size_t)n * sizeof(unsigned), st));
+    PIC_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    void* args[] = {(void*)&dev_insts, (void*)&n, (void*)&inst_of, (void*)&partials, (void*)&barriers,
+                    (void*)&err};
+    PIC_CUDA(cudaLaunchCooperativeKernel((const void*)k_poisson_batch, dim3(blocks), dim3(kFusedThreads),
+                                         args, smem, st));
+    return PIC_OK;
+}
+
+int poisson_batch_blocks(size_t smem, int* blocks) {
+    PIC_CUDA(cudaFuncSetAttribute(k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_poisson_batch, kFusedThreads, smem));
+    PIC_CUDA(cudaGetDevice(&dev));
+    PIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *blocks = per_sm * sms;
+    if (*blocks <= 0) return fail(PIC_ERR_CONFIG, "the batched solve does not fit on the device");
+    return PIC_OK;
+}
+
+// After a batched solve: the instance's statistics as poisson_solve leaves
+// them, from a host copy of its 16 scalars.
+int poisson_batch_finish(pic_ctx* c, const double* scal, float ms) {
+    PoissonState& ps = c->ps;
+    std::memcpy(ps.host_scal, scal, 16 * sizeof(double));
+    const double bb = scal[S_BB], trr = scal[S_TRUE_RR];
+    ps.last_iters = (int)scal[S_IT];
+    ps.last_relres = bb > 0 ? std::sqrt(trr / bb) : 0.0;
+    ps.last_ms = ms;
+    ps.have_prev = true;
+    c->fields_valid = true;
+    if (scal[S_STATUS] == 3.0) return fail(PIC_ERR_TIMEOUT, "batched Poisson solve: a block barrier timed out");
+    if (scal[S_STATUS] != 0.0)
+        return fail(PIC_ERR_NOT_CONVERGED, "Poisson PCG did not reach the tolerance within poisson_maxit");
     return PIC_OK;
 }
 

@@ -139,6 +139,17 @@ def lib():
         "pic_ws_set_params": (cint, [vp, vp, i64, dbl, dbl, dbl]),
         "pic_ws_grid": (cint, [vp, P(cint)]),
         "pic_ws_scales": (cint, [vp, P(dbl)]),
+        "pic_set_tile_shape": (cint, [vp, cint]),
+        "pic_ensemble_create": (cint, [vp, cint, P(vp)]),
+        "pic_ensemble_destroy": (None, [vp]),
+        "pic_ensemble_size": (cint, [vp]),
+        "pic_ensemble_instance": (vp, [vp, cint]),
+        "pic_ensemble_step": (cint, [vp, cint]),
+        "pic_ensemble_autotune": (cint, [vp, P(cint), P(dbl)]),
+        "pic_ensemble_use_graph": (cint, [vp, cint]),
+        "pic_ensemble_timing": (cint, [vp, P(dbl), P(dbl), P(dbl)]),
+        "pic_ensemble_info": (cint, [vp, P(cint), P(cint), P(cint)]),
+        "pic_autotune": (cint, [vp, P(cint), P(dbl)]),
         "pic_ws_debug_step": (cint, [vp, vp, vp, vp, vp, P(dbl)]),
         "pic_deposit_points_noalloc": (cint, [vp, i64, i32, i32, dbl, dbl, vp, dbl, dbl, vp, vp, vp]),
     }
@@ -377,7 +388,89 @@ class Pic:
         _check(lib().pic_ws_debug_step(self.h, _p(x0), _p(target), _p(out), _p(grad), ctypes.byref(loss)))
         return out, grad, loss.value
 
+    def autotune(self, timings: bool = False):
+        """Picks the fastest particle-kernel tile shape; returns it (and the
+        per-shape milliseconds when timings is set)."""
+        sh = ctypes.c_int(0)
+        ms = (ctypes.c_double * 4)() if timings else None
+        _check(lib().pic_autotune(self.h, ctypes.byref(sh), ms))
+        return (sh.value, list(ms)) if timings else sh.value
+
+    def set_tile_shape(self, shape: int):
+        _check(lib().pic_set_tile_shape(self.h, shape))
+
     def poisson_stats(self):
         it, rr, ms = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)
         _check(lib().pic_poisson_stats(self.h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(ms)))
         return it.value, rr.value, ms.value
+
+
+class _Instance(Pic):
+    """A context owned by an Ensemble (not destroyed by itself)."""
+
+    def __init__(self, handle, cfg: Config):
+        self.cfg = cfg
+        self.h = ctypes.c_void_p(handle)
+        self.GX, self.GY = cfg.nx + 1, cfg.ny + 1
+        self.nodes = self.GX * self.GY
+
+    def close(self):
+        self.h = ctypes.c_void_p()
+
+
+class Ensemble:
+    """pic_ensemble: many instances advanced together (include/pic_capi.h)."""
+
+    def __init__(self, cfgs):
+        arr = (Config * len(cfgs))(*cfgs)
+        self.h = ctypes.c_void_p()
+        _check(lib().pic_ensemble_create(arr, len(cfgs), ctypes.byref(self.h)))
+        self.instances = [_Instance(lib().pic_ensemble_instance(self.h, i), cfgs[i])
+                          for i in range(len(cfgs))]
+
+    def __len__(self):
+        return len(self.instances)
+
+    def __getitem__(self, i) -> Pic:
+        return self.instances[i]
+
+    def step(self, iteration: int = 0):
+        _check(lib().pic_ensemble_step(self.h, iteration))
+
+    def autotune(self):
+        sh = ctypes.c_int(0)
+        ms = (ctypes.c_double * 4)()
+        _check(lib().pic_ensemble_autotune(self.h, ctypes.byref(sh), ms))
+        return sh.value, list(ms)
+
+    def info(self):
+        g, sh, b = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(lib().pic_ensemble_info(self.h, ctypes.byref(g), ctypes.byref(sh), ctypes.byref(b)))
+        return dict(graph=bool(g.value), tile_shape=sh.value, solver_blocks=b.value)
+
+    def use_graph(self, on: bool):
+        _check(lib().pic_ensemble_use_graph(self.h, 1 if on else 0))
+
+    def timing(self):
+        d, p, q = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().pic_ensemble_timing(self.h, ctypes.byref(d), ctypes.byref(p), ctypes.byref(q)))
+        return d.value, p.value, q.value
+
+    def close(self):
+        if self.h:
+            for inst in self.instances:
+                inst.close()
+            lib().pic_ensemble_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -213,6 +213,20 @@ int pic_profile_read(pic_ctx* ctx, double* ms, int64_t* calls, int reset);
 /* Kernel launches issued by this context since creation. */
 int pic_launch_count(pic_ctx* ctx, int64_t* n);
 
+/* ---- tuning (no reference counterpart) -----------------------------------
+ * The particle kernels are built for PIC_NUM_TILE_SHAPES tile shapes of 256
+ * cells: 0 = 64x4 (default), 1 = 32x8, 2 = 128x2, 3 = 16x16. */
+#define PIC_NUM_TILE_SHAPES 4
+int pic_set_tile_shape(pic_ctx* ctx, int tile_shape);
+/* Times the push of the current particles with every tile shape (the
+ * simulation state is left as it was; the accumulators are redeposited at the
+ * next charge_deposition) and keeps the fastest.  When the environment
+ * variable PIC_TUNE_CACHE names a file and ms_per_shape is NULL, a choice
+ * recorded there for the same device, grid and particle count is used
+ * without timing; new choices are appended to it.  ms_per_shape, when not
+ * NULL, receives PIC_NUM_TILE_SHAPES timings (ms per push of all species). */
+int pic_autotune(pic_ctx* ctx, int* tile_shape, double* ms_per_shape);
+
 /* ---- allocation-free deposit ---------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory when they deposit -- a host framework that owns a fixed device
@@ -278,6 +292,38 @@ int pic_ws_grid(pic_ctx* ctx, int* P);
  * For gradient checks. */
 int pic_ws_debug_step(pic_ctx* ctx, const float* x0, const float* rhs, float* out,
                       float* grad, double* loss);
+
+/* ---- ensembles (no reference counterpart: the reference runs one
+ * simulation per process) ------------------------------------------------
+ * N independent instances on one device, advanced together: one step of all
+ * of them is one launch per phase -- the charge-deposit conversion of every
+ * species, ONE persistent cooperative launch for all the Poisson solves
+ * (MG-PCG to each instance's tolerance, then its E field), and per species
+ * one push launch and one side-list launch over all instances -- captured
+ * in a CUDA graph after the first step.  Instances may differ in grid size,
+ * electrodes, Bz, species weights and tolerances; they must share the
+ * device, the number of species and the energy-mesh mode, use the MG-PCG
+ * solver and no learned warm start.  Each instance is an ordinary context
+ * (pic_ensemble_instance) for loading particles and reading results; its
+ * step operators must not be called while it belongs to the ensemble. */
+typedef struct pic_ensemble pic_ensemble;
+int pic_ensemble_create(const pic_config* cfgs, int n, pic_ensemble** out);
+void pic_ensemble_destroy(pic_ensemble* ens);
+int pic_ensemble_size(pic_ensemble* ens);
+pic_ctx* pic_ensemble_instance(pic_ensemble* ens, int i);
+/* zero rho, deposit, Poisson + E, push: all instances.  Synchronises once. */
+int pic_ensemble_step(pic_ensemble* ens, int iteration);
+/* Times the batched push with every tile shape (state left as it was) and
+ * keeps the fastest; ms_per_shape may be NULL. */
+int pic_ensemble_autotune(pic_ensemble* ens, int* tile_shape, double* ms_per_shape);
+/* 0: launch the phases directly instead of replaying the captured graph. */
+int pic_ensemble_use_graph(pic_ensemble* ens, int on);
+/* Device milliseconds of the last step: deposit conversion, Poisson + E,
+ * push (all instances). */
+int pic_ensemble_timing(pic_ensemble* ens, double* deposit_ms, double* poisson_ms, double* push_ms);
+/* Whether the last step replayed a captured graph, the tile shape in use, and
+ * the blocks of the persistent Poisson launch. */
+int pic_ensemble_info(pic_ensemble* ens, int* graph_active, int* tile_shape, int* solver_blocks);
 
 /* ---- Poisson controls -------------------------------------------------- */
 int pic_set_poisson(pic_ctx* ctx, int solver, int warm_start, double tol, int maxit);
