@@ -53,7 +53,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg3", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--config", default="cfg3", choices=["cfg1", "cfg2", "cfg3", "cfg4"],
+                    help="cfg4: the learned warm-start protocol on the cfg3 run (train on the "
+                         "first --cfg4-train steps, evaluate on the next --cfg4-eval)")
+    ap.add_argument("--cfg4-train", type=int, default=2000)
+    ap.add_argument("--cfg4-eval", type=int, default=2000)
+    ap.add_argument("--cfg4-epochs", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -488,6 +493,73 @@ def run_ensemble(args, rank):
             "setup_s": setup_s}
 
 
+def run_cfg4(args):
+    """Learned vs plain warm start on the 1024^2 run: (input, RHS change)
+    pairs recorded over steps 0..T-1, the network trained on the GPU, then
+    every step of T..T+E-1 solved from the network's guess and, from the same
+    state, from phi_{n-1}; both to 1e-8.  Prints its own JSON line."""
+    import torch
+    import pic_b200 as P
+    import pic_configs as C
+    torch.cuda.set_device(0)
+    w = C.cfg3()
+    pic = P.Pic(C.library_config(w))
+    C.load_plasma(pic, w, seed=1234)
+    T, E = args.cfg4_train, args.cfg4_eval
+    t0 = time.perf_counter()
+    pic.ws_record(T)
+    plain_ms_rec, plain_it_rec = [], []
+    for it in range(T + 1):
+        pic.step(it)
+        n_it, _, ms = pic.poisson_stats()
+        plain_it_rec.append(n_it)
+        plain_ms_rec.append(ms)
+    pic.ws_record(0)
+    rec_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    losses = [pic.ws_train(1, 1e-3) for _ in range(args.cfg4_epochs)]
+    train_s = time.perf_counter() - t0
+    pic.ws_record(-1)
+    ml, mp, il, ip, dphi = [], [], [], [], []
+    it = T + 1
+    for _ in range(E):
+        pic.zero_rho()
+        for s in range(2):
+            pic.charge_deposition(s)
+        rho, phi_prev = pic.rho(), pic.phi()
+        pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_LEARNED, 1e-8, 500)
+        pic.poisson_solve(it)
+        n_l, r_l, ms_l = pic.poisson_stats()
+        phi_l = pic.phi()
+        pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_PREVIOUS, 1e-8, 500)
+        pic.set_phi(phi_prev)
+        pic.set_rho(rho)
+        pic.poisson_solve(it)
+        n_p, r_p, ms_p = pic.poisson_stats()
+        dphi.append(float(np.abs(phi_l - pic.phi()).max()))
+        for s in range(2):
+            pic.move_particles(s, it)
+        it += 1
+        ml.append(ms_l)
+        mp.append(ms_p)
+        il.append(n_l)
+        ip.append(n_p)
+    pic.close()
+    line = {"metric": "Poisson ms/step, learned warm start, relres 1e-8", "value": statistics.mean(ml),
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "impl": "ours", "data": "synthetic",
+            "config": {"workload": describe(w) + f"; train on steps 0-{T - 1}, evaluate on {T + 1}-{T + E}",
+                       "epochs": args.cfg4_epochs},
+            "plain_ms_per_step_same_state": statistics.mean(mp),
+            "iters_learned": statistics.mean(il), "iters_plain_same_state": statistics.mean(ip),
+            "iters_learned_hist": {str(k): il.count(k) for k in sorted(set(il))},
+            "iters_plain_hist": {str(k): ip.count(k) for k in sorted(set(ip))},
+            "max_abs_dphi_V": max(dphi), "loss_per_epoch": losses,
+            "record_s": rec_s, "train_s": train_s,
+            "plain_ms_during_recording": statistics.mean(plain_ms_rec)}
+    print(json.dumps(line))
+    return 0
+
+
 def run_e2e(pic, steps, n_part, it0):
     """Same metric through the public C ABI with host buffers: import both
     species from host Points, K x (zero rho, deposit, read rho to host, push),
@@ -557,6 +629,8 @@ def main():
         print(json.dumps(line))
         return 0
 
+    if args.config == "cfg4":
+        return run_cfg4(args) if rank == 0 else 0
     if world > 1:
         import datetime
         import torch

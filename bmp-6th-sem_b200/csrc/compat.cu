@@ -128,6 +128,8 @@ int sycl_pic_init(const char* dev_type, int wg, int ps, const char* input1, cons
 }
 
 int sycl_pic_get_grid_size(void) { return g.ctx ? (int)g.ctx->nodes : -1; }
+int sycl_pic_get_grid_x(void) { return g.ctx ? g.ctx->GX : -1; }
+int sycl_pic_get_grid_y(void) { return g.ctx ? g.ctx->GY : -1; }
 int sycl_pic_get_timesteps(void) { return g.ctx ? g.file.timesteps : -1; }
 int sycl_pic_get_print_interval(void) { return g.ctx ? g.file.print_interval : -1; }
 int sycl_pic_get_num_species(void) { return g.ctx ? g.ctx->cfg.num_species : -1; }
@@ -192,8 +194,8 @@ double sycl_pic_generate_new_particles(void) {
 void sycl_pic_update_fields_from_phi(void) {
     if (!ready()) return;
     if (pic_set_phi(g.ctx, g.phi.data()) != PIC_OK) return;
-    pic_update_fields_from_phi(g.ctx);
-    pic_synchronize(g.ctx);
+    if (pic_update_fields_from_phi(g.ctx) != PIC_OK) return;
+    refresh_host(false, true);  // the electrode potentials, as overwritePhi leaves them
 }
 
 // printNumberDensity / printEnergy / printElectricField / printPhi
@@ -222,6 +224,7 @@ void sycl_pic_print_diagnostics(const char* dir, int iteration) {
     std::vector<double> phi(n);
     pic_get_phi(c, phi.data());
     const double sf = g.file.scale_factor;
+    mkdir(d.c_str(), 0755);  // the output folder itself (an existing one is kept)
     auto path = [&](const char* q) {
         const std::string p = d + "/" + q;
         mkdir(p.c_str(), 0755);

@@ -573,6 +573,7 @@ int pic_set_phi(pic_ctx* c, const double* host) {
 
 int pic_update_fields_from_phi(pic_ctx* c) {
     if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_TRY(overwrite_phi(c));
     return fields_from_phi(c);
 }
 

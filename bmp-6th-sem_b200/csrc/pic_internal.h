@@ -256,6 +256,7 @@ int poisson_setup(pic_ctx* c);
 void poisson_free(pic_ctx* c);
 int poisson_solve(pic_ctx* c);
 int fields_from_phi(pic_ctx* c);
+int overwrite_phi(pic_ctx* c);  // electrode nodes take their potential
 int efield_export(pic_ctx* c);
 int fields_set_bz(pic_ctx* c);
 // batched solve of many contexts (poisson.cu)

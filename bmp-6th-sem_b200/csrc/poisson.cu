@@ -916,6 +916,21 @@ int poisson_solve(pic_ctx* c) {
     return PIC_OK;
 }
 
+// overwritePhi (src/poissonSolver.cpp:364-382): electrode nodes take their
+// potential.
+__global__ void k_overwrite_phi(int64_t nodes, const uint8_t* mask, const double* dv, double* phi) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nodes && mask[i]) phi[i] = dv[i];
+}
+
+int overwrite_phi(pic_ctx* c) {
+    k_overwrite_phi<<<(unsigned)((c->nodes + 255) / 256), 256, 0, c->stream>>>(c->nodes, c->mask, c->dir_val,
+                                                                              c->phi);
+    c->launches += 1;
+    PIC_CUDA(cudaGetLastError());
+    return PIC_OK;
+}
+
 int fields_from_phi(pic_ctx* c) {
     const dim3 b2(32, 8);
     k_efield<<<grid2d(c->GX, c->GY, b2), b2, 0, c->stream>>>(c->phi, c->bz, c->GX, c->GY, c->dx,

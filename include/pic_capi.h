@@ -191,9 +191,10 @@ int pic_get_final_mesh(pic_ctx* ctx, int species, double* host);
 int pic_get_energy_mesh(pic_ctx* ctx, int species, double* host);
 int pic_set_rho(pic_ctx* ctx, const double* host);
 int pic_set_phi(pic_ctx* ctx, const double* host);
-/* E from phi (calculateElectricField, src/poissonSolver.cpp:433-456); the
- * reference Python extension's update_fields_from_phi
- * (src/sycl_pic_module.cpp:216-223). */
+/* The reference Python extension's update_fields_from_phi
+ * (src/sycl_pic_module.cpp:216-223): electrode nodes of phi take their
+ * potential (overwritePhi, src/poissonSolver.cpp:364-382), then E from phi
+ * (calculateElectricField, src/poissonSolver.cpp:433-456). */
 int pic_update_fields_from_phi(pic_ctx* ctx);
 int pic_set_bz(pic_ctx* ctx, const double* host);
 

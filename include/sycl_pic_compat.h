@@ -29,6 +29,9 @@ extern "C" {
  * the reference (readPICDAT initialises particles randomly). */
 int sycl_pic_init(const char* dev_type, int wg, int ps, const char* input1, const char* input2);
 int sycl_pic_get_grid_size(void);        /* :91  GRID_X*GRID_Y            */
+/* sycl_pic_module.cpp:110-118 (Python extension): GRID_X, GRID_Y. */
+int sycl_pic_get_grid_x(void);
+int sycl_pic_get_grid_y(void);
 int sycl_pic_get_timesteps(void);        /* :95  TIMESTEPS                */
 int sycl_pic_get_print_interval(void);   /* :99  printInterval            */
 int sycl_pic_get_num_species(void);      /* :103 num_type                 */

@@ -189,3 +189,19 @@ def test_compat_surface_before_init(picb):
     assert L.sycl_pic_charge_deposition(0) == -1.0
     assert L.sycl_pic_get_grid_size() == -1
     assert L.sycl_pic_generate_new_particles() == -1.0
+
+
+def test_sycl_pic_module_surface():
+    """The Python module offers every function of the reference extension's
+    method table (SYCL-PIC-poissonsolver/src/sycl_pic_module.cpp:386-409)."""
+    import sycl_pic
+    names = ["init", "get_grid_size", "get_grid_x", "get_grid_y", "get_timesteps",
+             "get_print_interval", "get_num_species", "get_particle_counts", "get_rho", "get_phi",
+             "zero_rho", "charge_deposition", "poisson_solve", "update_fields_from_phi",
+             "move_particles", "compact_particles", "cleanup_map", "generate_new_particles",
+             "print_diagnostics", "save_meshes", "dump_rho_phi_cpp", "finalize"]
+    missing = [n for n in names if not callable(getattr(sycl_pic, n, None))]
+    assert not missing, missing
+    # without a context the calls fail the way the module documents
+    with pytest.raises(RuntimeError):
+        sycl_pic.get_grid_size()
