@@ -187,8 +187,16 @@ double sycl_pic_cleanup_map(int species) {
 }
 
 double sycl_pic_generate_new_particles(void) {
-    set_error("particle sources (re-injection, ionisation pairs) are not built");
-    return -1.0;
+    if (!ready()) return -1.0;
+    const double t0 = now();
+    pic_source_desc d;
+    pic_source_default(&d);
+    d.te_ev = g.file.te;  // electronTemp / ionTemp from M_PICDAT.DAT
+    d.ti_ev = g.file.ti;
+    if (const char* e = std::getenv("PIC_SEED")) d.seed = std::strtoull(e, nullptr, 10) ^ 0x5A1CE5ull;
+    int64_t ne = 0, np = 0;
+    if (pic_generate_new_particles(g.ctx, &d, &ne, &np) != PIC_OK) return -1.0;
+    return now() - t0;
 }
 
 void sycl_pic_update_fields_from_phi(void) {

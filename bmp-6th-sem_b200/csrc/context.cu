@@ -482,6 +482,28 @@ int pic_left_exits(pic_ctx* c, int s, int64_t* n) {
     return PIC_OK;
 }
 
+int pic_source_default(pic_source_desc* d) {
+    if (!d) return fail(PIC_ERR_ARG, "null argument");
+    *d = pic_source_desc{};
+    d->reinject_x = 0.024;  // src/utils.cpp:398
+    d->te_ev = 2.0;
+    d->ti_ev = 0.026;
+    d->x11 = 0.0025;  // src/types.cpp:103-105
+    d->x22 = 0.01;
+    d->xm = 0.00625;
+    d->ionimax = 5.23e23;  // src/utils.cpp:500
+    d->rate_div = 1.67e6;  // src/utils.cpp:502
+    d->reinject = 1;
+    d->pairs = 1;
+    d->seed = 0x5A1CE5ull;
+    return PIC_OK;
+}
+
+int pic_generate_new_particles(pic_ctx* c, const pic_source_desc* d, int64_t* n_e, int64_t* n_p) {
+    if (!c || !d) return fail(PIC_ERR_ARG, "null argument");
+    return particles_generate(c, d, n_e, n_p);
+}
+
 int pic_zero_rho(pic_ctx* c) {
     if (!c) return fail(PIC_ERR_ARG, "null context");
     PIC_CUDA(cudaMemsetAsync(c->rho, 0, (size_t)c->nodes * 8, c->stream));

@@ -2068,3 +2068,202 @@ int batch_time_shapes(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st, int r
 }
 
 }  // namespace picb200
+
+// ---------------------------------------------------------------------------
+// Particle sources: generate_new_electrons and generate_pairs
+// (SYCL-PIC-poissonsolver/src/utils.cpp:374-777, called per step by
+// src/sycl_pic_ctypes.cpp:212-236).  New particles are drawn on the device
+// (Philox-4x32-10, counter = (call, particle, stream)) and appended to the
+// species' side list: they are part of the state at once (deposited into
+// the accumulators when those hold the current positions) and are placed in
+// their cells by the next push or re-layout.
+// ---------------------------------------------------------------------------
+namespace picb200 {
+namespace {
+
+struct SourceArgs {
+    int nx, ny, GX;
+    double dx, dy, W, H;
+    double x_reinject;
+    double x11, x22, xm;
+    double ve, vi;  // sqrt(2|q/m|T) of electrons and ions
+    uint32_t n_reinject, n_pairs;
+    uint2 key;
+    uint32_t call;
+    ListDev e_list, i_list;
+    unsigned long long* e_acc_q;
+    unsigned long long* e_acc_e;
+    unsigned long long* i_acc_q;
+    unsigned long long* i_acc_e;
+    int deposit_e, deposit_i, energy;
+    float e_half_inv_abs_qm, i_half_inv_abs_qm;
+    unsigned long long* e_counters;
+    unsigned long long* i_counters;
+    unsigned* accepted;  // pairs created
+};
+
+__device__ __forceinline__ double u01d(uint32_t a, uint32_t b) {
+    // 53-bit uniform in [0, 1)
+    return (double)(((uint64_t)a << 21) ^ (uint64_t)(b >> 11)) * (1.0 / 9007199254740992.0);
+}
+
+// the reference's Maxwellian draw: v * sqrt(-ln u) * (cos, sin)(2 pi u'),
+// u clamped below at 1e-10 as ran2 (src/utils.cpp:51-56)
+__device__ __forceinline__ void maxwell(double v, uint4 r0, uint4 r1, double& vx, double& vy, double& vz) {
+    const double u1 = fmax(u01d(r0.x, r0.y), 1e-10), u2 = u01d(r0.z, r0.w);
+    const double u3 = fmax(u01d(r1.x, r1.y), 1e-10), u4 = u01d(r1.z, r1.w);
+    const double z1 = sqrt(-log(u1)), z3 = sqrt(-log(u3));
+    double s, c;
+    sincospi(2.0 * u2, &s, &c);
+    vx = v * z1 * c;
+    vy = v * z1 * s;
+    sincospi(2.0 * u4, &s, &c);
+    vz = v * z3 * c;
+}
+
+// Appends one particle (FP64 position) to a side list, deposit included.
+template <bool ENERGY>
+__device__ __forceinline__ void append_point(const SourceArgs& S, const ListDev& L, double x, double y,
+                                             double vx, double vy, double vz, bool deposit,
+                                             unsigned long long* acc_q, unsigned long long* acc_e,
+                                             float half_inv_abs_qm, unsigned long long* counters) {
+    const double sx = x * (1.0 / S.dx), sy = y * (1.0 / S.dy);
+    if (!(sx >= 0.0 && sy >= 0.0 && sx < (double)S.nx && sy < (double)S.ny)) return;
+    const int gx = (int)sx, gy = (int)sy;
+    const float fx = fminf((float)(sx - gx), kOneBelow), fy = fminf((float)(sy - gy), kOneBelow);
+    const uint32_t s = atomicAdd(L.count, 1u);
+    if (s >= L.cap) {
+        atomicOr(counters + 2, 1ull);
+        return;
+    }
+    L.a[s] = make_float4(fx, fy, (float)vx, (float)vy);
+    L.vz[s] = (float)vz;
+    L.cell[s] = (uint32_t)(gy * S.nx + gx);
+    if (deposit) {
+        const float en = ENERGY ? energy_ev((float)vx, (float)vy, (float)vz, half_inv_abs_qm) : 0.f;
+        deposit_one<ENERGY>(acc_q, acc_e, S.GX, (uint32_t)(gy * S.GX + gx), fx, fy, en);
+    }
+}
+
+template <bool ENERGY>
+__global__ void k_sources(SourceArgs S) {
+    const uint32_t total = S.n_reinject + S.n_pairs;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const uint4 r0 = philox(make_uint4(k, S.call, 0u, 0x50u), S.key);
+        const uint4 r1 = philox(make_uint4(k, S.call, 1u, 0x50u), S.key);
+        if (k < S.n_reinject) {
+            // generate_new_electrons (src/utils.cpp:397-425): x fixed, y uniform
+            double vx, vy, vz;
+            maxwell(S.ve, r0, r1, vx, vy, vz);
+            const uint4 r2 = philox(make_uint4(k, S.call, 2u, 0x50u), S.key);
+            append_point<ENERGY>(S, S.e_list, S.x_reinject, S.H * u01d(r2.x, r2.y), vx, vy, vz, S.deposit_e,
+                                 S.e_acc_q, S.e_acc_e, S.e_half_inv_abs_qm, S.e_counters);
+        } else {
+            // generate_pairs (src/utils.cpp:517-566): one electron and one
+            // ion at x = xm + asin(2u-1)(x22-x11)/pi, y uniform, kept inside (0, W)
+            const uint4 r2 = philox(make_uint4(k, S.call, 2u, 0x50u), S.key);
+            const uint4 r3 = philox(make_uint4(k, S.call, 3u, 0x50u), S.key);
+            const uint4 r4 = philox(make_uint4(k, S.call, 4u, 0x50u), S.key);
+            const double x = S.xm + asin(2.0 * u01d(r2.x, r2.y) - 1.0) * (S.x22 - S.x11) * (1.0 / 3.14159265358979323846);
+            const double y = S.H * u01d(r2.z, r2.w);
+            if (!(x > 0.0 && x < S.W)) continue;
+            double vx, vy, vz;
+            maxwell(S.ve, r0, r1, vx, vy, vz);
+            append_point<ENERGY>(S, S.e_list, x, y, vx, vy, vz, S.deposit_e, S.e_acc_q, S.e_acc_e,
+                                 S.e_half_inv_abs_qm, S.e_counters);
+            maxwell(S.vi, r3, r4, vx, vy, vz);
+            append_point<ENERGY>(S, S.i_list, x, y, vx, vy, vz, S.deposit_i, S.i_acc_q, S.i_acc_e,
+                                 S.i_half_inv_abs_qm, S.i_counters);
+            atomicAdd(S.accepted, 1u);
+        }
+    }
+}
+
+}  // namespace
+
+int particles_generate(pic_ctx* c, const pic_source_desc* d, int64_t* n_e, int64_t* n_p) {
+    if (c->cfg.num_species < 2) return fail(PIC_ERR_STATE, "particle sources need electrons (species 0) and ions (1)");
+    Species& E = c->sp[0];
+    Species& I = c->sp[1];
+    // re-injection count: electron exits through x < 0 beyond the ions'
+    unsigned long long ex[2] = {0, 0};
+    PIC_CUDA(cudaMemcpyAsync(&ex[0], E.counters, 8, cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaMemcpyAsync(&ex[1], I.counters, 8, cudaMemcpyDeviceToHost, c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    int64_t num_new = 0;
+    if (d->reinject) {
+        num_new = std::max<int64_t>((int64_t)ex[0] - (int64_t)ex[1], 0);
+        PIC_CUDA(cudaMemsetAsync(E.counters, 0, 8, c->stream));
+        PIC_CUDA(cudaMemsetAsync(I.counters, 0, 8, c->stream));
+    }
+    int64_t target = 0;
+    if (d->pairs) {
+        // fn = H dt (2/pi) (x22 - x11) ionimax / rate_div (src/utils.cpp:502)
+        const double fn = c->cfg.ymax * c->cfg.dt * (2.0 / 3.14159265358979323846) * (d->x22 - d->x11) *
+                          d->ionimax / d->rate_div;
+        if (fn > 0) target = (int64_t)std::ceil(fn);
+    }
+    if (n_e) *n_e = 0;
+    if (n_p) *n_p = 0;
+    if (num_new + target == 0) return PIC_OK;
+    if (num_new + target > 0x7fffffffll) return fail(PIC_ERR_CAPACITY, "too many new particles in one call");
+    // the side lists must hold them: make room first if needed
+    for (Species* sp : {&E, &I}) {
+        uint32_t n = 0;
+        PIC_CUDA(cudaMemcpy(&n, sp->list_counts + 1 + sp->lcur, 4, cudaMemcpyDeviceToHost));
+        if ((int64_t)n + num_new + target > (int64_t)sp->loose[sp->lcur].cap)
+            return fail(PIC_ERR_CAPACITY, "particle sources: more new particles than the side list holds");
+    }
+    unsigned* accepted = nullptr;
+    PIC_CUDA(cudaMalloc(&accepted, sizeof(unsigned)));
+    PIC_CUDA(cudaMemsetAsync(accepted, 0, sizeof(unsigned), c->stream));
+    SourceArgs S{};
+    S.nx = c->nx;
+    S.ny = c->ny;
+    S.GX = c->GX;
+    S.dx = c->dx;
+    S.dy = c->dy;
+    S.W = c->cfg.xmax;
+    S.H = c->cfg.ymax;
+    S.x_reinject = d->reinject_x;
+    S.x11 = d->x11;
+    S.x22 = d->x22;
+    S.xm = d->xm;
+    S.ve = std::sqrt(2.0 * std::fabs(E.ctom) * d->te_ev);
+    S.vi = std::sqrt(2.0 * std::fabs(I.ctom) * d->ti_ev);
+    S.n_reinject = (uint32_t)num_new;
+    S.n_pairs = (uint32_t)target;
+    S.key = make_uint2((uint32_t)d->seed, (uint32_t)(d->seed >> 32));
+    S.call = (uint32_t)c->source_calls++;
+    S.e_list = list_dev(E.loose[E.lcur]);
+    S.i_list = list_dev(I.loose[I.lcur]);
+    S.e_acc_q = E.acc_q;
+    S.e_acc_e = E.acc_e;
+    S.i_acc_q = I.acc_q;
+    S.i_acc_e = I.acc_e;
+    S.deposit_e = E.acc_fresh ? 1 : 0;
+    S.deposit_i = I.acc_fresh ? 1 : 0;
+    S.e_half_inv_abs_qm = E.k.half_inv_abs_qm;
+    S.i_half_inv_abs_qm = I.k.half_inv_abs_qm;
+    S.e_counters = E.counters;
+    S.i_counters = I.counters;
+    S.accepted = accepted;
+    const unsigned blocks = (unsigned)std::min<int64_t>((num_new + target + 255) / 256, 148 * 8);
+    if (c->cfg.deposit_energy)
+        k_sources<true><<<blocks, 256, 0, c->stream>>>(S);
+    else
+        k_sources<false><<<blocks, 256, 0, c->stream>>>(S);
+    c->launches += 1;
+    unsigned acc_h = 0;
+    cudaMemcpyAsync(&acc_h, accepted, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(accepted);
+    if (e != cudaSuccess) return fail(PIC_ERR_CUDA, std::string("particle sources: ") + cudaGetErrorString(e));
+    // the new particles make the side lists' host-side counts stale
+    E.flags_pending = I.flags_pending = false;
+    if (n_e) *n_e = num_new;
+    if (n_p) *n_p = acc_h;
+    return PIC_OK;
+}
+
+}  // namespace picb200

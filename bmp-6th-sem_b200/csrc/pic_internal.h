@@ -190,6 +190,7 @@ struct pic_ctx {
     picb200::PoissonState ps;
     bool fields_valid = false;
     int tile_shape = 0;            // particle-kernel tile shape (see particles.cu)
+    uint64_t source_calls = 0;     // particle-source calls (RNG counter)
     bool bz_uniform = true;        // every node has the same Bz (bz_value)
     double bz_value = 0.0;
     // instrumentation
@@ -242,6 +243,7 @@ int batch_push(ParticleBatchImpl* B, int shape, bool energy, cudaStream_t st);
 void batch_commit(pic_ctx** cs, int n);
 int batch_time_shapes(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st, int reps, bool energy,
                       double* ms);
+int particles_generate(pic_ctx* c, const pic_source_desc* d, int64_t* n_e, int64_t* n_p);
 int particles_num_tile_shapes();
 int particles_time_shapes(pic_ctx* c, int reps, double* ms);  // ms[particles_num_tile_shapes()]
 

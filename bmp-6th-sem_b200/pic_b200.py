@@ -59,6 +59,14 @@ class Config(ctypes.Structure):
     ]
 
 
+class SourceDesc(ctypes.Structure):
+    """pic_source_desc (include/pic_capi.h)."""
+    _fields_ = [("reinject_x", ctypes.c_double), ("te_ev", ctypes.c_double), ("ti_ev", ctypes.c_double),
+                ("x11", ctypes.c_double), ("x22", ctypes.c_double), ("xm", ctypes.c_double),
+                ("ionimax", ctypes.c_double), ("rate_div", ctypes.c_double),
+                ("reinject", ctypes.c_int32), ("pairs", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
 class PlasmaDesc(ctypes.Structure):
     """pic_plasma_desc (include/pic_capi.h)."""
     _fields_ = [("ppc", ctypes.c_int32), ("temperature_ev", ctypes.c_double),
@@ -140,6 +148,8 @@ def lib():
         "pic_ws_grid": (cint, [vp, P(cint)]),
         "pic_ws_scales": (cint, [vp, P(dbl)]),
         "pic_set_tile_shape": (cint, [vp, cint]),
+        "pic_source_default": (cint, [P(SourceDesc)]),
+        "pic_generate_new_particles": (cint, [vp, P(SourceDesc), P(i64), P(i64)]),
         "pic_ensemble_create": (cint, [vp, cint, P(vp)]),
         "pic_ensemble_destroy": (None, [vp]),
         "pic_ensemble_size": (cint, [vp]),
@@ -276,6 +286,18 @@ class Pic:
         out = np.zeros(self.nodes, np.int32)
         _check(lib().pic_bin_counts(self.h, s, _p(out)))
         return out
+
+    def generate_new_particles(self, **overrides):
+        """Re-injection and ionisation pairs (pic_generate_new_particles);
+        keyword arguments override pic_source_default's fields.  Returns
+        (electrons re-injected, pairs created)."""
+        d = SourceDesc()
+        _check(lib().pic_source_default(ctypes.byref(d)))
+        for k, v in overrides.items():
+            setattr(d, k, v)
+        ne, npair = ctypes.c_int64(0), ctypes.c_int64(0)
+        _check(lib().pic_generate_new_particles(self.h, ctypes.byref(d), ctypes.byref(ne), ctypes.byref(npair)))
+        return ne.value, npair.value
 
     def left_exits(self, s: int) -> int:
         n = ctypes.c_int64(0)

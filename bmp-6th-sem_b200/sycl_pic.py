@@ -17,7 +17,8 @@ driver finds the same surface:
   * failures raise RuntimeError with the library's message where the
     reference would exit.
 
-Particle sources (generate_new_particles) are not built: the call raises.
+generate_new_particles re-injects electrons and creates ionisation pairs
+with the reference's constants (pic_generate_new_particles).
 """
 from __future__ import annotations
 

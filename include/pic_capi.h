@@ -171,6 +171,33 @@ int pic_bin_counts(pic_ctx* ctx, int species, int32_t* host_counts);
  * src/mover.cpp:344-351); the counter is reset by the read. */
 int pic_left_exits(pic_ctx* ctx, int species, int64_t* n_out);
 
+/* Particle sources of the reference's generate_new_particles
+ * (src/sycl_pic_ctypes.cpp:212-236): generate_new_electrons re-injects, as
+ * electrons (species 0), the electrons lost through x < 0 beyond the ions
+ * (species 1) lost there since the last call, at x = reinject_x with y
+ * uniform (src/utils.cpp:374-489); generate_pairs creates ceil(fn) electron-
+ * ion pairs, fn = YMAX dt (2/pi) (x22 - x11) ionimax / rate_div, each at
+ * x = xm + asin(2u-1)(x22-x11)/pi, y uniform, kept inside (0, XMAX)
+ * (src/utils.cpp:495-566).  Velocities are the reference's Maxwellian draw
+ * v sqrt(-ln u) (cos, sin)(2 pi u'), v = sqrt(2|q/m|T).  The reference's
+ * constants are the defaults (pic_source_default); draws are Philox with
+ * the call number and particle index as counter (the reference uses rand()). */
+typedef struct pic_source_desc {
+    double reinject_x;    /* m (reference: 0.024)                         */
+    double te_ev, ti_ev;  /* temperatures of new electrons / ions (eV)    */
+    double x11, x22, xm;  /* ionisation band (m): 0.0025, 0.01, 0.00625   */
+    double ionimax;       /* 5.23e23                                      */
+    double rate_div;      /* 1.67e6                                       */
+    int32_t reinject;     /* 1: re-inject electrons                       */
+    int32_t pairs;        /* 1: create ionisation pairs                   */
+    uint64_t seed;
+} pic_source_desc;
+int pic_source_default(pic_source_desc* d);
+/* New particles join the state at once (placed in their cells by the next
+ * push); n_electrons / n_pairs receive what was created. */
+int pic_generate_new_particles(pic_ctx* ctx, const pic_source_desc* d, int64_t* n_electrons,
+                               int64_t* n_pairs);
+
 /* ---- step operators (reference order, src/main.cpp:130-257) ------------ */
 int pic_zero_rho(pic_ctx* ctx);
 int pic_charge_deposition(pic_ctx* ctx, int species);

@@ -44,8 +44,9 @@ double sycl_pic_poisson_solve(int iteration);            /* :153 */
 double sycl_pic_move_particles(int species, int iteration); /* :161 */
 double sycl_pic_compact_particles(int species, double* out_alloc_t, double* out_scan_t); /* :179 */
 double sycl_pic_cleanup_map(int species);                /* :201 */
-/* :212 particle sources (re-injection, ionisation pairs) are not built:
- * returns -1.0 with PIC_ERR_STATE. */
+/* :212 particle sources: re-injection of left-wall electron exits beyond the
+ * ions' and ionisation pairs (pic_generate_new_particles with the reference's
+ * constants, temperatures from M_PICDAT.DAT). */
 double sycl_pic_generate_new_particles(void);
 /* :239 text snapshots into dir/{electronDensity,ionDensity,potential,Ex,Ey}/<iter>. */
 void sycl_pic_print_diagnostics(const char* dir, int iteration);

@@ -188,7 +188,7 @@ def test_compat_surface_before_init(picb):
     assert L.sycl_pic_get_rho_ptr() is None
     assert L.sycl_pic_charge_deposition(0) == -1.0
     assert L.sycl_pic_get_grid_size() == -1
-    assert L.sycl_pic_generate_new_particles() == -1.0
+    assert L.sycl_pic_generate_new_particles() == -1.0   # no context
 
 
 def test_sycl_pic_module_surface():
