@@ -201,7 +201,11 @@ def test_push_matches_oracle(oracle, species, bz):
     pts["vz"] = np.arange(len(pts), dtype=np.float64) + 1.0
     phi = _random_fields(w)
     g = oracle_grid(oracle, w)
-    ef = oracle.efield(w.GX, w.GY, *lib_dx(w), phi)
+    # update_fields_from_phi first imposes the electrode potentials
+    # (overwritePhi), as the reference's extension does
+    phi_el = phi.copy()
+    oracle.overwrite_phi(w.GX, w.GY, oracle.Electrodes(w.rects), phi_el)
+    ef = oracle.efield(w.GX, w.GY, *lib_dx(w), phi_el)
     bzn = np.full(g.nodes, bz)
     ctom = w.species[species][0] / w.species[species][1]
     ref = pts.copy()
@@ -298,3 +302,66 @@ def test_load_plasma_counts_and_moments():
         assert abs(st[k].std() / sig - 1) < 0.02
         assert abs(st[k].mean()) < 0.02 * sig
     assert (st["fx"] >= 0).all() and (st["fx"] < 1).all()
+
+
+def test_converging_flow_overflow_and_far_jumps(oracle):
+    """Movers that find their target cell full (the side list, the fix-up,
+    particles carried on the list across steps, re-layout) and jumps of more
+    than one cell: after two pushes in a uniform field-free flow the
+    particles are those of the FP64 oracle, as a multiset."""
+    import pic_b200 as P
+    w = small_workload(nx=24, ny=24)
+    w.b0 = 0.0
+    dx, dy = lib_dx(w)
+    pts = []
+    rng = np.random.default_rng(9)
+    # 50 particles in each of the 8 cells around (12, 12), all moving exactly
+    # into the centre cell; the centre cell itself holds 50 stayers
+    for sx in (-1, 0, 1):
+        for sy in (-1, 0, 1):
+            p = np.zeros(50, P.POINT_DTYPE)
+            p["x"] = (12 + sx + rng.uniform(0.3, 0.7, 50)) * dx
+            p["y"] = (12 + sy + rng.uniform(0.3, 0.7, 50)) * dy
+            p["vx"] = -sx * dx / w.dt
+            p["vy"] = -sy * dy / w.dt
+            pts.append(p)
+    # far jumps: 3 cells per step to the right
+    far = np.zeros(40, P.POINT_DTYPE)
+    far["x"] = (3 + rng.uniform(0.2, 0.8, 40)) * dx
+    far["y"] = (5 + rng.uniform(0.2, 0.8, 40)) * dy
+    far["vx"] = 3 * dx / w.dt
+    pts.append(far)
+    pts = np.concatenate(pts)
+    pts["vz"] = np.arange(len(pts), dtype=np.float64) + 1.0   # tags
+    g = oracle_grid(oracle, w)
+    ef = np.zeros((g.nodes, 2))
+    bz = np.zeros(g.nodes)
+    ref = pts.copy()
+    with make_pic(w) as pic:
+        pic.import_points(0, pts)
+        pic.set_phi(np.zeros(g.nodes))
+        pic.update_fields()
+        for k in range(2):
+            pic.move_particles(0)
+            oracle.push(g, ref, w.species[0][0] / w.species[0][1], w.dt, ef, bz)
+            if k == 0:   # everything converged on one cell (its slots overflowed)
+                assert pic.bin_counts(0).reshape(w.GY, w.GX)[12, 12] == 450
+        got = export_state(pic, 0)
+        counts = pic.bin_counts(0)
+        # the deposit of the state equals a fresh deposit
+        pic.zero_rho()
+        pic.charge_deposition(0)
+        fin = pic.final_mesh(0)
+    live = ref[ref["pointer"] != -1]
+    assert len(got["cell"]) == len(live) == len(pts)
+    tag = got["vz"].astype(np.int64) - 1
+    order = np.argsort(tag)
+    assert np.array_equal(tag[order], np.arange(len(pts)))
+    lv = live[np.argsort((live["vz"] - 1).astype(np.int64))]
+    xg = (got["cell"][order] % w.nx + got["fx"][order].astype(np.float64)) * dx
+    yg = (got["cell"][order] // w.nx + got["fy"][order].astype(np.float64)) * dy
+    assert np.abs(xg - lv["x"]).max() <= 2e-6 * dx and np.abs(yg - lv["y"]).max() <= 2e-6 * dy
+    assert np.array_equal(counts, oracle.bucket_counts(g, lv))
+    sp, wgt = oracle_species(oracle, w, 0)
+    fin_o, _ = oracle.deposit(g, lv, sp, wgt, EPS0)
+    assert np.abs(fin - fin_o).max() <= 2e-6 * np.abs(fin_o).max()
