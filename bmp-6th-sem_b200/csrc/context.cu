@@ -301,12 +301,25 @@ int pic_create(const pic_config* cfg_in, pic_ctx** out) {
                 dval[(size_t)j * GX + i] = R.potential;
             }
     }
-    for (int i = 0; i < GX; ++i)
-        if (!mask[i] || !mask[(size_t)(GY - 1) * GX + i])
-            return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
-    for (int j = 0; j < GY; ++j)
-        if (!mask[(size_t)j * GX] || !mask[(size_t)j * GX + GX - 1])
-            return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
+    const bool periodic = cfg.periodic_y != 0;
+    if (!periodic) {
+        for (int i = 0; i < GX; ++i)
+            if (!mask[i] || !mask[(size_t)(GY - 1) * GX + i])
+                return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
+        for (int j = 0; j < GY; ++j)
+            if (!mask[(size_t)j * GX] || !mask[(size_t)j * GX + GX - 1])
+                return fail(PIC_ERR_CONFIG, "every wall node must be an electrode (generateCoeffs)");
+    } else {
+        // generateCoeffsPeriodic (src/poissonSolver.cpp:82-180) couples i-1
+        // and i+1 across row ends: the x walls of the solved rows must be
+        // electrodes
+        for (int j = 0; j < GY - 1; ++j)
+            if (!mask[(size_t)j * GX] || !mask[(size_t)j * GX + GX - 1])
+                return fail(PIC_ERR_CONFIG,
+                            "periodic in y: the x = 0 and x = nx node columns must be electrodes");
+        if (cfg.warm_start == PIC_WARM_LEARNED)
+            return fail(PIC_ERR_CONFIG, "periodic in y: the learned warm start is not available");
+    }
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -329,6 +342,9 @@ int pic_create(const pic_config* cfg_in, pic_ctx** out) {
     c->GY = GY;
     c->nodes = (int64_t)GX * GY;
     c->ncells = (int64_t)cfg.nx * cfg.ny;
+    c->periodic = periodic;
+    c->solve_rows = periodic ? GY - 1 : GY;
+    c->solve_nodes = (int64_t)GX * c->solve_rows;
     c->dx = cfg.xmax / cfg.nx;  // readPICDAT, src/particles.cpp:360-361
     c->dy = cfg.ymax / cfg.ny;
     c->device = cfg.device;
@@ -719,6 +735,8 @@ int pic_set_poisson(pic_ctx* c, int solver, int warm, double tol, int maxit) {
         return fail(PIC_ERR_ARG, "unknown solver");
     if (warm < PIC_WARM_ZERO || warm > PIC_WARM_LEARNED) return fail(PIC_ERR_ARG, "unknown warm start");
     if (!(tol > 0) || maxit <= 0) return fail(PIC_ERR_ARG, "tol and maxit must be positive");
+    if (c->periodic && warm == PIC_WARM_LEARNED)
+        return fail(PIC_ERR_CONFIG, "periodic in y: the learned warm start is not available");
     c->ps.solver = solver;
     c->ps.warm = warm;
     c->ps.tol = tol;

@@ -182,6 +182,12 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     const int sx = ok ? (int)fsx : 0, sy = ok ? (int)fsy : 0;
     o.gx = gx + sx;
     o.gy = gy + sy;
+    // periodic in y (modulo(y, H), src/mover.cpp:317-320): the cell row
+    // wraps, the offset stays
+    if (k.pery && (unsigned)o.gy >= (unsigned)ny) {
+        o.gy %= ny;
+        if (o.gy < 0) o.gy += ny;
+    }
     // absorbing walls (src/mover.cpp:325): outside [0,W) x [0,H)
     const bool alive = ok && (unsigned)o.gx < (unsigned)nx && (unsigned)o.gy < (unsigned)ny;
     o.left = ok ? (o.gx < 0) : (px < 0.0f);
@@ -1040,6 +1046,7 @@ int scan_cells(pic_ctx* c, Species& sp, const uint32_t* in, uint32_t* out, uint3
 SpeciesConsts push_consts(const pic_ctx* c, const Species& sp) {
     SpeciesConsts k = sp.k;
     k.bzu = c->bz_uniform ? 1 : 0;
+    k.pery = c->periodic ? 1 : 0;
     const float t = k.h * (float)c->bz_value;
     k.bt = t;
     k.bs = (float)(2.0 * (double)t / (1.0 + (double)t * (double)t));

@@ -64,6 +64,7 @@ struct SpeciesConsts {
     // s = 2t/(1+t^2), the same for every particle
     int bzu;
     float bt, bs;
+    int pery;  // periodic in y: the cell row wraps modulo ny
 };
 
 // Cell-sorted state of one species (one buffer of a double buffer):
@@ -118,6 +119,8 @@ struct Species {
 };
 
 // Multigrid level (FP32).
+// A multigrid level: GX x GY nodes.  Periodic in y, GY counts the distinct
+// rows (the row above the last is row 0).
 struct MGLevel {
     int nx, ny, GX, GY;
     int64_t nodes;
@@ -147,6 +150,10 @@ struct PoissonState {
     double last_relres = 0, last_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float* net_guess = nullptr;  // learned warm start output (nodes), optional
+    // false: no multigrid hierarchy (periodic in y with an odd row count, or
+    // a coarsest level too large for one block); the solve is
+    // Jacobi-preconditioned
+    bool mg_ok = true;
     // levels >= fused_first run in one thread block (k_mg_fused)
     int fused_first = 0;
     size_t fused_smem = 0;
@@ -167,6 +174,11 @@ struct pic_ctx {
     int nx = 0, ny = 0, GX = 0, GY = 0;
     int64_t nodes = 0, ncells = 0;
     double dx = 0, dy = 0;
+    // periodic in y: the potential is solved on node rows 0..GY-2 (row GY-1
+    // repeats row 0); otherwise on all GY rows.  solve_nodes = GX*solve_rows.
+    bool periodic = false;
+    int solve_rows = 0;
+    int64_t solve_nodes = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;

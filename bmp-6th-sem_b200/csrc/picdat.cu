@@ -125,7 +125,7 @@ int read_picdat(const char* path, PicdatFile& f) {
     return PIC_OK;
 }
 
-int read_geometry(const char* path, int GX, int GY, std::vector<pic_rect>& rects) {
+int read_geometry(const char* path, int GX, int GY, int periodic, std::vector<pic_rect>& rects) {
     std::vector<std::vector<std::string>> b;
     PIC_TRY(read_blocks(path, b));
     std::vector<std::vector<std::string>> blk;
@@ -135,6 +135,10 @@ int read_geometry(const char* path, int GX, int GY, std::vector<pic_rect>& rects
     int count = 0;
     if (!parse_line(blk[0].back(), count) || count < 0 || count > PIC_MAX_RECTS)
         return fail(PIC_ERR_CONFIG, "geometry.conf: bad rectangle count");
+    // readGeometry, src/particles.cpp:651-654: a periodic run has the two
+    // x walls and at most one more electrode
+    if (periodic && count > 3)
+        return fail(PIC_ERR_CONFIG, "geometry.conf: a periodic boundary expects at most 3 rectangles");
     rects.clear();
     for (const std::string& row : blk[1]) {
         if ((int)rects.size() == count) break;
@@ -160,10 +164,8 @@ int config_from_files(const char* picdat_path, const char* geometry_path, pic_co
                       PicdatFile* file_out) {
     PicdatFile f;
     PIC_TRY(read_picdat(picdat_path, f));
-    if (f.periodic != 0)
-        return fail(PIC_ERR_CONFIG, "periodic boundaries are not supported by this library");
     std::vector<pic_rect> rects;
-    PIC_TRY(read_geometry(geometry_path, f.nx + 1, f.ny + 1, rects));
+    PIC_TRY(read_geometry(geometry_path, f.nx + 1, f.ny + 1, f.periodic != 0, rects));
     pic_config_default(cfg);
     cfg->nx = f.nx;
     cfg->ny = f.ny;
@@ -187,6 +189,7 @@ int config_from_files(const char* picdat_path, const char* geometry_path, pic_co
     for (size_t r = 0; r < rects.size(); ++r) cfg->rects[r] = rects[r];
     cfg->timesteps = f.timesteps;
     cfg->print_interval = f.print_interval;
+    cfg->periodic_y = f.periodic != 0 ? 1 : 0;
     if (file_out) *file_out = f;
     return PIC_OK;
 }

@@ -41,7 +41,7 @@ struct PicdatFile {
 };
 
 int read_picdat(const char* path, PicdatFile& f);
-int read_geometry(const char* path, int GX, int GY, std::vector<pic_rect>& rects);
+int read_geometry(const char* path, int GX, int GY, int periodic, std::vector<pic_rect>& rects);
 int config_from_files(const char* picdat_path, const char* geometry_path, pic_config* cfg,
                       PicdatFile* file_out);
 

@@ -74,6 +74,7 @@ enum {
 
 struct Grid64 {
     int GX, GY;
+    int64_t n;  // solved nodes: GX * (GY, or GY-1 when periodic in y)
     double cx, cy, cd;
 };
 
@@ -133,6 +134,21 @@ __device__ __forceinline__ double dirv(const uint8_t* mask, const double* dv, in
     return mask[k] ? dv[k] : 0.0;
 }
 
+// The nodes one row up / down, rows wrapping at n = GX * rows.  Periodic in
+// y the system wraps (generateCoeffsPeriodic, src/poissonSolver.cpp:82-180);
+// with walls the first and last rows are electrodes, whose stencils are
+// never evaluated, so there the wrap is never taken.
+template <typename I>
+__device__ __forceinline__ I row_up(I k, I n, int GX) {
+    const I u = k + GX;
+    return u >= n ? u - n : u;
+}
+template <typename I>
+__device__ __forceinline__ I row_dn(I k, I n, int GX) {
+    const I d = k - GX;
+    return d < 0 ? d + n : d;
+}
+
 // overwriteRho (src/poissonSolver.cpp:384-402) in place: b = -rho, electrode
 // nodes b = -V.  Also imposes the electrode potentials on phi and, for a
 // zero warm start, clears phi.
@@ -163,16 +179,17 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_setup(Grid64 g, const uint8
                                                            float* r32, double* partials,
                                                            int nblocks, unsigned* arrive,
                                                            double* scal) {
-    const int64_t nodes = (int64_t)g.GX * g.GY;
+    const int64_t nodes = g.n;
     double acc[2] = {0.0, 0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
         double ri = 0.0;
         if (!mask[i]) {
-            const double ax = g.cd * x[i] - g.cx * (x[i - 1] + x[i + 1]) - g.cy * (x[i - g.GX] + x[i + g.GX]);
+            const int64_t up = row_up(i, nodes, g.GX), dn = row_dn(i, nodes, g.GX);
+            const double ax = g.cd * x[i] - g.cx * (x[i - 1] + x[i + 1]) - g.cy * (x[dn] + x[up]);
             ri = b[i] - ax;
             const double br = b[i] + g.cx * (dirv(mask, dv, i - 1) + dirv(mask, dv, i + 1)) +
-                              g.cy * (dirv(mask, dv, i - g.GX) + dirv(mask, dv, i + g.GX));
+                              g.cy * (dirv(mask, dv, dn) + dirv(mask, dv, up));
             acc[1] += br * br;
         }
         r[i] = ri;
@@ -226,13 +243,14 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_ap(Grid64 g, const uint8_t*
                                                         const double* p, double* q,
                                                         double* partials, int nblocks,
                                                         unsigned* arrive, double* scal) {
-    const int64_t nodes = (int64_t)g.GX * g.GY;
+    const int64_t nodes = g.n;
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
         double qi = 0.0;
         if (!mask[i])
-            qi = g.cd * p[i] - g.cx * (p[i - 1] + p[i + 1]) - g.cy * (p[i - g.GX] + p[i + g.GX]);
+            qi = g.cd * p[i] - g.cx * (p[i - 1] + p[i + 1]) -
+                 g.cy * (p[row_dn(i, nodes, g.GX)] + p[row_up(i, nodes, g.GX)]);
         q[i] = qi;
         acc[0] += p[i] * qi;
     }
@@ -283,12 +301,13 @@ __global__ void __launch_bounds__(kRedThreads) k_true_residual(Grid64 g, const u
                                                                const double* b, const double* x,
                                                                double* partials, int nblocks,
                                                                unsigned* arrive, double* scal) {
-    const int64_t nodes = (int64_t)g.GX * g.GY;
+    const int64_t nodes = g.n;
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
         if (!mask[i]) {
-            const double ax = g.cd * x[i] - g.cx * (x[i - 1] + x[i + 1]) - g.cy * (x[i - g.GX] + x[i + g.GX]);
+            const double ax = g.cd * x[i] - g.cx * (x[i - 1] + x[i + 1]) -
+                              g.cy * (x[row_dn(i, nodes, g.GX)] + x[row_up(i, nodes, g.GX)]);
             const double ri = b[i] - ax;
             acc[0] += ri * ri;
         }
@@ -326,17 +345,23 @@ __global__ void k_mg_rbgs(LevelDev L, int color) {
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = 2 * h + ((j + color) & 1);
     if (i >= L.GX || j >= L.GY) return;
-    const int64_t k = (int64_t)j * L.GX + i;
+    const int k = j * L.GX + i, n = L.GX * L.GY;
     if (L.mask[k]) return;
-    const float s = __fmaf_rn(L.cx, L.x[k - 1] + L.x[k + 1], __fmaf_rn(L.cy, L.x[k - L.GX] + L.x[k + L.GX], L.b[k]));
+    const float s = __fmaf_rn(L.cx, L.x[k - 1] + L.x[k + 1],
+                              __fmaf_rn(L.cy, L.x[row_dn(k, n, L.GX)] + L.x[row_up(k, n, L.GX)], L.b[k]));
     L.x[k] = s / L.cd;
 }
 
+// Residual at fine node (i, j); 0 outside the x range and at electrodes.
+// Rows wrap (only reached periodic in y: with walls the restriction of an
+// interior coarse node stays inside the fine rows).
 __device__ __forceinline__ float fine_residual(const LevelDev& F, int i, int j) {
-    if (i < 0 || j < 0 || i >= F.GX || j >= F.GY) return 0.0f;
-    const int64_t k = (int64_t)j * F.GX + i;
+    if (i < 0 || i >= F.GX) return 0.0f;
+    j = j < 0 ? j + F.GY : (j >= F.GY ? j - F.GY : j);
+    const int k = j * F.GX + i, n = F.GX * F.GY;
     if (F.mask[k]) return 0.0f;
-    const float ax = F.cd * F.x[k] - F.cx * (F.x[k - 1] + F.x[k + 1]) - F.cy * (F.x[k - F.GX] + F.x[k + F.GX]);
+    const float ax = F.cd * F.x[k] - F.cx * (F.x[k - 1] + F.x[k + 1]) -
+                     F.cy * (F.x[row_dn(k, n, F.GX)] + F.x[row_up(k, n, F.GX)]);
     return F.b[k] - ax;
 }
 
@@ -367,13 +392,14 @@ __global__ void k_mg_prolong(LevelDev F, LevelDev C) {
     const int64_t k = (int64_t)j * F.GX + i;
     if (F.mask[k]) return;
     const int I = i >> 1, J = j >> 1;
+    const int J1 = J + 1 == C.GY ? 0 : J + 1;  // wraps only periodic in y
     const bool ox = i & 1, oy = j & 1;
     auto X = [&](int a, int b) { return C.x[(int64_t)b * C.GX + a]; };
     float v;
     if (!ox && !oy) v = X(I, J);
     else if (ox && !oy) v = 0.5f * (X(I, J) + X(I + 1, J));
-    else if (!ox && oy) v = 0.5f * (X(I, J) + X(I, J + 1));
-    else v = 0.25f * (X(I, J) + X(I + 1, J) + X(I, J + 1) + X(I + 1, J + 1));
+    else if (!ox && oy) v = 0.5f * (X(I, J) + X(I, J1));
+    else v = 0.25f * (X(I, J) + X(I + 1, J) + X(I, J1) + X(I + 1, J1));
     F.x[k] += v;
 }
 
@@ -423,19 +449,22 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
             const int j = (int)__umulhi((uint32_t)h, rcp);
             const int i = 2 * (h - j * hw) + ((j + color) & 1);
             if (i >= GX) continue;
-            const int k = j * GX + i;
+            const int k = j * GX + i, n = GX * GY;
             if (m[k]) continue;
-            x[k] = __fmaf_rn(cx, x[k - 1] + x[k + 1], __fmaf_rn(cy, x[k - GX] + x[k + GX], b[k])) * icd;
+            x[k] = __fmaf_rn(cx, x[k - 1] + x[k + 1],
+                             __fmaf_rn(cy, x[row_dn(k, n, GX)] + x[row_up(k, n, GX)], b[k])) * icd;
         }
         __syncthreads();
     };
     auto residual = [&](int l, int i, int j) -> float {
-        const int GX = F.GX[l];
-        if (i < 0 || j < 0 || i >= GX || j >= F.GY[l]) return 0.0f;
-        const int k = j * GX + i;
+        const int GX = F.GX[l], GY = F.GY[l];
+        if (i < 0 || i >= GX) return 0.0f;
+        j = j < 0 ? j + GY : (j >= GY ? j - GY : j);  // wraps only periodic in y
+        const int k = j * GX + i, n = GX * GY;
         if (M(l)[k]) return 0.0f;
         const float* x = X(l);
-        const float ax = F.cd[l] * x[k] - F.cx[l] * (x[k - 1] + x[k + 1]) - F.cy[l] * (x[k - GX] + x[k + GX]);
+        const float ax = F.cd[l] * x[k] - F.cx[l] * (x[k - 1] + x[k + 1]) -
+                         F.cy[l] * (x[row_dn(k, n, GX)] + x[row_up(k, n, GX)]);
         return B(l)[k] - ax;
     };
     for (int l = 0; l < F.n - 1; ++l) {
@@ -485,12 +514,13 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
         for (int k = tid; k < n; k += kFusedThreads) {
             if (M(l)[k]) continue;
             const int i = k % GX, j = k / GX, I = i >> 1, J = j >> 1;
+            const int J1 = J + 1 == F.GY[l + 1] ? 0 : J + 1;  // wraps only periodic in y
             const bool ox = i & 1, oy = j & 1;
             float v;
             if (!ox && !oy) v = xc[J * CGX + I];
             else if (ox && !oy) v = 0.5f * (xc[J * CGX + I] + xc[J * CGX + I + 1]);
-            else if (!ox && oy) v = 0.5f * (xc[J * CGX + I] + xc[(J + 1) * CGX + I]);
-            else v = 0.25f * (xc[J * CGX + I] + xc[J * CGX + I + 1] + xc[(J + 1) * CGX + I] + xc[(J + 1) * CGX + I + 1]);
+            else if (!ox && oy) v = 0.5f * (xc[J * CGX + I] + xc[J1 * CGX + I]);
+            else v = 0.25f * (xc[J * CGX + I] + xc[J * CGX + I + 1] + xc[J1 * CGX + I] + xc[J1 * CGX + I + 1]);
             X(l)[k] += v;
         }
         __syncthreads();
@@ -510,25 +540,41 @@ __global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
     fused_body(F, smem);
 }
 
-// injected Dirichlet mask of a coarse level
+// injected Dirichlet mask of a coarse level: the x walls (and, unless
+// periodic in y, the y walls) are Dirichlet, inner nodes take the fine
+// node's flag
 __global__ void k_mg_coarse_mask(const uint8_t* fmask, int fGX, int fGY, uint8_t* cmask, int cGX,
-                                 int cGY) {
+                                 int cGY, int periodic) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= cGX || J >= cGY) return;
     const int i = 2 * I, j = 2 * J;
     uint8_t m = 1;
-    if (I > 0 && J > 0 && I < cGX - 1 && J < cGY - 1 && i < fGX && j < fGY)
+    if (I > 0 && I < cGX - 1 && (periodic || (J > 0 && J < cGY - 1)) && i < fGX && j < fGY)
         m = fmask[(int64_t)j * fGX + i];
     cmask[(int64_t)J * cGX + I] = m;
 }
 
-// ---- E field (calculateElectricField, src/poissonSolver.cpp:433-456) -----
-// Interior: central differences.  Boundary nodes take the value of the
-// nearest interior node (columns first, then rows, as the reference copies).
+// ---- E field ----------------------------------------------------------------
+// With walls (calculateElectricField, src/poissonSolver.cpp:433-456): central
+// differences inside; boundary nodes take the value of the nearest interior
+// node (columns first, then rows, as the reference copies).
+// Periodic in y (calculateElectricFieldPeriodic, :411-430): E_x one-sided at
+// the first and last column, central elsewhere; E_y central with rows taken
+// modulo GY-1; both on every row.
 
 __device__ __forceinline__ void efield_at(const double* phi, int GX, int GY, double dx, double dy,
-                                          int i, int j, double& ex, double& ey) {
+                                          int i, int j, int periodic, double& ex, double& ey) {
+    if (periodic) {
+        const int64_t k = (int64_t)j * GX + i;
+        if (i == 0) ex = -((phi[k + 1] - phi[k]) / dx);
+        else if (i == GX - 1) ex = -((phi[k] - phi[k - 1]) / dx);
+        else ex = -((phi[k + 1] - phi[k - 1]) / (2 * dx));
+        const int P = GY - 1;
+        const int ju = j + 1 >= P ? j + 1 - P : j + 1, jd = j == 0 ? P - 1 : j - 1;
+        ey = -((phi[(int64_t)ju * GX + i] - phi[(int64_t)jd * GX + i]) / (2 * dy));
+        return;
+    }
     const int ci = min(max(i, 1), GX - 2), cj = min(max(j, 1), GY - 2);
     const int64_t k = (int64_t)cj * GX + ci;
     ex = -((phi[k + 1] - phi[k - 1]) / (2 * dx));
@@ -536,22 +582,23 @@ __device__ __forceinline__ void efield_at(const double* phi, int GX, int GY, dou
 }
 
 __global__ void k_efield(const double* phi, const double* bz, int GX, int GY, double dx, double dy,
-                         float4* fld) {
+                         int periodic, float4* fld) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= GX || j >= GY) return;
     double ex, ey;
-    efield_at(phi, GX, GY, dx, dy, i, j, ex, ey);
+    efield_at(phi, GX, GY, dx, dy, i, j, periodic, ex, ey);
     const int64_t k = (int64_t)j * GX + i;
     fld[k] = make_float4((float)ex, (float)ey, (float)bz[k], 0.0f);
 }
 
-__global__ void k_efield64(const double* phi, int GX, int GY, double dx, double dy, double* out) {
+__global__ void k_efield64(const double* phi, int GX, int GY, double dx, double dy, int periodic,
+                           double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= GX || j >= GY) return;
     double ex, ey;
-    efield_at(phi, GX, GY, dx, dy, i, j, ex, ey);
+    efield_at(phi, GX, GY, dx, dy, i, j, periodic, ex, ey);
     const int64_t k = (int64_t)j * GX + i;
     out[2 * k] = ex;
     out[2 * k + 1] = ey;
@@ -573,6 +620,7 @@ Grid64 fine_grid(pic_ctx* c) {
     Grid64 g;
     g.GX = c->GX;
     g.GY = c->GY;
+    g.n = c->solve_nodes;
     g.cx = 1.0 / (c->dx * c->dx);
     g.cy = 1.0 / (c->dy * c->dy);
     g.cd = 2.0 * (g.cx + g.cy);
@@ -627,11 +675,11 @@ int enqueue_iteration(pic_ctx* c, cudaStream_t st, bool jacobi,
     unsigned* arrive = arrive_ptr(ps);
     int launches = 0;
     if (!jacobi) launches += enqueue_vcycle(c, st);
-    k_pcg_rz<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
+    k_pcg_rz<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
                                          jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
-    k_pcg_p<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.z, ps.p[0], ps.scal);
+    k_pcg_p<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.z, ps.p[0], ps.scal);
     k_pcg_ap<<<nb, kRedThreads, 0, st>>>(g, c->mask, ps.p[0], ps.q, ps.partials, nb, arrive, ps.scal);
-    k_pcg_update<<<nb, kRedThreads, 0, st>>>(c->nodes, c->mask, ps.p[0], ps.q, c->phi, ps.r,
+    k_pcg_update<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.p[0], ps.q, c->phi, ps.r,
                                              ps.levels[0].b, ps.partials, nb, arrive, ps.scal);
     k_pcg_cond<<<1, 1, 0, st>>>(ps.scal, handle, use_handle);
     return launches + 5;
@@ -708,17 +756,21 @@ int poisson_setup(pic_ctx* c) {
     PIC_CUDA(cudaMallocHost(&ps.host_scal, 16 * sizeof(double)));
     PIC_CUDA(cudaEventCreate(&ps.ev0));
     PIC_CUDA(cudaEventCreate(&ps.ev1));
-    // multigrid hierarchy
+    // multigrid hierarchy.  Periodic in y a level has `ny` distinct rows,
+    // which must be even for the red-black sweeps; coarsening halves them
+    // while the result stays even.
     int nx = c->nx, ny = c->ny;
+    const bool per = c->periodic;
+    ps.mg_ok = !per || ny % 2 == 0;
     double hx = c->dx, hy = c->dy;
     const uint8_t* prev_mask = c->mask;
-    int pGX = c->GX, pGY = c->GY;
+    int pGX = c->GX, pGY = c->solve_rows;
     for (int l = 0; l < 16; ++l) {
         MGLevel L{};
         L.nx = nx;
         L.ny = ny;
         L.GX = nx + 1;
-        L.GY = ny + 1;
+        L.GY = per ? ny : ny + 1;
         L.nodes = (int64_t)L.GX * L.GY;
         L.cx = (float)(1.0 / (hx * hx));
         L.cy = (float)(1.0 / (hy * hy));
@@ -733,16 +785,18 @@ int poisson_setup(pic_ctx* c) {
             PIC_CUDA(cudaMalloc(&L.mask, (size_t)L.nodes));
             const dim3 b2(32, 8);
             k_mg_coarse_mask<<<grid2d(L.GX, L.GY, b2), b2, 0, c->stream>>>(prev_mask, pGX, pGY,
-                                                                           L.mask, L.GX, L.GY);
+                                                                           L.mask, L.GX, L.GY,
+                                                                           per ? 1 : 0);
             PIC_CUDA(cudaGetLastError());
         }
         ps.levels.push_back(L);
-        if (std::min(nx, ny) <= 2) break;
+        if (!ps.mg_ok) break;  // level 0 only: the PCG's single-precision residual
+        if (per ? (nx <= 2 || ny % 4 != 0) : std::min(nx, ny) <= 2) break;
         prev_mask = L.mask;
         pGX = L.GX;
         pGY = L.GY;
         nx = (nx + 1) / 2;
-        ny = (ny + 1) / 2;
+        ny = per ? ny / 2 : (ny + 1) / 2;
         hx *= 2;
         hy *= 2;
     }
@@ -760,7 +814,15 @@ int poisson_setup(pic_ctx* c) {
         total += level_bytes(l);
         kf = l;
     }
-    if (kf == L) return fail(PIC_ERR_CONFIG, "coarsest multigrid level does not fit in shared memory");
+    if (kf == L && ps.mg_ok) {
+        // only periodic in y can stop coarsening early (rows no longer even)
+        if (!per) return fail(PIC_ERR_CONFIG, "coarsest multigrid level does not fit in shared memory");
+        ps.mg_ok = false;
+    }
+    if (!ps.mg_ok) {
+        PIC_CUDA(cudaStreamCreateWithFlags(&ps.cap_stream, cudaStreamNonBlocking));
+        return PIC_OK;
+    }
     ps.fused_first = kf;
     FusedLevels F{};
     F.n = L - kf;
@@ -826,7 +888,7 @@ int poisson_solve(pic_ctx* c) {
     const Grid64 g = fine_grid(c);
     const int nb = ps.nblocks;
     unsigned* arrive = arrive_ptr(ps);
-    const bool jacobi = ps.solver == PIC_SOLVER_JACOBI_PCG;
+    const bool jacobi = ps.solver == PIC_SOLVER_JACOBI_PCG || !ps.mg_ok;
     const int slot = jacobi ? 1 : 0;
     PIC_CUDA(cudaEventRecord(ps.ev0, c->stream));
     prof_begin(c, PIC_PHASE_POISSON);
@@ -901,6 +963,7 @@ int poisson_solve(pic_ctx* c) {
     const int it = (int)ps.host_scal[S_IT];
     if (ps.gexec[slot]) c->launches += (int64_t)it * ps.body_nodes[slot] + 1;
     if (ws_active && status == PIC_OK) PIC_TRY(ws_after_solve(c, c->ws_record));
+    if (c->periodic) PIC_TRY(overwrite_phi(c));  // the last row repeats row 0
     PIC_TRY(fields_from_phi(c));
     prof_end(c, PIC_PHASE_POISSON);
     PIC_CUDA(cudaEventRecord(ps.ev1, c->stream));
@@ -916,16 +979,30 @@ int poisson_solve(pic_ctx* c) {
     return PIC_OK;
 }
 
-// overwritePhi (src/poissonSolver.cpp:364-382): electrode nodes take their
-// potential.
-__global__ void k_overwrite_phi(int64_t nodes, const uint8_t* mask, const double* dv, double* phi) {
+// overwritePhi (src/poissonSolver.cpp:364-382): periodic in y, row 0 is
+// first copied into the last row; then electrode nodes take their potential.
+// The thread of a first-row node also writes the last-row node of its
+// column, from the first row's value before the electrodes.
+__global__ void k_overwrite_phi(int64_t nodes, int GX, int periodic, const uint8_t* mask,
+                                const double* dv, double* phi) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nodes && mask[i]) phi[i] = dv[i];
+    if (i >= nodes) return;
+    const int64_t last = nodes - GX;
+    if (periodic) {
+        if (i >= last) return;
+        if (i < GX) {
+            const double v0 = phi[i];
+            phi[last + i] = mask[last + i] ? dv[last + i] : v0;
+            phi[i] = mask[i] ? dv[i] : v0;
+            return;
+        }
+    }
+    if (mask[i]) phi[i] = dv[i];
 }
 
 int overwrite_phi(pic_ctx* c) {
-    k_overwrite_phi<<<(unsigned)((c->nodes + 255) / 256), 256, 0, c->stream>>>(c->nodes, c->mask, c->dir_val,
-                                                                              c->phi);
+    k_overwrite_phi<<<(unsigned)((c->nodes + 255) / 256), 256, 0, c->stream>>>(
+        c->nodes, c->GX, c->periodic ? 1 : 0, c->mask, c->dir_val, c->phi);
     c->launches += 1;
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
@@ -934,7 +1011,7 @@ int overwrite_phi(pic_ctx* c) {
 int fields_from_phi(pic_ctx* c) {
     const dim3 b2(32, 8);
     k_efield<<<grid2d(c->GX, c->GY, b2), b2, 0, c->stream>>>(c->phi, c->bz, c->GX, c->GY, c->dx,
-                                                             c->dy, c->fld);
+                                                             c->dy, c->periodic ? 1 : 0, c->fld);
     c->launches += 1;
     PIC_CUDA(cudaGetLastError());
     c->fields_valid = true;
@@ -944,7 +1021,7 @@ int fields_from_phi(pic_ctx* c) {
 int efield_export(pic_ctx* c) {
     const dim3 b2(32, 8);
     k_efield64<<<grid2d(c->GX, c->GY, b2), b2, 0, c->stream>>>(c->phi, c->GX, c->GY, c->dx, c->dy,
-                                                               c->efield64);
+                                                               c->periodic ? 1 : 0, c->efield64);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
@@ -977,7 +1054,9 @@ struct BatchInst {
     int GX, GY;
     double cx, cy, cd;
     double dx, dy;
-    int64_t nodes;
+    int64_t nodes;  // all GX*GY nodes
+    int64_t sn;     // solved nodes (GX*(GY-1) when periodic in y)
+    int periodic;
     const uint8_t* mask;
     const double* dv;
     double* rho;  // becomes the right-hand side b
@@ -1083,7 +1162,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
         return t;
     };
     auto stencil64 = [&](const double* x, int64_t k) {
-        return I->cd * x[k] - I->cx * (x[k - 1] + x[k + 1]) - I->cy * (x[k - I->GX] + x[k + I->GX]);
+        return I->cd * x[k] - I->cx * (x[k - 1] + x[k + 1]) -
+               I->cy * (x[row_dn(k, I->sn, I->GX)] + x[row_up(k, I->sn, I->GX)]);
     };
 
     // overwriteRho and the electrode potentials (zero start: phi = 0 elsewhere)
@@ -1102,12 +1182,13 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
     // r = b - A x, MG input r32; |r|^2 and |b_red|^2
     if (I) {
         double rr = 0.0, bb = 0.0;
-        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+        for (int64_t k = ltid; k < I->sn; k += lsize) {
             double ri = 0.0;
             if (!I->mask[k]) {
                 ri = I->rho[k] - stencil64(I->phi, k);
                 const double br = I->rho[k] + I->cx * (dirv(I->mask, I->dv, k - 1) + dirv(I->mask, I->dv, k + 1)) +
-                                  I->cy * (dirv(I->mask, I->dv, k - I->GX) + dirv(I->mask, I->dv, k + I->GX));
+                                  I->cy * (dirv(I->mask, I->dv, row_dn(k, I->sn, I->GX)) +
+                                           dirv(I->mask, I->dv, row_up(k, I->sn, I->GX)));
                 bb += br * br;
             }
             I->r[k] = ri;
@@ -1138,7 +1219,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
         auto half_sweep = [&](int l, int color) {
             if (on && l < I->kf) {
                 const LevelDev& L = I->lev[l];
-                const int hw = (L.GX + 1) >> 1, n = hw * L.GY, ls = (int)lsize;
+                const int hw = (L.GX + 1) >> 1, n = hw * L.GY, ls = (int)lsize, nl = L.GX * L.GY;
                 for (int h0 = (int)ltid; h0 < n; h0 += 4 * ls) {
                     int k[4];
                     bool ok[4];
@@ -1155,7 +1236,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
                         v[u] = ok[u] ? __fmaf_rn(L.cx, L.x[k[u] - 1] + L.x[k[u] + 1],
-                                                 __fmaf_rn(L.cy, L.x[k[u] - L.GX] + L.x[k[u] + L.GX], L.b[k[u]]))
+                                                 __fmaf_rn(L.cy, L.x[row_dn(k[u], nl, L.GX)] + L.x[row_up(k[u], nl, L.GX)],
+                                                           L.b[k[u]]))
                                      : 0.0f;
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
@@ -1219,13 +1301,14 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
                     if (F.mask[k]) continue;
                     const int j = k / F.GX, x = k - j * F.GX;
                     const int cI = x >> 1, cJ = j >> 1;
+                    const int cJ1 = cJ + 1 == C.GY ? 0 : cJ + 1;  // wraps only periodic in y
                     const bool ox = x & 1, oy = j & 1;
                     auto X = [&](int a, int b) { return cxv[b * C.GX + a]; };
                     float v;
                     if (!ox && !oy) v = X(cI, cJ);
                     else if (ox && !oy) v = 0.5f * (X(cI, cJ) + X(cI + 1, cJ));
-                    else if (!ox && oy) v = 0.5f * (X(cI, cJ) + X(cI, cJ + 1));
-                    else v = 0.25f * (X(cI, cJ) + X(cI + 1, cJ) + X(cI, cJ + 1) + X(cI + 1, cJ + 1));
+                    else if (!ox && oy) v = 0.5f * (X(cI, cJ) + X(cI, cJ1));
+                    else v = 0.25f * (X(cI, cJ) + X(cI + 1, cJ) + X(cI, cJ1) + X(cI + 1, cJ1));
                     fx[k] += v;
                 }
             }
@@ -1242,7 +1325,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             const double* __restrict__ rv = I->r;
             double* __restrict__ zv = I->z;
             const uint8_t* __restrict__ mk = I->mask;
-            const int nn = (int)I->nodes;
+            const int nn = (int)I->sn;
 #pragma unroll 4
             for (int k = (int)ltid; k < nn; k += (int)lsize) {
                 const double zi = mk[k] ? 0.0 : (double)x0[k];
@@ -1260,7 +1343,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             const double* __restrict__ zv = I->z;
             double* __restrict__ pv = I->p;
             const uint8_t* __restrict__ mk = I->mask;
-            const int nn = (int)I->nodes;
+            const int nn = (int)I->sn;
 #pragma unroll 4
             for (int k = (int)ltid; k < nn; k += (int)lsize) pv[k] = mk[k] ? 0.0 : zv[k] + beta * pv[k];
         }
@@ -1270,11 +1353,13 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             const double* __restrict__ pv = I->p;
             double* __restrict__ qv = I->q;
             const uint8_t* __restrict__ mk = I->mask;
-            const int nn = (int)I->nodes, GX = I->GX;
+            const int nn = (int)I->sn, GX = I->GX;
             const double cd = I->cd, cx = I->cx, cy = I->cy;
 #pragma unroll 4
             for (int k = (int)ltid; k < nn; k += (int)lsize) {
-                const double qi = mk[k] ? 0.0 : cd * pv[k] - cx * (pv[k - 1] + pv[k + 1]) - cy * (pv[k - GX] + pv[k + GX]);
+                const double qi = mk[k] ? 0.0
+                                        : cd * pv[k] - cx * (pv[k - 1] + pv[k + 1]) -
+                                              cy * (pv[row_dn(k, nn, GX)] + pv[row_up(k, nn, GX)]);
                 qv[k] = qi;
                 pq += pv[k] * qi;
             }
@@ -1292,7 +1377,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             double* __restrict__ rv = I->r;
             float* __restrict__ b0 = I->lev[0].b;
             const uint8_t* __restrict__ mk = I->mask;
-            const int nn = (int)I->nodes;
+            const int nn = (int)I->sn;
 #pragma unroll 4
             for (int k = (int)ltid; k < nn; k += (int)lsize) {
                 double ri = 0.0;
@@ -1327,7 +1412,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
     // true residual of every instance, then its E field
     if (I) {
         double rr = 0.0;
-        for (int64_t k = ltid; k < I->nodes; k += lsize) {
+        for (int64_t k = ltid; k < I->sn; k += lsize) {
             if (I->mask[k]) continue;
             const double ri = I->rho[k] - stencil64(I->phi, k);
             rr += ri * ri;
@@ -1339,11 +1424,19 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
         I->scal[S_TRUE_RR] = total(0);
         if (*err) I->scal[S_STATUS] = 3.0;
     }
+    if (I->periodic) {
+        // overwritePhi: the last row repeats row 0 (final, electrodes
+        // included), then takes its own electrodes
+        const int64_t last = I->nodes - I->GX;
+        for (int64_t i = ltid; i < I->GX; i += lsize)
+            I->phi[last + i] = I->mask[last + i] ? I->dv[last + i] : I->phi[i];
+        grid.sync();
+    }
     if (I) {
         for (int64_t k = ltid; k < I->nodes; k += lsize) {
             const int x = (int)(k % I->GX), j = (int)(k / I->GX);
             double ex, ey;
-            efield_at(I->phi, I->GX, I->GY, I->dx, I->dy, x, j, ex, ey);
+            efield_at(I->phi, I->GX, I->GY, I->dx, I->dy, x, j, I->periodic, ex, ey);
             I->fld[k] = make_float4((float)ex, (float)ey, (float)I->bz[k], 0.0f);
         }
     }
@@ -1360,7 +1453,8 @@ int poisson_batch_describe(pic_ctx* c, void* host_desc, const void* dev_fused, i
     PoissonState& ps = c->ps;
     if (ps.fused_first + 1 > kMaxBatchLevels) return fail(PIC_ERR_CONFIG, "too many multigrid levels for the batched solve");
     if (ps.warm == PIC_WARM_LEARNED) return fail(PIC_ERR_CONFIG, "the batched solve has no learned warm start");
-    if (ps.solver != PIC_SOLVER_MG_PCG) return fail(PIC_ERR_CONFIG, "the batched solve is MG-PCG only");
+    if (ps.solver != PIC_SOLVER_MG_PCG || !ps.mg_ok)
+        return fail(PIC_ERR_CONFIG, "the batched solve is MG-PCG only (periodic in y: ny must be even)");
     BatchInst I{};
     const Grid64 g = fine_grid(c);
     I.GX = g.GX;
@@ -1371,6 +1465,8 @@ int poisson_batch_describe(pic_ctx* c, void* host_desc, const void* dev_fused, i
     I.dx = c->dx;
     I.dy = c->dy;
     I.nodes = c->nodes;
+    I.sn = c->solve_nodes;
+    I.periodic = c->periodic ? 1 : 0;
     I.mask = c->mask;
     I.dv = c->dir_val;
     I.rho = c->rho;

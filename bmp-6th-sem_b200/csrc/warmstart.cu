@@ -1080,6 +1080,8 @@ int pic_ws_record(pic_ctx* c, int64_t max_pairs, double phi_scale, double db_sca
         c->ws_record = false;
         return PIC_OK;
     }
+    if (c->periodic && max_pairs > 0)
+        return fail(PIC_ERR_CONFIG, "periodic in y: the learned warm start is not available");
     PIC_TRY(ws_alloc(c));
     Net& N = c->ws->net;
     if (max_pairs < 0) {  // stop and release the dataset

@@ -56,6 +56,7 @@ class Config(ctypes.Structure):
         ("poisson_tol", ctypes.c_double), ("poisson_maxit", ctypes.c_int32),
         ("deposit_energy", ctypes.c_int32), ("device", ctypes.c_int32),
         ("timesteps", ctypes.c_int32), ("print_interval", ctypes.c_int32),
+        ("periodic_y", ctypes.c_int32),
     ]
 
 
@@ -196,9 +197,10 @@ def _p(a: np.ndarray):
 
 def make_config(nx, ny, xmax, ymax, dt, species, rects, b0=0.0, epsilon=8.854e-12,
                 surf_area=0.0, solver=SOLVER_MG_PCG, warm=WARM_PREVIOUS, tol=1e-8, maxit=500,
-                deposit_energy=True, device=0) -> Config:
+                deposit_energy=True, device=0, periodic_y=False) -> Config:
     """species: list of (charge, mass, sim_count, actual_count);
-    rects: list of (x1, y1, x2, y2, volts) node-index rectangles."""
+    rects: list of (x1, y1, x2, y2, volts) node-index rectangles;
+    periodic_y: the reference's periodicBoundary = 1."""
     cfg = Config()
     _check(lib().pic_config_default(ctypes.byref(cfg)))
     cfg.nx, cfg.ny, cfg.xmax, cfg.ymax = nx, ny, xmax, ymax
@@ -213,6 +215,7 @@ def make_config(nx, ny, xmax, ymax, dt, species, rects, b0=0.0, epsilon=8.854e-1
     cfg.poisson_tol, cfg.poisson_maxit = tol, maxit
     cfg.deposit_energy = 1 if deposit_energy else 0
     cfg.device = device
+    cfg.periodic_y = 1 if periodic_y else 0
     return cfg
 
 

@@ -82,6 +82,16 @@ def wall_rects(nx: int, ny: int, left=0.0, right=0.0, top=0.0, bottom=0.0) -> li
     return [(0, 0, 0, ny, left), (nx, 0, nx, ny, right), (0, ny, nx, ny, top), (0, 0, nx, 0, bottom)]
 
 
+def periodic_rects(nx: int, ny: int, left=0.0, right=0.0, inner=None) -> list:
+    """Electrodes of a run periodic in y: the two x walls over the full
+    height, plus at most one more rectangle (readGeometry allows three,
+    SYCL-PIC-poissonsolver/src/particles.cpp:651-654)."""
+    r = [(0, 0, 0, ny, left), (nx, 0, nx, ny, right)]
+    if inner is not None:
+        r.append(tuple(inner))
+    return r
+
+
 def _species(nx, ny, ppc, n0):
     sim = float(ppc * nx * ny)
     return [(-QE, ME, sim, n0), (QE, M_AR, sim, n0)]

@@ -112,6 +112,14 @@ typedef struct pic_config {
     int32_t device;           /* CUDA device ordinal                       */
     int32_t timesteps;        /* informational (M_PICDAT TIMESTEPS)        */
     int32_t print_interval;   /* informational (M_PICDAT printInterval)    */
+    /* 1: periodic in y (M_PICDAT periodicBoundary; src/poissonSolver.cpp:
+     * 82-180, 411-430, src/mover.cpp:317-320).  The potential is solved on
+     * node rows 0..ny-1, row ny is a copy of row 0 (then the electrodes),
+     * E_y wraps, E_x is one-sided at the x walls, and the push wraps y into
+     * [0, ymax).  The node columns x = 0 and x = nx must be electrodes on
+     * rows 0..ny-1.  Multigrid needs ny even (a Jacobi-preconditioned solve
+     * is used otherwise); the learned warm start is not available. */
+    int32_t periodic_y;
 } pic_config;
 
 /* Uniform Maxwellian plasma plus an optional Gaussian blob, generated on the

@@ -95,13 +95,17 @@ def lib():
             "orc_bucket_sort": (i64, [vp, i64, i32, vp, vp, vp]),
             "orc_deposit": (None, [P(Grid), vp, i64, dbl, dbl, dbl, dbl, vp, vp, vp]),
             "orc_push": (i64, [P(Grid), vp, i64, dbl, dbl, vp, vp, P(i64)]),
+            "orc_push_mode": (i64, [P(Grid), vp, i64, dbl, dbl, vp, vp, i32, P(i64)]),
             "orc_kinetic_energy": (dbl, [vp, i64, dbl]),
             "orc_geom_from_fractions": (None, [i32, i32, vp, i32, vp]),
             "orc_electrode_mask": (None, [i32, i32, vp, i32, vp]),
             "orc_build_csr": (i64, [i32, i32, dbl, dbl, vp, vp, vp, vp]),
+            "orc_build_csr_periodic": (i64, [i32, i32, dbl, dbl, vp, vp, vp, vp]),
             "orc_overwrite_rho": (None, [i32, i32, vp, i32, vp]),
             "orc_overwrite_phi": (None, [i32, i32, vp, i32, vp]),
+            "orc_overwrite_phi_periodic": (None, [i32, i32, vp, i32, vp]),
             "orc_efield": (None, [i32, i32, dbl, dbl, vp, vp]),
+            "orc_efield_periodic": (None, [i32, i32, dbl, dbl, vp, vp]),
             "orc_apply_a": (None, [i32, i32, dbl, dbl, vp, vp, vp]),
             "orc_cg_solve": (ctypes.c_int, [i32, i32, dbl, dbl, vp, vp, vp, dbl, ctypes.c_int, P(dbl)]),
             "orc_hm_create": (vp, [i32, i32, dbl]),
@@ -217,12 +221,14 @@ def deposit(g: Grid, pts: np.ndarray, sp: Species, weighing: float, eps: float,
 
 
 def push(g: Grid, pts: np.ndarray, ctom: float, dt: float, efield: np.ndarray,
-         bz: np.ndarray):
-    """MoverKernel semantics, in place.  Returns (deleted, left_exits)."""
+         bz: np.ndarray, periodic: bool = False):
+    """MoverKernel semantics, in place (periodic: y wrapped by modulo(y, H)
+    first).  Returns (deleted, left_exits)."""
     left = ctypes.c_int64(0)
     assert efield.shape == (g.nodes, 2) and efield.dtype == np.float64
-    deleted = lib().orc_push(ctypes.byref(g), _ptr(pts), len(pts), ctom, dt,
-                             _ptr(np.ascontiguousarray(efield)), _ptr(bz), ctypes.byref(left))
+    deleted = lib().orc_push_mode(ctypes.byref(g), _ptr(pts), len(pts), ctom, dt,
+                                  _ptr(np.ascontiguousarray(efield)), _ptr(bz),
+                                  1 if periodic else 0, ctypes.byref(left))
     return int(deleted), int(left.value)
 
 
@@ -257,14 +263,32 @@ def overwrite_rho(GX: int, GY: int, el: Electrodes, rho: np.ndarray) -> None:
     lib().orc_overwrite_rho(GX, GY, ctypes.cast(arr, ctypes.c_void_p), len(el.rects), _ptr(rho))
 
 
-def overwrite_phi(GX: int, GY: int, el: Electrodes, phi: np.ndarray) -> None:
+def build_csr_periodic(GX: int, GY: int, dx: float, dy: float, mask: np.ndarray):
+    """generateCoeffsPeriodic as a SciPy CSR matrix over GX*(GY-1) nodes."""
+    import scipy.sparse as sps
+    n = GX * (GY - 1)
+    row_ptr = np.zeros(n + 1, np.int64)
+    col = np.zeros(5 * n, np.int64)
+    val = np.zeros(5 * n)
+    nnz = lib().orc_build_csr_periodic(GX, GY, dx, dy, _ptr(mask), _ptr(row_ptr), _ptr(col),
+                                       _ptr(val))
+    if nnz < 0:
+        raise ValueError("periodic system: the first and last node columns must be electrodes")
+    return sps.csr_matrix((val[:nnz], col[:nnz], row_ptr), shape=(n, n))
+
+
+def overwrite_phi(GX: int, GY: int, el: Electrodes, phi: np.ndarray,
+                  periodic: bool = False) -> None:
     arr = el.c_array()
-    lib().orc_overwrite_phi(GX, GY, ctypes.cast(arr, ctypes.c_void_p), len(el.rects), _ptr(phi))
+    fn = lib().orc_overwrite_phi_periodic if periodic else lib().orc_overwrite_phi
+    fn(GX, GY, ctypes.cast(arr, ctypes.c_void_p), len(el.rects), _ptr(phi))
 
 
-def efield(GX: int, GY: int, dx: float, dy: float, phi: np.ndarray) -> np.ndarray:
+def efield(GX: int, GY: int, dx: float, dy: float, phi: np.ndarray,
+           periodic: bool = False) -> np.ndarray:
     ef = np.zeros((GX * GY, 2))
-    lib().orc_efield(GX, GY, dx, dy, _ptr(phi), _ptr(ef))
+    fn = lib().orc_efield_periodic if periodic else lib().orc_efield
+    fn(GX, GY, dx, dy, _ptr(phi), _ptr(ef))
     return ef
 
 
@@ -274,10 +298,18 @@ def apply_a(GX, GY, dx, dy, mask, x):
     return y
 
 
-def reduced_relres(GX, GY, dx, dy, mask, b, phi) -> float:
+def reduced_relres(GX, GY, dx, dy, mask, b, phi, periodic: bool = False) -> float:
     """||b_int - A_int phi|| / ||b_int|| over the non-electrode rows, where
     b_int carries the known electrode neighbours across (the measure used for
-    the 1e-8 target)."""
+    the 1e-8 target).  periodic: the system of rows 0..GY-2."""
+    if periodic:
+        n = GX * (GY - 1)
+        A = build_csr_periodic(GX, GY, dx, dy, mask)
+        m, bb, ph = mask[:n] == 1, b[:n], phi[:n]
+        r = (bb - A @ ph)[~m]
+        bi = (bb - A[:, np.flatnonzero(m)] @ ph[m])[~m]
+        nb = np.linalg.norm(bi)
+        return float(np.linalg.norm(r) / (nb if nb > 0 else 1.0))
     r = b - apply_a(GX, GY, dx, dy, mask, phi)
     inner = mask == 0
     cx, cy = 1.0 / dx ** 2, 1.0 / dy ** 2
@@ -303,23 +335,36 @@ class DirectPoisson:
     """PARDISO restatement: SuperLU on the generateCoeffs matrix, factored once
     (phases 11+22) and re-solved every step (phase 33).  Single-threaded."""
 
-    def __init__(self, GX: int, GY: int, dx: float, dy: float, el: Electrodes):
+    def __init__(self, GX: int, GY: int, dx: float, dy: float, el: Electrodes,
+                 periodic: bool = False):
         import scipy.sparse.linalg as spla
         self.GX, self.GY, self.dx, self.dy, self.el = GX, GY, dx, dy, el
+        self.periodic = periodic
         self.mask = electrode_mask(GX, GY, el)
-        self.A = build_csr(GX, GY, dx, dy, self.mask)
+        self.A = (build_csr_periodic if periodic else build_csr)(GX, GY, dx, dy, self.mask)
+        self.n = self.A.shape[0]
         self.lu = spla.splu(self.A.tocsc())
 
     def solve_rhs(self, b: np.ndarray) -> np.ndarray:
-        return self.lu.solve(b)
+        """LU solve plus two steps of iterative refinement.  PARDISO (mtype
+        11 defaults: scaling and weighted matching) reaches round-off on this
+        system; SuperLU on the unscaled matrix (electrode rows of order 1,
+        stencil rows of order 1/dx^2) can stop near 1e-8 relative without
+        the refinement."""
+        x = self.lu.solve(b)
+        for _ in range(2):
+            x += self.lu.solve(b - self.A @ x)
+        return x
 
     def step(self, rho: np.ndarray):
         """poissonSolver(): rho is overwritten in place (becomes the RHS);
-        returns (phi, efield)."""
+        returns (phi, efield).  Periodic: PARDISO sees the first GX*(GY-1)
+        entries of rho and writes those of phi; overwritePhi fills row GY-1."""
         overwrite_rho(self.GX, self.GY, self.el, rho)
-        phi = self.lu.solve(rho)
-        overwrite_phi(self.GX, self.GY, self.el, phi)
-        ef = efield(self.GX, self.GY, self.dx, self.dy, phi)
+        phi = np.zeros(self.GX * self.GY)
+        phi[:self.n] = self.solve_rhs(rho[:self.n])
+        overwrite_phi(self.GX, self.GY, self.el, phi, self.periodic)
+        ef = efield(self.GX, self.GY, self.dx, self.dy, phi, self.periodic)
         return phi, ef
 
 

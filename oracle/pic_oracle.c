@@ -222,12 +222,24 @@ static inline void mover_one(orc_point* q, const orc_grid* g, double pctm, doubl
     q->x = px; q->y = py; q->z = pz; q->vx = pvx; q->vy = pvy; q->vz = pvz;
 }
 
-/* MoverKernel, src/mover.cpp:304-366, semantic form (non-periodic):
- * push every live particle; a particle with x outside [0,W) or y outside
- * [0,H) is deleted (pointer = -1) and counted as a left exit when x < 0.
- * Returns the number deleted; *left_exits receives the x<0 count. */
-int64_t orc_push(const orc_grid* g, orc_point* p, int64_t n, double ctom, double dt,
-                 const double* efield, const double* bz, int64_t* left_exits) {
+/* modulo(), src/mover.cpp:13-22: x wrapped into [0, y); a negative exact
+ * multiple of y gives 0. */
+static inline double ref_modulo(double x, double y) {
+    if (x < 0) {
+        if ((int)(x / y) == x / y) return 0;
+        return y - fmod(-x, y);
+    }
+    return fmod(x, y);
+}
+
+/* MoverKernel, src/mover.cpp:304-366, semantic form: push every live
+ * particle; with periodic_y the new y is first wrapped by modulo(y, H)
+ * (:317-320).  A particle with x outside [0,W) or y outside [0,H) is deleted
+ * (pointer = -1) and counted as a left exit when x < 0.  Returns the number
+ * deleted; *left_exits receives the x<0 count. */
+int64_t orc_push_mode(const orc_grid* g, orc_point* p, int64_t n, double ctom, double dt,
+                      const double* efield, const double* bz, int32_t periodic_y,
+                      int64_t* left_exits) {
     const double W = g->nx * g->dx, H = g->ny * g->dy;
     int64_t deleted = 0, left = 0;
 #pragma omp parallel for schedule(static) reduction(+ : deleted, left)
@@ -235,6 +247,7 @@ int64_t orc_push(const orc_grid* g, orc_point* p, int64_t n, double ctom, double
         orc_point* q = &p[i];
         if (q->pointer == -1) continue;
         mover_one(q, g, ctom, dt, efield, bz);
+        if (periodic_y) q->y = ref_modulo(q->y, H);
         const double px = q->x, py = q->y;
         if (px >= W || px < 0.0 || py >= H || py < 0) {
             q->pointer = -1;
@@ -244,6 +257,11 @@ int64_t orc_push(const orc_grid* g, orc_point* p, int64_t n, double ctom, double
     }
     if (left_exits) *left_exits = left;
     return deleted;
+}
+
+int64_t orc_push(const orc_grid* g, orc_point* p, int64_t n, double ctom, double dt,
+                 const double* efield, const double* bz, int64_t* left_exits) {
+    return orc_push_mode(g, p, n, ctom, dt, efield, bz, 0, left_exits);
 }
 
 /* calculate_energy(), src/utils.cpp:77-118: sum of 0.5*v^2/|q/m| (eV). */
@@ -310,6 +328,37 @@ int64_t orc_build_csr(int32_t GX, int32_t GY, double dx, double dy, const uint8_
     return idx;
 }
 
+/* generateCoeffsPeriodic(), src/poissonSolver.cpp:82-180, 0-based CSR over
+ * the N = GX*(GY-1) nodes of rows 0..GY-2 (row GY-1 is row 0): electrode row
+ * = [-1]; other rows the 5-point stencil with the row above the last row
+ * being row 0 and the row below row 0 the last row (columns i+-GX modulo N).
+ * Returns nnz, or -1 when a non-electrode node lies in the first or last
+ * column (the reference's i-1 / i+1 would then reach into another row, or
+ * outside the matrix at node 0). */
+int64_t orc_build_csr_periodic(int32_t GX, int32_t GY, double dx, double dy, const uint8_t* mask,
+                               int64_t* row_ptr, int64_t* col, double* val) {
+    const double inv_dx2 = 1.0 / (dx * dx), inv_dy2 = 1.0 / (dy * dy);
+    const int64_t N = (int64_t)GX * (GY - 1);
+    int64_t idx = 0;
+    row_ptr[0] = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        if (mask[i] == 1) {
+            val[idx] = -1; col[idx] = i; idx++;
+        } else {
+            const int64_t c = i % GX;
+            if (c == 0 || c == GX - 1) return -1;
+            val[idx + 0] = -inv_dy2; col[idx + 0] = (i - GX + N) % N;
+            val[idx + 1] = -inv_dx2; col[idx + 1] = i - 1;
+            val[idx + 2] = 2 * (inv_dx2 + inv_dy2); col[idx + 2] = i;
+            val[idx + 3] = -inv_dx2; col[idx + 3] = i + 1;
+            val[idx + 4] = -inv_dy2; col[idx + 4] = (i + GX) % N;
+            idx += 5;
+        }
+        row_ptr[i + 1] = idx;
+    }
+    return idx;
+}
+
 /* overwriteRho(), src/poissonSolver.cpp:384-402: electrode nodes <- V, then
  * the whole array is negated (it becomes PARDISO's right-hand side). */
 void orc_overwrite_rho(int32_t GX, int32_t GY, const orc_geom* geo, int32_t count, double* rho) {
@@ -325,6 +374,35 @@ void orc_overwrite_phi(int32_t GX, int32_t GY, const orc_geom* geo, int32_t coun
     for (int32_t i = 0; i < count; ++i)
         for (int32_t j = geo[i].y1; j <= geo[i].y2; ++j)
             for (int32_t k = geo[i].x1; k <= geo[i].x2; ++k) phi[(size_t)j * GX + k] = geo[i].potential;
+}
+
+/* overwritePhi() with periodicBoundary, src/poissonSolver.cpp:364-382: row 0
+ * is copied into row GY-1, then the electrode potentials are imposed. */
+void orc_overwrite_phi_periodic(int32_t GX, int32_t GY, const orc_geom* geo, int32_t count,
+                                double* phi) {
+    memcpy(phi + (size_t)(GY - 1) * GX, phi, sizeof(double) * (size_t)GX);
+    orc_overwrite_phi(GX, GY, geo, count, phi);
+}
+
+/* calculateElectricFieldPeriodic(), src/poissonSolver.cpp:411-430: fx is
+ * one-sided at the first and last column and central elsewhere, on every
+ * row; fy is central with rows taken modulo GY-1, on every row. */
+void orc_efield_periodic(int32_t GX, int32_t GY, double dx, double dy, const double* phi,
+                         double* efield) {
+    for (int32_t i = 0; i < GY; ++i) {
+        const size_t a = (size_t)i * GX;
+        efield[2 * a] = -((phi[a + 1] - phi[a]) / dx);
+        for (int32_t j = 1; j < GX - 1; ++j)
+            efield[2 * (a + j)] = -((phi[a + j + 1] - phi[a + j - 1]) / (2 * dx));
+        const size_t b = a + GX - 1;
+        efield[2 * b] = -((phi[b] - phi[b - 1]) / dx);
+    }
+    const int32_t P = GY - 1;
+    for (int32_t j = 0; j < GX; ++j)
+        for (int32_t i = 0; i < GY; ++i) {
+            const size_t up = (size_t)((i + 1) % P) * GX + j, dn = (size_t)((i - 1 + P) % P) * GX + j;
+            efield[2 * ((size_t)i * GX + j) + 1] = -((phi[up] - phi[dn]) / (2 * dy));
+        }
 }
 
 /* calculateElectricField(), src/poissonSolver.cpp:433-456: central

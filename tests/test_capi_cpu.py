@@ -146,7 +146,8 @@ def test_config_box_init_surface_area(picb, tmp_path):
     assert np.isclose(cfg.surf_area, 0.5 * 0.064 * 0.5 * 0.032)
 
 
-def test_config_rejects_periodic_and_missing_files(picb, tmp_path):
+def test_config_rejects_bad_periodic_geometry_and_missing_files(picb, tmp_path):
+    # five rectangles with a periodic boundary (readGeometry: at most three)
     p, g = _write_inputs(tmp_path, periodic=1)
     cfg = picb.Config()
     assert picb.lib().pic_config_from_files(p.encode(), g.encode(), ctypes.byref(cfg)) == -2
