@@ -22,7 +22,10 @@
  * PARDISO dumps (SYCL-PIC-poissonsolver/validation_dumps, 257x257 nodes).
  * Binning, deposit and push have no reference fixtures; for them parity is
  * pinned only through this restatement of the reference source (unpinned by
- * golden vectors).
+ * golden vectors).  The same holds for the periodic-in-y variants
+ * (orc_push_mode, orc_build_csr_periodic, orc_overwrite_phi_periodic,
+ * orc_efield_periodic), which the tests pin by properties of the periodic
+ * system instead.
  */
 #include <math.h>
 #include <stdint.h>
