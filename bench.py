@@ -589,11 +589,16 @@ def run_e2e(pic, steps, n_part, it0):
     pic.synchronize()
     t = time.perf_counter() - t0
     split = {"import_s": t1 - t0, "steps_s": t2 - t1, "export_s": t0 + t - t2}
-    h2d = sum(len(h) for h in host) * P.POINT_DTYPE.itemsize
-    d2h = sum(len(o) for o in out) * P.POINT_DTYPE.itemsize
+    # bytes on the host link: the library moves 24-byte records (cell,
+    # FP32 offsets and velocities); the caller's arrays hold 56-byte Points
+    rec = 24
+    h2d = sum(len(h) for h in host) * rec
+    d2h = sum(len(o) for o in out) * rec
     return {"value": n_part * steps / t, "unit": UNIT,
             "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps + pic.nodes * 8,
+            "link_bytes_per_particle": rec,
+            "api_bytes_per_particle": P.POINT_DTYPE.itemsize,
             "wall_s": t, "split": split,
             "what": "pic_import_points (both species) + K x (zero_rho, charge_deposition x2, "
                     "pic_get_rho to host, move_particles x2) + pic_export_points; E held "

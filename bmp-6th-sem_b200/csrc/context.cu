@@ -9,12 +9,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "pic_internal.h"
+
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 namespace picb200 {
 
@@ -36,30 +41,33 @@ static int check_species(pic_ctx* c, int s) {
 // ---------------------------------------------------------------------------
 // Host <-> device streaming of large arrays (particles, grids).  Caller memory
 // is ordinary pageable memory, so every copy passes through pinned staging:
-// two kPipeChunk buffers alternate, the host-side copy of one chunk (split
-// over a pool of threads) overlapping the DMA of the other.
+// two kPipeChunk buffers alternate, the host-side work on one chunk (a copy,
+// or the Point <-> record conversion, split over a pool of threads)
+// overlapping the DMA of the other.
 // ---------------------------------------------------------------------------
 namespace {
 
-class CopyPool {
+class HostPool {
   public:
-    static CopyPool& get() {
-        static CopyPool pool;
+    static HostPool& get() {
+        static HostPool pool;
         return pool;
     }
 
-    void copy(void* dst, const void* src, size_t bytes) {
-        if (bytes < (4u << 20) || workers_.empty()) {
-            std::memcpy(dst, src, bytes);
+    // fn(begin, end) over [0, n) in one part per thread, part boundaries
+    // multiples of `align`; on the calling thread alone below `serial_below`.
+    void run(size_t n, size_t align, size_t serial_below, const std::function<void(size_t, size_t)>& fn) {
+        if (n < serial_below || workers_.empty()) {
+            if (n) fn(0, n);
             return;
         }
         std::lock_guard<std::mutex> one_at_a_time(call_mu_);
         const int parts = (int)workers_.size() + 1;
         {
             std::lock_guard<std::mutex> lk(mu_);
-            dst_ = static_cast<char*>(dst);
-            src_ = static_cast<const char*>(src);
-            bytes_ = bytes;
+            job_ = &fn;
+            n_ = n;
+            align_ = align;
             parts_ = parts;
             pending_ = parts - 1;
             ++gen_;
@@ -68,9 +76,16 @@ class CopyPool {
         part(0);
         std::unique_lock<std::mutex> lk(mu_);
         done_.wait(lk, [&] { return pending_ == 0; });
+        job_ = nullptr;
     }
 
-    ~CopyPool() {
+    void copy(void* dst, const void* src, size_t bytes) {
+        char* d = static_cast<char*>(dst);
+        const char* s = static_cast<const char*>(src);
+        run(bytes, 64, 4u << 20, [&](size_t a, size_t b) { std::memcpy(d + a, s + a, b - a); });
+    }
+
+    ~HostPool() {
         {
             std::lock_guard<std::mutex> lk(mu_);
             stop_ = true;
@@ -80,17 +95,16 @@ class CopyPool {
     }
 
   private:
-    CopyPool() {
+    HostPool() {
         const unsigned hw = std::thread::hardware_concurrency();
         const int n = (int)std::min<unsigned>(hw ? hw : 1u, 16u) - 1;
         for (int i = 0; i < n; ++i) workers_.emplace_back([this, i] { loop(i + 1); });
     }
 
     void part(int i) {
-        // 64-byte aligned part boundaries
-        const size_t per = ((bytes_ / parts_) + 63) & ~(size_t)63;
-        const size_t a = std::min(bytes_, per * (size_t)i), b = std::min(bytes_, per * (size_t)(i + 1));
-        if (b > a) std::memcpy(dst_ + a, src_ + a, b - a);
+        const size_t per = ((n_ / parts_) + align_ - 1) / align_ * align_;
+        const size_t a = std::min(n_, per * (size_t)i), b = std::min(n_, per * (size_t)(i + 1));
+        if (b > a) (*job_)(a, b);
     }
 
     void loop(int i) {
@@ -113,9 +127,8 @@ class CopyPool {
     uint64_t gen_ = 0;
     int pending_ = 0, parts_ = 1;
     bool stop_ = false;
-    char* dst_ = nullptr;
-    const char* src_ = nullptr;
-    size_t bytes_ = 0;
+    const std::function<void(size_t, size_t)>* job_ = nullptr;
+    size_t n_ = 0, align_ = 1;
 };
 
 constexpr size_t kPipeChunk = 32u << 20;
@@ -139,7 +152,7 @@ static int stream_to_device(pic_ctx* c, void* dev, const void* host, size_t byte
         const size_t m = std::min(kPipeChunk, bytes - off);
         const int b = (int)(k & 1);
         if (k >= 2) PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));  // its previous DMA is done
-        CopyPool::get().copy(c->pipe_buf[b], static_cast<const char*>(host) + off, m);
+        HostPool::get().copy(c->pipe_buf[b], static_cast<const char*>(host) + off, m);
         PIC_CUDA(cudaMemcpyAsync(static_cast<char*>(dev) + off, c->pipe_buf[b], m,
                                  cudaMemcpyHostToDevice, c->stream));
         PIC_CUDA(cudaEventRecord(c->pipe_ev[b], c->stream));
@@ -167,7 +180,7 @@ static int stream_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes)
         const int b = (int)(k & 1);
         PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));
         const size_t off = k * kPipeChunk, m = std::min(kPipeChunk, bytes - off);
-        CopyPool::get().copy(static_cast<char*>(host) + off, c->pipe_buf[b], m);
+        HostPool::get().copy(static_cast<char*>(host) + off, c->pipe_buf[b], m);
     }
     return PIC_OK;
 }
@@ -179,6 +192,140 @@ static int copy_to_host(pic_ctx* c, void* host, const void* dev, size_t bytes) {
 
 static int copy_to_device(pic_ctx* c, void* dev, const void* host, size_t bytes) {
     return stream_to_device(c, dev, host, bytes);
+}
+
+// Reference Point -> record, as InsertKernel bins it (src/particles.cpp:
+// 230-235): cell ((int)(y*(1/dy)), (int)(x*(1/dx))), the FP32 offset being
+// the FP64 remainder clamped below 1.  Dead (pointer == -1) and out-of-domain
+// points get kNoCell.  Plain IEEE double arithmetic (the host build does not
+// contract products into FMAs).
+static inline PointRec point_to_rec(const pic_point& p, int nx, int ny, double inv_dx,
+                                    double inv_dy) {
+    PointRec r{kNoCell, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (p.pointer == -1) return r;
+    const double sx = p.x * inv_dx, sy = p.y * inv_dy;
+    if (!(sx >= 0.0 && sy >= 0.0 && sx < (double)nx && sy < (double)ny)) return r;
+    const int gx = (int)sx, gy = (int)sy;
+    constexpr float kOneBelow = 0x1.fffffep-1f;
+    r.cell = (uint32_t)gy * (uint32_t)nx + (uint32_t)gx;
+    r.fx = std::min((float)(sx - gx), kOneBelow);
+    r.fy = std::min((float)(sy - gy), kOneBelow);
+    r.vx = (float)p.vx;
+    r.vy = (float)p.vy;
+    r.vz = (float)p.vz;
+    return r;
+}
+
+// Record -> reference Point: x = (gx + fx)*dx in FP64; pointer = the
+// particle's index in the output.
+static inline void rec_to_point(const PointRec& r, int nx, double dx, double dy, int64_t index,
+                                pic_point& p) {
+    const int gx = (int)(r.cell % (uint32_t)nx), gy = (int)(r.cell / (uint32_t)nx);
+    p.x = ((double)gx + (double)r.fx) * dx;
+    p.y = ((double)gy + (double)r.fy) * dy;
+    p.z = 0.0;
+    p.vx = r.vx;
+    p.vy = r.vy;
+    p.vz = r.vz;
+    p.pointer = (int32_t)index;
+    p.pad_ = 0;
+}
+
+// Stores of 8-byte words that bypass the cache (no read-for-ownership of
+// the destination line): the conversions below are bound by host memory
+// traffic, and their outputs are not read again by this thread.
+static inline void put8(void* dst, const void* src) {
+#if defined(__x86_64__)
+    long long v;
+    std::memcpy(&v, src, 8);
+    _mm_stream_si64(static_cast<long long*>(dst), v);
+#else
+    std::memcpy(dst, src, 8);
+#endif
+}
+
+static inline void store_fence() {
+#if defined(__x86_64__)
+    _mm_sfence();
+#endif
+}
+
+static inline void stream_rec(PointRec* dst, const PointRec& r) {
+    const char* s = reinterpret_cast<const char*>(&r);
+    char* d = reinterpret_cast<char*>(dst);
+    put8(d, s);
+    put8(d + 8, s + 8);
+    put8(d + 16, s + 16);
+}
+
+static inline void stream_point(pic_point* dst, const pic_point& p) {
+    const char* s = reinterpret_cast<const char*>(&p);
+    char* d = reinterpret_cast<char*>(dst);
+    for (int w = 0; w < 7; ++w) put8(d + 8 * w, s + 8 * w);
+}
+
+constexpr size_t kRecsPerChunk = kPipeChunk / sizeof(PointRec);
+
+// Host Points -> device records: the pool converts a chunk into a pinned
+// buffer while the DMA engine moves the previous one.
+static int points_to_device(pic_ctx* c, PointRec* dev, const pic_point* host, int64_t n) {
+    PIC_TRY(ensure_pipe(c));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    const int nx = c->nx, ny = c->ny;
+    const double inv_dx = 1.0 / c->dx, inv_dy = 1.0 / c->dy;
+    for (int64_t off = 0, k = 0; off < n; off += (int64_t)kRecsPerChunk, ++k) {
+        const size_t m = (size_t)std::min<int64_t>((int64_t)kRecsPerChunk, n - off);
+        const int b = (int)(k & 1);
+        if (k >= 2) PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));
+        PointRec* buf = static_cast<PointRec*>(c->pipe_buf[b]);
+        const pic_point* src = host + off;
+        HostPool::get().run(m, 64, 1u << 16, [&](size_t a, size_t e) {
+            for (size_t i = a; i < e; ++i) stream_rec(buf + i, point_to_rec(src[i], nx, ny, inv_dx, inv_dy));
+            store_fence();
+        });
+        PIC_CUDA(cudaMemcpyAsync(dev + off, buf, m * sizeof(PointRec), cudaMemcpyHostToDevice,
+                                 c->stream));
+        PIC_CUDA(cudaEventRecord(c->pipe_ev[b], c->stream));
+    }
+    return PIC_OK;
+}
+
+// Device records -> host Points, after the work queued on the stream;
+// synchronous.  The DMA of chunk k+1 overlaps the pool's expansion of chunk k.
+static int points_to_host(pic_ctx* c, pic_point* host, const PointRec* dev, int64_t n) {
+    PIC_TRY(ensure_pipe(c));
+    const int64_t nchunks = (n + (int64_t)kRecsPerChunk - 1) / (int64_t)kRecsPerChunk;
+    auto span = [&](int64_t k) {
+        return (size_t)std::min<int64_t>((int64_t)kRecsPerChunk, n - k * (int64_t)kRecsPerChunk);
+    };
+    auto issue = [&](int64_t k) -> int {
+        const int b = (int)(k & 1);
+        PIC_CUDA(cudaMemcpyAsync(c->pipe_buf[b], dev + k * (int64_t)kRecsPerChunk,
+                                 span(k) * sizeof(PointRec), cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaEventRecord(c->pipe_ev[b], c->stream));
+        return PIC_OK;
+    };
+    if (nchunks == 0) return PIC_OK;
+    const int nx = c->nx;
+    const double dx = c->dx, dy = c->dy;
+    PIC_TRY(issue(0));
+    for (int64_t k = 0; k < nchunks; ++k) {
+        if (k + 1 < nchunks) PIC_TRY(issue(k + 1));
+        const int b = (int)(k & 1);
+        PIC_CUDA(cudaEventSynchronize(c->pipe_ev[b]));
+        const PointRec* buf = static_cast<const PointRec*>(c->pipe_buf[b]);
+        const int64_t off = k * (int64_t)kRecsPerChunk;
+        pic_point* dst = host + off;
+        HostPool::get().run(span(k), 64, 1u << 16, [&](size_t a, size_t e) {
+            for (size_t i = a; i < e; ++i) {
+                pic_point p;
+                rec_to_point(buf[i], nx, dx, dy, off + (int64_t)i, p);
+                stream_point(dst + i, p);
+            }
+            store_fence();
+        });
+    }
+    return PIC_OK;
 }
 
 static cudaEvent_t pool_event(pic_ctx* c) {
@@ -423,9 +570,9 @@ int pic_import_points(pic_ctx* c, int s, const pic_point* host, int64_t n) {
     PIC_TRY(check_species(c, s));
     if (n < 0 || (n > 0 && !host)) return fail(PIC_ERR_ARG, "bad point array");
     if (n > (int64_t)0xF0000000ll) return fail(PIC_ERR_CAPACITY, "too many points");
-    pic_point* dev = nullptr;
+    PointRec* dev = nullptr;
     PIC_TRY(particles_import_staging(c, n, &dev));
-    PIC_TRY(stream_to_device(c, dev, host, (size_t)n * sizeof(pic_point)));
+    PIC_TRY(points_to_device(c, dev, host, n));
     return particles_import(c, s, n);
 }
 
@@ -437,11 +584,11 @@ int pic_export_points(pic_ctx* c, int s, pic_point* host, int64_t capacity, int6
     if (!host) return PIC_OK;  // size query
     if (capacity < n) return fail(PIC_ERR_CAPACITY, "export buffer smaller than the particle count");
     if (n == 0) return PIC_OK;
-    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(pic_point)));
-    pic_point* dev = static_cast<pic_point*>(c->staging);
+    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(PointRec)));
+    PointRec* dev = static_cast<PointRec*>(c->staging);
     int64_t n2 = 0;
     PIC_TRY(particles_export(c, s, dev, &n2));
-    return stream_to_host(c, host, dev, (size_t)n * sizeof(pic_point));
+    return points_to_host(c, host, dev, n);
 }
 
 int pic_export_state(pic_ctx* c, int s, int32_t* cell, float* fx, float* fy, float* vx,

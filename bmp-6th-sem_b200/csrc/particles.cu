@@ -828,69 +828,48 @@ __global__ void k_relayout_list(ListDev L, const uint32_t* __restrict__ nbase, u
 // Reference Point -> cell.  The cell follows InsertKernel: gx = (int)(x *
 // (1/dx)) in FP64 (src/particles.cpp:230-235); dead (pointer == -1) and
 // out-of-domain points get no cell.
-__device__ __forceinline__ uint32_t point_cell(const pic_point& p, int nx, int ny, double inv_dx,
-                                               double inv_dy, double& sx, double& sy) {
-    if (p.pointer == -1) return 0xffffffffu;
-    sx = p.x * inv_dx;
-    sy = p.y * inv_dy;
-    if (!(sx >= 0.0 && sy >= 0.0 && sx < (double)nx && sy < (double)ny)) return 0xffffffffu;
-    return (uint32_t)(int)sy * (uint32_t)nx + (uint32_t)(int)sx;
-}
-
-__global__ void k_import_count(const pic_point* __restrict__ pts, int64_t n, int nx, int ny,
-                               double inv_dx, double inv_dy, uint32_t* cell_of, uint32_t* cnt) {
+// Import of records (converted from reference Points on the host): count
+// per cell, then place each record in its cell's front run.
+__global__ void k_import_count(const PointRec* __restrict__ recs, int64_t n, uint32_t* cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double sx, sy;
-    const uint32_t cell = point_cell(pts[i], nx, ny, inv_dx, inv_dy, sx, sy);
-    cell_of[i] = cell;
-    if (cell != 0xffffffffu) atomicAdd(cnt + cell, 1u);
+    const uint32_t cell = recs[i].cell;
+    if (cell != kNoCell) atomicAdd(cnt + cell, 1u);
 }
 
-// The FP32 in-cell offset is the FP64 remainder (clamped below 1).
-__global__ void k_import_place(const pic_point* __restrict__ pts, const uint32_t* __restrict__ cell_of,
-                               int64_t n, int nx, int ny, double inv_dx, double inv_dy,
+__global__ void k_import_place(const PointRec* __restrict__ recs, int64_t n,
                                const uint32_t* __restrict__ base, uint32_t* front, float4* dst_a,
                                float* dst_vz) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t c = cell_of[i];
-    if (c == 0xffffffffu) return;
-    const pic_point p = pts[i];
-    const double sx = p.x * inv_dx, sy = p.y * inv_dy;
-    const int gx = (int)sx, gy = (int)sy;
-    const uint32_t d = base[c] + atomicAdd(front + c, 1u);
-    dst_a[d] = make_float4(fminf((float)(sx - gx), kOneBelow), fminf((float)(sy - gy), kOneBelow),
-                           (float)p.vx, (float)p.vy);
-    dst_vz[d] = (float)p.vz;
-    (void)nx;
-    (void)ny;
+    const PointRec r = recs[i];
+    if (r.cell == kNoCell) return;
+    const uint32_t d = base[r.cell] + atomicAdd(front + r.cell, 1u);
+    dst_a[d] = make_float4(r.fx, r.fy, r.vx, r.vy);
+    dst_vz[d] = r.vz;
 }
 
-// Layout -> reference Point AoS in cell order (dense[c] = particles before
-// cell c).  x = (gx + fx)*dx in FP64.
+// Layout -> records in cell order (dense[c] = particles before cell c); the
+// host expands them into reference Points.
 __global__ void k_export(const float4* __restrict__ a, const float* __restrict__ vz,
                          const uint32_t* __restrict__ base, const uint32_t* __restrict__ front,
                          const uint32_t* __restrict__ back, const uint32_t* __restrict__ dense,
-                         int nx, int64_t ncells, double dx, double dy, pic_point* out) {
+                         int64_t ncells, PointRec* out) {
     const int64_t c = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (c >= ncells) return;
     const int lane = threadIdx.x & 31;
-    const int gx = (int)(c % nx), gy = (int)(c / nx);
     const uint32_t nf = front[c], nb = back[c], b0 = base[c], back0 = base[c + 1] - nb, d0 = dense[c];
     for (uint32_t j = lane; j < nf + nb; j += 32) {
         const uint32_t i = j < nf ? b0 + j : back0 + (j - nf);
         const float4 v = a[i];
-        pic_point p;
-        p.x = ((double)gx + (double)v.x) * dx;
-        p.y = ((double)gy + (double)v.y) * dy;
-        p.z = 0.0;
-        p.vx = v.z;
-        p.vy = v.w;
-        p.vz = vz[i];
-        p.pointer = (int32_t)(d0 + j);
-        p.pad_ = 0;
-        out[d0 + j] = p;
+        PointRec r;
+        r.cell = (uint32_t)c;
+        r.fx = v.x;
+        r.fy = v.y;
+        r.vx = v.z;
+        r.vy = v.w;
+        r.vz = vz[i];
+        out[d0 + j] = r;
     }
 }
 
@@ -1385,13 +1364,9 @@ int ensure_staging(pic_ctx* c, size_t bytes) {
     return PIC_OK;
 }
 
-static size_t aligned_points_bytes(int64_t n) {
-    return ((size_t)n * sizeof(pic_point) + 255) & ~(size_t)255;
-}
-
-int particles_import_staging(pic_ctx* c, int64_t n, pic_point** dev_points) {
-    PIC_TRY(ensure_staging(c, aligned_points_bytes(n) + (size_t)n * 4 + 256));
-    *dev_points = static_cast<pic_point*>(c->staging);
+int particles_import_staging(pic_ctx* c, int64_t n, PointRec** dev_recs) {
+    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(PointRec) + 256));
+    *dev_recs = static_cast<PointRec*>(c->staging);
     return PIC_OK;
 }
 
@@ -1426,23 +1401,18 @@ static int fresh_layout(pic_ctx* c, int s) {
 
 int particles_import(pic_ctx* c, int s, int64_t n) {
     Species& sp = c->sp[s];
-    if (aligned_points_bytes(n) + (size_t)n * 4 > c->staging_bytes)
+    if ((size_t)n * sizeof(PointRec) > c->staging_bytes)
         return fail(PIC_ERR_STATE, "import staging too small");
-    const pic_point* dev_points = static_cast<const pic_point*>(c->staging);
-    uint32_t* cell_of =
-        reinterpret_cast<uint32_t*>(static_cast<char*>(c->staging) + aligned_points_bytes(n));
+    const PointRec* recs = static_cast<const PointRec*>(c->staging);
     PIC_CUDA(cudaMemsetAsync(sp.cnt, 0, (size_t)c->ncells * 4, c->stream));
-    if (n > 0)
-        k_import_count<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, n, c->nx, c->ny, 1.0 / c->dx,
-                                                              1.0 / c->dy, cell_of, sp.cnt);
+    if (n > 0) k_import_count<<<grid1d(n, 256), 256, 0, c->stream>>>(recs, n, sp.cnt);
     PIC_TRY(fresh_layout(c, s));
     const int b = sp.cur;
     PIC_CUDA(cudaMemsetAsync(sp.front[b], 0, (size_t)c->ncells * 4, c->stream));
     PIC_CUDA(cudaMemsetAsync(sp.back[b], 0, (size_t)c->ncells * 4, c->stream));
     if (n > 0)
-        k_import_place<<<grid1d(n, 256), 256, 0, c->stream>>>(dev_points, cell_of, n, c->nx, c->ny,
-                                                              1.0 / c->dx, 1.0 / c->dy, sp.base,
-                                                              sp.front[b], sp.buf[b].a, sp.buf[b].vz);
+        k_import_place<<<grid1d(n, 256), 256, 0, c->stream>>>(recs, n, sp.base, sp.front[b],
+                                                              sp.buf[b].a, sp.buf[b].vz);
     c->launches += 2;
     PIC_CUDA(cudaGetLastError());
     PIC_CUDA(cudaMemsetAsync(sp.acc_q, 0, (size_t)c->nodes * 8, c->stream));
@@ -1451,7 +1421,7 @@ int particles_import(pic_ctx* c, int s, int64_t n) {
     return PIC_OK;
 }
 
-int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out) {
+int particles_export(pic_ctx* c, int s, PointRec* dev_out, int64_t* n_out) {
     Species& sp = c->sp[s];
     int64_t n = 0;
     PIC_TRY(count_cells(c, s, &n));
@@ -1459,8 +1429,8 @@ int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out) {
     if (n == 0) return PIC_OK;
     const int b = sp.cur;
     k_export<<<grid1d(c->ncells, 8), 256, 0, c->stream>>>(sp.buf[b].a, sp.buf[b].vz, sp.base,
-                                                          sp.front[b], sp.back[b], sp.dense, c->nx,
-                                                          c->ncells, c->dx, c->dy, dev_out);
+                                                          sp.front[b], sp.back[b], sp.dense,
+                                                          c->ncells, dev_out);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }

@@ -67,6 +67,16 @@ struct SpeciesConsts {
     int pery;  // periodic in y: the cell row wraps modulo ny
 };
 
+// A particle as it crosses the host link: cell index (gy*nx + gx;
+// kNoCell: dropped) and the FP32 state, 24 bytes where the reference Point
+// has 56.  The host's thread pool converts between the two.
+struct PointRec {
+    uint32_t cell;
+    float fx, fy, vx, vy, vz;
+};
+static_assert(sizeof(PointRec) == 24, "PointRec layout");
+constexpr uint32_t kNoCell = 0xffffffffu;
+
 // Cell-sorted state of one species (one buffer of a double buffer):
 // a[i] = {fx, fy, vx, vy}, vz[i].
 struct ParticleSoA {
@@ -232,11 +242,12 @@ void prof_end(pic_ctx* c, int phase);
 int species_setup(pic_ctx* c, int s);
 int species_reserve(pic_ctx* c, int s, int64_t capacity);
 void species_free(Species& sp);
-// Stages n points for import; returns the device address to copy them to.
-int particles_import_staging(pic_ctx* c, int64_t n, pic_point** dev_points);
-int particles_import(pic_ctx* c, int s, int64_t n);  // points already staged
+// Stages n records for import; returns the device address to copy them to.
+int particles_import_staging(pic_ctx* c, int64_t n, PointRec** dev_recs);
+int particles_import(pic_ctx* c, int s, int64_t n);  // records already staged
 int ensure_staging(pic_ctx* c, size_t bytes);
-int particles_export(pic_ctx* c, int s, pic_point* dev_out, int64_t* n_out);
+// The species as records in cell order (dev_out: n records).
+int particles_export(pic_ctx* c, int s, PointRec* dev_out, int64_t* n_out);
 int particles_load_plasma(pic_ctx* c, int s, const pic_plasma_desc* d);
 // raw state into 6 consecutive arrays of n entries (int32 cell, 5 floats)
 int particles_export_state(pic_ctx* c, int s, void* dev, int64_t n);
