@@ -59,6 +59,8 @@ constexpr uint32_t kAxisOne = 1u << kAxisBits;
 constexpr float kAxisScale = (float)(1u << kAxisBits);
 constexpr float kOneBelow = 0x1.fffffep-1f;   // largest float < 1
 constexpr float kEnergyScale = 4194304.0f;    // eV -> 2^-22 eV units
+constexpr float kFloorMagic = 12582912.0f;    // 1.5 * 2^23
+constexpr uint32_t kFloorMagicBits = 0x4B400000u;
 constexpr int kFixupBlocks = 296;
 
 enum Mode { kPush = 0, kDeposit = 1 };
@@ -174,12 +176,17 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     // the integer part moves the cell, the remainder is the new offset.
     const float px = __fmaf_rn(o.vx, k.dtdx, fx);
     const float py = __fmaf_rn(o.vy, k.dtdy, fy);
-    const float fsx = floorf(px), fsy = floorf(py);
+    // floor without the conversion unit: for |p| < 2^22, p + 1.5*2^23
+    // rounded down is floor(p) + 1.5*2^23 exactly, an integer held in the
+    // low mantissa bits; subtracting 1.5*2^23 again is exact
+    const float tx = __fadd_rd(px, kFloorMagic), ty = __fadd_rd(py, kFloorMagic);
+    const float fsx = __fsub_rn(tx, kFloorMagic), fsy = __fsub_rn(ty, kFloorMagic);
     o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
     o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
     // beyond 2^20 cells (or NaN) a particle is lost whatever the grid
     const bool ok = fabsf(px) < 1048576.0f && fabsf(py) < 1048576.0f;
-    const int sx = ok ? (int)fsx : 0, sy = ok ? (int)fsy : 0;
+    const int sx = ok ? (int)(__float_as_uint(tx) - kFloorMagicBits) : 0;
+    const int sy = ok ? (int)(__float_as_uint(ty) - kFloorMagicBits) : 0;
     o.gx = gx + sx;
     o.gy = gy + sy;
     // periodic in y (modulo(y, H), src/mover.cpp:317-320): the cell row
@@ -261,18 +268,21 @@ __device__ __forceinline__ void deposit_one(unsigned long long* acc_q, unsigned 
 //   Q00 = N 2^40 - (SX + SY) 2^20 + SXY,  Q10 = SX 2^20 - SXY,
 //   Q01 = SY 2^20 - SXY,                   Q11 = SXY.
 // A lane holds at most kMaxPerCell/32 = 2^11 particles: SX, SY < 2^31,
-// SXY < 2^51, energy sums < 2^43.
+// SXY < 2^51.  The energy mesh (a diagnostic) sums its corner weights per
+// lane in FP32, in 2^-22 eV units (< 2^43), rounded to integers once per
+// lane and cell: exact integer sums from there on, but the per-lane FP32
+// rounding depends on the order of the lane's particles.
 struct StayAcc {
     uint32_t n, sx, sy;
     unsigned long long sxy;
-    unsigned long long e[4];
+    float e[4];
 };
 
 __device__ __forceinline__ void acc_zero(StayAcc& s) {
     s.n = s.sx = s.sy = 0u;
     s.sxy = 0ull;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) s.e[k] = 0ull;
+    for (int k = 0; k < 4; ++k) s.e[k] = 0.f;
 }
 
 template <bool ENERGY>
@@ -283,11 +293,13 @@ __device__ __forceinline__ void acc_add(StayAcc& s, float fx, float fy, float en
     s.sy += ay;
     s.sxy += (unsigned long long)ax * ay;
     if (ENERGY) {
-        const EWeights e = energy_weights(fx, fy, en);
-        s.e[0] += e.e00;
-        s.e[1] += e.e10;
-        s.e[2] += e.e01;
-        s.e[3] += e.e11;
+        const float es = __fmul_rn(en, kEnergyScale);
+        const float a = __fmul_rn(es, __fsub_rn(1.0f, fx)), b = __fmul_rn(es, fx);
+        const float ofy = __fsub_rn(1.0f, fy);
+        s.e[0] = __fmaf_rn(a, ofy, s.e[0]);
+        s.e[1] = __fmaf_rn(b, ofy, s.e[1]);
+        s.e[2] = __fmaf_rn(a, fy, s.e[2]);
+        s.e[3] = __fmaf_rn(b, fy, s.e[3]);
     }
 }
 
@@ -310,7 +322,7 @@ __device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, in
     unsigned long long E[4] = {0ull, 0ull, 0ull, 0ull};
     if (ENERGY) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) E[k] = warp_sum_limbs<22>(s.e[k]);
+        for (int k = 0; k < 4; ++k) E[k] = warp_sum_limbs<22>(__float2ull_rn(s.e[k]));
     }
     if (lane == 0 && N) {
         const int64_t n = (int64_t)gy * A.GX + gx;
@@ -1356,6 +1368,10 @@ static int count_cells(pic_ctx* c, int s, int64_t* total) {
 
 int ensure_staging(pic_ctx* c, size_t bytes) {
     if (bytes <= c->staging_bytes) return PIC_OK;
+    // whole 32 MiB granules: requests of nearly the same size (an export,
+    // then an import of the same particles) reuse the buffer
+    constexpr size_t kGranule = 32u << 20;
+    bytes = (bytes + kGranule - 1) / kGranule * kGranule;
     cudaFree(c->staging);
     c->staging = nullptr;
     c->staging_bytes = 0;
@@ -1365,7 +1381,7 @@ int ensure_staging(pic_ctx* c, size_t bytes) {
 }
 
 int particles_import_staging(pic_ctx* c, int64_t n, PointRec** dev_recs) {
-    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(PointRec) + 256));
+    PIC_TRY(ensure_staging(c, (size_t)n * sizeof(PointRec)));
     *dev_recs = static_cast<PointRec*>(c->staging);
     return PIC_OK;
 }
