@@ -448,49 +448,75 @@ def run_learned(pic, args, it):
                     "32 channels, bf16 mma.sync tensor cores, FP32 accumulation"}, it
 
 
-def run_ensemble(args, rank):
+def run_ensemble(args, rank, world, local_rank):
     """The 64-instance ensemble (grids 128^2..384^2, left electrode 50-300 V,
     Bz 0-0.02 T, 32 particles/cell/species, 5e14-2e15 m^-3, seeded per
     instance): one launch per phase over all instances, the Poisson solves
     in one persistent launch, the step replayed as a CUDA graph, tile shape
-    autotuned.  Times from the ensemble's own CUDA events."""
+    autotuned.  With N ranks the 64 instances are placed whole on the GPUs by
+    the greedy longest-first rule on their cell counts (sharding.py): the
+    total work is fixed ("strong" scaling), no data-path collective; times
+    from each rank's ensemble CUDA events, max over ranks; per-instance
+    results gathered to rank 0."""
     import pic_b200 as P
     import pic_configs as C
+    import sharding as S
     ws = C.cfg5_instances()
+    cells = [w.nx * w.ny for w in ws]
+    mine = S.local(cells, world, rank)
     t0 = time.perf_counter()
-    E = P.Ensemble([C.library_config(w) for w in ws])
-    for k, w in enumerate(ws):
-        C.load_plasma(E[k], w, seed=5000 + 97 * k + 7919 * rank)
+    E = P.Ensemble([C.library_config(ws[k], device=local_rank) for k in mine]) if mine else None
+    for j, k in enumerate(mine):
+        C.load_plasma(E[j], ws[k], seed=5000 + 97 * k)
     setup_s = time.perf_counter() - t0
-    n_part = sum(E[k].count(s) for k in range(len(ws)) for s in range(2))
-    shape, ms_shapes = E.autotune()
+    n_local = sum(E[j].count(s) for j in range(len(mine)) for s in range(2)) if E else 0
+    shape, ms_shapes = E.autotune() if E else (0, [])
     for it in range(args.warmup):
-        E.step(it)
+        if E:
+            E.step(it)
     dep, pois, push, iters = [], [], [], []
     for it in range(args.warmup, args.warmup + args.ensemble_steps):
-        E.step(it)
-        d, p, q = E.timing()
+        if E:
+            E.step(it)
+            d, p, q = E.timing()
+        else:
+            d = p = q = 0.0
         dep.append(d)
         pois.append(p)
         push.append(q)
-        iters.append(statistics.mean(E[k].poisson_stats()[0] for k in range(len(ws))))
-    info = E.info()
-    worst_rel = max(E[k].poisson_stats()[1] for k in range(len(ws)))
-    E.close()
-    part_ms = statistics.mean(d + q for d, q in zip(dep, push))
+    metrics = {}
+    if E:
+        info = E.info()
+        for j, k in enumerate(mine):
+            it_k, rel_k, _ = E[j].poisson_stats()
+            metrics[k] = {"rank": rank, "cells": cells[k], "iters": it_k, "relres": rel_k,
+                          "particles": [E[j].count(s) for s in range(2)]}
+        E.close()
+    else:
+        info = {"graph": False, "solver_blocks": 0}
+    every = S.gather_metrics(metrics)
+    part_ms = S.max_over_ranks(statistics.mean(d + q for d, q in zip(dep, push)))
+    push_ms = S.max_over_ranks(statistics.mean(push))
+    pois_ms = S.max_over_ranks(statistics.mean(pois))
+    total_ms = S.max_over_ranks(statistics.mean(a + b + c for a, b, c in zip(dep, pois, push)))
+    n_part = S.sum_over_ranks(n_local)
+    if rank != 0:
+        return None
     peak, peak_kind = measured_peaks()
-    push_ms = statistics.mean(push)
     return {"workload": f"{len(ws)} instances, grids {min(w.nx for w in ws)}^2..{max(w.nx for w in ws)}^2, "
                         "left electrode 50-300 V, Bz 0-0.02 T, 32 ppc/species, 5e14-2e15 m^-3",
-            "instances": len(ws), "particles": n_part,
+            "instances": len(ws), "particles": int(n_part),
             "particle_steps_per_s": n_part / (part_ms * 1e-3),
-            "ms_per_step_particles": part_ms, "ms_per_step_poisson_all": statistics.mean(pois),
-            "ms_per_step_total": statistics.mean(a + b + c for a, b, c in zip(dep, pois, push)),
-            "poisson_iters_mean": statistics.mean(iters), "worst_relres": worst_rel,
-            "push_roofline_frac": BYTES_PUSH_PASS * n_part / (push_ms * 1e-3) / 1e9 / peak,
+            "ms_per_step_particles": part_ms, "ms_per_step_poisson_all": pois_ms,
+            "ms_per_step_total": total_ms,
+            "poisson_iters_mean": statistics.mean(m["iters"] for m in every.values()),
+            "worst_relres": max(m["relres"] for m in every.values()),
+            "push_roofline_frac": BYTES_PUSH_PASS * n_part / world / (push_ms * 1e-3) / 1e9 / peak,
             "tile_shape": ["64x4", "32x8", "128x2", "16x16"][shape], "ms_per_shape": ms_shapes,
             "graph": info["graph"], "solver_blocks": info["solver_blocks"], "steps": args.ensemble_steps,
-            "setup_s": setup_s}
+            "setup_s": setup_s, "scaling": "strong", "n_gpus": world,
+            "placement": "whole instances, greedy longest-first on cell counts; rank loads (cells) "
+                         + str([int(x) for x in S.loads(cells, world)])}
 
 
 def run_cfg4(args):
@@ -645,7 +671,9 @@ def main():
     line, pic, w = run_ours(args, rank, world, local_rank)
     pic.close()
     if not args.no_ensemble and args.config == "cfg3":
-        line["ensemble"] = run_ensemble(args, rank)
+        ens = run_ensemble(args, rank, world, local_rank)
+        if rank == 0:
+            line["ensemble"] = ens
     if rank == 0 and not args.no_cpu_baseline:
         scale = 4 if w.nx >= 512 else 1
         value, pois_ms, sample, threads, _, _ = cpu_reference_run(w, scale, args.cpu_seconds)

@@ -54,6 +54,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = kWarps * 32;
+constexpr int kCellBlocksPerSM = 4;           // k_cells residency (register budget)
 constexpr int kScanTile = 2048;               // cells per scan block
 constexpr uint32_t kAxisOne = 1u << kAxisBits;
 constexpr float kAxisScale = (float)(1u << kAxisBits);
@@ -607,14 +608,14 @@ constexpr int kTileShapeX[kNumTileShapes] = {64, 32, 128, 16};
 constexpr int kTileShapeY[kNumTileShapes] = {4, 8, 2, 16};
 
 template <int MODE, bool ENERGY, int TX, int TY>
-__global__ void __launch_bounds__(kThreads, 4) k_cells(KArgs A) {
+__global__ void __launch_bounds__(kThreads, kCellBlocksPerSM) k_cells(KArgs A) {
     cells_body<MODE, ENERGY, TX, TY>(A, blockIdx.x, blockIdx.y);
 }
 
 // One launch over many instances: block b works on tile (work[b].y & 0xffff,
 // work[b].y >> 16) of instance work[b].x, whose arguments are args[work[b].x].
 template <int MODE, bool ENERGY, int TX, int TY>
-__global__ void __launch_bounds__(kThreads, 4) k_cells_batch(const KArgs* __restrict__ args,
+__global__ void __launch_bounds__(kThreads, kCellBlocksPerSM) k_cells_batch(const KArgs* __restrict__ args,
                                                              const uint2* __restrict__ work) {
     __shared__ KArgs s_args;
     const uint2 w = work[blockIdx.x];
