@@ -264,8 +264,9 @@ __device__ __forceinline__ void deposit_one(unsigned long long* acc_q, unsigned 
 }
 
 // Per-lane sums of the particles that stay in the warp's cell.  Charge as
-// moments of the 20-bit axis weights -- count, sum ax, sum ay, sum ax*ay --
-// from which the four corner sums follow exactly:
+// moments of the 20-bit axis weights -- count N (the warp's stayer count,
+// kept by the caller), sum ax, sum ay, sum ax*ay -- from which the four
+// corner sums follow exactly:
 //   Q00 = N 2^40 - (SX + SY) 2^20 + SXY,  Q10 = SX 2^20 - SXY,
 //   Q01 = SY 2^20 - SXY,                   Q11 = SXY.
 // A lane holds at most kMaxPerCell/32 = 2^11 particles: SX, SY < 2^31,
@@ -274,13 +275,13 @@ __device__ __forceinline__ void deposit_one(unsigned long long* acc_q, unsigned 
 // lane and cell: exact integer sums from there on, but the per-lane FP32
 // rounding depends on the order of the lane's particles.
 struct StayAcc {
-    uint32_t n, sx, sy;
+    uint32_t sx, sy;
     unsigned long long sxy;
     float e[4];
 };
 
 __device__ __forceinline__ void acc_zero(StayAcc& s) {
-    s.n = s.sx = s.sy = 0u;
+    s.sx = s.sy = 0u;
     s.sxy = 0ull;
 #pragma unroll
     for (int k = 0; k < 4; ++k) s.e[k] = 0.f;
@@ -289,7 +290,6 @@ __device__ __forceinline__ void acc_zero(StayAcc& s) {
 template <bool ENERGY>
 __device__ __forceinline__ void acc_add(StayAcc& s, float fx, float fy, float en) {
     const uint32_t ax = axis_fixed(fx), ay = axis_fixed(fy);
-    s.n += 1u;
     s.sx += ax;
     s.sy += ay;
     s.sxy += (unsigned long long)ax * ay;
@@ -314,9 +314,10 @@ __device__ __forceinline__ unsigned long long warp_sum_limbs(unsigned long long 
 }
 
 // Warp-reduce the cell's stayer sums and add them to its four nodes (lane 0).
+// N: the cell's stayer count (known to the whole warp).
 template <bool ENERGY>
-__device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane) {
-    const unsigned long long N = __reduce_add_sync(kFull, s.n);
+__device__ __forceinline__ void acc_flush(StayAcc& s, const KArgs& A, int gx, int gy, int lane,
+                                          unsigned long long N) {
     const unsigned long long SX = warp_sum_limbs<26>(s.sx);
     const unsigned long long SY = warp_sum_limbs<26>(s.sy);
     const unsigned long long SXY = warp_sum_limbs<26>(s.sxy);
@@ -395,21 +396,26 @@ struct MoverQueue {
     float4 a[kQueue];
     float vz[kQueue];
     uint2 tn[kQueue];  // target cell, its lower-left node
+    uint16_t loc[kQueue];  // target's index in the block's tile, kOffTile outside
 };
+constexpr uint16_t kOffTile = 0xffffu;
 
 // Places `count` (<= 32) queued movers, entries 0..count-1.
 template <bool ENERGY>
-__device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q, int count, int lane,
-                                             unsigned lt) {
+__device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
+                                             const CellMeta* __restrict__ s_meta, int count,
+                                             int lane, unsigned lt) {
     __syncwarp();
     const bool on = lane < count;
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
     float vz = 0.f;
     uint2 tn = make_uint2(0u, 0u);
+    uint32_t loc = kOffTile;
     if (on) {
         a = q.a[lane];
         vz = q.vz[lane];
         tn = q.tn[lane];
+        loc = q.loc[lane];
     }
     const uint32_t t = tn.x;
     const float en = (ENERGY && on) ? energy_ev(a.z, a.w, vz, A.k.half_inv_abs_qm) : 0.f;
@@ -418,10 +424,23 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q, int 
     // minus its current count (the most stayers it can have)
     const unsigned grp = __match_any_sync(kFull, on ? t : (0x80000000u | (uint32_t)lane));
     const int leader = __ffs(grp) - 1;
-    uint32_t old = 0, lim = 0;
+    uint32_t old = 0, lim = 0, top = 0;
     if (on && lane == leader) {
         const uint32_t cnt = __popc(grp);
-        lim = (A.base[t + 1] - A.base[t]) - (A.front_src[t] + A.back_src[t]);
+        // the target's slots and source counts: from the tile's shared
+        // metadata when it lies in this block's tile (most movers go one
+        // cell), else from global memory
+        CellMeta m;
+        if (loc != kOffTile) {
+            m = s_meta[loc];
+        } else {
+            m.b0 = A.base[t];
+            m.b1 = A.base[t + 1];
+            m.nf = A.front_src[t];
+            m.nb = A.back_src[t];
+        }
+        lim = (m.b1 - m.b0) - (m.nf + m.nb);
+        top = m.b1;
         old = atomicAdd(A.back_dst + t, cnt);
         // give back what does not fit (the count then ends at
         // min(requested, lim) with slots 0.. taken)
@@ -430,12 +449,13 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q, int 
     if (on) deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, tn.y, a.x, a.y, en);
     old = __shfl_sync(kFull, old, leader);
     lim = __shfl_sync(kFull, lim, leader);
+    top = __shfl_sync(kFull, top, leader);
     bool spill = false;
     Pushed p;
     p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
     if (on) {
         const uint32_t k = old + __popc(grp & lt);
-        if (k < lim) store_slot(A.dst_a, A.dst_vz, A.base[t + 1] - 1u - k, p, vz);
+        if (k < lim) store_slot(A.dst_a, A.dst_vz, top - 1u - k, p, vz);
         else spill = true;
     }
     list_append(A.ovf, spill, t, p, vz, lt, lane, A.counters + 2);
@@ -476,7 +496,7 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     }
     __syncthreads();
 
-    unsigned long long left_exits = 0;
+    uint32_t left_exits = 0;  // per lane
     // the warp's cells are lc = warp + kWarps*k; empty ones only get their
     // front count written
     auto next_cell = [&](int lc, bool mark_empty) {
@@ -556,7 +576,7 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
             const float en = (ENERGY && live) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
             if (stay) acc_add<ENERGY>(acc, p.fx, p.fy, en);
             if (MODE == kPush) {
-                left_exits += __popc(__ballot_sync(kFull, valid && !live && p.left));
+                left_exits += (valid && !live && p.left) ? 1u : 0u;
                 const unsigned sm = __ballot_sync(kFull, stay);
                 if (stay) store_slot(A.dst_a, A.dst_vz, m.b0 + stay_run + __popc(sm & lt), p, vz);
                 stay_run += __popc(sm);
@@ -568,10 +588,13 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                         q.a[e] = make_float4(p.fx, p.fy, p.vx, p.vy);
                         q.vz[e] = vz;
                         q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
+                        const int llx = p.gx - tgx0, lly = p.gy - tgy0;
+                        q.loc[e] = ((unsigned)llx < (unsigned)kTileX && (unsigned)lly < (unsigned)kTileY)
+                                       ? (uint16_t)(lly * kTileX + llx) : kOffTile;
                     }
                     queued += __popc(mm);
                     if (queued >= 32) {
-                        place_movers<ENERGY>(A, q, 32, lane, lt);
+                        place_movers<ENERGY>(A, q, s_meta, 32, lane, lt);
                         // the rest (< 32) moves to the front of the queue
                         queued -= 32;
                         __syncwarp();
@@ -579,13 +602,14 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                             q.a[lane] = q.a[32 + lane];
                             q.vz[lane] = q.vz[32 + lane];
                             q.tn[lane] = q.tn[32 + lane];
+                            q.loc[lane] = q.loc[32 + lane];
                         }
                         __syncwarp();
                     }
                 }
             }
             if (last) {
-                acc_flush<ENERGY>(acc, A, gx, gy, lane);
+                acc_flush<ENERGY>(acc, A, gx, gy, lane, MODE == kPush ? stay_run : n);
                 if (MODE == kPush && lane == 0) A.front_dst[(int64_t)gy * A.nx + gx] = stay_run;
                 stay_run = 0;
                 if (lcn >= kTileCells) break;
@@ -596,8 +620,11 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
         }
         cp_async_wait<0>();
     }
-    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, queued, lane, lt);
-    if (MODE == kPush && lane == 0 && left_exits) atomicAdd(A.counters, left_exits);
+    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, s_meta, queued, lane, lt);
+    if (MODE == kPush) {
+        const uint32_t left = __reduce_add_sync(kFull, left_exits);
+        if (lane == 0 && left) atomicAdd(A.counters, (unsigned long long)left);
+    }
 }
 
 // Tile shapes the kernels are built for (cells per block in x, y); every
