@@ -65,7 +65,6 @@ constexpr uint32_t kFloorMagicBits = 0x4B400000u;
 constexpr int kFixupBlocks = 296;
 
 enum Mode { kPush = 0, kDeposit = 1 };
-constexpr int kStay = 4;      // d = (sy+1)*3 + (sx+1) of a particle that keeps its cell
 constexpr int kFar = 9;       // moved more than one cell in x or y
 
 // list_counts slots
@@ -136,6 +135,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // Result of one gather + Boris + position update.
 struct Pushed {
     float fx, fy, vx, vy;
+    float px, py;  // new position in units of the old cell (its corner at 0)
+    int sx, sy;    // cell step: 0, 0 exactly when the particle keeps its cell
+    // set by resolve_move
     int gx, gy;
     int dir;  // 0..8 near (4 = same cell), kFar, or -1 when absorbed
     bool left;
@@ -146,9 +148,11 @@ struct Pushed {
 // (1-fx)(1-fy), fx(1-fy), (1-fx)fy, fx*fy == the reference's unnormalised
 // weights divided by dx*dy.  Every operation is an explicit _rn intrinsic:
 // the result does not depend on how the compiler contracts the code.
-__device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, float4 n01,
-                                           float4 n11, const SpeciesConsts& k, int gx, int gy,
-                                           int nx, int ny) {
+//
+// push_move does the arithmetic of every particle; resolve_move the cell
+// bookkeeping that only particles leaving their cell need.
+__device__ __forceinline__ Pushed push_move(float4 a, float4 n00, float4 n10, float4 n01,
+                                            float4 n11, const SpeciesConsts& k) {
     const float fx = a.x, fy = a.y;
     const float ofx = __fsub_rn(1.0f, fx), ofy = __fsub_rn(1.0f, fy);
     const float w00 = __fmul_rn(ofx, ofy), w10 = __fmul_rn(fx, ofy);
@@ -177,17 +181,30 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     // the integer part moves the cell, the remainder is the new offset.
     const float px = __fmaf_rn(o.vx, k.dtdx, fx);
     const float py = __fmaf_rn(o.vy, k.dtdy, fy);
+    o.px = px;
+    o.py = py;
     // floor without the conversion unit: for |p| < 2^22, p + 1.5*2^23
     // rounded down is floor(p) + 1.5*2^23 exactly, an integer held in the
-    // low mantissa bits; subtracting 1.5*2^23 again is exact
+    // low mantissa bits; subtracting 1.5*2^23 again is exact.  The step's
+    // bits are 0 exactly when floor(p) == 0: for NaN or |p| >= 2^22 the sum
+    // is not 1.5*2^23, so those never read as staying.
     const float tx = __fadd_rd(px, kFloorMagic), ty = __fadd_rd(py, kFloorMagic);
     const float fsx = __fsub_rn(tx, kFloorMagic), fsy = __fsub_rn(ty, kFloorMagic);
     o.fx = fminf(__fsub_rn(px, fsx), kOneBelow);
     o.fy = fminf(__fsub_rn(py, fsy), kOneBelow);
+    o.sx = (int)(__float_as_uint(tx) - kFloorMagicBits);
+    o.sy = (int)(__float_as_uint(ty) - kFloorMagicBits);
+    return o;
+}
+
+// Cell bookkeeping of a pushed particle that was in cell (gx, gy).
+__device__ __forceinline__ void resolve_move(Pushed& o, const SpeciesConsts& k, int gx, int gy,
+                                             int nx, int ny) {
+    const float px = o.px, py = o.py;
     // beyond 2^20 cells (or NaN) a particle is lost whatever the grid
     const bool ok = fabsf(px) < 1048576.0f && fabsf(py) < 1048576.0f;
-    const int sx = ok ? (int)(__float_as_uint(tx) - kFloorMagicBits) : 0;
-    const int sy = ok ? (int)(__float_as_uint(ty) - kFloorMagicBits) : 0;
+    const int sx = ok ? o.sx : 0;
+    const int sy = ok ? o.sy : 0;
     o.gx = gx + sx;
     o.gy = gy + sy;
     // periodic in y (modulo(y, H), src/mover.cpp:317-320): the cell row
@@ -201,6 +218,13 @@ __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, flo
     o.left = ok ? (o.gx < 0) : (px < 0.0f);
     const bool near = (unsigned)(sx + 1) < 3u && (unsigned)(sy + 1) < 3u;
     o.dir = !alive ? -1 : (near ? (sy + 1) * 3 + (sx + 1) : kFar);
+}
+
+__device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, float4 n01,
+                                           float4 n11, const SpeciesConsts& k, int gx, int gy,
+                                           int nx, int ny) {
+    Pushed o = push_move(a, n00, n10, n01, n11, k);
+    resolve_move(o, k, gx, gy, nx, ny);
     return o;
 }
 
@@ -563,24 +587,32 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
             const int gx = tgx0 + lx, gy = tgy0 + ly;
             const bool valid = j0 + lane < n;
             Pushed p;
+            bool stay;
             if (MODE == kDeposit) {
                 p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
-                p.gx = gx; p.gy = gy; p.dir = kStay; p.left = false;
+                stay = valid;
             } else {
                 const float4* f = s_fld + ly * kTileNodesX + lx;
-                p = push_one(a, f[0], f[1], f[kTileNodesX], f[kTileNodesX + 1], A.k, gx, gy, A.nx, A.ny);
+                p = push_move(a, f[0], f[1], f[kTileNodesX], f[kTileNodesX + 1], A.k);
+                stay = valid && (p.sx | p.sy) == 0;
             }
-            const int dir = valid ? p.dir : -1;
-            const bool stay = dir == kStay;
-            const bool live = dir >= 0;
-            const float en = (ENERGY && live) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
+            const float en = (ENERGY && stay) ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
             if (stay) acc_add<ENERGY>(acc, p.fx, p.fy, en);
             if (MODE == kPush) {
-                left_exits += (valid && !live && p.left) ? 1u : 0u;
                 const unsigned sm = __ballot_sync(kFull, stay);
                 if (stay) store_slot(A.dst_a, A.dst_vz, m.b0 + stay_run + __popc(sm & lt), p, vz);
                 stay_run += __popc(sm);
-                const bool mv = live && !stay;
+                // the cell bookkeeping of the rest (absorbed or moving), only
+                // in chunks that have any (most chunks of slow species do not)
+                const bool other = valid && !stay;
+                bool mv = false;
+                if (__any_sync(kFull, other)) {
+                    if (other) {
+                        resolve_move(p, A.k, gx, gy, A.nx, A.ny);
+                        mv = p.dir >= 0;
+                        left_exits += (p.dir < 0 && p.left) ? 1u : 0u;
+                    }
+                }
                 const unsigned mm = __ballot_sync(kFull, mv);
                 if (mm) {  // warp-uniform: queue the movers
                     if (mv) {
