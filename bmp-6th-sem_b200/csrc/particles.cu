@@ -406,6 +406,7 @@ __device__ __forceinline__ void list_append(const ListDev& L, bool on, uint32_t 
 // chunks ahead of the one being processed -- across cell boundaries, so the
 // load pipeline never drains.
 constexpr int kDepth = 4;
+static_assert((kDepth & (kDepth - 1)) == 0, "ring depth: a power of two");
 
 struct CellMeta {
     uint32_t b0, b1, nf, nb;
@@ -535,21 +536,30 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     };
     // producer: issues the copies of the chunk (plc, pj0) into ring slot r
     // and advances; every call commits one (possibly empty) copy group
+    // the producer's cell as the source index of its j-th particle: the
+    // front run for j < nf, then the back run (index back + j)
+    struct ProdCell {
+        uint32_t front, back, nf, n;
+    };
+    auto prod_cell = [&](int c) {
+        const CellMeta pm = c < kTileCells ? s_meta[c] : CellMeta{0u, 0u, 0u, 0u};
+        return ProdCell{pm.b0, pm.b1 - pm.nb - pm.nf, pm.nf, pm.nf + pm.nb};
+    };
     int plc = next_cell(warp, false);
-    CellMeta pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
+    ProdCell pc = prod_cell(plc);
     uint32_t pj0 = 0;
     const uint32_t ring_a0 = smem_u32(&s_ring_a[warp][0][lane]);
     const uint32_t ring_vz0 = smem_u32(&s_ring_vz[warp][0][lane]);
     auto issue = [&](int r) {
         if (plc < kTileCells) {
-            const uint32_t jj = pj0 + lane, np = pm.nf + pm.nb;
-            const bool v = jj < np;
-            const uint32_t i = !v ? 0u : (jj < pm.nf ? pm.b0 + jj : pm.b1 - pm.nb + (jj - pm.nf));
+            const uint32_t jj = pj0 + lane;
+            const bool v = jj < pc.n;
+            const uint32_t i = !v ? 0u : (jj < pc.nf ? pc.front : pc.back) + jj;
             cp_async16(ring_a0 + (uint32_t)r * (32u * 16u), A.src_a + i, v);
             cp_async4(ring_vz0 + (uint32_t)r * (32u * 4u), A.src_vz + i, v);
-            if (pj0 + 32 >= np) {
+            if (pj0 + 32 >= pc.n) {
                 plc = next_cell(plc + kWarps, false);
-                pm = plc < kTileCells ? s_meta[plc] : CellMeta{0u, 0u, 0u, 0u};
+                pc = prod_cell(plc);
                 pj0 = 0;
             } else {
                 pj0 += 32;
@@ -577,11 +587,11 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
             const int lcn = last ? next_cell(lc + kWarps, true) : lc;
             const uint32_t jn0 = last ? 0u : j0 + 32;
             // refill the slot freed by the previous chunk, then wait for this one
-            issue(r == 0 ? kDepth - 1 : r - 1);
+            issue((r + kDepth - 1) & (kDepth - 1));
             cp_async_wait<kDepth - 1>();
             const float4 a = s_ring_a[warp][r][lane];
             const float vz = s_ring_vz[warp][r][lane];
-            r = (r + 1 == kDepth) ? 0 : r + 1;
+            r = (r + 1) & (kDepth - 1);
 
             const int lx = lc % kTileX, ly = lc / kTileX;
             const int gx = tgx0 + lx, gy = tgy0 + ly;
