@@ -574,18 +574,29 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     if (lc < kTileCells) {
 #pragma unroll
         for (int r = 0; r < kDepth - 1; ++r) issue(r);
-        CellMeta m = s_meta[lc];
-        uint32_t j0 = 0;
+        // the consumer's cell: particle count, coordinates, its field
+        // corner in the shared tile, and the next free front slot
+        uint32_t n, front;
+        int gx, gy;
+        const float4* f;
+        auto enter = [&](int c) {
+            const CellMeta m = s_meta[c];
+            n = m.nf + m.nb;
+            front = m.b0;
+            const int lx = c % kTileX, ly = c / kTileX;
+            gx = tgx0 + lx;
+            gy = tgy0 + ly;
+            f = s_fld + ly * kTileNodesX + lx;
+        };
+        enter(lc);
+        uint32_t j0 = 0, front0 = front;
         int r = 0;
         StayAcc acc;
         acc_zero(acc);
-        uint32_t stay_run = 0;
         for (;;) {
-            const uint32_t n = m.nf + m.nb;
             const bool last = j0 + 32 >= n;
             // the next chunk: same cell, or the warp's next non-empty cell
             const int lcn = last ? next_cell(lc + kWarps, true) : lc;
-            const uint32_t jn0 = last ? 0u : j0 + 32;
             // refill the slot freed by the previous chunk, then wait for this one
             issue((r + kDepth - 1) & (kDepth - 1));
             cp_async_wait<kDepth - 1>();
@@ -593,8 +604,6 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
             const float vz = s_ring_vz[warp][r][lane];
             r = (r + 1) & (kDepth - 1);
 
-            const int lx = lc % kTileX, ly = lc / kTileX;
-            const int gx = tgx0 + lx, gy = tgy0 + ly;
             const bool valid = j0 + lane < n;
             Pushed p;
             bool stay;
@@ -602,7 +611,6 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                 p.fx = a.x; p.fy = a.y; p.vx = a.z; p.vy = a.w;
                 stay = valid;
             } else {
-                const float4* f = s_fld + ly * kTileNodesX + lx;
                 p = push_move(a, f[0], f[1], f[kTileNodesX], f[kTileNodesX + 1], A.k);
                 stay = valid && (p.sx | p.sy) == 0;
             }
@@ -610,55 +618,58 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
             if (stay) acc_add<ENERGY>(acc, p.fx, p.fy, en);
             if (MODE == kPush) {
                 const unsigned sm = __ballot_sync(kFull, stay);
-                if (stay) store_slot(A.dst_a, A.dst_vz, m.b0 + stay_run + __popc(sm & lt), p, vz);
-                stay_run += __popc(sm);
+                if (stay) store_slot(A.dst_a, A.dst_vz, front + __popc(sm & lt), p, vz);
+                front += __popc(sm);
                 // the cell bookkeeping of the rest (absorbed or moving), only
                 // in chunks that have any (most chunks of slow species do not)
                 const bool other = valid && !stay;
-                bool mv = false;
                 if (__any_sync(kFull, other)) {
+                    bool mv = false;
                     if (other) {
                         resolve_move(p, A.k, gx, gy, A.nx, A.ny);
                         mv = p.dir >= 0;
                         left_exits += (p.dir < 0 && p.left) ? 1u : 0u;
                     }
-                }
-                const unsigned mm = __ballot_sync(kFull, mv);
-                if (mm) {  // warp-uniform: queue the movers
-                    if (mv) {
-                        const int e = queued + __popc(mm & lt);
-                        q.a[e] = make_float4(p.fx, p.fy, p.vx, p.vy);
-                        q.vz[e] = vz;
-                        q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
-                        const int llx = p.gx - tgx0, lly = p.gy - tgy0;
-                        q.loc[e] = ((unsigned)llx < (unsigned)kTileX && (unsigned)lly < (unsigned)kTileY)
-                                       ? (uint16_t)(lly * kTileX + llx) : kOffTile;
-                    }
-                    queued += __popc(mm);
-                    if (queued >= 32) {
-                        place_movers<ENERGY>(A, q, s_meta, 32, lane, lt);
-                        // the rest (< 32) moves to the front of the queue
-                        queued -= 32;
-                        __syncwarp();
-                        if (lane < queued) {
-                            q.a[lane] = q.a[32 + lane];
-                            q.vz[lane] = q.vz[32 + lane];
-                            q.tn[lane] = q.tn[32 + lane];
-                            q.loc[lane] = q.loc[32 + lane];
+                    const unsigned mm = __ballot_sync(kFull, mv);
+                    if (mm) {  // warp-uniform: queue the movers
+                        if (mv) {
+                            const int e = queued + __popc(mm & lt);
+                            q.a[e] = make_float4(p.fx, p.fy, p.vx, p.vy);
+                            q.vz[e] = vz;
+                            q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
+                            const int llx = p.gx - tgx0, lly = p.gy - tgy0;
+                            q.loc[e] = ((unsigned)llx < (unsigned)kTileX && (unsigned)lly < (unsigned)kTileY)
+                                           ? (uint16_t)(lly * kTileX + llx) : kOffTile;
                         }
-                        __syncwarp();
+                        queued += __popc(mm);
+                        if (queued >= 32) {
+                            place_movers<ENERGY>(A, q, s_meta, 32, lane, lt);
+                            // the rest (< 32) moves to the front of the queue
+                            queued -= 32;
+                            __syncwarp();
+                            if (lane < queued) {
+                                q.a[lane] = q.a[32 + lane];
+                                q.vz[lane] = q.vz[32 + lane];
+                                q.tn[lane] = q.tn[32 + lane];
+                                q.loc[lane] = q.loc[32 + lane];
+                            }
+                            __syncwarp();
+                        }
                     }
                 }
             }
             if (last) {
-                acc_flush<ENERGY>(acc, A, gx, gy, lane, MODE == kPush ? stay_run : n);
-                if (MODE == kPush && lane == 0) A.front_dst[(int64_t)gy * A.nx + gx] = stay_run;
-                stay_run = 0;
+                const uint32_t stayers = front - front0;
+                acc_flush<ENERGY>(acc, A, gx, gy, lane, MODE == kPush ? stayers : n);
+                if (MODE == kPush && lane == 0) A.front_dst[(int64_t)gy * A.nx + gx] = stayers;
                 if (lcn >= kTileCells) break;
-                m = s_meta[lcn];
+                enter(lcn);
+                front0 = front;
+                j0 = 0;
+            } else {
+                j0 += 32;
             }
             lc = lcn;
-            j0 = jn0;
         }
         cp_async_wait<0>();
     }
