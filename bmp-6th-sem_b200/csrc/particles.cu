@@ -421,15 +421,21 @@ struct MoverQueue {
     float4 a[kQueue];
     float vz[kQueue];
     uint2 tn[kQueue];  // target cell, its lower-left node
-    uint16_t loc[kQueue];  // target's index in the block's tile, kOffTile outside
+    uint16_t loc[kQueue];  // target's index in the block's tile (| kOwned), kOffTile outside
 };
 constexpr uint16_t kOffTile = 0xffffu;
+// A cell strictly inside the block's tile (not on the tile's border, not on
+// the periodic seam) receives direct placements only from cells of the
+// same tile: movers placed here go at most one cell (longer jumps go to the
+// side list).  Its back count is kept in shared memory and written out when
+// the block ends, instead of a global atomic per group of movers.
+constexpr uint16_t kOwned = 0x8000u;
 
 // Places `count` (<= 32) queued movers, entries 0..count-1.
 template <bool ENERGY>
 __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
-                                             const CellMeta* __restrict__ s_meta, int count,
-                                             int lane, unsigned lt) {
+                                             const CellMeta* __restrict__ s_meta,
+                                             uint32_t* s_back, int count, int lane, unsigned lt) {
     __syncwarp();
     const bool on = lane < count;
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -457,7 +463,7 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
         // cell), else from global memory
         CellMeta m;
         if (loc != kOffTile) {
-            m = s_meta[loc];
+            m = s_meta[loc & ~(uint32_t)kOwned];
         } else {
             m.b0 = A.base[t];
             m.b1 = A.base[t + 1];
@@ -466,10 +472,13 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
         }
         lim = (m.b1 - m.b0) - (m.nf + m.nb);
         top = m.b1;
-        old = atomicAdd(A.back_dst + t, cnt);
+        // the back count: in shared memory for a cell this block owns
+        uint32_t* ctr = (loc != kOffTile && (loc & kOwned)) ? s_back + (loc & ~(uint32_t)kOwned)
+                                                            : A.back_dst + t;
+        old = atomicAdd(ctr, cnt);
         // give back what does not fit (the count then ends at
         // min(requested, lim) with slots 0.. taken)
-        if (old + cnt > lim) atomicSub(A.back_dst + t, old >= lim ? cnt : old + cnt - lim);
+        if (old + cnt > lim) atomicSub(ctr, old >= lim ? cnt : old + cnt - lim);
     }
     if (on) deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, tn.y, a.x, a.y, en);
     old = __shfl_sync(kFull, old, leader);
@@ -495,11 +504,21 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     __shared__ CellMeta s_meta[kTileCells];
     __shared__ float4 s_fld[MODE == kPush ? kTileNodes : 1];
     __shared__ MoverQueue s_q[MODE == kPush ? kWarps : 1];
+    __shared__ uint32_t s_back[MODE == kPush ? kTileCells : 1];
     __shared__ float4 s_ring_a[kWarps][kDepth][32];
     __shared__ float s_ring_vz[kWarps][kDepth][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tgx0 = tile_x * kTileX, tgy0 = tile_y * kTileY;
     const unsigned lt = lanemask_lt();
+    // tile cell (lx, ly) is owned: inside the grid, off the tile's border
+    // and off the periodic seam (rows 0 and ny-1 exchange wrapped movers)
+    auto owned = [&](int lx, int ly) {
+        const int gy = tgy0 + ly;
+        return lx >= 1 && lx <= kTileX - 2 && ly >= 1 && ly <= kTileY - 2 && tgx0 + lx < A.nx &&
+               gy < A.ny && !(A.k.pery && (gy == 0 || gy == A.ny - 1));
+    };
+    if (MODE == kPush)
+        for (int i = threadIdx.x; i < kTileCells; i += kThreads) s_back[i] = 0u;
     for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
         const int gx = tgx0 + (i % kTileX), gy = tgy0 + (i / kTileX);
         CellMeta m{0u, 0u, 0u, 0u};
@@ -624,11 +643,23 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                 // in chunks that have any (most chunks of slow species do not)
                 const bool other = valid && !stay;
                 if (__any_sync(kFull, other)) {
-                    bool mv = false;
+                    bool mv = false, far = false;
                     if (other) {
                         resolve_move(p, A.k, gx, gy, A.nx, A.ny);
-                        mv = p.dir >= 0;
+                        mv = p.dir >= 0 && p.dir != kFar;
+                        far = p.dir == kFar;
                         left_exits += (p.dir < 0 && p.left) ? 1u : 0u;
+                    }
+                    // a jump of more than one cell: deposited here, placed
+                    // from the side list after the pass (rare)
+                    if (__any_sync(kFull, far)) {
+                        const uint32_t tc = (uint32_t)(p.gy * A.nx + p.gx);
+                        if (far) {
+                            const float ef = ENERGY ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;
+                            deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, (uint32_t)(p.gy * A.GX + p.gx),
+                                                p.fx, p.fy, ef);
+                        }
+                        list_append(A.ovf, far, tc, p, vz, lt, lane, A.counters + 2);
                     }
                     const unsigned mm = __ballot_sync(kFull, mv);
                     if (mm) {  // warp-uniform: queue the movers
@@ -639,11 +670,12 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                             q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
                             const int llx = p.gx - tgx0, lly = p.gy - tgy0;
                             q.loc[e] = ((unsigned)llx < (unsigned)kTileX && (unsigned)lly < (unsigned)kTileY)
-                                           ? (uint16_t)(lly * kTileX + llx) : kOffTile;
+                                           ? (uint16_t)((lly * kTileX + llx) | (owned(llx, lly) ? kOwned : 0u))
+                                           : kOffTile;
                         }
                         queued += __popc(mm);
                         if (queued >= 32) {
-                            place_movers<ENERGY>(A, q, s_meta, 32, lane, lt);
+                            place_movers<ENERGY>(A, q, s_meta, s_back, 32, lane, lt);
                             // the rest (< 32) moves to the front of the queue
                             queued -= 32;
                             __syncwarp();
@@ -673,10 +705,16 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
         }
         cp_async_wait<0>();
     }
-    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, s_meta, queued, lane, lt);
+    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, s_meta, s_back, queued, lane, lt);
     if (MODE == kPush) {
         const uint32_t left = __reduce_add_sync(kFull, left_exits);
         if (lane == 0 && left) atomicAdd(A.counters, (unsigned long long)left);
+        // the owned cells' back counts (no other block placed into them)
+        __syncthreads();
+        for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
+            const int lx = i % kTileX, ly = i / kTileX;
+            if (owned(lx, ly) && s_back[i]) A.back_dst[(int64_t)(tgy0 + ly) * A.nx + tgx0 + lx] = s_back[i];
+        }
     }
 }
 
