@@ -380,7 +380,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": part_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": describe(w), "particles_per_gpu": n_part,
-                   "tile_shape": ["64x4", "32x8", "128x2", "16x16"][tile_shape],
+                   "tile_shape": ["64x4", "256x1", "128x2", "16x16"][tile_shape],
                    "ms_per_tile_shape": tile_ms,
                    "particles_per_species": counts, "grid_nodes": (w.nx + 1) * (w.ny + 1),
                    "l2": "inputs larger than L2 (particle state ~%.1f GB per GPU)" % (n_part * 40 / 1e9),
@@ -517,7 +517,7 @@ def run_ensemble(args, rank, world, local_rank):
             "poisson_iters_mean": statistics.mean(m["iters"] for m in every.values()),
             "worst_relres": max(m["relres"] for m in every.values()),
             "push_roofline_frac": BYTES_PUSH_PASS * n_part / world / (push_ms * 1e-3) / 1e9 / peak,
-            "tile_shape": ["64x4", "32x8", "128x2", "16x16"][shape], "ms_per_shape": ms_shapes,
+            "tile_shape": ["64x4", "256x1", "128x2", "16x16"][shape], "ms_per_shape": ms_shapes,
             "graph": info["graph"], "solver_blocks": info["solver_blocks"], "steps": args.ensemble_steps,
             "setup_s": setup_s, "scaling": "strong", "n_gpus": world,
             "placement": "whole instances, greedy longest-first on cell counts; rank loads (cells) "

@@ -504,7 +504,8 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     __shared__ CellMeta s_meta[kTileCells];
     __shared__ float4 s_fld[MODE == kPush ? kTileNodes : 1];
     __shared__ MoverQueue s_q[MODE == kPush ? kWarps : 1];
-    __shared__ uint32_t s_back[MODE == kPush ? kTileCells : 1];
+    // tiles of one or two rows own no cell
+    __shared__ uint32_t s_back[MODE == kPush && kTileY > 2 ? kTileCells : 1];
     __shared__ float4 s_ring_a[kWarps][kDepth][32];
     __shared__ float s_ring_vz[kWarps][kDepth][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -517,7 +518,7 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
         return lx >= 1 && lx <= kTileX - 2 && ly >= 1 && ly <= kTileY - 2 && tgx0 + lx < A.nx &&
                gy < A.ny && !(A.k.pery && (gy == 0 || gy == A.ny - 1));
     };
-    if (MODE == kPush)
+    if (MODE == kPush && kTileY > 2)
         for (int i = threadIdx.x; i < kTileCells; i += kThreads) s_back[i] = 0u;
     for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
         const int gx = tgx0 + (i % kTileX), gy = tgy0 + (i / kTileX);
@@ -710,20 +711,23 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
         const uint32_t left = __reduce_add_sync(kFull, left_exits);
         if (lane == 0 && left) atomicAdd(A.counters, (unsigned long long)left);
         // the owned cells' back counts (no other block placed into them)
-        __syncthreads();
-        for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
-            const int lx = i % kTileX, ly = i / kTileX;
-            if (owned(lx, ly) && s_back[i]) A.back_dst[(int64_t)(tgy0 + ly) * A.nx + tgx0 + lx] = s_back[i];
+        if (kTileY > 2) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < kTileCells; i += kThreads) {
+                const int lx = i % kTileX, ly = i / kTileX;
+                if (owned(lx, ly) && s_back[i])
+                    A.back_dst[(int64_t)(tgy0 + ly) * A.nx + tgx0 + lx] = s_back[i];
+            }
         }
     }
 }
 
 // Tile shapes the kernels are built for (cells per block in x, y); every
 // shape has 256 cells.
-#define PIC_TILE_SHAPES(X) X(64, 4) X(32, 8) X(128, 2) X(16, 16)
+#define PIC_TILE_SHAPES(X) X(64, 4) X(256, 1) X(128, 2) X(16, 16)
 constexpr int kNumTileShapes = 4;
-constexpr int kTileShapeX[kNumTileShapes] = {64, 32, 128, 16};
-constexpr int kTileShapeY[kNumTileShapes] = {4, 8, 2, 16};
+constexpr int kTileShapeX[kNumTileShapes] = {64, 256, 128, 16};
+constexpr int kTileShapeY[kNumTileShapes] = {4, 1, 2, 16};
 
 template <int MODE, bool ENERGY, int TX, int TY>
 __global__ void __launch_bounds__(kThreads, kCellBlocksPerSM) k_cells(KArgs A) {
@@ -1196,7 +1200,7 @@ dim3 tile_grid(const pic_ctx* c, int shape) {
 template <int MODE, bool ENERGY>
 void launch_cells(int shape, dim3 grid, cudaStream_t st, const KArgs& A) {
     switch (shape) {
-        case 1: k_cells<MODE, ENERGY, 32, 8><<<grid, kThreads, 0, st>>>(A); break;
+        case 1: k_cells<MODE, ENERGY, 256, 1><<<grid, kThreads, 0, st>>>(A); break;
         case 2: k_cells<MODE, ENERGY, 128, 2><<<grid, kThreads, 0, st>>>(A); break;
         case 3: k_cells<MODE, ENERGY, 16, 16><<<grid, kThreads, 0, st>>>(A); break;
         default: k_cells<MODE, ENERGY, 64, 4><<<grid, kThreads, 0, st>>>(A); break;
@@ -1207,7 +1211,7 @@ template <int MODE, bool ENERGY>
 void launch_cells_batch(int shape, unsigned nblocks, cudaStream_t st, const KArgs* args,
                         const uint2* work) {
     switch (shape) {
-        case 1: k_cells_batch<MODE, ENERGY, 32, 8><<<nblocks, kThreads, 0, st>>>(args, work); break;
+        case 1: k_cells_batch<MODE, ENERGY, 256, 1><<<nblocks, kThreads, 0, st>>>(args, work); break;
         case 2: k_cells_batch<MODE, ENERGY, 128, 2><<<nblocks, kThreads, 0, st>>>(args, work); break;
         case 3: k_cells_batch<MODE, ENERGY, 16, 16><<<nblocks, kThreads, 0, st>>>(args, work); break;
         default: k_cells_batch<MODE, ENERGY, 64, 4><<<nblocks, kThreads, 0, st>>>(args, work); break;

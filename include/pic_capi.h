@@ -251,7 +251,7 @@ int pic_launch_count(pic_ctx* ctx, int64_t* n);
 
 /* ---- tuning (no reference counterpart) -----------------------------------
  * The particle kernels are built for PIC_NUM_TILE_SHAPES tile shapes of 256
- * cells: 0 = 64x4 (default), 1 = 32x8, 2 = 128x2, 3 = 16x16. */
+ * cells: 0 = 64x4 (default), 1 = 256x1, 2 = 128x2, 3 = 16x16. */
 #define PIC_NUM_TILE_SHAPES 4
 int pic_set_tile_shape(pic_ctx* ctx, int tile_shape);
 /* Times the push of the current particles with every tile shape (the

@@ -365,3 +365,35 @@ def test_converging_flow_overflow_and_far_jumps(oracle):
     sp, wgt = oracle_species(oracle, w, 0)
     fin_o, _ = oracle.deposit(g, lv, sp, wgt, EPS0)
     assert np.abs(fin - fin_o).max() <= 2e-6 * np.abs(fin_o).max()
+
+
+@pytest.mark.parametrize("shape,periodic", [(1, False), (2, False), (3, False), (1, True)])
+def test_tile_shapes_agree(shape, periodic):
+    """Every tile shape of the particle kernels gives the same run as the
+    default one: bit-identical charge density, the same particle state as a
+    multiset, the same counts -- on a grid that no tile shape divides, with
+    the fields of a solve and Bz, over several steps."""
+    import pic_b200 as P
+    import pic_configs as C
+    w = small_workload(nx=300, ny=37, ppc=12)
+    w.b0 = 0.01
+    if periodic:
+        w.rects = C.periodic_rects(w.nx, w.ny, 30.0, -5.0)
+    out = []
+    for sh in (0, shape):
+        with P.Pic(C.library_config(w, periodic_y=periodic)) as pic:
+            pic.set_tile_shape(sh)
+            C.load_plasma(pic, w, seed=21)
+            rho = []
+            for it in range(4):
+                pic.step(it)
+                rho.append(pic.rho())
+            out.append((rho, [multiset(export_state(pic, s)) for s in range(2)],
+                        [pic.count(s) for s in range(2)], [pic.bin_counts(s) for s in range(2)]))
+    (r0, m0, c0, b0), (r1, m1, c1, b1) = out
+    assert c0 == c1
+    for a, b in zip(r0, r1):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        assert np.array_equal(m0[s], m1[s])
+        assert np.array_equal(b0[s], b1[s])
