@@ -426,9 +426,10 @@ struct MoverQueue {
 constexpr uint16_t kOffTile = 0xffffu;
 // A cell strictly inside the block's tile (not on the tile's border, not on
 // the periodic seam) receives direct placements only from cells of the
-// same tile: movers placed here go at most one cell (longer jumps go to the
-// side list).  Its back count is kept in shared memory and written out when
-// the block ends, instead of a global atomic per group of movers.
+// same tile: one-cell movers from elsewhere cannot reach it, and longer
+// jumps into it from other tiles go to the side list.  Its back count is
+// kept in shared memory and written out when the block ends, instead of a
+// global atomic per group of movers.
 constexpr uint16_t kOwned = 0x8000u;
 
 // Places `count` (<= 32) queued movers, entries 0..count-1.
@@ -513,10 +514,13 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     const unsigned lt = lanemask_lt();
     // tile cell (lx, ly) is owned: inside the grid, off the tile's border
     // and off the periodic seam (rows 0 and ny-1 exchange wrapped movers)
+    // (the same rule for a cell of any tile: position (lx, ly) in its tile, row gy)
+    auto owned_at = [&](int lx, int ly, int gy) {
+        return lx >= 1 && lx <= kTileX - 2 && ly >= 1 && ly <= kTileY - 2 &&
+               !(A.k.pery && (gy == 0 || gy == A.ny - 1));
+    };
     auto owned = [&](int lx, int ly) {
-        const int gy = tgy0 + ly;
-        return lx >= 1 && lx <= kTileX - 2 && ly >= 1 && ly <= kTileY - 2 && tgx0 + lx < A.nx &&
-               gy < A.ny && !(A.k.pery && (gy == 0 || gy == A.ny - 1));
+        return tgx0 + lx < A.nx && tgy0 + ly < A.ny && owned_at(lx, ly, tgy0 + ly);
     };
     if (MODE == kPush && kTileY > 2)
         for (int i = threadIdx.x; i < kTileCells; i += kThreads) s_back[i] = 0u;
@@ -647,13 +651,19 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                     bool mv = false, far = false;
                     if (other) {
                         resolve_move(p, A.k, gx, gy, A.nx, A.ny);
-                        mv = p.dir >= 0 && p.dir != kFar;
-                        far = p.dir == kFar;
+                        mv = p.dir >= 0;
+                        // a jump of more than one cell into a cell that
+                        // another block owns: deposited here, placed from
+                        // the side list after the pass (rare)
+                        if (kTileY > 2 && p.dir == kFar) {
+                            const int olx = p.gx % kTileX, oly = p.gy % kTileY;
+                            const bool mine = p.gx - olx == tgx0 && p.gy - oly == tgy0;
+                            far = !mine && owned_at(olx, oly, p.gy);
+                            mv = mv && !far;
+                        }
                         left_exits += (p.dir < 0 && p.left) ? 1u : 0u;
                     }
-                    // a jump of more than one cell: deposited here, placed
-                    // from the side list after the pass (rare)
-                    if (__any_sync(kFull, far)) {
+                    if (kTileY > 2 && __any_sync(kFull, far)) {
                         const uint32_t tc = (uint32_t)(p.gy * A.nx + p.gx);
                         if (far) {
                             const float ef = ENERGY ? energy_ev(p.vx, p.vy, vz, A.k.half_inv_abs_qm) : 0.f;

@@ -159,7 +159,9 @@ int pic_reserve(pic_ctx* ctx, int species, int64_t capacity);
 /* Replace a species' particles with n host Points (reference AoS).  The cell
  * is (int)(x*(1/dx)), (int)(y*(1/dy)) as in InsertKernel
  * (src/particles.cpp:230-235); the FP32 offset is the FP64 remainder.
- * Dead (pointer == -1) or out-of-domain points are dropped. */
+ * Dead (pointer == -1) or out-of-domain points are dropped.  A cell holds at
+ * most 43,680 particles (its slots, n + n/2 + 16, stay within 2^16):
+ * PIC_ERR_CAPACITY beyond that. */
 int pic_import_points(pic_ctx* ctx, int species, const pic_point* host, int64_t n);
 int pic_export_points(pic_ctx* ctx, int species, pic_point* host, int64_t capacity,
                       int64_t* n_out);

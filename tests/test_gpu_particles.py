@@ -397,3 +397,36 @@ def test_tile_shapes_agree(shape, periodic):
     for s in range(2):
         assert np.array_equal(m0[s], m1[s])
         assert np.array_equal(b0[s], b1[s])
+
+
+@pytest.mark.parametrize("shape", [1, 2, 3])
+def test_fast_particles_every_tile_shape(shape):
+    """A beam whose particles jump 2-3 cells a step (longer than the one-cell
+    moves the placement is built around), with thermal electrons beside it:
+    every tile shape keeps every particle and gives the default shape's
+    state and charge density."""
+    import pic_b200 as P
+    import pic_configs as C
+    w = small_workload(nx=96, ny=80, ppc=10)
+    rng = np.random.default_rng(8)
+    pts = C.host_points(w, 0, seed=8)
+    beam = rng.random(len(pts)) < 0.4
+    pts["vx"][beam] = rng.uniform(2.0, 3.0, beam.sum()) * w.dx / w.dt * rng.choice([-1, 1], beam.sum())
+    pts["vy"][beam] = rng.uniform(-2.5, 2.5, beam.sum()) * w.dx / w.dt
+    out = []
+    for sh in (0, shape):
+        with make_pic(w) as pic:
+            pic.set_tile_shape(sh)
+            pic.import_points(0, pts)
+            rho = []
+            for it in range(3):
+                pic.zero_rho()
+                pic.charge_deposition(0)
+                rho.append(pic.rho())
+                pic.move_particles(0, it)
+            out.append((rho, multiset(export_state(pic, 0)), pic.count(0), pic.left_exits(0)))
+    (r0, m0, c0, l0), (r1, m1, c1, l1) = out
+    assert c0 == c1 and l0 == l1 and c0 > 0.5 * len(pts)
+    for a, b in zip(r0, r1):
+        assert np.array_equal(a, b)
+    assert np.array_equal(m0, m1)
