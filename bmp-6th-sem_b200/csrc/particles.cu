@@ -139,7 +139,7 @@ struct Pushed {
     int sx, sy;    // cell step: 0, 0 exactly when the particle keeps its cell
     // set by resolve_move
     int gx, gy;
-    int dir;  // 0..8 near (4 = same cell), kFar, or -1 when absorbed
+    int dir;  // 0: moved at most one cell in x and y, kFar: farther, -1: absorbed
     bool left;
 };
 
@@ -217,7 +217,7 @@ __device__ __forceinline__ void resolve_move(Pushed& o, const SpeciesConsts& k, 
     const bool alive = ok && (unsigned)o.gx < (unsigned)nx && (unsigned)o.gy < (unsigned)ny;
     o.left = ok ? (o.gx < 0) : (px < 0.0f);
     const bool near = (unsigned)(sx + 1) < 3u && (unsigned)(sy + 1) < 3u;
-    o.dir = !alive ? -1 : (near ? (sy + 1) * 3 + (sx + 1) : kFar);
+    o.dir = !alive ? -1 : (near ? 0 : kFar);
 }
 
 __device__ __forceinline__ Pushed push_one(float4 a, float4 n00, float4 n10, float4 n01,
@@ -420,36 +420,40 @@ constexpr int kQueue = 64;
 struct MoverQueue {
     float4 a[kQueue];
     float vz[kQueue];
-    uint2 tn[kQueue];  // target cell, its lower-left node
-    uint16_t loc[kQueue];  // target's index in the block's tile (| kOwned), kOffTile outside
+    uint2 g[kQueue];  // target cell (gx, gy)
 };
-constexpr uint16_t kOffTile = 0xffffu;
-// A cell strictly inside the block's tile (not on the tile's border, not on
+
+// A cell strictly inside its block's tile (not on the tile's border, not on
 // the periodic seam) receives direct placements only from cells of the
 // same tile: one-cell movers from elsewhere cannot reach it, and longer
 // jumps into it from other tiles go to the side list.  Its back count is
 // kept in shared memory and written out when the block ends, instead of a
-// global atomic per group of movers.
-constexpr uint16_t kOwned = 0x8000u;
+// global atomic per group of movers.  (lx, ly): the cell's position in its
+// tile; gy: its row.
+template <int TX, int TY>
+__device__ __forceinline__ bool tile_owned(int lx, int ly, int gy, const KArgs& A) {
+    return TY > 2 && lx >= 1 && lx <= TX - 2 && ly >= 1 && ly <= TY - 2 &&
+           !(A.k.pery && (gy == 0 || gy == A.ny - 1));
+}
 
-// Places `count` (<= 32) queued movers, entries 0..count-1.
-template <bool ENERGY>
+// Places `count` (<= 32) queued movers, entries 0..count-1, from the block
+// of tile (tgx0, tgy0): all lanes busy on the target's bookkeeping.
+template <bool ENERGY, int TX, int TY>
 __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
                                              const CellMeta* __restrict__ s_meta,
-                                             uint32_t* s_back, int count, int lane, unsigned lt) {
+                                             uint32_t* s_back, int tgx0, int tgy0, int count,
+                                             int lane, unsigned lt) {
     __syncwarp();
     const bool on = lane < count;
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
     float vz = 0.f;
-    uint2 tn = make_uint2(0u, 0u);
-    uint32_t loc = kOffTile;
+    uint2 g = make_uint2(0u, 0u);
     if (on) {
         a = q.a[lane];
         vz = q.vz[lane];
-        tn = q.tn[lane];
-        loc = q.loc[lane];
+        g = q.g[lane];
     }
-    const uint32_t t = tn.x;
+    const uint32_t t = g.y * (uint32_t)A.nx + g.x;
     const float en = (ENERGY && on) ? energy_ev(a.z, a.w, vz, A.k.half_inv_abs_qm) : 0.f;
     // movers bound for the same cell form a group; its leader reserves the
     // group's slots at the back of the cell, capped at the cell's capacity
@@ -459,12 +463,14 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
     uint32_t old = 0, lim = 0, top = 0;
     if (on && lane == leader) {
         const uint32_t cnt = __popc(grp);
+        const int lx = (int)g.x - tgx0, ly = (int)g.y - tgy0;
+        const bool in_tile = (unsigned)lx < (unsigned)TX && (unsigned)ly < (unsigned)TY;
         // the target's slots and source counts: from the tile's shared
         // metadata when it lies in this block's tile (most movers go one
         // cell), else from global memory
         CellMeta m;
-        if (loc != kOffTile) {
-            m = s_meta[loc & ~(uint32_t)kOwned];
+        if (in_tile) {
+            m = s_meta[ly * TX + lx];
         } else {
             m.b0 = A.base[t];
             m.b1 = A.base[t + 1];
@@ -474,14 +480,14 @@ __device__ __forceinline__ void place_movers(const KArgs& A, MoverQueue& q,
         lim = (m.b1 - m.b0) - (m.nf + m.nb);
         top = m.b1;
         // the back count: in shared memory for a cell this block owns
-        uint32_t* ctr = (loc != kOffTile && (loc & kOwned)) ? s_back + (loc & ~(uint32_t)kOwned)
-                                                            : A.back_dst + t;
+        uint32_t* ctr = (in_tile && tile_owned<TX, TY>(lx, ly, (int)g.y, A)) ? s_back + (ly * TX + lx)
+                                                                              : A.back_dst + t;
         old = atomicAdd(ctr, cnt);
         // give back what does not fit (the count then ends at
         // min(requested, lim) with slots 0.. taken)
         if (old + cnt > lim) atomicSub(ctr, old >= lim ? cnt : old + cnt - lim);
     }
-    if (on) deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, tn.y, a.x, a.y, en);
+    if (on) deposit_one<ENERGY>(A.acc_q, A.acc_e, A.GX, g.y * (uint32_t)A.GX + g.x, a.x, a.y, en);
     old = __shfl_sync(kFull, old, leader);
     lim = __shfl_sync(kFull, lim, leader);
     top = __shfl_sync(kFull, top, leader);
@@ -514,13 +520,8 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
     const unsigned lt = lanemask_lt();
     // tile cell (lx, ly) is owned: inside the grid, off the tile's border
     // and off the periodic seam (rows 0 and ny-1 exchange wrapped movers)
-    // (the same rule for a cell of any tile: position (lx, ly) in its tile, row gy)
-    auto owned_at = [&](int lx, int ly, int gy) {
-        return lx >= 1 && lx <= kTileX - 2 && ly >= 1 && ly <= kTileY - 2 &&
-               !(A.k.pery && (gy == 0 || gy == A.ny - 1));
-    };
     auto owned = [&](int lx, int ly) {
-        return tgx0 + lx < A.nx && tgy0 + ly < A.ny && owned_at(lx, ly, tgy0 + ly);
+        return tgx0 + lx < A.nx && tgy0 + ly < A.ny && tile_owned<TX, TY>(lx, ly, tgy0 + ly, A);
     };
     if (MODE == kPush && kTileY > 2)
         for (int i = threadIdx.x; i < kTileCells; i += kThreads) s_back[i] = 0u;
@@ -658,7 +659,7 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                         if (kTileY > 2 && p.dir == kFar) {
                             const int olx = p.gx % kTileX, oly = p.gy % kTileY;
                             const bool mine = p.gx - olx == tgx0 && p.gy - oly == tgy0;
-                            far = !mine && owned_at(olx, oly, p.gy);
+                            far = !mine && tile_owned<TX, TY>(olx, oly, p.gy, A);
                             mv = mv && !far;
                         }
                         left_exits += (p.dir < 0 && p.left) ? 1u : 0u;
@@ -678,23 +679,18 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
                             const int e = queued + __popc(mm & lt);
                             q.a[e] = make_float4(p.fx, p.fy, p.vx, p.vy);
                             q.vz[e] = vz;
-                            q.tn[e] = make_uint2((uint32_t)(p.gy * A.nx + p.gx), (uint32_t)(p.gy * A.GX + p.gx));
-                            const int llx = p.gx - tgx0, lly = p.gy - tgy0;
-                            q.loc[e] = ((unsigned)llx < (unsigned)kTileX && (unsigned)lly < (unsigned)kTileY)
-                                           ? (uint16_t)((lly * kTileX + llx) | (owned(llx, lly) ? kOwned : 0u))
-                                           : kOffTile;
+                            q.g[e] = make_uint2((uint32_t)p.gx, (uint32_t)p.gy);
                         }
                         queued += __popc(mm);
                         if (queued >= 32) {
-                            place_movers<ENERGY>(A, q, s_meta, s_back, 32, lane, lt);
+                            place_movers<ENERGY, TX, TY>(A, q, s_meta, s_back, tgx0, tgy0, 32, lane, lt);
                             // the rest (< 32) moves to the front of the queue
                             queued -= 32;
                             __syncwarp();
                             if (lane < queued) {
                                 q.a[lane] = q.a[32 + lane];
                                 q.vz[lane] = q.vz[32 + lane];
-                                q.tn[lane] = q.tn[32 + lane];
-                                q.loc[lane] = q.loc[32 + lane];
+                                q.g[lane] = q.g[32 + lane];
                             }
                             __syncwarp();
                         }
@@ -716,7 +712,8 @@ __device__ __forceinline__ void cells_body(const KArgs& A, int tile_x, int tile_
         }
         cp_async_wait<0>();
     }
-    if (MODE == kPush && queued > 0) place_movers<ENERGY>(A, q, s_meta, s_back, queued, lane, lt);
+    if (MODE == kPush && queued > 0)
+        place_movers<ENERGY, TX, TY>(A, q, s_meta, s_back, tgx0, tgy0, queued, lane, lt);
     if (MODE == kPush) {
         const uint32_t left = __reduce_add_sync(kFull, left_exits);
         if (lane == 0 && left) atomicAdd(A.counters, (unsigned long long)left);
