@@ -39,6 +39,7 @@
 // launch and one host synchronisation.  Without conditional-node support the
 // same kernels run from a host loop.
 #include <cooperative_groups.h>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -149,6 +150,16 @@ __device__ __forceinline__ I row_dn(I k, I n, int GX) {
     return d < 0 ? d + n : d;
 }
 
+// Programmatic dependent launch (the PCG iteration's kernels are launched
+// with it): wait until the grid before this one in the stream has finished
+// and its writes are visible, then let the next grid start launching its
+// blocks, which wait here in turn.  The launch of each small kernel then
+// overlaps the end of the one before.  Called first thing, by every thread.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // overwriteRho (src/poissonSolver.cpp:384-402) in place: b = -rho, electrode
 // nodes b = -V.  Also imposes the electrode potentials on phi and, for a
 // zero warm start, clears phi.
@@ -216,6 +227,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t nodes, const uin
                                                         double inv_diag, int jacobi, double* z,
                                                         double* partials, int nblocks,
                                                         unsigned* arrive, double* scal) {
+    pdl_enter();
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -231,6 +243,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t nodes, const uin
 // (re)start, marked by rz_old == 0)
 __global__ void k_pcg_p(int64_t nodes, const uint8_t* mask, const double* z, double* p,
                         const double* scal) {
+    pdl_enter();
     const double ro = scal[S_RZ_OLD];
     const double beta = ro == 0.0 ? 0.0 : scal[S_RZ] / ro;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
@@ -243,6 +256,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_ap(Grid64 g, const uint8_t*
                                                         const double* p, double* q,
                                                         double* partials, int nblocks,
                                                         unsigned* arrive, double* scal) {
+    pdl_enter();
     const int64_t nodes = g.n;
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
@@ -263,6 +277,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int64_t nodes, const
                                                             double* x, double* r, float* r32,
                                                             double* partials, int nblocks,
                                                             unsigned* arrive, double* scal) {
+    pdl_enter();
     const double alpha = scal[S_RZ] / scal[S_PQ];
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
@@ -282,6 +297,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int64_t nodes, const
 // End of an iteration: count it, keep rz for the next beta, decide whether
 // to go on (and tell the graph's while node when there is one).
 __global__ void k_pcg_cond(double* scal, cudaGraphConditionalHandle handle, int use_handle) {
+    pdl_enter();
     const double it = scal[S_IT] + 1.0;
     scal[S_IT] = it;
     scal[S_RZ_OLD] = scal[S_RZ];
@@ -332,6 +348,7 @@ __host__ __device__ __forceinline__ LevelDev as_dev(const MGLevel& L) {
 // x = b/cd on red non-Dirichlet nodes, 0 elsewhere: the first red sweep from
 // a zero guess.
 __global__ void k_mg_init(LevelDev L) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= L.GX || j >= L.GY) return;
@@ -341,6 +358,7 @@ __global__ void k_mg_init(LevelDev L) {
 
 // one Gauss-Seidel half sweep over the nodes of one colour
 __global__ void k_mg_rbgs(LevelDev L, int color) {
+    pdl_enter();
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = 2 * h + ((j + color) & 1);
@@ -367,6 +385,7 @@ __device__ __forceinline__ float fine_residual(const LevelDev& F, int i, int j) 
 
 // b_coarse = full weighting of the fine residual
 __global__ void k_mg_restrict(LevelDev F, LevelDev C) {
+    pdl_enter();
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= C.GX || J >= C.GY) return;
@@ -386,6 +405,7 @@ __global__ void k_mg_restrict(LevelDev F, LevelDev C) {
 
 // x_fine += bilinear interpolation of x_coarse (non-Dirichlet fine nodes)
 __global__ void k_mg_prolong(LevelDev F, LevelDev C) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= F.GX || j >= F.GY) return;
@@ -536,6 +556,7 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
 }
 
 __global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem[];
     fused_body(F, smem);
 }
@@ -631,6 +652,22 @@ unsigned* arrive_ptr(PoissonState& ps) { return reinterpret_cast<unsigned*>(ps.s
 
 // V-cycle on level 0 (b = r32 -> x = z32) enqueued on stream st; returns
 // the number of kernels launched.
+// Launch with programmatic stream serialisation (see pdl_enter).
+template <typename... P, typename... A>
+void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
     PoissonState& ps = c->ps;
     const int kf = ps.fused_first;
@@ -641,25 +678,26 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const dim3 gn = grid2d(F.GX, F.GY, b2);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        k_mg_init<<<gn, b2, 0, st>>>(F);
-        k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
+        launch_pdl(k_mg_init, gn, b2, 0, st, F);
+        launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
         for (int s = 1; s < kNu; ++s) {
-            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 0);
-            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
+            launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
+            launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
         }
-        k_mg_restrict<<<grid2d(C.GX, C.GY, b2), b2, 0, st>>>(F, C);
+        launch_pdl(k_mg_restrict, grid2d(C.GX, C.GY, b2), b2, 0, st, F, C);
         launches += 3 + 2 * kNu - 1;
     }
-    k_mg_fused<<<1, kFusedThreads, ps.fused_smem, st>>>(*reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
+               *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
     launches += 1;
     for (int l = kf - 1; l >= 0; --l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        k_mg_prolong<<<grid2d(F.GX, F.GY, b2), b2, 0, st>>>(F, C);
+        launch_pdl(k_mg_prolong, grid2d(F.GX, F.GY, b2), b2, 0, st, F, C);
         for (int s = 0; s < kNu; ++s) {
-            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 1);
-            k_mg_rbgs<<<gh, b2, 0, st>>>(F, 0);
+            launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
+            launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
         }
         launches += 1 + 2 * kNu;
     }
@@ -675,13 +713,14 @@ int enqueue_iteration(pic_ctx* c, cudaStream_t st, bool jacobi,
     unsigned* arrive = arrive_ptr(ps);
     int launches = 0;
     if (!jacobi) launches += enqueue_vcycle(c, st);
-    k_pcg_rz<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
-                                         jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
-    k_pcg_p<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.z, ps.p[0], ps.scal);
-    k_pcg_ap<<<nb, kRedThreads, 0, st>>>(g, c->mask, ps.p[0], ps.q, ps.partials, nb, arrive, ps.scal);
-    k_pcg_update<<<nb, kRedThreads, 0, st>>>(g.n, c->mask, ps.p[0], ps.q, c->phi, ps.r,
-                                             ps.levels[0].b, ps.partials, nb, arrive, ps.scal);
-    k_pcg_cond<<<1, 1, 0, st>>>(ps.scal, handle, use_handle);
+    const dim3 gb(nb), tb(kRedThreads);
+    launch_pdl(k_pcg_rz, gb, tb, 0, st, g.n, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
+               jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
+    launch_pdl(k_pcg_p, gb, tb, 0, st, g.n, c->mask, ps.z, ps.p[0], ps.scal);
+    launch_pdl(k_pcg_ap, gb, tb, 0, st, g, c->mask, ps.p[0], ps.q, ps.partials, nb, arrive, ps.scal);
+    launch_pdl(k_pcg_update, gb, tb, 0, st, g.n, c->mask, ps.p[0], ps.q, c->phi, ps.r,
+               ps.levels[0].b, ps.partials, nb, arrive, ps.scal);
+    launch_pdl(k_pcg_cond, dim3(1), dim3(1), 0, st, ps.scal, handle, use_handle);
     return launches + 5;
 }
 
