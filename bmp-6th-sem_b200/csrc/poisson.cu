@@ -81,8 +81,9 @@ struct Grid64 {
 
 // ---- deterministic block reduction with last-block finalisation ---------
 
+// Returns true in the last block (after `out` is written).
 template <int ND>
-__device__ __forceinline__ void reduce_finalize(double (&v)[ND], double* partials, int nblocks,
+__device__ __forceinline__ bool reduce_finalize(double (&v)[ND], double* partials, int nblocks,
                                                 unsigned int* arrive, double* out, int slot0) {
     __shared__ double sh[ND][kRedThreads / 32];
     __shared__ bool last;
@@ -107,7 +108,7 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[ND], double* partial
         last = (prev == (unsigned)nblocks - 1);
     }
     __syncthreads();
-    if (!last) return;
+    if (!last) return false;
     __threadfence();
     // the last block sums the partials in block order: fixed order, fixed result
 #pragma unroll
@@ -129,6 +130,7 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[ND], double* partial
         }
     }
     if (threadIdx.x == 0) *arrive = 0u;
+    return true;
 }
 
 __device__ __forceinline__ double dirv(const uint8_t* mask, const double* dv, int64_t k) {
@@ -239,44 +241,47 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t nodes, const uin
     reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_RZ);
 }
 
-// p = z + beta p (beta = rz/rz_old; 0 on the first iteration after a
-// (re)start, marked by rz_old == 0)
-__global__ void k_pcg_p(int64_t nodes, const uint8_t* mask, const double* z, double* p,
-                        const double* scal) {
-    pdl_enter();
-    const double ro = scal[S_RZ_OLD];
-    const double beta = ro == 0.0 ? 0.0 : scal[S_RZ] / ro;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
-         i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = mask[i] ? 0.0 : z[i] + beta * p[i];
-}
-
-// q = A p; partial p.q
-__global__ void __launch_bounds__(kRedThreads) k_pcg_ap(Grid64 g, const uint8_t* mask,
-                                                        const double* p, double* q,
+// p = z + beta p and q = A p, the latter as A z + beta q (q holds A p of the
+// previous direction), so one pass reads z's neighbours and no kernel
+// boundary is needed between the two; partial p.q.  beta = rz/rz_old, 0 on
+// the first iteration after a (re)start (marked by rz_old == 0).
+__global__ void __launch_bounds__(kRedThreads) k_pcg_pq(Grid64 g, const uint8_t* mask,
+                                                        const double* z, double* p, double* q,
                                                         double* partials, int nblocks,
                                                         unsigned* arrive, double* scal) {
     pdl_enter();
+    const double ro = scal[S_RZ_OLD];
+    const double beta = ro == 0.0 ? 0.0 : scal[S_RZ] / ro;
     const int64_t nodes = g.n;
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
-        double qi = 0.0;
-        if (!mask[i])
-            qi = g.cd * p[i] - g.cx * (p[i - 1] + p[i + 1]) -
-                 g.cy * (p[row_dn(i, nodes, g.GX)] + p[row_up(i, nodes, g.GX)]);
+        double pi = 0.0, qi = 0.0;
+        if (!mask[i]) {
+            const double az = g.cd * z[i] - g.cx * (z[i - 1] + z[i + 1]) -
+                              g.cy * (z[row_dn(i, nodes, g.GX)] + z[row_up(i, nodes, g.GX)]);
+            // (after a restart p and q are not read: beta == 0)
+            pi = beta == 0.0 ? z[i] : z[i] + beta * p[i];
+            qi = beta == 0.0 ? az : az + beta * q[i];
+        }
+        p[i] = pi;
         q[i] = qi;
-        acc[0] += p[i] * qi;
+        acc[0] += pi * qi;
     }
     reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_PQ);
 }
 
 // x += alpha p; r -= alpha q; r32 = r; partial r.r.  Also shifts rz -> rz_old.
+// The last block then ends the iteration: counts it, keeps rz for the next
+// beta, decides whether to go on (and tells the graph's while node when
+// there is one).
 __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int64_t nodes, const uint8_t* mask,
                                                             const double* p, const double* q,
                                                             double* x, double* r, float* r32,
                                                             double* partials, int nblocks,
-                                                            unsigned* arrive, double* scal) {
+                                                            unsigned* arrive, double* scal,
+                                                            cudaGraphConditionalHandle handle,
+                                                            int use_handle) {
     pdl_enter();
     const double alpha = scal[S_RZ] / scal[S_PQ];
     double acc[1] = {0.0};
@@ -291,13 +296,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int64_t nodes, const
         r32[i] = (float)ri;
         acc[0] += ri * ri;
     }
-    reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_RR);
-}
-
-// End of an iteration: count it, keep rz for the next beta, decide whether
-// to go on (and tell the graph's while node when there is one).
-__global__ void k_pcg_cond(double* scal, cudaGraphConditionalHandle handle, int use_handle) {
-    pdl_enter();
+    if (!reduce_finalize<1>(acc, partials, nblocks, arrive, scal, S_RR) || threadIdx.x != 0) return;
     const double it = scal[S_IT] + 1.0;
     scal[S_IT] = it;
     scal[S_RZ_OLD] = scal[S_RZ];
@@ -716,12 +715,11 @@ int enqueue_iteration(pic_ctx* c, cudaStream_t st, bool jacobi,
     const dim3 gb(nb), tb(kRedThreads);
     launch_pdl(k_pcg_rz, gb, tb, 0, st, g.n, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
                jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
-    launch_pdl(k_pcg_p, gb, tb, 0, st, g.n, c->mask, ps.z, ps.p[0], ps.scal);
-    launch_pdl(k_pcg_ap, gb, tb, 0, st, g, c->mask, ps.p[0], ps.q, ps.partials, nb, arrive, ps.scal);
+    launch_pdl(k_pcg_pq, gb, tb, 0, st, g, c->mask, ps.z, ps.p[0], ps.q, ps.partials, nb, arrive,
+               ps.scal);
     launch_pdl(k_pcg_update, gb, tb, 0, st, g.n, c->mask, ps.p[0], ps.q, c->phi, ps.r,
-               ps.levels[0].b, ps.partials, nb, arrive, ps.scal);
-    launch_pdl(k_pcg_cond, dim3(1), dim3(1), 0, st, ps.scal, handle, use_handle);
-    return launches + 5;
+               ps.levels[0].b, ps.partials, nb, arrive, ps.scal, handle, use_handle);
+    return launches + 3;
 }
 
 __global__ void k_cond_init(const double* scal, cudaGraphConditionalHandle handle) {
@@ -788,6 +786,7 @@ int poisson_setup(pic_ctx* c) {
     PIC_CUDA(cudaMalloc(&ps.q, n * 8));
     PIC_CUDA(cudaMemsetAsync(ps.p[0], 0, n * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(ps.p[1], 0, n * 8, c->stream));
+    PIC_CUDA(cudaMemsetAsync(ps.q, 0, n * 8, c->stream));
     ps.nblocks = (int)std::min<int64_t>((c->nodes + kRedThreads - 1) / kRedThreads, 148 * 8);
     PIC_CUDA(cudaMalloc(&ps.partials, (size_t)ps.nblocks * 4 * sizeof(double)));
     PIC_CUDA(cudaMalloc(&ps.scal, 16 * sizeof(double)));
