@@ -344,17 +344,6 @@ __host__ __device__ __forceinline__ LevelDev as_dev(const MGLevel& L) {
     return LevelDev{L.nx, L.ny, L.GX, L.GY, L.cx, L.cy, L.cd, L.mask, L.x, L.b};
 }
 
-// x = b/cd on red non-Dirichlet nodes, 0 elsewhere: the first red sweep from
-// a zero guess.
-__global__ void k_mg_init(LevelDev L) {
-    pdl_enter();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= L.GX || j >= L.GY) return;
-    const int64_t k = (int64_t)j * L.GX + i;
-    L.x[k] = (((i + j) & 1) == 0 && !L.mask[k]) ? L.b[k] / L.cd : 0.0f;
-}
-
 // one Gauss-Seidel half sweep over the nodes of one colour
 __global__ void k_mg_rbgs(LevelDev L, int color) {
     pdl_enter();
@@ -402,14 +391,36 @@ __global__ void k_mg_restrict(LevelDev F, LevelDev C) {
     C.b[kc] = s * 0.0625f;
 }
 
-// x_fine += bilinear interpolation of x_coarse (non-Dirichlet fine nodes)
-__global__ void k_mg_prolong(LevelDev F, LevelDev C) {
+// The first black half sweep after a zero start or after the coarse
+// correction, fused with what precedes it.  A Gauss-Seidel update of a node
+// reads only its neighbours, and the red sweep that follows overwrites every
+// red node without reading it, so the red values these steps would write
+// are only needed here: each black node computes its four red neighbours'
+// values itself (the same arithmetic as the separate kernels, so the same
+// bits) and nothing else is written.  Both need kNu >= 2 (a red sweep
+// before anything reads red nodes again).
+static_assert(kNu >= 2, "the fused first sweeps need a later red sweep");
+
+// zero start: red x = b/cd (Dirichlet 0), then the black sweep
+__global__ void k_mg_init_black(LevelDev L) {
     pdl_enter();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= F.GX || j >= F.GY) return;
-    const int64_t k = (int64_t)j * F.GX + i;
-    if (F.mask[k]) return;
+    const int i = 2 * h + ((j + 1) & 1);
+    if (i >= L.GX || j >= L.GY) return;
+    const int k = j * L.GX + i, n = L.GX * L.GY;
+    if (L.mask[k]) return;
+    auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] / L.cd; };
+    const float s = __fmaf_rn(L.cx, xr(k - 1) + xr(k + 1),
+                              __fmaf_rn(L.cy, xr(row_dn(k, n, L.GX)) + xr(row_up(k, n, L.GX)), L.b[k]));
+    L.x[k] = s / L.cd;
+}
+
+// x at fine node (i, j) plus the bilinear interpolation of the coarse
+// correction (Dirichlet nodes unchanged)
+__device__ __forceinline__ float prolonged(const LevelDev& F, const LevelDev& C, int i, int j) {
+    const int k = j * F.GX + i;
+    if (F.mask[k]) return F.x[k];
     const int I = i >> 1, J = j >> 1;
     const int J1 = J + 1 == C.GY ? 0 : J + 1;  // wraps only periodic in y
     const bool ox = i & 1, oy = j & 1;
@@ -419,8 +430,24 @@ __global__ void k_mg_prolong(LevelDev F, LevelDev C) {
     else if (ox && !oy) v = 0.5f * (X(I, J) + X(I + 1, J));
     else if (!ox && oy) v = 0.5f * (X(I, J) + X(I, J1));
     else v = 0.25f * (X(I, J) + X(I + 1, J) + X(I, J1) + X(I + 1, J1));
-    F.x[k] += v;
+    return F.x[k] + v;
 }
+
+// coarse correction, then the black sweep
+__global__ void k_mg_prolong_black(LevelDev F, LevelDev C) {
+    pdl_enter();
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = 2 * h + ((j + 1) & 1);
+    if (i >= F.GX || j >= F.GY) return;
+    const int k = j * F.GX + i;
+    if (F.mask[k]) return;
+    const int jd = j == 0 ? F.GY - 1 : j - 1, ju = j + 1 == F.GY ? 0 : j + 1;
+    const float s = __fmaf_rn(F.cx, prolonged(F, C, i - 1, j) + prolonged(F, C, i + 1, j),
+                              __fmaf_rn(F.cy, prolonged(F, C, i, jd) + prolonged(F, C, i, ju), F.b[k]));
+    F.x[k] = s / F.cd;
+}
+
 
 // All levels from `first` down to the coarsest in one thread block, in
 // shared memory: the same operations as the per-level kernels (zero-start red
@@ -675,16 +702,14 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
     for (int l = 0; l < kf; ++l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
-        const dim3 gn = grid2d(F.GX, F.GY, b2);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        launch_pdl(k_mg_init, gn, b2, 0, st, F);
-        launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
+        launch_pdl(k_mg_init_black, gh, b2, 0, st, F);
         for (int s = 1; s < kNu; ++s) {
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
         }
         launch_pdl(k_mg_restrict, grid2d(C.GX, C.GY, b2), b2, 0, st, F, C);
-        launches += 3 + 2 * kNu - 1;
+        launches += 2 * kNu;
     }
     launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
                *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
@@ -693,12 +718,13 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const dim3 gh = grid2d((F.GX + 1) / 2, F.GY, b2);
-        launch_pdl(k_mg_prolong, grid2d(F.GX, F.GY, b2), b2, 0, st, F, C);
-        for (int s = 0; s < kNu; ++s) {
+        launch_pdl(k_mg_prolong_black, gh, b2, 0, st, F, C);
+        launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
+        for (int s = 1; s < kNu; ++s) {
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
         }
-        launches += 1 + 2 * kNu;
+        launches += 2 * kNu;
     }
     return launches;
 }
