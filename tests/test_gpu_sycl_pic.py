@@ -68,3 +68,46 @@ def test_reference_driver_loop(oracle, tmp_path, monkeypatch):
         assert ne2 > ne1 and ni2 > ni1 and ne2 - ne1 >= ni2 - ni1
     finally:
         sp.finalize()
+
+
+def test_reference_driver_loop_periodic(oracle, tmp_path, monkeypatch):
+    """The same loop on input files with periodicBoundary = 1 and three
+    electrodes (the x walls and a central block): the solve is the periodic
+    system, the last node row repeats row 0, and update_fields_from_phi
+    applies the periodic overwritePhi."""
+    import sycl_pic as sp
+    from test_capi_cpu import GEOMETRY, _write_inputs
+    _write_inputs(tmp_path, nx=64, ny=32, xmax=0.016, ymax=0.008, steps=3, pint=10, periodic=1)
+    rows = GEOMETRY.splitlines()
+    keep = [r for r in rows if not (r.strip().startswith("0.     1.") or r.strip().startswith("0.     0.      1."))]
+    geo = "\n".join(keep).replace("  5\n", "  3\n")
+    (tmp_path / "geometry.conf").write_text(geo)
+    monkeypatch.chdir(tmp_path)
+    sp.init("gpu", 256, 24, "e.inp", "i.inp")
+    try:
+        GX, GY = sp.get_grid_x(), sp.get_grid_y()
+        rho, phi = sp.get_rho(), sp.get_phi()
+        g = oracle.Electrodes.from_fractions(GX, GY, [(0, 0, 0, 1, 100.0), (1, 0, 1, 1, 0.0),
+                                                      (0.46875, 0.46875, 0.53125, 0.53125, 200.0)])
+        mask = oracle.electrode_mask(GX, GY, g)
+        dx, dy = 0.016 / 64, 0.008 / 32
+        for it in range(sp.get_timesteps()):
+            sp.zero_rho()
+            for s in range(sp.get_num_species()):
+                sp.charge_deposition(s)
+            assert sp.poisson_solve(it) >= 0
+            assert oracle.reduced_relres(GX, GY, dx, dy, mask, rho.copy(), phi.copy(),
+                                         periodic=True) <= 1e-8
+            p = phi.reshape(GY, GX)
+            assert np.array_equal(p[-1], p[0])
+            for s in range(sp.get_num_species()):
+                assert sp.move_particles(s, it) >= 0
+        ne, ni = sp.get_particle_counts()
+        assert ne > 0 and ni > 0
+        phi[:] = np.arange(GX * GY, dtype=np.float64)
+        sp.update_fields_from_phi()
+        p = phi.reshape(GY, GX)
+        # row 0 copied into the last row, then the electrodes
+        assert p[-1, 5] == 5.0 and p[-1, 0] == 100.0 and p[0, 0] == 100.0
+    finally:
+        sp.finalize()
