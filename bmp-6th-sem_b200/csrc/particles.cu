@@ -1051,21 +1051,41 @@ __global__ void k_bin_counts(const uint32_t* __restrict__ cnt, int nx, int ny, i
 
 // final_mesh = weighing * sum of unnormalised corner weights; rho += final *
 // (-q/eps) (src/interpolation.cpp:139-171).  Resets the accumulators.
-__global__ void k_flush(int64_t nodes, unsigned long long* acc_q, unsigned long long* acc_e,
-                        double qscale, double escale, double chrg, double* final_mesh,
-                        double* energy_mesh, double* rho, int energy) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nodes) return;
-    const double f = (double)acc_q[i] * qscale;
-    acc_q[i] = 0ull;
-    final_mesh[i] = f;
-    if (energy) {
-        energy_mesh[i] = (double)acc_e[i] * escale;
-        acc_e[i] = 0ull;
-    } else {
-        energy_mesh[i] = 0.0;
+// kFlushNodes nodes a thread, blockDim apart (coalesced), all loads issued
+// before any store: the arrays are distinct, so the loads need not wait on
+// each other's stores, and several are in flight per thread.
+constexpr int kFlushNodes = 4;
+
+__global__ void k_flush(int64_t nodes, unsigned long long* __restrict__ acc_q,
+                        unsigned long long* __restrict__ acc_e, double qscale, double escale,
+                        double chrg, double* __restrict__ final_mesh,
+                        double* __restrict__ energy_mesh, double* __restrict__ rho, int energy) {
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kFlushNodes + threadIdx.x;
+    unsigned long long q[kFlushNodes], e[kFlushNodes];
+    double r[kFlushNodes];
+#pragma unroll
+    for (int u = 0; u < kFlushNodes; ++u) {
+        const int64_t i = i0 + (int64_t)u * blockDim.x;
+        const bool in = i < nodes;
+        q[u] = in ? acc_q[i] : 0ull;
+        e[u] = (in && energy) ? acc_e[i] : 0ull;
+        r[u] = in ? rho[i] : 0.0;
     }
-    rho[i] += f * chrg;
+#pragma unroll
+    for (int u = 0; u < kFlushNodes; ++u) {
+        const int64_t i = i0 + (int64_t)u * blockDim.x;
+        if (i >= nodes) break;
+        const double f = (double)q[u] * qscale;
+        acc_q[i] = 0ull;
+        final_mesh[i] = f;
+        if (energy) {
+            energy_mesh[i] = (double)e[u] * escale;
+            acc_e[i] = 0ull;
+        } else {
+            energy_mesh[i] = 0.0;
+        }
+        rho[i] = r[u] + f * chrg;
+    }
 }
 
 // ---- device plasma loading (Philox-4x32-10, Salmon et al., SC'11) ----------
@@ -1674,7 +1694,7 @@ int particles_flush_rho(pic_ctx* c, int s) {
     const double chrg = -sp.desc.charge / c->cfg.epsilon;
     prof_begin(c, PIC_PHASE_FLUSH);
     c->launches += 1;
-    k_flush<<<grid1d(c->nodes, 256), 256, 0, c->stream>>>(c->nodes, sp.acc_q, sp.acc_e, qscale,
+    k_flush<<<grid1d(c->nodes, 256 * kFlushNodes), 256, 0, c->stream>>>(c->nodes, sp.acc_q, sp.acc_e, qscale,
                                                           escale, chrg, sp.final_mesh,
                                                           sp.energy_mesh, c->rho,
                                                           c->cfg.deposit_energy ? 1 : 0);
