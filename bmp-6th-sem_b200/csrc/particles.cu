@@ -1051,41 +1051,54 @@ __global__ void k_bin_counts(const uint32_t* __restrict__ cnt, int nx, int ny, i
 
 // final_mesh = weighing * sum of unnormalised corner weights; rho += final *
 // (-q/eps) (src/interpolation.cpp:139-171).  Resets the accumulators.
-// kFlushNodes nodes a thread, blockDim apart (coalesced), all loads issued
-// before any store: the arrays are distinct, so the loads need not wait on
-// each other's stores, and several are in flight per thread.
+// The conversion of one species' accumulators into its final/energy mesh
+// (and rho += final * chrg).
+struct FlushEntry {
+    int64_t nodes;
+    unsigned long long* acc_q;
+    unsigned long long* acc_e;
+    double qscale, escale, chrg;
+    double* final_mesh;
+    double* energy_mesh;
+    double* rho;
+    int energy;
+};
+
+// kFlushNodes nodes from i0 on, `stride` apart (coalesced across a block),
+// all loads issued before any store: the arrays are distinct, so the loads
+// need not wait on each other's stores, and several are in flight at once.
 constexpr int kFlushNodes = 4;
 
-__global__ void k_flush(int64_t nodes, unsigned long long* __restrict__ acc_q,
-                        unsigned long long* __restrict__ acc_e, double qscale, double escale,
-                        double chrg, double* __restrict__ final_mesh,
-                        double* __restrict__ energy_mesh, double* __restrict__ rho, int energy) {
-    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kFlushNodes + threadIdx.x;
+__device__ __forceinline__ void flush_nodes(const FlushEntry& F, int64_t i0, int stride) {
     unsigned long long q[kFlushNodes], e[kFlushNodes];
     double r[kFlushNodes];
 #pragma unroll
     for (int u = 0; u < kFlushNodes; ++u) {
-        const int64_t i = i0 + (int64_t)u * blockDim.x;
-        const bool in = i < nodes;
-        q[u] = in ? acc_q[i] : 0ull;
-        e[u] = (in && energy) ? acc_e[i] : 0ull;
-        r[u] = in ? rho[i] : 0.0;
+        const int64_t i = i0 + (int64_t)u * stride;
+        const bool in = i < F.nodes;
+        q[u] = in ? F.acc_q[i] : 0ull;
+        e[u] = (in && F.energy) ? F.acc_e[i] : 0ull;
+        r[u] = in ? F.rho[i] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < kFlushNodes; ++u) {
-        const int64_t i = i0 + (int64_t)u * blockDim.x;
-        if (i >= nodes) break;
-        const double f = (double)q[u] * qscale;
-        acc_q[i] = 0ull;
-        final_mesh[i] = f;
-        if (energy) {
-            energy_mesh[i] = (double)e[u] * escale;
-            acc_e[i] = 0ull;
+        const int64_t i = i0 + (int64_t)u * stride;
+        if (i >= F.nodes) break;
+        const double f = (double)q[u] * F.qscale;
+        F.acc_q[i] = 0ull;
+        F.final_mesh[i] = f;
+        if (F.energy) {
+            F.energy_mesh[i] = (double)e[u] * F.escale;
+            F.acc_e[i] = 0ull;
         } else {
-            energy_mesh[i] = 0.0;
+            F.energy_mesh[i] = 0.0;
         }
-        rho[i] = r[u] + f * chrg;
+        F.rho[i] = r[u] + f * F.chrg;
     }
+}
+
+__global__ void k_flush(FlushEntry F) {
+    flush_nodes(F, (int64_t)blockIdx.x * blockDim.x * kFlushNodes + threadIdx.x, blockDim.x);
 }
 
 // ---- device plasma loading (Philox-4x32-10, Salmon et al., SC'11) ----------
@@ -1694,10 +1707,9 @@ int particles_flush_rho(pic_ctx* c, int s) {
     const double chrg = -sp.desc.charge / c->cfg.epsilon;
     prof_begin(c, PIC_PHASE_FLUSH);
     c->launches += 1;
-    k_flush<<<grid1d(c->nodes, 256 * kFlushNodes), 256, 0, c->stream>>>(c->nodes, sp.acc_q, sp.acc_e, qscale,
-                                                          escale, chrg, sp.final_mesh,
-                                                          sp.energy_mesh, c->rho,
-                                                          c->cfg.deposit_energy ? 1 : 0);
+    const FlushEntry F{c->nodes, sp.acc_q, sp.acc_e, qscale, escale, chrg, sp.final_mesh,
+                       sp.energy_mesh, c->rho, c->cfg.deposit_energy ? 1 : 0};
+    k_flush<<<grid1d(c->nodes, 256 * kFlushNodes), 256, 0, c->stream>>>(F);
     prof_end(c, PIC_PHASE_FLUSH);
     PIC_CUDA(cudaGetLastError());
     sp.acc_fresh = false;
@@ -1864,35 +1876,15 @@ __global__ void k_batch_zero(const ZeroEntry* __restrict__ e, int n) {
     }
 }
 
-struct FlushEntry {
-    int64_t nodes;
-    unsigned long long* acc_q;
-    unsigned long long* acc_e;
-    double qscale, escale, chrg;
-    double* final_mesh;
-    double* energy_mesh;
-    double* rho;
-    int energy;
-};
-
-__global__ void k_batch_flush(const FlushEntry* __restrict__ e, int n) {
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
-    for (int i = 0; i < n; ++i) {
-        const FlushEntry F = e[i];
-        for (int64_t k = gtid; k < F.nodes; k += gsize) {
-            const double f = (double)F.acc_q[k] * F.qscale;
-            F.acc_q[k] = 0ull;
-            F.final_mesh[k] = f;
-            if (F.energy) {
-                F.energy_mesh[k] = (double)F.acc_e[k] * F.escale;
-                F.acc_e[k] = 0ull;
-            } else {
-                F.energy_mesh[k] = 0.0;
-            }
-            F.rho[k] += f * F.chrg;
-        }
-    }
+// Every species of every instance: block (x, i) works on kFlushNodes x 256
+// nodes of instance i, each thread on the same nodes of every species in
+// turn (species order, as rho sums them one species at a time).
+// e[s * n + i]: species s of instance i.
+__global__ void k_batch_flush(const FlushEntry* __restrict__ e, int n, int ns) {
+    const int i = blockIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kFlushNodes + threadIdx.x;
+    if (i0 >= e[i].nodes) return;
+    for (int s = 0; s < ns; ++s) flush_nodes(e[(size_t)s * n + i], i0, blockDim.x);
 }
 
 constexpr int kFixupBlocksPerInstance = 4;
@@ -1981,6 +1973,7 @@ struct ParticleBatchImpl {
     char* d_tables = nullptr;
     size_t table_bytes = 0;
     unsigned long long* h_flags = nullptr;
+    int64_t max_nodes = 0;  // nodes of the largest instance
 };
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -1990,6 +1983,7 @@ int batch_create(pic_ctx** cs, int n, ParticleBatchImpl** out) {
     *out = B;
     B->n = n;
     B->ns = cs[0]->cfg.num_species;
+    for (int i = 0; i < n; ++i) B->max_nodes = std::max<int64_t>(B->max_nodes, cs[i]->nodes);
     for (int sh = 0; sh < kNumTileShapes; ++sh) {
         std::vector<uint2> w;
         for (int i = 0; i < n; ++i) {
@@ -2110,7 +2104,8 @@ int batch_prepare(ParticleBatchImpl* B, pic_ctx** cs, cudaStream_t st) {
 int batch_deposit(ParticleBatchImpl* B, cudaStream_t st) {
     const int n = B->n, ns = B->ns;
     k_batch_zero<<<296, 256, 0, st>>>(B->d_zero + (size_t)ns * 5 * n, n);
-    k_batch_flush<<<296, 256, 0, st>>>(B->d_flush, ns * n);
+    const dim3 fg(grid1d(B->max_nodes, 256 * kFlushNodes), (unsigned)n);
+    k_batch_flush<<<fg, 256, 0, st>>>(B->d_flush, n, ns);
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
 }
