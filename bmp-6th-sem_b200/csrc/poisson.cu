@@ -1310,21 +1310,41 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             }
             grid.sync();
         };
-        for (int l = 0; l < maxkf; ++l) {
+        // the first black sweep fused with the zero start (mode 0) or with
+        // the coarse correction (mode 1): each black node computes its red
+        // neighbours' values itself (as k_mg_init_black / k_mg_prolong_black)
+        auto first_black = [&](int l, int mode) {
             if (on && l < I->kf) {
                 const LevelDev& L = I->lev[l];
-                float* __restrict__ lx = L.x;
-                const float* __restrict__ lb = L.b;
-                const uint8_t* __restrict__ lm = L.mask;
-                const int nn = L.GX * L.GY;
-#pragma unroll 4
-                for (int k = (int)ltid; k < nn; k += (int)lsize) {
-                    const int j = k / L.GX, x = k - j * L.GX;
-                    lx[k] = (((x + j) & 1) == 0 && !lm[k]) ? lb[k] / L.cd : 0.0f;
+                const LevelDev& C = I->lev[l + 1];
+                const int hw = (L.GX + 1) >> 1, n = hw * L.GY, ls = (int)lsize, nl = L.GX * L.GY;
+                for (int h = (int)ltid; h < n; h += ls) {
+                    const int j = h / hw;
+                    const int x = 2 * (h - j * hw) + ((j + 1) & 1);
+                    if (x >= L.GX) continue;
+                    const int k = j * L.GX + x;
+                    if (L.mask[k]) continue;
+                    float w, e, d, u;
+                    if (mode == 0) {
+                        auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] / L.cd; };
+                        w = xr(k - 1);
+                        e = xr(k + 1);
+                        d = xr(row_dn(k, nl, L.GX));
+                        u = xr(row_up(k, nl, L.GX));
+                    } else {
+                        const int jd = j == 0 ? L.GY - 1 : j - 1, ju = j + 1 == L.GY ? 0 : j + 1;
+                        w = prolonged(L, C, x - 1, j);
+                        e = prolonged(L, C, x + 1, j);
+                        d = prolonged(L, C, x, jd);
+                        u = prolonged(L, C, x, ju);
+                    }
+                    L.x[k] = __fmaf_rn(L.cx, w + e, __fmaf_rn(L.cy, d + u, L.b[k])) / L.cd;
                 }
             }
             grid.sync();
-            half_sweep(l, 1);
+        };
+        for (int l = 0; l < maxkf; ++l) {
+            first_black(l, 0);
             for (int s = 1; s < kNu; ++s) {
                 half_sweep(l, 0);
                 half_sweep(l, 1);
@@ -1354,30 +1374,9 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
         if (on && first) fused_body(*I->fused, smem);
         grid.sync();
         for (int l = maxkf - 1; l >= 0; --l) {
-            if (on && l < I->kf) {
-                const LevelDev& F = I->lev[l];
-                const LevelDev& C = I->lev[l + 1];
-                const int nf = F.GX * F.GY;
-                float* __restrict__ fx = F.x;
-                const float* __restrict__ cxv = C.x;
-#pragma unroll 4
-                for (int k = (int)ltid; k < nf; k += (int)lsize) {
-                    if (F.mask[k]) continue;
-                    const int j = k / F.GX, x = k - j * F.GX;
-                    const int cI = x >> 1, cJ = j >> 1;
-                    const int cJ1 = cJ + 1 == C.GY ? 0 : cJ + 1;  // wraps only periodic in y
-                    const bool ox = x & 1, oy = j & 1;
-                    auto X = [&](int a, int b) { return cxv[b * C.GX + a]; };
-                    float v;
-                    if (!ox && !oy) v = X(cI, cJ);
-                    else if (ox && !oy) v = 0.5f * (X(cI, cJ) + X(cI + 1, cJ));
-                    else if (!ox && oy) v = 0.5f * (X(cI, cJ) + X(cI, cJ1));
-                    else v = 0.25f * (X(cI, cJ) + X(cI + 1, cJ) + X(cI, cJ1) + X(cI + 1, cJ1));
-                    fx[k] += v;
-                }
-            }
-            grid.sync();
-            for (int s = 0; s < kNu; ++s) {
+            first_black(l, 1);
+            half_sweep(l, 0);
+            for (int s = 1; s < kNu; ++s) {
                 half_sweep(l, 1);
                 half_sweep(l, 0);
             }
