@@ -916,7 +916,12 @@ int poisson_setup(pic_ctx* c) {
     static_assert(sizeof(FusedLevels) <= sizeof(ps.fused_desc), "fused level table");
     std::memcpy(ps.fused_desc, &F, sizeof(F));
     ps.fused_smem = off;
-    PIC_CUDA(cudaFuncSetAttribute(k_mg_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
+    // the attribute belongs to the kernel, shared by every context of the
+    // process: it only ever grows, so contexts created earlier keep working
+    cudaFuncAttributes fa{};
+    PIC_CUDA(cudaFuncGetAttributes(&fa, k_mg_fused));
+    if ((int)off > fa.maxDynamicSharedSizeBytes)
+        PIC_CUDA(cudaFuncSetAttribute(k_mg_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
     PIC_CUDA(cudaStreamCreateWithFlags(&ps.cap_stream, cudaStreamNonBlocking));
     return PIC_OK;
 }
@@ -1574,7 +1579,10 @@ int poisson_batch_launch(const void* dev_insts, int n, const int* inst_of, doubl
 }
 
 int poisson_batch_blocks(size_t smem, int* blocks) {
-    PIC_CUDA(cudaFuncSetAttribute(k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaFuncAttributes fa{};  // (grows only: other ensembles may be alive)
+    PIC_CUDA(cudaFuncGetAttributes(&fa, k_poisson_batch));
+    if ((int)smem > fa.maxDynamicSharedSizeBytes)
+        PIC_CUDA(cudaFuncSetAttribute(k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, dev = 0, sms = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_poisson_batch, kFusedThreads, smem));
     PIC_CUDA(cudaGetDevice(&dev));

@@ -120,3 +120,26 @@ def test_warm_start_cuts_iterations():
         pic.poisson_solve(1)          # same rho again from the previous phi
         warm = pic.poisson_stats()[0]
     assert warm < cold
+
+
+def test_contexts_of_different_sizes_alive_together(oracle):
+    """A context keeps solving after a smaller one is created: the coarse-level
+    kernel's shared-memory size is a property of the kernel, shared by every
+    context of the process, and must cover the largest of them."""
+    import pic_b200 as P
+    import pic_configs as C
+    out = []
+    with P.Pic(P.make_config(250, 250, 1.0, 1.0, 1e-9, [(-1.6e-19, 9.1e-31, 1.0, 1.0)],
+                             C.wall_rects(250, 250, left=5.0))) as big:
+        with P.Pic(P.make_config(40, 40, 1.0, 1.0, 1e-9, [(-1.6e-19, 9.1e-31, 1.0, 1.0)],
+                                 C.wall_rects(40, 40, left=5.0))) as small:
+            for pic, n in ((big, 250), (small, 40)):
+                rho = np.random.default_rng(n).normal(size=(n + 1) ** 2)
+                pic.set_rho(rho)
+                pic.poisson_solve(0)
+                it, rel, _ = pic.poisson_stats()
+                GX = n + 1
+                mask = oracle.electrode_mask(GX, GX, oracle.Electrodes(C.wall_rects(n, n, left=5.0)))
+                out.append((rel, oracle.reduced_relres(GX, GX, 1.0 / n, 1.0 / n, mask, pic.rho(), pic.phi())))
+    for rel, rel_o in out:
+        assert rel <= 1e-8 and rel_o <= 1e-8
