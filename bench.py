@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-instance batched ensemble measurement")
     ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--tile-shape", type=int, default=None, choices=[0, 1, 2, 3],
+                    help="particle-kernel tile shape (0 64x4, 1 256x1, 2 128x2, 3 16x16); "
+                         "default: the library's tuner picks it (under a profiler, fix it: "
+                         "the tuner's timings change there)")
     return ap.parse_args()
 
 
@@ -289,7 +293,11 @@ def run_ours(args, rank, world, local_rank):
     it = 0
     # the library's tuner picks the particle kernels' tile shape for this
     # workload (it times the push on the loaded particles without keeping it)
-    tile_shape, tile_ms = pic.autotune(timings=True)
+    if args.tile_shape is None:
+        tile_shape, tile_ms = pic.autotune(timings=True)
+    else:
+        tile_shape, tile_ms = args.tile_shape, None
+        pic.set_tile_shape(tile_shape)
     for _ in range(args.warmup):
         pic.step(it)
         it += 1
