@@ -23,9 +23,13 @@
 // bf16 with FP32 master copies and Adam moments.  The 32->32 convolutions
 // (forward, data gradient, weight gradient) are implicit GEMMs on the tensor
 // cores with mma.sync.m16n8k16 bf16 x bf16 -> fp32 (K = 9 taps x 32
-// channels); the 3->32 input and 32->1 output convolutions are small and run
-// on the FP32 cores.  Weight gradients are reduced through per-block
-// partials in a fixed order, so training is deterministic.
+// channels); in the forward pass the 3->32 input and 32->1 output
+// convolutions are tensor-core GEMMs too (K = 12 taps x 4 channels, and N = 8
+// of which one column is used), their bf16 weights prepacked as B fragments;
+// their gradients run on the FP32 cores.  The forward pass fuses the pools
+// and the decoder's upsample-and-skip sums into the 32->32 convolutions.
+// Weight gradients are reduced through per-block partials in a fixed order,
+// so training is deterministic.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -73,19 +77,78 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// Load a (TH+2) x (TW+2) x 32 halo tile of an NHWC bf16 image into shared
-// memory ([row][col][CP]); pixels outside the image read as zero.
-__device__ __forceinline__ void load_halo(__nv_bfloat16* dst, const __nv_bfloat16* src, int P,
-                                          int y0, int x0) {
+// x += c for 8 bf16 channels, each sum rounded to bf16
+__device__ __forceinline__ void add_bf16x8(uint4& x, const uint4& c) {
+    __nv_bfloat162* px = reinterpret_cast<__nv_bfloat162*>(&x);
+    const __nv_bfloat162* pc = reinterpret_cast<const __nv_bfloat162*>(&c);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float2 a = __bfloat1622float2(pc[e]), b = __bfloat1622float2(px[e]);
+        px[e] = __floats2bfloat162_rn(a.x + b.x, a.y + b.y);
+    }
+}
+
+// Asynchronous global -> shared copies; with valid == false the destination
+// is zero-filled and nothing is read.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Start the copy of a (TH+2) x (TW+2) x 32 halo tile of an NHWC bf16 image
+// into shared memory ([row][col][CP]); pixels outside the image read as zero.
+__device__ __forceinline__ void load_halo_async(__nv_bfloat16* dst, const __nv_bfloat16* src, int P,
+                                                int y0, int x0) {
     constexpr int kChunks = (TH + 2) * (TW + 2) * (C / 8);  // 16-byte chunks
     for (int i = threadIdx.x; i < kChunks; i += blockDim.x) {
         const int q = i & 3, pix = i >> 2;
         const int r = pix / (TW + 2), col = pix % (TW + 2);
         const int y = y0 + r - 1, x = x0 + col - 1;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (y >= 0 && x >= 0 && y < P && x < P)
-            v = *reinterpret_cast<const uint4*>(src + ((int64_t)y * P + x) * C + q * 8);
-        *reinterpret_cast<uint4*>(dst + (r * (TW + 2) + col) * CP + q * 8) = v;
+        const bool in = y >= 0 && x >= 0 && y < P && x < P;
+        cp_async16(dst + pix * CP + q * 8, in ? src + ((int64_t)y * P + x) * C + q * 8 : src, in);
+    }
+}
+
+// The half-size image under a halo tile: rows y0/2-1 .. y0/2+TH/2 and columns
+// x0/2-1 .. x0/2+TW/2 (y0, x0 even), [row][col][CP] in shared memory.
+constexpr int kUpRows = TH / 2 + 2, kUpCols = TW / 2 + 2;
+
+__device__ __forceinline__ void load_up_async(__nv_bfloat16* dst, const __nv_bfloat16* up, int P,
+                                              int y0, int x0) {
+    const int Q = P / 2, Y0 = y0 / 2 - 1, X0 = x0 / 2 - 1;
+    for (int i = threadIdx.x; i < kUpRows * kUpCols * (C / 8); i += blockDim.x) {
+        const int q = i & 3, pix = i >> 2;
+        const int Y = Y0 + pix / kUpCols, X = X0 + pix % kUpCols;
+        const bool in = Y >= 0 && X >= 0 && Y < Q && X < Q;
+        cp_async16(dst + pix * CP + q * 8, in ? up + ((int64_t)Y * Q + X) * C + q * 8 : up, in);
+    }
+}
+
+// Once both tiles have landed: the halo tile's in-image pixels become
+// up2(up) + tile (each sum rounded to bf16); the tile's interior sums are also
+// written to u_out when given.
+__device__ __forceinline__ void add_up(__nv_bfloat16* in_s, const __nv_bfloat16* up_s, int P, int y0,
+                                       int x0, __nv_bfloat16* u_out) {
+    constexpr int kChunks = (TH + 2) * (TW + 2) * (C / 8);
+    const int Y0 = y0 / 2 - 1, X0 = x0 / 2 - 1;
+    for (int i = threadIdx.x; i < kChunks; i += blockDim.x) {
+        const int q = i & 3, pix = i >> 2;
+        const int r = pix / (TW + 2), col = pix % (TW + 2);
+        const int y = y0 + r - 1, x = x0 + col - 1;
+        if (y < 0 || x < 0 || y >= P || x >= P) continue;
+        uint4* d = reinterpret_cast<uint4*>(in_s + pix * CP + q * 8);
+        uint4 v = *d;
+        add_bf16x8(v, *reinterpret_cast<const uint4*>(up_s + (((y >> 1) - Y0) * kUpCols + (x >> 1) - X0) * CP + q * 8));
+        *d = v;
+        if (u_out && r >= 1 && r <= TH && col >= 1 && col <= TW)
+            *reinterpret_cast<uint4*>(u_out + ((int64_t)y * P + x) * C + q * 8) = v;
     }
 }
 
@@ -93,8 +156,10 @@ __device__ __forceinline__ void load_halo(__nv_bfloat16* dst, const __nv_bfloat1
 // 32 -> 32 3x3 convolution (forward, or data gradient with transformed
 // weights).  Weights in global memory as [tap][n][k] bf16 (n = output
 // channel, k = input channel).  Epilogue: out = act(acc + bias), where act is
-// relu (forward) or a gate (out *= gate[p] > 0, data gradient); an optional
-// bf16 image is added before the gate.
+// relu (forward) or a gate (out *= gate[p] > 0, data gradient).  Forward
+// options fused into the same pass: the input may be up2(up) + in (the
+// decoder's upsample-and-skip, its sum kept in u_out for training), and the
+// output's 2x2 average pool may be written to pool_out.
 // ---------------------------------------------------------------------------
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -102,24 +167,34 @@ struct ConvArgs {
     const float* bias;        // [32] or null
     const __nv_bfloat16* gate;  // [P][P][32] or null: multiply by (gate > 0)
     __nv_bfloat16* out;
+    const __nv_bfloat16* up;  // [P/2][P/2][32] or null: input is up2(up) + in
+    __nv_bfloat16* u_out;     // [P][P][32] or null: that input sum
+    __nv_bfloat16* pool_out;  // [P/2][P/2][32] or null: avgpool2 of the output
     int P;
     int relu;
 };
 
 constexpr int kConvSmem = ((TH + 2) * (TW + 2) * CP + 9 * C * CP) * 2;
+constexpr int kConvSmemUp = kConvSmem + kUpRows * kUpCols * CP * 2;  // with the half-size tile
 
 __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* in_s = reinterpret_cast<__nv_bfloat16*>(smem);
     __nv_bfloat16* w_s = in_s + (TH + 2) * (TW + 2) * CP;
     const int y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
-    load_halo(in_s, A.in, A.P, y0, x0);
+    __nv_bfloat16* up_s = w_s + 9 * C * CP;  // with A.up only
+    load_halo_async(in_s, A.in, A.P, y0, x0);
+    if (A.up) load_up_async(up_s, A.up, A.P, y0, x0);
     for (int i = threadIdx.x; i < 9 * C * (C / 8); i += blockDim.x) {
         const int q = i & 3, row = i >> 2;  // row = tap*32 + n
-        *reinterpret_cast<uint4*>(w_s + row * CP + q * 8) =
-            *reinterpret_cast<const uint4*>(A.w + row * C + q * 8);
+        cp_async16(w_s + row * CP + q * 8, A.w + row * C + q * 8, true);
     }
+    cp_async_wait_all();
     __syncthreads();
+    if (A.up) {
+        add_up(in_s, up_s, A.P, y0, x0, A.u_out);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // warp = output row in the tile
     float acc[2][4][4];
 #pragma unroll
@@ -200,6 +275,31 @@ __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
         }
         *reinterpret_cast<uint4*>(A.out + go) = v;
     }
+    if (A.pool_out) {
+        // 2x2 averages of the tile (y0, x0 even): (TH/2) x (TW/2) pixels x 4 chunks
+        const int Q = A.P / 2;
+        for (int i = threadIdx.x; i < (TH / 2) * (TW / 2) * (C / 8); i += blockDim.x) {
+            const int q = i & 3, pp = i >> 2;
+            const int py = pp / (TW / 2), px = pp % (TW / 2);
+            const int Y = y0 / 2 + py, X = x0 / 2 + px;
+            if (Y >= Q || X >= Q) continue;
+            const __nv_bfloat16* s00 = o_s + (2 * py * TW + 2 * px) * CP + q * 8;
+            uint4 c4[4] = {*reinterpret_cast<const uint4*>(s00), *reinterpret_cast<const uint4*>(s00 + CP),
+                           *reinterpret_cast<const uint4*>(s00 + TW * CP),
+                           *reinterpret_cast<const uint4*>(s00 + (TW + 1) * CP)};
+            uint4 o;
+            __nv_bfloat162* po = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float2 f0 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[0])[e]);
+                const float2 f1 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[1])[e]);
+                const float2 f2 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[2])[e]);
+                const float2 f3 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[3])[e]);
+                po[e] = __floats2bfloat162_rn(0.25f * (f0.x + f1.x + f2.x + f3.x), 0.25f * (f0.y + f1.y + f2.y + f3.y));
+            }
+            *reinterpret_cast<uint4*>(A.pool_out + ((int64_t)Y * Q + X) * C + q * 8) = o;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -229,14 +329,14 @@ __global__ void __launch_bounds__(256) k_wgrad32(const __nv_bfloat16* X, const _
     for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
         const int y0 = (tile / tiles_x) * TH, x0 = (tile % tiles_x) * TW;
         __syncthreads();
-        load_halo(x_s, X, P, y0, x0);
+        load_halo_async(x_s, X, P, y0, x0);
         for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
             const int q = i & 3, pix = i >> 2;
             const int y = y0 + pix / TW, x = x0 + pix % TW;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (y < P && x < P) v = *reinterpret_cast<const uint4*>(dY + ((int64_t)y * P + x) * C + q * 8);
-            *reinterpret_cast<uint4*>(d_s + pix * CP + q * 8) = v;
+            const bool in = y < P && x < P;
+            cp_async16(d_s + pix * CP + q * 8, in ? dY + ((int64_t)y * P + x) * C + q * 8 : dY, in);
         }
+        cp_async_wait_all();
         __syncthreads();
         if (threadIdx.x < C) {
             float s = 0.f;
@@ -306,60 +406,128 @@ __global__ void k_sum_partials(const float* partial, int nblocks, int n, float* 
 }
 
 // ---------------------------------------------------------------------------
-// FP32-core layers: input conv 3->32, output conv 32->1
+// Input conv 3->32, output conv 32->1
 // ---------------------------------------------------------------------------
-// x0 layout: [P][P][4] bf16 (channel 3 unused).  w_in: [tap][ci(3)][co(32)] fp32.
-__global__ void k_conv_in(const __nv_bfloat16* x0, const float* w, const float* bias, int P,
-                          __nv_bfloat16* out) {
-    __shared__ float ws[9 * 3 * C + C];
-    for (int i = threadIdx.x; i < 9 * 3 * C; i += blockDim.x) ws[i] = w[i];
-    if (threadIdx.x < C) ws[9 * 3 * C + threadIdx.x] = bias[threadIdx.x];
+// Both are implicit GEMMs on the tensor cores over TH x TW output tiles (warp
+// = tile row, two m16 tiles of pixels), with the input tile and its halo
+// staged in shared memory and the weights as bf16 B fragments prepacked per
+// lane by k_pack_frags (FP32 accumulation).
+//
+// Input: x0 is [P][P][4] bf16 (channel 3 zero); K index = tap*4 + ci over 12
+// taps (taps 9..11 zero), three k16 steps; N = 32 output channels.
+// out = relu(b + sum_K W[K][:] x0[p+tap][ci]), stored through a shared-memory
+// stage so that the 64-byte pixels leave in 16-byte chunks.
+constexpr int kInSteps = 3, kOutSteps = 18;  // k16 steps of the two GEMMs
+
+__global__ void __launch_bounds__(256) k_conv_in(const __nv_bfloat16* x0, const uint2* wfrag,
+                                                 const float* bias, int P, __nv_bfloat16* out) {
+    __shared__ __align__(16) uint2 xs[(TH + 2) * (TW + 2)];
+    __shared__ __align__(16) __nv_bfloat16 os[TH * TW * CP];
+    const int y0 = blockIdx.y * TH, x0p = blockIdx.x * TW;
+    for (int i = threadIdx.x; i < (TH + 2) * (TW + 2); i += blockDim.x) {
+        const int y = y0 + i / (TW + 2) - 1, x = x0p + i % (TW + 2) - 1;
+        const bool in = y >= 0 && x >= 0 && y < P && x < P;
+        cp_async8(xs + i, in ? x0 + ((int64_t)y * P + x) * 4 : x0, in);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    uint2 b[kInSteps][4];
+#pragma unroll
+    for (int s = 0; s < kInSteps; ++s)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) b[s][n] = wfrag[(s * 4 + n) * 32 + lane];
+    cp_async_wait_all();
     __syncthreads();
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (int64_t)P * P) return;
-    const int y = (int)(p / P), x = (int)(p % P);
-    float acc[C];
+    const uint32_t* xw = reinterpret_cast<const uint32_t*>(xs);
+    float acc[2][4][4];
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[c] = ws[9 * 3 * C + c];
-    for (int tap = 0; tap < 9; ++tap) {
-        const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
-        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
-        const __nv_bfloat16* src = x0 + ((int64_t)yy * P + xx) * 4;
+    for (int m = 0; m < 2; ++m)
 #pragma unroll
-        for (int ci = 0; ci < 3; ++ci) {
-            const float v = __bfloat162float(src[ci]);
+        for (int n = 0; n < 4; ++n)
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[c] = fmaf(ws[(tap * 3 + ci) * C + c], v, acc[c]);
+            for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
+#pragma unroll
+    for (int s = 0; s < kInSteps; ++s) {
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            uint32_t a[4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {  // k offset 0 / 8 of the step
+                const int tap = 4 * s + 2 * h + (t >> 1);
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {  // pixel row g / g + 8 of the m tile
+                    const int px = m * 16 + g + 8 * r;
+                    a[h * 2 + r] = tap < 9 ? xw[2 * ((warp + tap / 3) * (TW + 2) + px + tap % 3) + (t & 1)] : 0u;
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < 4; ++n) mma_bf16(acc[m][n], a[0], a[1], a[2], a[3], b[s][n].x, b[s][n].y);
         }
     }
-    __nv_bfloat16* dst = out + p * C;
 #pragma unroll
-    for (int c = 0; c < C; c += 2)
-        *reinterpret_cast<__nv_bfloat162*>(dst + c) = __floats2bfloat162_rn(fmaxf(acc[c], 0.f), fmaxf(acc[c + 1], 0.f));
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int px = m * 16 + g + 8 * r, ch = n * 8 + 2 * t;
+                const float v0 = fmaxf(acc[m][n][2 * r] + bias[ch], 0.f);
+                const float v1 = fmaxf(acc[m][n][2 * r + 1] + bias[ch + 1], 0.f);
+                *reinterpret_cast<__nv_bfloat162*>(os + (warp * TW + px) * CP + ch) = __floats2bfloat162_rn(v0, v1);
+            }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
+        const int q = i & 3, pix = i >> 2;
+        const int y = y0 + pix / TW, x = x0p + pix % TW;
+        if (y >= P || x >= P) continue;
+        *reinterpret_cast<uint4*>(out + ((int64_t)y * P + x) * C + q * 8) =
+            *reinterpret_cast<const uint4*>(os + pix * CP + q * 8);
+    }
 }
 
-// out[p] = b + sum_tap sum_ci w[tap][ci] a[p+tap][ci]   (w_out: [tap][ci] fp32)
-__global__ void k_conv_out(const __nv_bfloat16* a, const float* w, const float* bias, int P,
-                           float* out) {
-    __shared__ float ws[9 * C];
-    for (int i = threadIdx.x; i < 9 * C; i += blockDim.x) ws[i] = w[i];
+// Output: out[p] = b + sum_tap sum_ci w[tap][ci] a[p+tap][ci]; K = tap*32 + ci,
+// eighteen k16 steps; N = 8 with only column 0 non-zero (lanes t == 0 hold
+// the result).
+__global__ void __launch_bounds__(256) k_conv_out(const __nv_bfloat16* a, const uint2* wfrag,
+                                                  const float* bias, int P, float* out) {
+    __shared__ __align__(16) __nv_bfloat16 in_s[(TH + 2) * (TW + 2) * CP];
+    const int y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
+    load_halo_async(in_s, a, P, y0, x0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    cp_async_wait_all();
     __syncthreads();
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (int64_t)P * P) return;
-    const int y = (int)(p / P), x = (int)(p % P);
-    float s = bias[0];
-    for (int tap = 0; tap < 9; ++tap) {
-        const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
-        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
-        const __nv_bfloat162* src = reinterpret_cast<const __nv_bfloat162*>(a + ((int64_t)yy * P + xx) * C);
+    float acc[2][4];
 #pragma unroll
-        for (int c = 0; c < C / 2; ++c) {
-            const float2 v = __bfloat1622float2(src[c]);
-            s = fmaf(ws[tap * C + 2 * c], v.x, s);
-            s = fmaf(ws[tap * C + 2 * c + 1], v.y, s);
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[m][e] = 0.f;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+            const uint2 b = wfrag[(tap * 2 + kc) * 32 + lane];
+#pragma unroll
+            for (int m = 0; m < 2; ++m) {
+                uint32_t f[4];
+                const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
+                const int koff = (lane >> 4) * 8;
+                ldsm_x4(smem_u32(in_s + ((warp + dy) * (TW + 2) + m * 16 + r + dx) * CP + kc * 16 + koff),
+                        f[0], f[1], f[2], f[3]);
+                mma_bf16(acc[m], f[0], f[1], f[2], f[3], b.x, b.y);
+            }
         }
     }
-    out[p] = s;
+    if ((lane & 3) == 0) {
+        const int g = lane >> 2, y = y0 + warp;
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int x = x0 + m * 16 + g + 8 * r;
+                if (y < P && x < P) out[(int64_t)y * P + x] = acc[m][2 * r] + bias[0];
+            }
+    }
 }
 
 // dA[p][ci] = (sum_tap w[tap][ci] dout[p - tap]) gated by (a[p][ci] > 0)
@@ -491,29 +659,6 @@ __global__ void __launch_bounds__(256) k_wgrad_out(const __nv_bfloat16* a, const
 // ---------------------------------------------------------------------------
 // Pooling, upsampling, gates
 // ---------------------------------------------------------------------------
-__global__ void k_pool(const __nv_bfloat16* in, int P, __nv_bfloat16* out) {  // P = input size
-    const int Q = P / 2;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)Q * Q * C) return;
-    const int c = (int)(i % C);
-    const int64_t q = i / C;
-    const int Y = (int)(q / Q), X = (int)(q % Q);
-    auto at = [&](int y, int x) { return __bfloat162float(in[((int64_t)y * P + x) * C + c]); };
-    out[i] = __float2bfloat16_rn(0.25f * (at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1) + at(2 * Y + 1, 2 * X) + at(2 * Y + 1, 2 * X + 1)));
-}
-
-// u = up2(coarse) + skip   (P = fine size)
-__global__ void k_up_add(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, int P,
-                         __nv_bfloat16* out) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)P * P * C) return;
-    const int c = (int)(i % C);
-    const int64_t p = i / C;
-    const int y = (int)(p / P), x = (int)(p % P), Q = P / 2;
-    const float v = __bfloat162float(coarse[((int64_t)(y / 2) * Q + x / 2) * C + c]) + __bfloat162float(skip[i]);
-    out[i] = __float2bfloat16_rn(v);
-}
-
 // dcoarse[Y][X] = sum of the 2x2 fine gradients, gated by (act > 0)
 __global__ void k_down_sum_gate(const __nv_bfloat16* dfine, const __nv_bfloat16* act, int P,
                                 __nv_bfloat16* dcoarse) {
@@ -720,6 +865,9 @@ struct Net {
     // their data-gradient transposes
     __nv_bfloat16* w16 = nullptr;
     __nv_bfloat16* w16t = nullptr;
+    // bf16 B fragments of the input and output convolutions (k_pack_frags)
+    uint2* in_frag = nullptr;
+    uint2* out_frag = nullptr;
     // activations (P = fine, Q = P/2, R = P/4)
     __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
     float* out = nullptr;
@@ -755,7 +903,7 @@ static int64_t param_off(int block) {
 
 static void net_free(Net& N) {
     cudaFree(N.w); cudaFree(N.m); cudaFree(N.v); cudaFree(N.g);
-    cudaFree(N.w16); cudaFree(N.w16t);
+    cudaFree(N.w16); cudaFree(N.w16t); cudaFree(N.in_frag); cudaFree(N.out_frag);
     cudaFree(N.x0);
     for (auto* p : N.a) cudaFree(p);
     cudaFree(N.p1); cudaFree(N.p2); cudaFree(N.u0); cudaFree(N.u1); cudaFree(N.out);
@@ -812,6 +960,8 @@ static int ws_alloc(pic_ctx* c) {
     if (cudaMalloc(&N.w, kParams * 4) || cudaMalloc(&N.m, kParams * 4) ||
         cudaMalloc(&N.v, kParams * 4) || cudaMalloc(&N.g, kParams * 4) ||
         balloc(&N.w16, (int64_t)kNumConv32 * kW32) || balloc(&N.w16t, (int64_t)kNumConv32 * kW32) ||
+        cudaMalloc(&N.in_frag, kInSteps * 4 * 32 * sizeof(uint2)) ||
+        cudaMalloc(&N.out_frag, kOutSteps * 32 * sizeof(uint2)) ||
         balloc(&N.x0, P * P * 4))
         return fail(PIC_ERR_CUDA, "warm start: parameter allocation failed");
     const int64_t sizes[11] = {P, P, Q, Q, R, R, Q, Q, P, P, 0};  // a1..a10 at index 1..10
@@ -841,7 +991,7 @@ static int ws_alloc(pic_ctx* c) {
     PIC_CUDA(cudaMemcpy(N.w, w.data(), kParams * 4, cudaMemcpyHostToDevice));
     PIC_CUDA(cudaMemset(N.m, 0, kParams * 4));
     PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
-    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemUp));
     PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
     return PIC_OK;
 }
@@ -857,6 +1007,36 @@ __global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16, _
     w16t[i] = __float2bfloat16_rn(w[l * stride + ((8 - tap) * C + n) * C + k]);
 }
 
+// B fragments (m16n8k16, per lane: {k 2t, 2t+1 | k 2t+8, 2t+9} of column g)
+// of the input and output convolutions, from the FP32 masters.
+//   input  [step s][n tile][lane]: B[K][co] = w_in[tap][ci][co], K = 16s + k =
+//          tap*4 + ci, zero for ci == 3 or tap >= 9;
+//   output [step j = tap*2 + kc][lane]: B[K][0] = w_out[tap][kc*16 + k], other
+//          columns zero.
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__global__ void k_pack_frags(const float* w_in, const float* w_out, uint2* in_frag, uint2* out_frag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = i & 31, g = lane >> 2, t = lane & 3;
+    if (i < kInSteps * 4 * 32) {
+        const int s = i / 128, n = (i / 32) % 4, co = n * 8 + g;
+        auto w = [&](int k) {
+            const int K = 16 * s + k, tap = K / 4, ci = K % 4;
+            return (ci < 3 && tap < 9) ? w_in[(tap * 3 + ci) * C + co] : 0.f;
+        };
+        in_frag[i] = make_uint2(pack_bf16x2(w(2 * t), w(2 * t + 1)), pack_bf16x2(w(2 * t + 8), w(2 * t + 9)));
+    } else if (i < kInSteps * 4 * 32 + kOutSteps * 32) {
+        const int j = (i - kInSteps * 4 * 32) / 32, tap = j / 2, kc = j % 2;
+        const float* wt = w_out + tap * C + kc * 16;
+        out_frag[j * 32 + lane] = g == 0 ? make_uint2(pack_bf16x2(wt[2 * t], wt[2 * t + 1]),
+                                                      pack_bf16x2(wt[2 * t + 8], wt[2 * t + 9]))
+                                         : make_uint2(0u, 0u);
+    }
+}
+
 // Refresh the bf16 working weights and their transposes from the masters
 // (only after the masters changed).
 static int ws_pack(pic_ctx* c) {
@@ -864,14 +1044,17 @@ static int ws_pack(pic_ctx* c) {
     if (N.packed) return PIC_OK;
     k_pack_w16<<<g1((int64_t)kNumConv32 * kW32), 256, 0, c->stream>>>(N.w + param_off(1), kW32 + kB32,
                                                                        N.w16, N.w16t);
-    c->launches += 1;
+    k_pack_frags<<<g1((kInSteps * 4 + kOutSteps) * 32), 256, 0, c->stream>>>(
+        N.w, N.w + param_off(kNumConv32 + 1), N.in_frag, N.out_frag);
+    c->launches += 2;
     PIC_CUDA(cudaGetLastError());
     N.packed = true;
     return PIC_OK;
 }
 
 static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
-                   bool transposed, const __nv_bfloat16* gate) {
+                   bool transposed, const __nv_bfloat16* gate, const __nv_bfloat16* up = nullptr,
+                   __nv_bfloat16* u_out = nullptr, __nv_bfloat16* pool_out = nullptr) {
     Net& N = c->ws->net;
     ConvArgs A;
     A.in = in;
@@ -879,10 +1062,13 @@ static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16
     A.bias = transposed ? nullptr : N.w + param_off(layer + 1) + kW32;
     A.gate = gate;
     A.out = out;
+    A.up = up;
+    A.u_out = u_out;
+    A.pool_out = pool_out;
     A.P = P;
     A.relu = transposed ? 0 : 1;
     const dim3 grid((P + TW - 1) / TW, (P + TH - 1) / TH);
-    k_conv32<<<grid, 256, kConvSmem, c->stream>>>(A);
+    k_conv32<<<grid, 256, up ? kConvSmemUp : kConvSmem, c->stream>>>(A);
 }
 
 // [tap][co][ci] (+ bias) -> the parameter layout [tap][ci][co] (+ bias)
@@ -905,27 +1091,27 @@ static void wgrad32(pic_ctx* c, int layer, const __nv_bfloat16* X, const __nv_bf
     k_scatter_wgrad<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.gsum, N.g + param_off(layer + 1));
 }
 
-// Forward pass on the image N.xin; result in N.out.
-static void forward(pic_ctx* c) {
+// Forward pass on the image N.xin; result in N.out.  Eleven launches: the
+// pools and the decoder's upsample-and-skip sums run inside the 32->32
+// convolutions.  `train` keeps the skip sums u0, u1 that the backward pass
+// needs.
+static void forward(pic_ctx* c, bool train) {
     Net& N = c->ws->net;
     const int P = N.P, Q = P / 2, R = P / 4;
-    k_conv_in<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.xin, N.w, N.w + kInW, P, N.a[1]);
-    conv32(c, 0, N.a[1], N.a[2], P, false, nullptr);
-    k_pool<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(N.a[2], P, N.p1);
+    const dim3 gP((P + TW - 1) / TW, (P + TH - 1) / TH);
+    k_conv_in<<<gP, 256, 0, c->stream>>>(N.xin, N.in_frag, N.w + kInW, P, N.a[1]);
+    conv32(c, 0, N.a[1], N.a[2], P, false, nullptr, nullptr, nullptr, N.p1);
     conv32(c, 1, N.p1, N.a[3], Q, false, nullptr);
-    conv32(c, 2, N.a[3], N.a[4], Q, false, nullptr);
-    k_pool<<<g1((int64_t)R * R * C), 256, 0, c->stream>>>(N.a[4], Q, N.p2);
+    conv32(c, 2, N.a[3], N.a[4], Q, false, nullptr, nullptr, nullptr, N.p2);
     conv32(c, 3, N.p2, N.a[5], R, false, nullptr);
     conv32(c, 4, N.a[5], N.a[6], R, false, nullptr);
-    k_up_add<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(N.a[6], N.a[4], Q, N.u1);
-    conv32(c, 5, N.u1, N.a[7], Q, false, nullptr);
+    conv32(c, 5, N.a[4], N.a[7], Q, false, nullptr, N.a[6], train ? N.u1 : nullptr);
     conv32(c, 6, N.a[7], N.a[8], Q, false, nullptr);
-    k_up_add<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(N.a[8], N.a[2], P, N.u0);
-    conv32(c, 7, N.u0, N.a[9], P, false, nullptr);
+    conv32(c, 7, N.a[2], N.a[9], P, false, nullptr, N.a[8], train ? N.u0 : nullptr);
     conv32(c, 8, N.a[9], N.a[10], P, false, nullptr);
     const int64_t ob = param_off(kNumConv32 + 1);
-    k_conv_out<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.a[10], N.w + ob, N.w + ob + kOutW, P, N.out);
-    c->launches += 18;
+    k_conv_out<<<gP, 256, 0, c->stream>>>(N.a[10], N.out_frag, N.w + ob + kOutW, P, N.out);
+    c->launches += 11;
 }
 
 // Loss of the guess N.out against the scaled right-hand-side change rhs
@@ -1016,7 +1202,7 @@ int ws_before_solve(pic_ctx* c, bool want_guess) {
         k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
             N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1, N.x0);
         N.xin = N.x0;
-        forward(c);
+        forward(c, false);
         if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)n * 4));
         k_make_guess<<<g1(n), 256, 0, c->stream>>>(N.phi_prev, N.out, c->mask, N.GX, N.GY, N.P, N.s2,
                                                    c->ps.net_guess);
@@ -1144,7 +1330,7 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
         for (int64_t s = 0; s < N.n_pairs; ++s) {
             PIC_TRY(ws_pack(c));
             N.xin = N.ds_x + s * (int64_t)P * P * 4;
-            forward(c);
+            forward(c, true);
             enqueue_loss(c, N.ds_t + s * c->nodes, N.loss_acc + s);
             backward(c);
             N.adam_t += 1;
@@ -1217,7 +1403,7 @@ int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* rhs_host, f
     PIC_CUDA(cudaMemcpy(t, rhs_host, (size_t)c->nodes * 4, cudaMemcpyHostToDevice));
     PIC_TRY(ws_pack(c));
     N.xin = N.x0;
-    forward(c);
+    forward(c, true);
     enqueue_loss(c, t, l);
     backward(c);
     float lh = 0.f;
