@@ -77,6 +77,11 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 // x += c for 8 bf16 channels, each sum rounded to bf16
 __device__ __forceinline__ void add_bf16x8(uint4& x, const uint4& c) {
     __nv_bfloat162* px = reinterpret_cast<__nv_bfloat162*>(&x);
@@ -101,6 +106,10 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// every committed group but the newest N has landed
+template <int N>
+__device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Start the copy of a (TH+2) x (TW+2) x 32 halo tile of an NHWC bf16 image
 // into shared memory ([row][col][CP]); pixels outside the image read as zero.
@@ -300,6 +309,320 @@ __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
             *reinterpret_cast<uint4*>(A.pool_out + ((int64_t)Y * Q + X) * C + q * 8) = o;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// 32 -> 32 3x3 convolution, forward pass, on the fifth-generation tensor
+// cores (tcgen05), warp-specialised and persistent (one CTA per SM).
+// Work unit: output rows y0, y0 + 1 (y0 even) x kTcW pixels from x0.  Per row
+// and k16 step one tcgen05.mma (M = 128 pixels, N = 32 channels, K = 16),
+// both operands in shared memory in the no-swizzle K-major layout:
+//   A: the unit's 4-row halo tile as [chunk q of 8 channels][row][pixel], 16
+//      bytes a pixel, so the A tile of tap (dy, dx) for row r starts at halo
+//      row r + dy, pixel dx; 8-pixel groups 128 bytes apart (SBO), the two
+//      chunk planes of a k16 step kTcPlane apart (LBO);
+//   B: the weights as [tap][chunk][n][8]: SBO 128 bytes (eight n), LBO 512.
+// Roles (warps):
+//   0-2  producers: copy unit k's halo into ring stage k % kTcStages with
+//        cp.async, then wait for the copies of unit k - kTcLag, fence them to
+//        the async proxy and arrive on that stage's `full` barrier;
+//   3    MMA: waits `full[s]` and `acc_empty[a]`, issues the 36 MMAs into
+//        TMEM accumulator a (64 columns: row r in 32r .. 32r+31) and commits
+//        them to `empty[s]` and `acc_full[a]`;
+//   4-11 epilogue, a warpgroup a row (TMEM lanes 32(w%4)..): tcgen05.ld of
+//        its 32 pixels, releases the accumulator, adds the bias, relu, bf16
+//        into a double-buffered shared stage; after a named barrier of the
+//        two warpgroups, 16-byte stores of both rows and the 2x2 average pool
+//        read from the stage.
+// Every wait is bounded (about a second): a role that gives up records
+// g_ws_fault and all roles leave their loops.
+// ---------------------------------------------------------------------------
+constexpr int kTcW = 128;                                // pixels of a unit row
+constexpr int kTcRows = 4;                               // halo rows
+constexpr int kTcPix = kTcW + 2;                         // halo pixels a row
+constexpr int kTcPlane = kTcRows * kTcPix * 16 + 32;     // bytes a chunk plane (+32: bank offset)
+constexpr int kTcHalo = 4 * kTcPlane;
+constexpr int kTcW16 = 9 * 4 * 32 * 16;                  // weight bytes
+constexpr int kTcStages = 3;
+constexpr int kTcLag = 1;                                // units in flight behind the one handed over
+// Accumulation chains a row: the taps split into kTcHalves partial sums
+// (taps 0-4 and 5-8 when 2), so that 2 * kTcHalves independent MMA chains
+// interleave; the epilogue adds the partials.
+constexpr int kTcHalves = 1;
+constexpr int kTcAccCols = 2 * kTcHalves * 32;           // TMEM columns of one accumulator set
+constexpr int kTcTmemCols = 2 * kTcAccCols;              // two sets (power of two, >= 32)
+constexpr int kTcProducers = 3 * 32;                     // producer threads (warps 0-2)
+constexpr int kTcStage = 2 * kTcW * C * 2;               // epilogue stage: 2 rows x kTcW px x 64 B
+constexpr int kTcEpi = 8 * 32;                           // epilogue threads (warps 4-11)
+constexpr int kTcThreads = 4 * 32 + kTcEpi;
+constexpr int kTcHead = 128;                             // barriers, TMEM address, abort flag
+constexpr int kTcSmem = kTcHead + kTcW16 + kTcStages * kTcHalo + 2 * kTcStage;
+// kind::f16 instruction descriptor: FP32 accumulator, bf16 A and B, both
+// K-major, N = 32, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+static_assert(kTcSmem <= 227 * 1024, "shared memory of one CTA");
+
+__device__ int g_ws_fault;  // a bounded wait of the warm-start kernels gave up
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+          "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+          "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+          "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16* __restrict__ in,
+                                                      const __nv_bfloat16* __restrict__ w,
+                                                      const float* __restrict__ bias, int P,
+                                                      __nv_bfloat16* __restrict__ out,
+                                                      __nv_bfloat16* __restrict__ pool_out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    // head: full[4] @0, empty[4] @32, acc_full[2] @64, acc_empty[2] @80, TMEM address @96, abort @100
+    static_assert(kTcStages <= 4, "barrier head layout");
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t full0 = sbase, empty0 = sbase + 32, accf0 = sbase + 64, acce0 = sbase + 80;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 96);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 100);
+    unsigned char* wsm = smem + kTcHead;
+    unsigned char* ring = wsm + kTcW16;
+    unsigned char* stage0 = ring + kTcStages * kTcHalo;
+    const int Q = P / 2;
+    const int units_x = (P + kTcW - 1) / kTcW, units = ((P + 1) / 2) * units_x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 3) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "n"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            mbar_init(full0 + 8 * s, kTcProducers);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(accf0 + 8 * a, 1);
+            mbar_init(acce0 + 8 * a, kTcEpi / 32);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+    auto give_up = [&]() {
+        if (!*abort_flag) atomicExch(&g_ws_fault, 1);
+        *abort_flag = 1;
+    };
+
+    if (warp < 3) {
+        // ---------------- producers ----------------
+        const int pt = threadIdx.x;  // 0 .. kTcProducers-1
+        int k = 0;
+        for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
+            const int s = k % kTcStages;
+            if (k >= kTcStages && !mbar_wait_bounded(empty0 + 8 * s, ((k / kTcStages) & 1) ^ 1)) {
+                give_up();
+                break;
+            }
+            if (*abort_flag) break;
+            if (k == 0)  // weights [tap][n][k] -> [tap][chunk][n][8], with the first unit
+                for (int i = pt; i < 9 * 32 * 4; i += kTcProducers) {
+                    const int q = i & 3, n = (i >> 2) & 31, tap = i >> 7;
+                    cp_async16(wsm + ((tap * 4 + q) * 32 + n) * 16, w + (tap * 32 + n) * C + q * 8, true);
+                }
+            const int y0 = (u / units_x) * 2, x0 = (u % units_x) * kTcW;
+            unsigned char* halo = ring + s * kTcHalo;
+            for (int i = pt; i < kTcRows * kTcPix * 4; i += kTcProducers) {
+                const int q = i & 3, pix = i >> 2;
+                const int y = y0 - 1 + pix / kTcPix, x = x0 - 1 + pix % kTcPix;
+                const bool ok = y >= 0 && x >= 0 && y < P && x < P;
+                cp_async16(halo + q * kTcPlane + pix * 16, ok ? in + ((int64_t)y * P + x) * C + q * 8 : in, ok);
+            }
+            cp_async_commit();
+            if (k >= kTcLag) {  // unit k - kTcLag has landed: hand it to the tensor cores
+                cp_async_wait_groups<kTcLag>();
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                mbar_arrive(full0 + 8 * ((k - kTcLag) % kTcStages));
+            }
+        }
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        for (int j = std::max(k - kTcLag, 0); j < k; ++j) mbar_arrive(full0 + 8 * (j % kTcStages));
+    } else if (warp == 3) {
+        // ---------------- MMA issue ----------------
+        if (lane == 0) {
+            const uint64_t bd = tc_desc(smem_u32(wsm), 512, 128);
+            int k = 0;
+            for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
+                const int s = k % kTcStages, a = k & 1;
+                if (!mbar_wait_bounded(full0 + 8 * s, (k / kTcStages) & 1) ||
+                    (k >= 2 && !mbar_wait_bounded(acce0 + 8 * a, ((k >> 1) & 1) ^ 1))) {
+                    give_up();
+                    break;
+                }
+                if (*abort_flag) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                // descriptors differ only in the start address field (addresses >> 4 stay below 2^14)
+                const uint64_t ad = tc_desc(smem_u32(ring + s * kTcHalo), kTcPlane, 128);
+                // k16 step j of chain h covers tap h * 5 + j / 2 (chain 1: taps 5-8), chunk pair j % 2;
+                // the chains of both rows are issued in turn
+#pragma unroll
+                for (int j = 0; j < 18 / kTcHalves + 1; ++j)
+#pragma unroll
+                    for (int h = 0; h < kTcHalves; ++h) {
+                        const int tap = (kTcHalves == 1 ? 0 : h * 5) + j / 2, kc = j % 2;
+                        if (j >= (kTcHalves == 1 ? 18 : (h == 0 ? 10 : 8))) continue;
+#pragma unroll
+                        for (int r = 0; r < 2; ++r)
+                            tc_mma(tmem + a * kTcAccCols + (r * kTcHalves + h) * 32,
+                                   ad + (uint64_t)((2 * kc * kTcPlane + ((r + tap / 3) * kTcPix + tap % 3) * 16) >> 4),
+                                   bd + (uint64_t)(((tap * 4 + 2 * kc) * 512) >> 4), j ? 1u : 0u);
+                    }
+                tc_commit(empty0 + 8 * s);
+                tc_commit(accf0 + 8 * a);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue ----------------
+        const int row = (warp - 4) >> 2;  // unit row of this warpgroup
+        const int wl = warp & 3;          // TMEM lanes 32 wl .. 32 wl + 31 = pixels of the row
+        const int et = threadIdx.x - 4 * 32;
+        float bz[C];
+#pragma unroll
+        for (int ch = 0; ch < C; ++ch) bz[ch] = bias[ch];
+        int k = 0;
+        for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
+            const int a = k & 1;
+            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * a, (k >> 1) & 1));
+            if (!ok && lane == 0) give_up();
+            __nv_bfloat16* st = reinterpret_cast<__nv_bfloat16*>(stage0 + (k & 1) * kTcStage);
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                uint32_t v[32];
+                tc_ld32(tmem + ((uint32_t)(32 * wl) << 16) + (uint32_t)(a * kTcAccCols + row * 32), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acce0 + 8 * a);
+                // bias, relu, bf16 into stage k & 1: [row][pixel][32 ch], chunk q of pixel p at
+                // position q ^ ((p >> 1) & 3) so that the eight lanes of a store phase hit distinct banks
+                const int px = 32 * wl + lane;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t w4[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int ch = 8 * q + 2 * e;
+                        w4[e] = pack_bf16x2(fmaxf(__uint_as_float(v[ch]) + bz[ch], 0.f),
+                                            fmaxf(__uint_as_float(v[ch + 1]) + bz[ch + 1], 0.f));
+                    }
+                    *reinterpret_cast<uint4*>(st + (row * kTcW + px) * C + (q ^ ((px >> 1) & 3)) * 8) =
+                        make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                }
+            }
+            // both rows staged; every epilogue thread takes the same quit decision here
+            uint32_t quit;
+            asm volatile(
+                "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred q, 1, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+                : "=r"(quit)
+                : "r"((!ok || *abort_flag) ? 1u : 0u), "n"(kTcEpi)
+                : "memory");
+            if (quit) break;
+            const int y0 = (u / units_x) * 2, x0 = (u % units_x) * kTcW;
+            // 2 rows x kTcW pixels x 4 chunks, consecutive threads consecutive 16-byte chunks
+#pragma unroll
+            for (int j = 0; j < 2 * kTcW * 4 / kTcEpi; ++j) {
+                const int i = j * kTcEpi + et, r = i / (kTcW * 4), pix = (i >> 2) % kTcW, q = i & 3;
+                const int y = y0 + r, x = x0 + pix;
+                if (y < P && x < P)
+                    *reinterpret_cast<uint4*>(out + ((int64_t)y * P + x) * C + q * 8) =
+                        *reinterpret_cast<const uint4*>(st + (r * kTcW + pix) * C + (q ^ ((pix >> 1) & 3)) * 8);
+            }
+            if (pool_out) {
+                // 0.25 (v(y0, x) + v(y0, x+1) + v(y0+1, x) + v(y0+1, x+1)) of the bf16 outputs
+                const int q = et & 3, pxp = et >> 2;  // kTcW / 2 pooled pixels x 4 chunks
+                const int X = x0 / 2 + pxp, Y = y0 / 2;
+                if (X < Q && Y < Q) {
+                    auto at = [&](int r, int p) {
+                        return *reinterpret_cast<const uint4*>(st + (r * kTcW + p) * C + (q ^ ((p >> 1) & 3)) * 8);
+                    };
+                    const uint4 c4[4] = {at(0, 2 * pxp), at(0, 2 * pxp + 1), at(1, 2 * pxp), at(1, 2 * pxp + 1)};
+                    uint4 o;
+                    __nv_bfloat162* po = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float2 f0 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[0])[e]);
+                        const float2 f1 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[1])[e]);
+                        const float2 f2 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[2])[e]);
+                        const float2 f3 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[3])[e]);
+                        po[e] = __floats2bfloat162_rn(0.25f * (f0.x + f1.x + f2.x + f3.x), 0.25f * (f0.y + f1.y + f2.y + f3.y));
+                    }
+                    *reinterpret_cast<uint4*>(pool_out + ((int64_t)Y * Q + X) * C + q * 8) = o;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 3) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(kTcTmemCols) : "memory");
+    }
+}
+
+// u = up2(coarse) + skip, 16 bytes a thread (P = fine size; each sum rounded to bf16)
+__global__ void k_up_add8(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, int P, __nv_bfloat16* u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * P * 4) return;
+    const int q = i & 3, p = i >> 2, y = p / P, x = p % P, Q = P / 2;
+    uint4 v = reinterpret_cast<const uint4*>(skip)[i];
+    add_bf16x8(v, *reinterpret_cast<const uint4*>(coarse + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + q * 8));
+    reinterpret_cast<uint4*>(u)[i] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -854,6 +1177,7 @@ constexpr int kParams = kInW + kInB + kNumConv32 * (kW32 + kB32) + kOutW + kOutB
 
 struct Net {
     int P = 0, GX = 0, GY = 0;
+    int sms = 148;  // streaming multiprocessors of the device (persistent grids)
     float s0 = 1, s1 = 1, s2 = 1;  // input / target scales
     // parameters (fp32 master, Adam moments, gradient)
     float* w = nullptr;
@@ -953,6 +1277,8 @@ static int ws_alloc(pic_ctx* c) {
     N.GX = c->GX;
     N.GY = c->GY;
     N.P = ((std::max(c->GX, c->GY) + 3) / 4) * 4;
+    if (cudaDeviceGetAttribute(&N.sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || N.sms < 1)
+        return fail(PIC_ERR_CUDA, "warm start: device query failed");
     const int64_t P = N.P, Q = P / 2, R = P / 4;
     auto balloc = [&](__nv_bfloat16** p, int64_t n) {
         return cudaMalloc(p, (size_t)n * sizeof(__nv_bfloat16));
@@ -992,6 +1318,7 @@ static int ws_alloc(pic_ctx* c) {
     PIC_CUDA(cudaMemset(N.m, 0, kParams * 4));
     PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
     PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemUp));
+    PIC_CUDA(cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
     return PIC_OK;
 }
@@ -1013,11 +1340,6 @@ __global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16, _
 //          tap*4 + ci, zero for ci == 3 or tap >= 9;
 //   output [step j = tap*2 + kc][lane]: B[K][0] = w_out[tap][kc*16 + k], other
 //          columns zero.
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
-
 __global__ void k_pack_frags(const float* w_in, const float* w_out, uint2* in_frag, uint2* out_frag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = i & 31, g = lane >> 2, t = lane & 3;
@@ -1071,6 +1393,35 @@ static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16
     k_conv32<<<grid, 256, up ? kConvSmemUp : kConvSmem, c->stream>>>(A);
 }
 
+// Forward 32->32 convolution on the tcgen05 tensor cores (k_conv32_tc), the
+// decoder's upsample-and-skip sum (into u) first when `up` is given.
+static void conv32_tc(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
+                      const __nv_bfloat16* up = nullptr, __nv_bfloat16* u = nullptr,
+                      __nv_bfloat16* pool_out = nullptr) {
+    Net& N = c->ws->net;
+    if (up) {
+        k_up_add8<<<g1((int64_t)P * P * 4), 256, 0, c->stream>>>(up, in, P, u);
+        in = u;
+        c->launches += 1;
+    }
+    const int units = ((P + 1) / 2) * ((P + kTcW - 1) / kTcW);
+    k_conv32_tc<<<std::min(units, N.sms), kTcThreads, kTcSmem, c->stream>>>(
+        in, N.w16 + (int64_t)layer * kW32, N.w + param_off(layer + 1) + kW32, P, out, pool_out);
+}
+
+// A bounded device wait of the warm-start kernels gave up (read after a
+// synchronisation; clears the flag).
+static int ws_check_fault() {
+    int f = 0;
+    PIC_CUDA(cudaMemcpyFromSymbol(&f, g_ws_fault, sizeof(int)));
+    if (f) {
+        const int z = 0;
+        PIC_CUDA(cudaMemcpyToSymbol(g_ws_fault, &z, sizeof(int)));
+        return fail(PIC_ERR_TIMEOUT, "warm start: a tensor-core wait timed out");
+    }
+    return PIC_OK;
+}
+
 // [tap][co][ci] (+ bias) -> the parameter layout [tap][ci][co] (+ bias)
 __global__ void k_scatter_wgrad(const float* src, float* g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1100,15 +1451,15 @@ static void forward(pic_ctx* c, bool train) {
     const int P = N.P, Q = P / 2, R = P / 4;
     const dim3 gP((P + TW - 1) / TW, (P + TH - 1) / TH);
     k_conv_in<<<gP, 256, 0, c->stream>>>(N.xin, N.in_frag, N.w + kInW, P, N.a[1]);
-    conv32(c, 0, N.a[1], N.a[2], P, false, nullptr, nullptr, nullptr, N.p1);
-    conv32(c, 1, N.p1, N.a[3], Q, false, nullptr);
-    conv32(c, 2, N.a[3], N.a[4], Q, false, nullptr, nullptr, nullptr, N.p2);
-    conv32(c, 3, N.p2, N.a[5], R, false, nullptr);
-    conv32(c, 4, N.a[5], N.a[6], R, false, nullptr);
-    conv32(c, 5, N.a[4], N.a[7], Q, false, nullptr, N.a[6], train ? N.u1 : nullptr);
-    conv32(c, 6, N.a[7], N.a[8], Q, false, nullptr);
-    conv32(c, 7, N.a[2], N.a[9], P, false, nullptr, N.a[8], train ? N.u0 : nullptr);
-    conv32(c, 8, N.a[9], N.a[10], P, false, nullptr);
+    conv32_tc(c, 0, N.a[1], N.a[2], P, nullptr, nullptr, N.p1);
+    conv32_tc(c, 1, N.p1, N.a[3], Q);
+    conv32_tc(c, 2, N.a[3], N.a[4], Q, nullptr, nullptr, N.p2);
+    conv32_tc(c, 3, N.p2, N.a[5], R);
+    conv32_tc(c, 4, N.a[5], N.a[6], R);
+    conv32_tc(c, 5, N.a[4], N.a[7], Q, N.a[6], N.u1);
+    conv32_tc(c, 6, N.a[7], N.a[8], Q);
+    conv32_tc(c, 7, N.a[2], N.a[9], P, N.a[8], N.u0);
+    conv32_tc(c, 8, N.a[9], N.a[10], P);
     const int64_t ob = param_off(kNumConv32 + 1);
     k_conv_out<<<gP, 256, 0, c->stream>>>(N.a[10], N.out_frag, N.w + ob + kOutW, P, N.out);
     c->launches += 11;
@@ -1345,6 +1696,7 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
         std::vector<float> ls((size_t)N.n_pairs);
         PIC_CUDA(cudaMemcpyAsync(ls.data(), N.loss_acc, ls.size() * 4, cudaMemcpyDeviceToHost, c->stream));
         PIC_CUDA(cudaStreamSynchronize(c->stream));
+        PIC_TRY(ws_check_fault());
         for (float v : ls) ep += v;
         last = ep / (double)N.n_pairs;
     }
@@ -1411,6 +1763,7 @@ int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* rhs_host, f
     PIC_CUDA(cudaStreamSynchronize(c->stream));
     cudaFree(t);
     cudaFree(l);
+    PIC_TRY(ws_check_fault());
     if (out_host) PIC_CUDA(cudaMemcpy(out_host, N.out, (size_t)P * P * 4, cudaMemcpyDeviceToHost));
     if (grad_host) PIC_CUDA(cudaMemcpy(grad_host, N.g, kParams * 4, cudaMemcpyDeviceToHost));
     if (loss) *loss = lh;
