@@ -1409,6 +1409,13 @@ static void conv32_tc(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloa
         in, N.w16 + (int64_t)layer * kW32, N.w + param_off(layer + 1) + kW32, P, out, pool_out);
 }
 
+// The solve's guess buffer, allocated when a network becomes usable (so
+// that no allocation falls inside a timed solve).
+static int ws_guess_buffer(pic_ctx* c) {
+    if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)c->nodes * 4));
+    return PIC_OK;
+}
+
 // A bounded device wait of the warm-start kernels gave up (read after a
 // synchronisation; clears the flag).
 static int ws_check_fault() {
@@ -1554,7 +1561,7 @@ int ws_before_solve(pic_ctx* c, bool want_guess) {
             N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1, N.x0);
         N.xin = N.x0;
         forward(c, false);
-        if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)n * 4));
+        PIC_TRY(ws_guess_buffer(c));
         k_make_guess<<<g1(n), 256, 0, c->stream>>>(N.phi_prev, N.out, c->mask, N.GX, N.GY, N.P, N.s2,
                                                    c->ps.net_guess);
         c->launches += 3;
@@ -1701,6 +1708,7 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
         last = ep / (double)N.n_pairs;
     }
     N.trained = true;
+    PIC_TRY(ws_guess_buffer(c));
     if (loss_out) *loss_out = last;
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
@@ -1727,6 +1735,7 @@ int pic_ws_set_params(pic_ctx* c, const float* host, int64_t n, double phi_scale
     N.s1 = (float)db_scale;
     N.s2 = (float)target_scale;
     N.trained = true;
+    PIC_TRY(ws_guess_buffer(c));
     return PIC_OK;
 }
 
