@@ -461,7 +461,7 @@ def run_learned(pic, args, it):
             "train_s": train_s, "loss_first_epoch": loss0, "loss_last_epoch": loss,
             "eval_steps": args.ws_eval, "scales": list(pic.ws_scales()),
             "what": "residual loss |db - A guess|^2 (scaled); network: 3-level conv encoder-decoder, "
-                    "32 channels, bf16 mma.sync tensor cores, FP32 accumulation"}, it
+                    "32 channels, 32->32 forward convolutions on tcgen05 (TMEM accumulators), the rest on mma.sync; bf16 operands, FP32 accumulation"}, it
 
 
 def run_ensemble(args, rank, world, local_rank):

@@ -77,6 +77,32 @@ def test_forward_backward_match_oracle(oracle, n):
         assert np.linalg.norm(g[a:b] - g_o[a:b]) <= 1e-1 * np.linalg.norm(g_o[a:b]), (a, b)
 
 
+def test_forward_many_units_per_block(oracle):
+    """A grid large enough (P = 388) that every persistent block of the
+    tcgen05 convolution walks several two-row units: the ring of staged
+    tiles wraps and both TMEM accumulators alternate.  The quarter-size
+    level (97) is odd, so its last unit has one row outside the image.  The
+    forward output matches the oracle's bf16-mode forward and repeats bit
+    for bit."""
+    import convnet as N
+    n = 387
+    pic, rects = small_pic(n)
+    with pic:
+        GX = GY = n + 1
+        P = pic.ws_grid()
+        assert P == 388
+        mask = oracle.electrode_mask(GX, GY, oracle.Electrodes(rects)).astype(np.uint8)
+        theta, x0, rhs = random_case(P, GX, GY, mask, seed=7)
+        pic.ws_set_params(theta, 1.0, 2.0, 1.5)
+        out, _, _ = pic.ws_debug_step(x0, rhs)
+        out2, _, _ = pic.ws_debug_step(x0, rhs)
+    assert np.array_equal(out, out2)
+    out_o, _ = N.forward(theta.astype(np.float64), x0)
+    err = np.abs(out.reshape(P, P) - out_o).max() / np.abs(out_o).max()
+    print(f"P={P}: out {err:.2e}")
+    assert err <= 2e-2
+
+
 def test_scales_and_recording_controls():
     import pic_b200 as P
     import pic_configs as C
