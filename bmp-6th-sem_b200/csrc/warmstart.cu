@@ -20,14 +20,15 @@
 // by linearity the target is A_red^-1 db.
 //
 // Storage: activations and their gradients NHWC bf16 (32 channels), weights
-// bf16 with FP32 master copies and Adam moments.  The 32->32 convolutions
-// (forward, data gradient, weight gradient) are implicit GEMMs on the tensor
-// cores with mma.sync.m16n8k16 bf16 x bf16 -> fp32 (K = 9 taps x 32
-// channels); in the forward pass the 3->32 input and 32->1 output
-// convolutions are tensor-core GEMMs too (K = 12 taps x 4 channels, and N = 8
-// of which one column is used), their bf16 weights prepacked as B fragments;
-// their gradients run on the FP32 cores.  The forward pass fuses the pools
-// and the decoder's upsample-and-skip sums into the 32->32 convolutions.
+// bf16 with FP32 master copies and Adam moments.  Convolutions are implicit
+// GEMMs on the tensor cores, bf16 operands and FP32 accumulation (K = 9 taps
+// x 32 channels for the 32->32 layers): the forward 32->32 layers on tcgen05
+// with TMEM accumulators (k_conv32_tc, the average pools fused into its
+// epilogue); the forward 3->32 input and 32->1 output layers with
+// mma.sync.m16n8k16 (K = 12 taps x 4 channels, and N = 8 of which one column
+// is used), their bf16 weights prepacked as B fragments; the training-only
+// data and weight gradients of the 32->32 layers with mma.sync, those of the
+// outer layers on the FP32 cores.
 // Weight gradients are reduced through per-block partials in a fixed order,
 // so training is deterministic.
 #include <cuda_bf16.h>
@@ -1449,11 +1450,10 @@ static void wgrad32(pic_ctx* c, int layer, const __nv_bfloat16* X, const __nv_bf
     k_scatter_wgrad<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.gsum, N.g + param_off(layer + 1));
 }
 
-// Forward pass on the image N.xin; result in N.out.  Eleven launches: the
-// pools and the decoder's upsample-and-skip sums run inside the 32->32
-// convolutions.  `train` keeps the skip sums u0, u1 that the backward pass
-// needs.
-static void forward(pic_ctx* c, bool train) {
+// Forward pass on the image N.xin; result in N.out.  Thirteen launches: the
+// pools run inside the 32->32 convolutions, the decoder's upsample-and-skip
+// sums (kept in u0, u1 for the backward pass) as vector kernels before them.
+static void forward(pic_ctx* c) {
     Net& N = c->ws->net;
     const int P = N.P, Q = P / 2, R = P / 4;
     const dim3 gP((P + TW - 1) / TW, (P + TH - 1) / TH);
@@ -1560,7 +1560,7 @@ int ws_before_solve(pic_ctx* c, bool want_guess) {
         k_make_input<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(
             N.phi_prev, N.db, c->mask, N.GX, N.GY, N.P, 1.f / N.s0, (float)(c->dx * c->dx) / N.s1, N.x0);
         N.xin = N.x0;
-        forward(c, false);
+        forward(c);
         PIC_TRY(ws_guess_buffer(c));
         k_make_guess<<<g1(n), 256, 0, c->stream>>>(N.phi_prev, N.out, c->mask, N.GX, N.GY, N.P, N.s2,
                                                    c->ps.net_guess);
@@ -1688,7 +1688,7 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
         for (int64_t s = 0; s < N.n_pairs; ++s) {
             PIC_TRY(ws_pack(c));
             N.xin = N.ds_x + s * (int64_t)P * P * 4;
-            forward(c, true);
+            forward(c);
             enqueue_loss(c, N.ds_t + s * c->nodes, N.loss_acc + s);
             backward(c);
             N.adam_t += 1;
@@ -1764,7 +1764,7 @@ int pic_ws_debug_step(pic_ctx* c, const float* x0_host, const float* rhs_host, f
     PIC_CUDA(cudaMemcpy(t, rhs_host, (size_t)c->nodes * 4, cudaMemcpyHostToDevice));
     PIC_TRY(ws_pack(c));
     N.xin = N.x0;
-    forward(c, true);
+    forward(c);
     enqueue_loss(c, t, l);
     backward(c);
     float lh = 0.f;
