@@ -274,6 +274,7 @@ int particles_time_shapes(pic_ctx* c, int reps, double* ms);  // ms[particles_nu
 void ws_free(pic_ctx* c);
 bool ws_tracking(const pic_ctx* c);  // hooks must run at every solve
 int ws_before_solve(pic_ctx* c, bool want_guess);  // 1 when a guess is in ps.net_guess
+int ws_check_fault();  // after a synchronisation: PIC_ERR_TIMEOUT if a warm-start kernel gave up
 int ws_after_solve(pic_ctx* c, bool record);
 
 // poisson.cu

@@ -1043,6 +1043,7 @@ int poisson_solve(pic_ctx* c) {
     ps.last_iters = it;
     ps.last_relres = bb > 0 ? std::sqrt(true_rr / bb) : 0.0;
     ps.have_prev = true;
+    if (learned) PIC_TRY(ws_check_fault());  // the guess's kernels gave up a bounded wait
     if (status != PIC_OK)
         return fail(status, "Poisson PCG did not reach the tolerance within poisson_maxit");
     return PIC_OK;

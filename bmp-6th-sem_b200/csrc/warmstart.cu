@@ -126,50 +126,12 @@ __device__ __forceinline__ void load_halo_async(__nv_bfloat16* dst, const __nv_b
     }
 }
 
-// The half-size image under a halo tile: rows y0/2-1 .. y0/2+TH/2 and columns
-// x0/2-1 .. x0/2+TW/2 (y0, x0 even), [row][col][CP] in shared memory.
-constexpr int kUpRows = TH / 2 + 2, kUpCols = TW / 2 + 2;
-
-__device__ __forceinline__ void load_up_async(__nv_bfloat16* dst, const __nv_bfloat16* up, int P,
-                                              int y0, int x0) {
-    const int Q = P / 2, Y0 = y0 / 2 - 1, X0 = x0 / 2 - 1;
-    for (int i = threadIdx.x; i < kUpRows * kUpCols * (C / 8); i += blockDim.x) {
-        const int q = i & 3, pix = i >> 2;
-        const int Y = Y0 + pix / kUpCols, X = X0 + pix % kUpCols;
-        const bool in = Y >= 0 && X >= 0 && Y < Q && X < Q;
-        cp_async16(dst + pix * CP + q * 8, in ? up + ((int64_t)Y * Q + X) * C + q * 8 : up, in);
-    }
-}
-
-// Once both tiles have landed: the halo tile's in-image pixels become
-// up2(up) + tile (each sum rounded to bf16); the tile's interior sums are also
-// written to u_out when given.
-__device__ __forceinline__ void add_up(__nv_bfloat16* in_s, const __nv_bfloat16* up_s, int P, int y0,
-                                       int x0, __nv_bfloat16* u_out) {
-    constexpr int kChunks = (TH + 2) * (TW + 2) * (C / 8);
-    const int Y0 = y0 / 2 - 1, X0 = x0 / 2 - 1;
-    for (int i = threadIdx.x; i < kChunks; i += blockDim.x) {
-        const int q = i & 3, pix = i >> 2;
-        const int r = pix / (TW + 2), col = pix % (TW + 2);
-        const int y = y0 + r - 1, x = x0 + col - 1;
-        if (y < 0 || x < 0 || y >= P || x >= P) continue;
-        uint4* d = reinterpret_cast<uint4*>(in_s + pix * CP + q * 8);
-        uint4 v = *d;
-        add_bf16x8(v, *reinterpret_cast<const uint4*>(up_s + (((y >> 1) - Y0) * kUpCols + (x >> 1) - X0) * CP + q * 8));
-        *d = v;
-        if (u_out && r >= 1 && r <= TH && col >= 1 && col <= TW)
-            *reinterpret_cast<uint4*>(u_out + ((int64_t)y * P + x) * C + q * 8) = v;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // 32 -> 32 3x3 convolution (forward, or data gradient with transformed
 // weights).  Weights in global memory as [tap][n][k] bf16 (n = output
 // channel, k = input channel).  Epilogue: out = act(acc + bias), where act is
-// relu (forward) or a gate (out *= gate[p] > 0, data gradient).  Forward
-// options fused into the same pass: the input may be up2(up) + in (the
-// decoder's upsample-and-skip, its sum kept in u_out for training), and the
-// output's 2x2 average pool may be written to pool_out.
+// relu (forward) or a gate (out *= gate[p] > 0, data gradient).  Training
+// uses it for the data gradients; the forward pass runs k_conv32_tc.
 // ---------------------------------------------------------------------------
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -177,34 +139,24 @@ struct ConvArgs {
     const float* bias;        // [32] or null
     const __nv_bfloat16* gate;  // [P][P][32] or null: multiply by (gate > 0)
     __nv_bfloat16* out;
-    const __nv_bfloat16* up;  // [P/2][P/2][32] or null: input is up2(up) + in
-    __nv_bfloat16* u_out;     // [P][P][32] or null: that input sum
-    __nv_bfloat16* pool_out;  // [P/2][P/2][32] or null: avgpool2 of the output
     int P;
     int relu;
 };
 
 constexpr int kConvSmem = ((TH + 2) * (TW + 2) * CP + 9 * C * CP) * 2;
-constexpr int kConvSmemUp = kConvSmem + kUpRows * kUpCols * CP * 2;  // with the half-size tile
 
 __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* in_s = reinterpret_cast<__nv_bfloat16*>(smem);
     __nv_bfloat16* w_s = in_s + (TH + 2) * (TW + 2) * CP;
     const int y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
-    __nv_bfloat16* up_s = w_s + 9 * C * CP;  // with A.up only
     load_halo_async(in_s, A.in, A.P, y0, x0);
-    if (A.up) load_up_async(up_s, A.up, A.P, y0, x0);
     for (int i = threadIdx.x; i < 9 * C * (C / 8); i += blockDim.x) {
         const int q = i & 3, row = i >> 2;  // row = tap*32 + n
         cp_async16(w_s + row * CP + q * 8, A.w + row * C + q * 8, true);
     }
     cp_async_wait_all();
     __syncthreads();
-    if (A.up) {
-        add_up(in_s, up_s, A.P, y0, x0, A.u_out);
-        __syncthreads();
-    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // warp = output row in the tile
     float acc[2][4][4];
 #pragma unroll
@@ -284,31 +236,6 @@ __global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
             }
         }
         *reinterpret_cast<uint4*>(A.out + go) = v;
-    }
-    if (A.pool_out) {
-        // 2x2 averages of the tile (y0, x0 even): (TH/2) x (TW/2) pixels x 4 chunks
-        const int Q = A.P / 2;
-        for (int i = threadIdx.x; i < (TH / 2) * (TW / 2) * (C / 8); i += blockDim.x) {
-            const int q = i & 3, pp = i >> 2;
-            const int py = pp / (TW / 2), px = pp % (TW / 2);
-            const int Y = y0 / 2 + py, X = x0 / 2 + px;
-            if (Y >= Q || X >= Q) continue;
-            const __nv_bfloat16* s00 = o_s + (2 * py * TW + 2 * px) * CP + q * 8;
-            uint4 c4[4] = {*reinterpret_cast<const uint4*>(s00), *reinterpret_cast<const uint4*>(s00 + CP),
-                           *reinterpret_cast<const uint4*>(s00 + TW * CP),
-                           *reinterpret_cast<const uint4*>(s00 + (TW + 1) * CP)};
-            uint4 o;
-            __nv_bfloat162* po = reinterpret_cast<__nv_bfloat162*>(&o);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float2 f0 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[0])[e]);
-                const float2 f1 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[1])[e]);
-                const float2 f2 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[2])[e]);
-                const float2 f3 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[3])[e]);
-                po[e] = __floats2bfloat162_rn(0.25f * (f0.x + f1.x + f2.x + f3.x), 0.25f * (f0.y + f1.y + f2.y + f3.y));
-            }
-            *reinterpret_cast<uint4*>(A.pool_out + ((int64_t)Y * Q + X) * C + q * 8) = o;
-        }
     }
 }
 
@@ -1318,7 +1245,7 @@ static int ws_alloc(pic_ctx* c) {
     PIC_CUDA(cudaMemcpy(N.w, w.data(), kParams * 4, cudaMemcpyHostToDevice));
     PIC_CUDA(cudaMemset(N.m, 0, kParams * 4));
     PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
-    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemUp));
+    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     PIC_CUDA(cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
     return PIC_OK;
@@ -1376,8 +1303,7 @@ static int ws_pack(pic_ctx* c) {
 }
 
 static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
-                   bool transposed, const __nv_bfloat16* gate, const __nv_bfloat16* up = nullptr,
-                   __nv_bfloat16* u_out = nullptr, __nv_bfloat16* pool_out = nullptr) {
+                   bool transposed, const __nv_bfloat16* gate) {
     Net& N = c->ws->net;
     ConvArgs A;
     A.in = in;
@@ -1385,13 +1311,10 @@ static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16
     A.bias = transposed ? nullptr : N.w + param_off(layer + 1) + kW32;
     A.gate = gate;
     A.out = out;
-    A.up = up;
-    A.u_out = u_out;
-    A.pool_out = pool_out;
     A.P = P;
     A.relu = transposed ? 0 : 1;
     const dim3 grid((P + TW - 1) / TW, (P + TH - 1) / TH);
-    k_conv32<<<grid, 256, up ? kConvSmemUp : kConvSmem, c->stream>>>(A);
+    k_conv32<<<grid, 256, kConvSmem, c->stream>>>(A);
 }
 
 // Forward 32->32 convolution on the tcgen05 tensor cores (k_conv32_tc), the
@@ -1419,7 +1342,7 @@ static int ws_guess_buffer(pic_ctx* c) {
 
 // A bounded device wait of the warm-start kernels gave up (read after a
 // synchronisation; clears the flag).
-static int ws_check_fault() {
+int ws_check_fault() {
     int f = 0;
     PIC_CUDA(cudaMemcpyFromSymbol(&f, g_ws_fault, sizeof(int)));
     if (f) {
