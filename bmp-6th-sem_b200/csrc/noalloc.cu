@@ -15,6 +15,7 @@
 // offset is rounded to 20 bits and the four corner weights are exact 40-bit
 // products summed in 64-bit integers -- so the result is bit-for-bit the
 // final_mesh / rho that pic_import_points + pic_charge_deposition produce.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,24 +33,71 @@ constexpr int kMaxDevices = 64;
 __device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxNodes];
 
 std::mutex g_mu;
-unsigned long long* g_acc_addr[kMaxDevices] = {};
+// Per device: the device address of the scratch array and the unique id of
+// the CUDA context it was looked up in.  The address belongs to the module
+// as loaded into that context; after cudaDeviceReset the next primary
+// context loads the module again, possibly at another address, so a change
+// of context id means a new lookup.
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    unsigned long long* addr;
+};
+ScratchSlot g_slot[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device, looked up once
-// per device (the host-side name of the array is not a device address).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// The current context's unique id through the driver entry points (no link
+// against libcuda); 0 when the driver cannot tell, which disables the cache.
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+            get_id = reinterpret_cast<CtxGetIdFn>(f2);
+        }
+        cudaGetLastError();
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device (the host-side
+// name of the array is not a device address), looked up with the device
+// current once per device and context.
 int scratch_address(unsigned long long** out) {
     int dev = 0;
     PIC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(PIC_ERR_NO_DEVICE, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_acc_addr[dev]) {
+    // 0 before the runtime has made the device's primary context current: the
+    // lookup below does that, and the id is read again after it
+    const unsigned long long id = current_context_id();
+    ScratchSlot& slot = g_slot[dev];
+    if (!slot.addr || id == 0 || slot.ctx_id != id) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_acc);
-        if (e != cudaSuccess)
+        if (e != cudaSuccess) {
+            slot.addr = nullptr;
             return fail(PIC_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_acc): ") +
                                           cudaGetErrorString(e));
-        g_acc_addr[dev] = static_cast<unsigned long long*>(p);
+        }
+        slot.addr = static_cast<unsigned long long*>(p);
+        slot.ctx_id = current_context_id();
     }
-    *out = g_acc_addr[dev];
+    *out = slot.addr;
     return PIC_OK;
 }
 
@@ -121,7 +169,7 @@ extern "C" int pic_deposit_points_noalloc(const pic_point* dev_points, int64_t n
     const double surf = surf_area > 0 ? surf_area : xmax * ymax;
     // updateWeighingFactor, src/particles.cpp:303-305
     const double weighing = species->actual_count * surf / (species->sim_count * dx * dy * dx * dy);
-    const double qscale = kChargeUnit * dx * dy * weighing;
+    const double qscale = kChargeUnit * (dx * dy) * weighing;  // as the context's flush rounds it
     const double chrg = -species->charge / epsilon;  // RhoKernel, src/interpolation.cpp:164-170
     k_na_clear<<<(unsigned)((nodes + 255) / 256), 256, 0, st>>>(acc, nodes);
     if (n > 0)

@@ -284,7 +284,10 @@ int pic_autotune(pic_ctx* ctx, int* tile_shape, double* ms_per_shape);
  *     process exits, cleared at the start of every call.
  *   - The first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     before any stream capture.  The address is kept per device and CUDA
+ *     context: after a cudaDeviceReset the next call sees a new context and
+ *     looks the address up again (so, after a reset too, make one call
+ *     before capturing).
  *   - All calls share the one array: calls that overlap on the GPU (other
  *     streams, other host threads) race and must be serialised by the caller. */
 int pic_deposit_points_noalloc(const pic_point* dev_points, int64_t n, int32_t nx, int32_t ny,

@@ -1,24 +1,27 @@
 """Copies the reference's PARDISO golden vectors into small committed fixtures.
 
-Source: SYCL-PIC-poissonsolver/validation_dumps/iter000{0,4}_{rho_input,phi_cpp}.npy
+Source: SYCL-PIC-poissonsolver/validation_dumps/iter000{0-4}_{rho_input,phi_cpp}.npy
 (257x257 nodes, XMAX=YMAX=1 m, NX=NY=256 from SYCL-PIC-poissonsolver/M_PICDAT.DAT:6,
 four grounded walls from SYCL-PIC-poissonsolver/geometry.conf:6-9).  rho_input is
 the deposited rho handed to poissonSolver() before overwriteRho; phi_cpp is the
-MKL PARDISO result after overwritePhi.  Only iterations 0 and 4 are kept to
-keep the fixtures small.  Run once in a checkout that has the reference tree:
+MKL PARDISO result after overwritePhi.  All five dumped iterations are kept
+(about 1 MB each, compressed).  Run once in a checkout that has the reference
+tree, naming its root:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout root>
 """
+import argparse
 import os
-import sys
 
 import numpy as np
 
-ITERS = (0, 4)
+ITERS = (0, 1, 2, 3, 4)
 
 
 def main(ref_root: str) -> None:
     src = os.path.join(ref_root, "SYCL-PIC-poissonsolver", "validation_dumps")
+    if not os.path.isdir(src):
+        raise SystemExit(f"no validation_dumps folder under {ref_root}")
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for it in ITERS:
         rho = np.load(os.path.join(src, f"iter{it:04d}_rho_input.npy"))
@@ -29,4 +32,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("reference_root", help="root of the vansh268p/BMP-6th-sem checkout")
+    main(ap.parse_args().reference_root)

@@ -6,9 +6,9 @@ memory budget, or a time-critical loop where cudaMalloc/cudaFree and their
 device-wide synchronisation are not allowed): its only scratch is a fixed
 array inside the library.  This test checks that two calls in a row give the
 same final_mesh and rho as the library's regular path (pic_import_points +
-pic_charge_deposition), within the deposit tolerance of the other GPU tests
-(2e-6 of max|final_mesh|; the arithmetic is in fact identical), so the
-shared scratch is cleared between calls.  The test's own buffers come from
+pic_charge_deposition): within the deposit tolerance of the other GPU tests
+(2e-6 of max|final_mesh|) and, since the fixed-point arithmetic is the same,
+bit for bit -- so the shared scratch is cleared between calls.  The test's own buffers come from
 torch; the entry point itself allocates nothing.
 
 The file name sorts last so that a run stopping at the first failure has
@@ -70,8 +70,12 @@ def test_noalloc_deposit_matches_regular_deposit_twice():
         torch.cuda.synchronize()
         got_final = final.cpu().numpy()
         got_rho = rho.cpu().numpy()
+        # same fixed-point arithmetic as the regular path: final_mesh and rho
+        # are bit-identical (the 2e-6 deposit tolerance is the outer bound)
         assert np.abs(got_final - final_ref).max() <= tol, call
+        assert np.array_equal(got_final, final_ref), call
         assert np.abs(got_rho - rho_ref).max() <= 2e-6 * np.abs(rho_ref).max(), call
+        assert np.array_equal(got_rho, rho_ref), call
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
