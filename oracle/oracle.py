@@ -17,8 +17,10 @@ This module adds the pieces that are easiest in NumPy/SciPy:
   (src/poissonSolver.cpp:459-544).
 
 The Poisson part is pinned against the reference's own PARDISO dumps
-(tests/golden/poisson_257_*.npz).  Binning, deposit and push have no reference
-fixtures and are pinned only through the line-by-line restatement.
+(tests/golden/poisson_257_*.npz).  Binning, deposit and push are pinned
+against the reference's own kernel bodies compiled here into a host harness
+(oracle/ref_build.py, loaded by ``ref_lib``; tests/test_oracle_ref_pin.py:
+bit for bit).
 """
 from __future__ import annotations
 
@@ -45,9 +47,12 @@ EPS0 = 8.854e-12
 
 
 class Grid(ctypes.Structure):
-    """GridParams subset (include/species_ds.hpp:6-10)."""
+    """GridParams subset (include/species_ds.hpp:6-10).  width/height are
+    GRID_WIDTH/GRID_HEIGHT (XMAX/YMAX as read from M_PICDAT.DAT), the bounds
+    of the mover's wall test; left 0 they are nx*dx / ny*dy."""
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
-                ("dx", ctypes.c_double), ("dy", ctypes.c_double)]
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("width", ctypes.c_double), ("height", ctypes.c_double)]
 
     @property
     def GX(self):
@@ -424,3 +429,47 @@ class RefHashmapSpecies:
 
     def cleanup(self):
         lib().orc_ref_cleanup(self.m, _ptr(self.pts))
+
+
+# ---------------------------------------------------------------------------
+# The reference's own particle code, compiled here (oracle/ref_build.py)
+# ---------------------------------------------------------------------------
+
+class RefGridParams(ctypes.Structure):
+    """GridParams as the reference declares it (include/species_ds.hpp:6-10)."""
+    _fields_ = [("NX", ctypes.c_int), ("NY", ctypes.c_int), ("GRID_X", ctypes.c_int),
+                ("GRID_Y", ctypes.c_int), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("GRID_WIDTH", ctypes.c_double), ("GRID_HEIGHT", ctypes.c_double)]
+
+
+_ref_lib = None
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_pic.so")
+
+
+def ref_lib():
+    """oracle/_ref/libref_pic.so (the reference's kernel bodies in a host
+    harness), built from a reference checkout when absent; None when it is
+    absent and no checkout is available."""
+    global _ref_lib
+    if _ref_lib is None:
+        if not os.path.exists(REF_LIB_PATH):
+            try:
+                import ref_build
+                ref_build.build()
+            except (FileNotFoundError, ImportError, subprocess.CalledProcessError):
+                return None
+        L = ctypes.CDLL(REF_LIB_PATH)
+        vp, i32, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.ref_mover_kernel.restype = i32
+        L.ref_mover_kernel.argtypes = [vp, i32, ctypes.POINTER(RefGridParams), vp, i32, dbl, vp, vp,
+                                       vp, i32, vp, vp, ctypes.POINTER(i32)]
+        L.ref_interpolate.restype = i32
+        L.ref_interpolate.argtypes = [vp, i32, vp, ctypes.POINTER(RefGridParams), i32, i32, vp, vp,
+                                      vp, dbl, i32, vp, vp, vp]
+        _ref_lib = L
+    return _ref_lib
+
+
+def ref_grid_params(nx: int, ny: int, width: float, height: float) -> RefGridParams:
+    """The reference's params1 (src/particles.cpp:357-368): dx = XMAX/NX."""
+    return RefGridParams(nx, ny, nx + 1, ny + 1, width / nx, height / ny, width, height)

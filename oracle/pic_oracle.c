@@ -20,12 +20,15 @@
  *
  * Parity status: the Poisson layer is pinned against the reference's own
  * PARDISO dumps (SYCL-PIC-poissonsolver/validation_dumps, 257x257 nodes).
- * Binning, deposit and push have no reference fixtures; for them parity is
- * pinned only through this restatement of the reference source (unpinned by
- * golden vectors).  The same holds for the periodic-in-y variants
- * (orc_push_mode, orc_build_csr_periodic, orc_overwrite_phi_periodic,
- * orc_efield_periodic), which the tests pin by properties of the periodic
- * system instead.
+ * Binning, deposit and push are pinned against the reference's own code run
+ * here: oracle/ref_build.py compiles the bodies of deterministic_mover,
+ * MoverKernel and interpolate's kernels from a reference checkout into a
+ * host harness, and tests/test_oracle_ref_pin.py finds the push (walled and
+ * periodic in y), the wall deletions, left exits, re-binned buckets and the
+ * deposit equal to this file's bit for bit.  The periodic Poisson variants
+ * (orc_build_csr_periodic, orc_overwrite_phi_periodic, orc_efield_periodic)
+ * have no reference fixtures; the tests pin them by properties of the
+ * periodic system instead.
  */
 #include <math.h>
 #include <stdint.h>
@@ -42,11 +45,18 @@ typedef struct {
     int32_t pad_;
 } orc_point;
 
-/* GridParams subset: include/species_ds.hpp:6-10.  nodes = (nx+1) x (ny+1). */
+/* GridParams subset: include/species_ds.hpp:6-10.  nodes = (nx+1) x (ny+1).
+ * width/height are GRID_WIDTH/GRID_HEIGHT (the XMAX/YMAX read from
+ * M_PICDAT.DAT, src/particles.cpp:352-368), the bounds of the mover's wall
+ * test; 0 means nx*dx / ny*dy. */
 typedef struct {
     int32_t nx, ny;
     double dx, dy;
+    double width, height;
 } orc_grid;
+
+static inline double grid_width(const orc_grid* g) { return g->width > 0 ? g->width : g->nx * g->dx; }
+static inline double grid_height(const orc_grid* g) { return g->height > 0 ? g->height : g->ny * g->dy; }
 
 /* Geometry: include/point.hpp:21-24 (inclusive node-index rectangle + volts). */
 typedef struct {
@@ -192,24 +202,28 @@ void orc_deposit(const orc_grid* g, const orc_point* p, int64_t n, double weighi
 
 /* deterministic_mover(), src/mover.cpp:103-176.  efield is the interleaved
  * Field array (fx, fy per node), bz the node magnetic field.  The cell used
- * for the gather is (int)(x/dx) -- a division, as at :115-116. */
+ * for the gather is (int)(x/dx) -- a division, as at :115-116.  Every
+ * expression keeps the reference's operand order and association (products
+ * left to right, e.g. (E*(dx-lx))*(dy-ly)), so that with the same compiler
+ * flags (no FMA contraction) the result is the reference's bit for bit. */
 static inline void mover_one(orc_point* q, const orc_grid* g, double pctm, double dt,
                              const double* efield, const double* bz) {
     const int GX = g->nx + 1;
+    const double dx = g->dx, dy = g->dy;
     double px = q->x, py = q->y, pz = q->z, pvx = q->vx, pvy = q->vy, pvz = q->vz;
-    const int gx = (int)(px / g->dx);
-    const int gy = (int)(py / g->dy);
-    const double lx = px - gx * g->dx;
-    const double ly = py - gy * g->dy;
-    const int n1 = gy * GX + gx, n2 = gy * GX + gx + 1, n3 = (gy + 1) * GX + gx,
-              n4 = (gy + 1) * GX + gx + 1;
-    const double a1 = (g->dx - lx) * (g->dy - ly), a2 = lx * (g->dy - ly),
-                 a3 = (g->dx - lx) * ly, a4 = lx * ly, area = g->dx * g->dy;
-    const double Epx = (efield[2 * n1] * a1 + efield[2 * n2] * a2 + efield[2 * n3] * a3 +
-                        efield[2 * n4] * a4) / area;
-    const double Epy = (efield[2 * n1 + 1] * a1 + efield[2 * n2 + 1] * a2 +
-                        efield[2 * n3 + 1] * a3 + efield[2 * n4 + 1] * a4) / area;
-    const double Bpz = (bz[n1] * a1 + bz[n2] * a2 + bz[n3] * a3 + bz[n4] * a4) / area;
+    const int gx = (int)(px / dx);
+    const int gy = (int)(py / dy);
+    const double lx = px - gx * dx;
+    const double ly = py - gy * dy;
+    const int n1 = gy * GX + gx, n2 = gy * GX + (gx + 1), n3 = (gy + 1) * GX + gx,
+              n4 = (gy + 1) * GX + (gx + 1);
+    const double Epx = (efield[2 * n1] * (dx - lx) * (dy - ly) + efield[2 * n2] * lx * (dy - ly) +
+                        efield[2 * n3] * (dx - lx) * ly + efield[2 * n4] * lx * ly) / (dx * dy);
+    const double Epy = (efield[2 * n1 + 1] * (dx - lx) * (dy - ly) +
+                        efield[2 * n2 + 1] * lx * (dy - ly) + efield[2 * n3 + 1] * (dx - lx) * ly +
+                        efield[2 * n4 + 1] * lx * ly) / (dx * dy);
+    const double Bpz = (bz[n1] * (dx - lx) * (dy - ly) + bz[n2] * lx * (dy - ly) +
+                        bz[n3] * (dx - lx) * ly + bz[n4] * lx * ly) / (dx * dy);
     /* Boris with Bz only, :151-166. */
     const double Vxminus = pvx + 0.5 * pctm * Epx * dt;
     const double Vyminus = pvy + 0.5 * pctm * Epy * dt;
@@ -243,7 +257,7 @@ static inline double ref_modulo(double x, double y) {
 int64_t orc_push_mode(const orc_grid* g, orc_point* p, int64_t n, double ctom, double dt,
                       const double* efield, const double* bz, int32_t periodic_y,
                       int64_t* left_exits) {
-    const double W = g->nx * g->dx, H = g->ny * g->dy;
+    const double W = grid_width(g), H = grid_height(g);
     int64_t deleted = 0, left = 0;
 #pragma omp parallel for schedule(static) reduction(+ : deleted, left)
     for (int64_t i = 0; i < n; ++i) {
@@ -692,7 +706,7 @@ void orc_ref_deposit(const orc_hmap* m, const orc_grid* g, const orc_point* p, d
 int64_t orc_ref_mover(orc_hmap* m, const orc_grid* g, orc_point* p, int64_t n, double ctom,
                       double dt, const double* efield, const double* bz, int32_t* empty_space,
                       int64_t* n_empty, int64_t* new_additions) {
-    const double W = g->nx * g->dx, H = g->ny * g->dy;
+    const double W = grid_width(g), H = grid_height(g);
     const double inv_dx = 1.0 / g->dx, inv_dy = 1.0 / g->dy;
     const int32_t GX = g->nx + 1;
     int64_t holes = *n_empty, left = 0;
