@@ -18,7 +18,8 @@ ranks run N independent replicas with different seeds ("scaling": "weak").
 
 --impl reference times the reference's algorithm on the host cores (the
 hashmap port in oracle/, the reference's own CPU path being unbuildable here)
-on a bounded sample of the same workload, and prints the same JSON line.
+on the same full-size workload, every step a full step, and prints the same
+JSON line.
 """
 import argparse
 import json
@@ -99,65 +100,63 @@ def describe(w):
 # CPU side: the reference's algorithm (hashmap port) on a bounded sample
 # ---------------------------------------------------------------------------
 
-def sample_points(w, s, scale, seed):
-    """Host Points for the workload shrunk by `scale` per axis, same per-cell
-    densities (background ppc + blob profile)."""
-    import pic_b200 as P
-    import pic_configs as C
-    nx, ny = w.nx // scale, w.ny // scale
-    rng = np.random.default_rng(seed)
-    ps = w.plasma[s]
-    gx, gy = np.meshgrid(np.arange(nx), np.arange(ny))
-    cnt = np.full(nx * ny, ps.ppc, np.int64)
-    if ps.blob_peak_ppc > 0:
-        cx, cy, sig = ps.blob_cx / scale, ps.blob_cy / scale, ps.blob_sigma / scale
-        r2 = ((gx + 0.5 - cx) ** 2 + (gy + 0.5 - cy) ** 2).ravel()
-        blob = np.floor(ps.blob_peak_ppc * np.exp(-r2 / (2 * sig * sig)) + rng.random(nx * ny))
-        cnt = cnt + blob.astype(np.int64)
-    cells = np.repeat(np.arange(nx * ny), cnt)
-    first = np.repeat(np.cumsum(cnt) - cnt, cnt)
-    is_blob = (np.arange(len(cells)) - first) >= ps.ppc
-    n = len(cells)
-    pts = np.zeros(n, P.POINT_DTYPE)
-    pts["x"] = (cells % nx + rng.random(n)) * w.dx
-    pts["y"] = (cells // nx + rng.random(n)) * w.dx
-    sig_v = np.sqrt(C.QE * ps.temperature_ev / w.species[s][1])
-    pts["vx"] = rng.normal(0, sig_v, n) + np.where(is_blob, ps.drift_vx, 0.0)
-    pts["vy"] = rng.normal(0, sig_v, n) + np.where(is_blob, ps.drift_vy, 0.0)
-    pts["vz"] = rng.normal(0, sig_v, n)
-    # the reference's arrays are in random order (initParticlesRandomly)
-    return pts[rng.permutation(n)], nx, ny
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
-def cpu_reference_run(w, scale, max_seconds, min_steps=2, max_steps=None, steps=None):
-    """Times the reference's step structure (src/main.cpp:130-230) on the host:
-    per species hashmap deposit, then the Poisson solve (SuperLU, factored
-    once), then per species mover + compaction + map cleanup.  Returns
-    (particle-steps/s of the particle phases, poisson ms/step, sample text,
-    threads, per-step particle seconds list)."""
+# The reference's hashmap gives every node key probing_length slots
+# (prob_size * wg = 24 * 256 = 6144 by default, src/particles.cpp:181), with
+# slot indices in int.  On the 1024^2 workload 6144 slots a node would take
+# 62 GB per species and overflow int (1.05e6 nodes * 6144 * 1.2 > 2^31), so
+# the port sizes the buckets to the data instead: the next power of two of
+# 1.3 x the fullest bucket, capped where the slot index still fits an int.
+def probing_length(peak: int, nodes: int) -> int:
+    want = 1 << max(4, int(np.ceil(np.log2(1.3 * max(peak, 1)))))
+    cap = int((2 ** 31 - 1) / (nodes * 1.2))
+    return min(want, cap)
+
+
+def cpu_reference_run(w, max_seconds=None, steps=None, min_steps=2):
+    """Times the reference's step structure (src/main.cpp:130-230) on the
+    host cores, on the full workload: per species the hashmap deposit, the
+    Poisson solve (SuperLU, factored once beforehand), then per species the
+    mover, compaction and map cleanup.  Runs `steps` steps, or steps until
+    max_seconds of particle-phase time (at least min_steps).  Returns a dict:
+    particle-steps/s of the particle phases, Poisson ms/step, per-step
+    particle seconds, the sample description, threads, CPU model."""
     import oracle as O
     import pic_configs as C
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    sp_pts, nx, ny = [], 0, 0
+    t_setup = time.perf_counter()
+    nx, ny = w.nx, w.ny
+    dx = w.xmax / nx
+    g = O.Grid(nx, ny, dx, dx, w.xmax, w.ymax)
+    pts = []
     for s in range(2):
-        pts, nx, ny = sample_points(w, s, scale, seed=900 + s)
-        sp_pts.append(pts)
-    dx = dy = w.dx
-    g = O.Grid(nx, ny, dx, dy)
-    scale_rects = [(0, 0, 0, ny, w.rects[0][4]), (nx, 0, nx, ny, w.rects[1][4]),
-                   (0, ny, nx, ny, w.rects[2][4]), (0, 0, nx, 0, w.rects[3][4])]
-    for (x1, y1, x2, y2, v) in w.rects[4:]:
-        scale_rects.append((x1 // scale, y1 // scale, x2 // scale, y2 // scale, v))
-    el = O.Electrodes(scale_rects)
-    D = O.DirectPoisson(nx + 1, ny + 1, dx, dy, el)
-    species = [O.Species(str(s), *C._species(nx, ny, w.ppc, w.n0)[s]) for s in range(2)]
-    weigh = [O.weighing_factor(sp, nx * dx * ny * dy, dx, dy) for sp in species]
-    # the reference sizes each bucket for prob_size*wg slots; the blob peak
-    # needs ~1.1k per bucket here
-    H = [O.RefHashmapSpecies(g, sp_pts[s], probing_length=2048) for s in range(2)]
+        ps = w.plasma[s]
+        v_th = float(np.sqrt(C.QE * ps.temperature_ev / w.species[s][1]))
+        pts.append(O.generate_plasma(nx, ny, dx, dx, ps.ppc, v_th, ps.blob_peak_ppc, ps.blob_cx,
+                                     ps.blob_cy, ps.blob_sigma or 1.0, ps.drift_vx, ps.drift_vy,
+                                     seed=900 + s))
+    el = O.Electrodes(w.rects)
+    t0 = time.perf_counter()
+    D = O.DirectPoisson(w.GX, w.GY, dx, dx, el)
+    factor_s = time.perf_counter() - t0
+    species = [O.Species(str(s), *w.species[s]) for s in range(2)]
+    weigh = [O.weighing_factor(sp, w.xmax * w.ymax, dx, dx) for sp in species]
+    peak = max(int(O.bucket_counts(g, p).max()) for p in pts)
+    probing = probing_length(peak, g.nodes)
+    H = [O.RefHashmapSpecies(g, pts[s], probing_length=probing) for s in range(2)]
     bz = np.full(g.nodes, w.b0)
-    n_particles = sum(len(p) for p in sp_pts)
+    n_particles = sum(len(p) for p in pts)
+    setup_s = time.perf_counter() - t_setup
     part_t, pois_t = [], []
     t_start = time.perf_counter()
     it = 0
@@ -180,15 +179,16 @@ def cpu_reference_run(w, scale, max_seconds, min_steps=2, max_steps=None, steps=
         if steps is not None:
             if it >= steps:
                 break
-        elif (it >= min_steps and time.perf_counter() - t_start > max_seconds) or (
-                max_steps and it >= max_steps):
+        elif it >= min_steps and sum(part_t) > max_seconds:
             break
     value = n_particles * len(part_t) / sum(part_t)
-    sample = (f"{w.name} at 1/{scale} scale per axis: {nx}x{ny} cells, {n_particles} particles "
-              f"(same per-cell densities, blob and electrode scaled), {len(part_t)} steps of the "
-              f"reference hashmap algorithm (deposit, mover, compaction, cleanup) on {threads} "
-              f"OpenMP threads; Poisson by SuperLU on one thread")
-    return value, 1e3 * statistics.mean(pois_t), sample, threads, part_t, n_particles
+    sample = (f"{w.name} at full size: {nx}x{ny} cells, {n_particles} particles, {len(part_t)} steps "
+              f"of the reference hashmap algorithm (deposit, mover, compaction, cleanup) on "
+              f"{threads} OpenMP threads, {probing} slots a bucket (fullest bucket {peak}); "
+              f"Poisson by SuperLU on one thread (factored once in {factor_s:.1f} s)")
+    return {"value": value, "poisson_ms": 1e3 * statistics.mean(pois_t), "part_t": part_t,
+            "sample": sample, "threads": threads, "cpu": cpu_model(), "n": n_particles,
+            "setup_s": setup_s, "factor_s": factor_s, "probing": probing}
 
 
 # ---------------------------------------------------------------------------
@@ -656,21 +656,22 @@ def main():
         if rank != 0:
             return 0
         w = workload(args.config)
-        # bounded sample per step: 1/4 scale per axis of the workload
-        scale = 4 if w.nx >= 512 else 1
-        steps = args.steps + args.warmup
-        value, pois_ms, sample, threads, part_t, n = cpu_reference_run(w, scale, 0, steps=steps)
-        timed = part_t[args.warmup:]
-        value = n * len(timed) / sum(timed)
+        # every step is one full step of the workload
+        r = cpu_reference_run(w, steps=args.steps + args.warmup)
+        timed = r["part_t"][args.warmup:]
+        value = r["n"] * len(timed) / sum(timed)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * sum(timed) / len(timed), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "impl": "reference",
-                "config": {"workload": describe(w), "parallelism": "host cores"},
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": sample},
-                "poisson": {"ms_per_step": pois_ms, "solver": "SuperLU (PARDISO restatement)"},
+                "config": {"workload": describe(w), "particles": r["n"],
+                           "parallelism": "host cores"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "port",
+                                 "cpu": r["cpu"], "sample": r["sample"]},
+                "poisson": {"ms_per_step": r["poisson_ms"], "solver": "SuperLU (PARDISO restatement)",
+                            "factor_s": r["factor_s"]},
+                "setup_s": r["setup_s"],
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -691,10 +692,10 @@ def main():
         if rank == 0:
             line["ensemble"] = ens
     if rank == 0 and not args.no_cpu_baseline:
-        scale = 4 if w.nx >= 512 else 1
-        value, pois_ms, sample, threads, _, _ = cpu_reference_run(w, scale, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": sample, "poisson_ms_per_step": pois_ms}
+        r = cpu_reference_run(w, max_seconds=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": r["threads"],
+                                "kind": "port", "cpu": r["cpu"], "sample": r["sample"],
+                                "poisson_ms_per_step": r["poisson_ms"]}
     if world > 1:
         import torch
         torch.distributed.barrier()

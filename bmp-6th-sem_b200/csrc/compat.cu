@@ -5,6 +5,8 @@
 // refreshed after every operator that changes them.
 #include <sys/stat.h>
 
+#include <cerrno>
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -24,6 +26,7 @@ struct Global {
     pic_ctx* ctx = nullptr;
     PicdatFile file;
     std::vector<double> rho, phi;
+    int status = PIC_OK;  // of the last void operator (diagnostics writers)
 };
 Global g;
 
@@ -89,16 +92,32 @@ bool ready() {
     return true;
 }
 
+// One grid as the reference's print* functions write it: GY lines of GX
+// "%lf" values, space separated.  Every write and the close are checked (a
+// full disk shows up at fclose at the latest).
 int write_grid(const std::string& path, int GX, int GY, const std::vector<double>& v,
                double scale) {
     FILE* fd = std::fopen(path.c_str(), "w");
-    if (!fd) return fail(PIC_ERR_IO, "cannot create " + path);
-    for (int i = 0; i < GY; ++i) {
-        for (int j = 0; j < GX - 1; ++j) std::fprintf(fd, "%lf ", v[(size_t)i * GX + j] * scale);
-        std::fprintf(fd, "%lf\n", v[(size_t)i * GX + GX - 1] * scale);
+    if (!fd) return fail(PIC_ERR_IO, "cannot create " + path + ": " + std::strerror(errno));
+    bool ok = true;
+    for (int i = 0; i < GY && ok; ++i) {
+        for (int j = 0; j < GX - 1 && ok; ++j)
+            ok = std::fprintf(fd, "%lf ", v[(size_t)i * GX + j] * scale) > 0;
+        ok = ok && std::fprintf(fd, "%lf\n", v[(size_t)i * GX + GX - 1] * scale) > 0;
     }
-    std::fclose(fd);
+    const int err = ok ? 0 : errno;
+    if (std::fclose(fd) != 0 && ok) return fail(PIC_ERR_IO, "cannot write " + path + ": " + std::strerror(errno));
+    if (!ok) return fail(PIC_ERR_IO, "cannot write " + path + ": " + std::strerror(err));
     return PIC_OK;
+}
+
+// mkdir that accepts an existing folder.
+int ensure_dir(const std::string& d) {
+    if (mkdir(d.c_str(), 0755) == 0 || errno == EEXIST) {
+        struct stat st;
+        if (stat(d.c_str(), &st) == 0 && S_ISDIR(st.st_mode)) return PIC_OK;
+    }
+    return fail(PIC_ERR_IO, "cannot create folder " + d + ": " + std::strerror(errno));
 }
 
 }  // namespace
@@ -208,38 +227,37 @@ void sycl_pic_update_fields_from_phi(void) {
 
 // printNumberDensity / printEnergy / printElectricField / printPhi
 // (src/utils.cpp:829-1025): one text grid per quantity under
-// dir/<quantity>/<iteration>, "%lf" values, space separated.
-void sycl_pic_print_diagnostics(const char* dir, int iteration) {
-    if (!ready() || !dir) return;
-    pic_ctx* c = g.ctx;
+// dir/<quantity>/<iteration>, "%lf" values, space separated.  The reference
+// prints a message and exits when a file cannot be created; this returns
+// PIC_ERR_IO (or the status of the failing read-back) instead.
+int pic_write_diagnostics(pic_ctx* c, const char* dir, int iteration, double scale_factor) {
+    if (!c || !dir) return fail(PIC_ERR_ARG, "pic_write_diagnostics: null argument");
     const int GX = c->GX, GY = c->GY;
     const size_t n = (size_t)c->nodes;
     const std::string it = std::to_string(iteration);
     const std::string d = dir;
-    std::vector<double> f0(n, 0.0), f1(n, 0.0), e0(n, 0.0), e1(n, 0.0), ex(n), ey(n);
-    pic_get_final_mesh(c, 0, f0.data());
-    pic_get_energy_mesh(c, 0, e0.data());
+    std::vector<double> f0(n, 0.0), f1(n, 0.0), e0(n, 0.0), e1(n, 0.0), ex(n), ey(n), phi(n);
+    PIC_TRY(pic_get_final_mesh(c, 0, f0.data()));
+    PIC_TRY(pic_get_energy_mesh(c, 0, e0.data()));
     if (c->cfg.num_species > 1) {
-        pic_get_final_mesh(c, 1, f1.data());
-        pic_get_energy_mesh(c, 1, e1.data());
+        PIC_TRY(pic_get_final_mesh(c, 1, f1.data()));
+        PIC_TRY(pic_get_energy_mesh(c, 1, e1.data()));
     }
     std::vector<pic_field> ef(n);
-    pic_get_efield(c, ef.data());
+    PIC_TRY(pic_get_efield(c, ef.data()));
     for (size_t i = 0; i < n; ++i) {
         ex[i] = ef[i].fx;
         ey[i] = ef[i].fy;
     }
-    std::vector<double> phi(n);
-    pic_get_phi(c, phi.data());
-    const double sf = g.file.scale_factor;
-    mkdir(d.c_str(), 0755);  // the output folder itself (an existing one is kept)
-    auto path = [&](const char* q) {
+    PIC_TRY(pic_get_phi(c, phi.data()));
+    PIC_TRY(ensure_dir(d));  // the output folder itself (an existing one is kept)
+    auto put = [&](const char* q, const std::vector<double>& v, double scale) {
         const std::string p = d + "/" + q;
-        mkdir(p.c_str(), 0755);
-        return p + "/" + it;
+        PIC_TRY(ensure_dir(p));
+        return write_grid(p + "/" + it, GX, GY, v, scale);
     };
-    write_grid(path("electronDensity"), GX, GY, f0, sf);
-    write_grid(path("ionDensity"), GX, GY, f1, sf);
+    PIC_TRY(put("electronDensity", f0, scale_factor));
+    PIC_TRY(put("ionDensity", f1, scale_factor));
     // temperature-like energy: 0.66667*E/(n+1); the reference's last electron
     // column divides by (energy+1) (src/utils.cpp printEnergy), kept as is
     std::vector<double> te(n), ti(n);
@@ -250,29 +268,53 @@ void sycl_pic_print_diagnostics(const char* dir, int iteration) {
             te[k] = 0.66667 * e0[k] / den0;
             ti[k] = 0.66667 * e1[k] / (f1[k] + 1.0);
         }
-    write_grid(path("electronenergy"), GX, GY, te, 1.0);
-    write_grid(path("ionenergy"), GX, GY, ti, 1.0);
-    write_grid(path("Ex"), GX, GY, ex, 1.0);
-    write_grid(path("Ey"), GX, GY, ey, 1.0);
-    write_grid(path("potential"), GX, GY, phi, 1.0);
+    PIC_TRY(put("electronenergy", te, 1.0));
+    PIC_TRY(put("ionenergy", ti, 1.0));
+    PIC_TRY(put("Ex", ex, 1.0));
+    PIC_TRY(put("Ey", ey, 1.0));
+    PIC_TRY(put("potential", phi, 1.0));
+    return PIC_OK;
+}
+
+// The reference's signature returns nothing; a failure leaves its reason in
+// pic_last_error() and in sycl_pic_last_status().
+void sycl_pic_print_diagnostics(const char* dir, int iteration) {
+    if (!ready() || !dir) {
+        g.status = PIC_ERR_STATE;
+        return;
+    }
+    g.status = pic_write_diagnostics(g.ctx, dir, iteration, g.file.scale_factor);
 }
 
 // Mesh_<s>.out: the final_mesh of each species (src/main.cpp:260-274).
 void sycl_pic_save_meshes(void) {
-    if (!ready()) return;
+    if (!ready()) {
+        g.status = PIC_ERR_STATE;
+        return;
+    }
     pic_ctx* c = g.ctx;
     std::vector<double> f((size_t)c->nodes);
-    for (int s = 0; s < c->cfg.num_species; ++s) {
-        if (pic_get_final_mesh(c, s, f.data()) != PIC_OK) continue;
-        FILE* fd = std::fopen(("Mesh_" + std::to_string(s) + ".out").c_str(), "w");
-        if (!fd) continue;
-        for (int y = 0; y < c->GY; ++y) {
-            for (int x = 0; x < c->GX; ++x) std::fprintf(fd, "%g ", f[(size_t)y * c->GX + x]);
-            std::fprintf(fd, "\n");
+    g.status = PIC_OK;
+    for (int s = 0; s < c->cfg.num_species && g.status == PIC_OK; ++s) {
+        g.status = pic_get_final_mesh(c, s, f.data());
+        if (g.status != PIC_OK) break;
+        const std::string path = "Mesh_" + std::to_string(s) + ".out";
+        FILE* fd = std::fopen(path.c_str(), "w");
+        if (!fd) {
+            g.status = fail(PIC_ERR_IO, "cannot create " + path + ": " + std::strerror(errno));
+            break;
         }
-        std::fclose(fd);
+        bool ok = true;
+        for (int y = 0; y < c->GY && ok; ++y) {
+            for (int x = 0; x < c->GX && ok; ++x) ok = std::fprintf(fd, "%g ", f[(size_t)y * c->GX + x]) > 0;
+            ok = ok && std::fprintf(fd, "\n") > 0;
+        }
+        if (std::fclose(fd) != 0 || !ok)
+            g.status = fail(PIC_ERR_IO, "cannot write " + path + ": " + std::strerror(errno));
     }
 }
+
+int sycl_pic_last_status(void) { return g.status; }
 
 void sycl_pic_finalize(void) {
     if (g.ctx) pic_destroy(g.ctx);

@@ -102,7 +102,8 @@ class HostPool {
     }
 
     void part(int i) {
-        const size_t per = ((n_ / parts_) + align_ - 1) / align_ * align_;
+        // ceil(n / parts) rounded up to the alignment: the parts cover [0, n)
+        const size_t per = ((n_ + parts_ - 1) / parts_ + align_ - 1) / align_ * align_;
         const size_t a = std::min(n_, per * (size_t)i), b = std::min(n_, per * (size_t)(i + 1));
         if (b > a) (*job_)(a, b);
     }
@@ -867,6 +868,15 @@ int pic_autotune(pic_ctx* c, int* shape_out, double* ms_per_shape) {
             std::fclose(f);
         }
     }
+    return PIC_OK;
+}
+
+int pic_debug_set_wait_limits(pic_ctx* c, int64_t barrier_polls, int64_t tensor_wait_cycles) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    PIC_CUDA(cudaSetDevice(c->cfg.device));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    PIC_TRY(poisson_set_spin_limit(barrier_polls));
+    PIC_TRY(ws_set_wait_limit(tensor_wait_cycles));
     return PIC_OK;
 }
 

@@ -275,6 +275,8 @@ void ws_free(pic_ctx* c);
 bool ws_tracking(const pic_ctx* c);  // hooks must run at every solve
 int ws_before_solve(pic_ctx* c, bool want_guess);  // 1 when a guess is in ps.net_guess
 int ws_check_fault();  // after a synchronisation: PIC_ERR_TIMEOUT if a warm-start kernel gave up
+int ws_set_wait_limit(int64_t cycles);     // tensor-core pipeline wait bound (<= 0: default)
+int poisson_set_spin_limit(int64_t polls); // batched-solve barrier poll bound (<= 0: default)
 int ws_after_solve(pic_ctx* c, bool record);
 
 // poisson.cu

@@ -1159,6 +1159,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 // *err and lets the block go on, so a fault can never hang the GPU (the
 // host then reports PIC_ERR_TIMEOUT).
 constexpr unsigned kSpinLimit = 1u << 26;
+__device__ unsigned g_spin_limit = kSpinLimit;  // a test lowers it to make the barriers give up
 
 struct GroupBarrier {
     unsigned* ctr;
@@ -1172,8 +1173,9 @@ struct GroupBarrier {
             __threadfence();
             atomicAdd(ctr, 1u);
             unsigned polls = 0;
+            const unsigned limit = g_spin_limit;
             while (ld_acquire(ctr) < target) {
-                if (++polls > kSpinLimit) {
+                if (++polls > limit) {
                     atomicExch(err, 1);
                     break;
                 }
@@ -1414,7 +1416,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
             const uint8_t* __restrict__ mk = I->mask;
             const int nn = (int)I->sn;
 #pragma unroll 4
-            for (int k = (int)ltid; k < nn; k += (int)lsize) pv[k] = mk[k] ? 0.0 : zv[k] + beta * pv[k];
+            // (the first iteration does not read p: what a solve that gave up
+            // left there, NaN included, never reaches the next one)
+            for (int k = (int)ltid; k < nn; k += (int)lsize)
+                pv[k] = mk[k] ? 0.0 : (beta == 0.0 ? zv[k] : zv[k] + beta * pv[k]);
         }
         grid.sync();
         if (on) {
@@ -1576,6 +1581,14 @@ int poisson_batch_launch(const void* dev_insts, int n, const int* inst_of, doubl
                     (void*)&err};
     PIC_CUDA(cudaLaunchCooperativeKernel((const void*)k_poisson_batch, dim3(blocks), dim3(kFusedThreads),
                                          args, smem, st));
+    return PIC_OK;
+}
+
+// Poll bound of the batched solve's barriers on the current device; polls <=
+// 0 restores the default.
+int poisson_set_spin_limit(int64_t polls) {
+    const unsigned v = polls > 0 ? (unsigned)std::min<int64_t>(polls, kSpinLimit) : kSpinLimit;
+    PIC_CUDA(cudaMemcpyToSymbol(g_spin_limit, &v, sizeof(v)));
     return PIC_OK;
 }
 

@@ -31,6 +31,7 @@
 // outer layers on the FP32 cores.
 // Weight gradients are reduced through per-block partials in a fixed order,
 // so training is deterministic.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -291,13 +292,17 @@ constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) <
 static_assert(kTcSmem <= 227 * 1024, "shared memory of one CTA");
 
 __device__ int g_ws_fault;  // a bounded wait of the warm-start kernels gave up
+// Bound of the tensor-core kernels' pipeline waits, in SM clock cycles (about
+// a second by default); a test lowers it to make the waits give up.
+constexpr long long kWsWaitCycles = 1ll << 31;
+__device__ long long g_ws_wait_cycles = kWsWaitCycles;
 
 __device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit) {
     const long long t0 = clock64();
     for (;;) {
         uint32_t done;
@@ -307,7 +312,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > (1ll << 31)) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -347,10 +352,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
                                                       __nv_bfloat16* __restrict__ out,
                                                       __nv_bfloat16* __restrict__ pool_out) {
     extern __shared__ __align__(16) unsigned char smem[];
-    // head: full[4] @0, empty[4] @32, acc_full[2] @64, acc_empty[2] @80, TMEM address @96, abort @100
+    // head: full[4] @0, empty[4] @32, acc_full[2] @64, acc_empty[2] @80, TMEM address @96, abort @100,
+    // drain @104 (the MMA warp's last commit: every MMA issued has completed)
     static_assert(kTcStages <= 4, "barrier head layout");
     const uint32_t sbase = smem_u32(smem);
     const uint32_t full0 = sbase, empty0 = sbase + 32, accf0 = sbase + 64, acce0 = sbase + 80;
+    const uint32_t drain = sbase + 104;
+    const long long wl = g_ws_wait_cycles;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 96);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 100);
     unsigned char* wsm = smem + kTcHead;
@@ -374,6 +382,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
             mbar_init(accf0 + 8 * a, 1);
             mbar_init(acce0 + 8 * a, kTcEpi / 32);
         }
+        mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -392,7 +401,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
         int k = 0;
         for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
             const int s = k % kTcStages;
-            if (k >= kTcStages && !mbar_wait_bounded(empty0 + 8 * s, ((k / kTcStages) & 1) ^ 1)) {
+            if (k >= kTcStages && !mbar_wait_bounded(empty0 + 8 * s, ((k / kTcStages) & 1) ^ 1, wl)) {
                 give_up();
                 break;
             }
@@ -425,14 +434,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
         if (lane == 0) {
             const uint64_t bd = tc_desc(smem_u32(wsm), 512, 128);
             int k = 0;
+            bool quit = false;
             for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
                 const int s = k % kTcStages, a = k & 1;
-                if (!mbar_wait_bounded(full0 + 8 * s, (k / kTcStages) & 1) ||
-                    (k >= 2 && !mbar_wait_bounded(acce0 + 8 * a, ((k >> 1) & 1) ^ 1))) {
+                if (!mbar_wait_bounded(full0 + 8 * s, (k / kTcStages) & 1, wl) ||
+                    (k >= 2 && !mbar_wait_bounded(acce0 + 8 * a, ((k >> 1) & 1) ^ 1, wl))) {
                     give_up();
+                    quit = true;
                     break;
                 }
-                if (*abort_flag) break;
+                if (*abort_flag) {
+                    quit = true;
+                    break;
+                }
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 // descriptors differ only in the start address field (addresses >> 4 stay below 2^14)
                 const uint64_t ad = tc_desc(smem_u32(ring + s * kTcHalo), kTcPlane, 128);
@@ -453,6 +467,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
                 tc_commit(empty0 + 8 * s);
                 tc_commit(accf0 + 8 * a);
             }
+            // Leaving early, MMAs whose accumulator the epilogue will not
+            // wait for may still be running: no MMA may write TMEM when it is
+            // freed below.  One more commit tracks every MMA issued; its wait
+            // has the fixed bound, not the test's.  (On the normal path the
+            // epilogue has waited for every accumulator.)
+            if (quit) {
+                tc_commit(drain);
+                if (!mbar_wait_bounded(drain, 0, kWsWaitCycles)) atomicExch(&g_ws_fault, 1);
+            }
         }
         __syncwarp();
     } else {
@@ -466,7 +489,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16
         int k = 0;
         for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
             const int a = k & 1;
-            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * a, (k >> 1) & 1));
+            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * a, (k >> 1) & 1, wl));
             if (!ok && lane == 0) give_up();
             __nv_bfloat16* st = reinterpret_cast<__nv_bfloat16*>(stage0 + (k & 1) * kTcStage);
             if (ok) {
@@ -551,6 +574,386 @@ __global__ void k_up_add8(const __nv_bfloat16* coarse, const __nv_bfloat16* skip
     uint4 v = reinterpret_cast<const uint4*>(skip)[i];
     add_bf16x8(v, *reinterpret_cast<const uint4*>(coarse + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + q * 8));
     reinterpret_cast<uint4*>(u)[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Row-streaming 32->32 convolution on tcgen05 (the forward 32->32 layers).
+//
+// Implicit GEMM with the pixels of one input row as M and (column tap dx,
+// output channel co) as N.  For output row y of a column strip whose first
+// output column is x0 (a multiple of 126), tile pixel i = 0..127 being input
+// column x0 - 1 + i:
+//   D[i][32 dx + co] = sum_{dy, ci} in[y + dy - 1][x0 - 1 + i][ci] W[dy][dx][ci][co]
+// -- six MMAs of M = 128, N = 96, K = 16 (three row taps x two halves of the
+// input channels), FP32 accumulators in TMEM.  The column taps are summed in
+// the epilogue, where TMEM lane i holds tile pixel i:
+//   out[y][x0 + j][co] = D[j][co] + D[j + 1][32 + co] + D[j + 2][64 + co],
+// the neighbours' values taken by warp shuffles (and across the four warps
+// of a warpgroup through shared memory).  126 outputs a strip row.
+//
+// Every input row is loaded once by TMA (four boxes of 8 channels x 128
+// pixels, zero filled outside the image) into a ring of row slots and used
+// by three consecutive output rows: each CTA walks down its share of the
+// (strip, row) units.  Roles, 12 warps:
+//   warp 0   TMA producer (one lane);
+//   warp 1   TMEM allocation, MMA issue (one lane);
+//   warps 4-7 and 8-11  two epilogue warpgroups, each taking output rows in
+//            pairs (2m, 2m + 1) with accumulators 2e, 2e + 1 (four in TMEM):
+//            bias, relu, bf16 store and, for the encoder layers, the 2x2
+//            average pool of the pair.
+// Every wait is bounded (g_ws_wait_cycles); a role that gives up records
+// g_ws_fault, the CTA's roles leave their loops together, the MMA lane waits
+// (fixed bound) for the MMAs it issued and the producer for its copies before
+// the tensor memory is freed.
+// ---------------------------------------------------------------------------
+constexpr int kRwStrip = 126;                 // output columns a strip
+constexpr int kRwSlots = 8;                   // input row slots
+constexpr int kRwRowBytes = 4 * 128 * 16;     // one input row: 4 boxes [128 px][8 ch] bf16
+constexpr int kRwWBytes = 6 * 2 * 96 * 16;    // weights: [dy][kc][g][n 96][8 ci] bf16
+constexpr int kRwThreads = 12 * 32;
+// shared memory: head @0 (full[8] @0, empty[8] @64, accf[4] @128, acce[4]
+// @160, drain @192, TMEM address @200, abort @204), weights @1024, row slots
+// (1024-aligned), edge exchange [wg][buf][side][warp][16] floats, bias
+constexpr int kRwXchg = 2 * 2 * 2 * 4 * 16 * 4;
+constexpr int kRwOffW = 1024;
+constexpr int kRwOffRows = kRwOffW + kRwWBytes;
+constexpr int kRwOffX = kRwOffRows + kRwSlots * kRwRowBytes;
+constexpr int kRwOffBias = kRwOffX + kRwXchg;
+constexpr int kRwSmemUsed = kRwOffBias + 32 * 4;
+static_assert(kRwOffRows % 1024 == 0, "row slots 1024-aligned");
+// more than half an SM's shared memory: one CTA an SM (its TMEM is all 512 columns)
+constexpr int kRwSmem = 120 * 1024;
+static_assert(kRwSmemUsed + 1024 <= kRwSmem, "row-conv shared memory");
+// kind::f16: FP32 accumulator, bf16 A and B, both K-major, N = 96, M = 128
+constexpr uint32_t kRwIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((96u >> 3) << 17) | ((128u >> 4) << 24);
+
+struct RowConvArgs {
+    const __nv_bfloat16* w;   // packed [dy][kc][g][n][8]
+    const float* bias;        // [32]
+    __nv_bfloat16* out;       // [P][P][32]
+    __nv_bfloat16* pool;      // [P/2][P/2][32] or null
+    int P;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void rw_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kRwIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The CTA's share of the (strip, row) units [g0, g1), in pairs of rows when
+// pooling (P is a multiple of 4, so a pair never straddles two strips).
+__device__ __forceinline__ void rw_share(int units, int pool, int& g0, int& g1) {
+    const int b = blockIdx.x, n = gridDim.x;
+    g0 = (int)(((int64_t)units * b) / n);
+    g1 = (int)(((int64_t)units * (b + 1)) / n);
+    if (pool) {
+        g0 &= ~1;
+        g1 = b + 1 == n ? units : (g1 & ~1);
+    }
+}
+
+__global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_constant__ CUtensorMap tmap,
+                                                            RowConvArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // offsets below are from the first 1024-byte boundary of the buffer
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t full0 = sbase, empty0 = sbase + 64, accf0 = sbase + 128, acce0 = sbase + 160;
+    const uint32_t drain = sbase + 192;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 200);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 204);
+    unsigned char* wsm = smem + kRwOffW;
+    unsigned char* rows = smem + kRwOffRows;
+    float* xch = reinterpret_cast<float*>(smem + kRwOffX);
+    float* sbias = reinterpret_cast<float*>(smem + kRwOffBias);
+    const long long wl = g_ws_wait_cycles;
+    const int P = A.P;
+    const int strips = (P + kRwStrip - 1) / kRwStrip;
+    const int units = strips * P;
+    const int pool = A.pool != nullptr;
+    int g0, g1;
+    rw_share(units, pool, g0, g1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kRwSlots; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int a = 0; a < 4; ++a) {
+            mbar_init(accf0 + 8 * a, 1);
+            mbar_init(acce0 + 8 * a, 4);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    // weights and bias into shared memory (generic stores, then a fence to
+    // the async proxy the MMAs read through)
+    for (int i = threadIdx.x; i < kRwWBytes / 16; i += kRwThreads)
+        reinterpret_cast<uint4*>(wsm)[i] = reinterpret_cast<const uint4*>(A.w)[i];
+    if (threadIdx.x < 32) sbias[threadIdx.x] = A.bias[threadIdx.x];
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+    auto give_up = [&]() {
+        if (!*abort_flag) atomicExch(&g_ws_fault, 1);
+        *abort_flag = 1;
+    };
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int ld = 0;
+            bool quit = false;
+            for (int g = g0; g < g1 && !quit;) {
+                const int strip = g / P, r0 = g % P, r1 = min(P, r0 + (g1 - g));
+                const int x0 = strip * kRwStrip;
+                for (int i = 0; i < r1 - r0 + 2; ++i, ++ld) {
+                    const int s = ld % kRwSlots;
+                    if (ld >= kRwSlots && !mbar_wait_bounded(empty0 + 8 * s, ((ld / kRwSlots) & 1) ^ 1, wl)) {
+                        give_up();
+                        quit = true;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        quit = true;
+                        break;
+                    }
+                    const uint32_t dst = smem_u32(rows + s * kRwRowBytes);
+                    mbar_expect_tx(full0 + 8 * s, kRwRowBytes);
+#pragma unroll
+                    for (int gch = 0; gch < 4; ++gch)
+                        tma_load_3d(dst + gch * 2048, &tmap, 8 * gch, x0 - 1, r0 - 1 + i, full0 + 8 * s);
+                }
+                g += r1 - r0;
+            }
+            // every copy issued has landed before the CTA leaves (the last
+            // use of each slot; fixed bound)
+            for (int j = max(0, ld - kRwSlots); j < ld; ++j)
+                if (!mbar_wait_bounded(full0 + 8 * (j % kRwSlots), (j / kRwSlots) & 1, kWsWaitCycles))
+                    atomicExch(&g_ws_fault, 1);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMA issue ----------------
+        if (lane == 0) {
+            const uint32_t rows_u32 = smem_u32(rows), w_u32 = smem_u32(wsm);
+            int ld = 0, o = 0, waited = 0;  // loads [0, waited) are known to have landed
+            bool quit = false;
+            for (int g = g0; g < g1 && !quit;) {
+                const int r0 = g % P, r1 = min(P, r0 + (g1 - g)), n = r1 - r0;
+                for (int j = 0; j < n; ++j, ++o) {
+                    for (; waited < ld + j + 3 && !quit; ++waited)
+                        if (!mbar_wait_bounded(full0 + 8 * (waited % kRwSlots), (waited / kRwSlots) & 1, wl)) {
+                            give_up();
+                            quit = true;
+                        }
+                    const int q = o & 3;
+                    if (!quit && o >= 4 && !mbar_wait_bounded(acce0 + 8 * q, ((o >> 2) & 1) ^ 1, wl)) {
+                        give_up();
+                        quit = true;
+                    }
+                    if (quit || *abort_flag) {
+                        quit = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+                    for (int dy = 0; dy < 3; ++dy) {
+                        const uint32_t rb = rows_u32 + ((ld + j + dy) % kRwSlots) * kRwRowBytes;
+#pragma unroll
+                        for (int kc = 0; kc < 2; ++kc)
+                            rw_mma(tmem + q * 128, tc_desc(rb + kc * 4096, 2048, 128),
+                                   tc_desc(w_u32 + (dy * 2 + kc) * 3072, 1536, 128), (dy | kc) ? 1u : 0u);
+                    }
+                    tc_commit(accf0 + 8 * q);
+                    tc_commit(empty0 + 8 * ((ld + j) % kRwSlots));  // row y - 1 is done with
+                }
+                if (quit) break;
+                tc_commit(empty0 + 8 * ((ld + n) % kRwSlots));
+                tc_commit(empty0 + 8 * ((ld + n + 1) % kRwSlots));
+                ld += n + 2;
+                g += n;
+            }
+            if (quit) {  // MMAs the epilogue will not wait for may still run
+                tc_commit(drain);
+                if (!mbar_wait_bounded(drain, 0, kWsWaitCycles)) atomicExch(&g_ws_fault, 1);
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // ---------------- epilogue ----------------
+        const int e = (warp - 4) >> 2;    // warpgroup
+        const int wq = warp & 3;          // TMEM lanes 32 wq .. 32 wq + 31
+        const int t = 32 * wq + lane;     // tile pixel
+        const int Q = P / 2;
+        float* xl = xch + (e * 2) * 2 * 4 * 16;  // [buf][side][warp][16]
+        uint32_t prev[16];                       // even row of a pooled pair, bf16x2
+        int o = 0;
+        bool quit = false;
+        for (int g = g0; g < g1 && !quit;) {
+            const int strip = g / P, r0 = g % P, r1 = min(P, r0 + (g1 - g)), n = r1 - r0;
+            const int x0 = strip * kRwStrip;
+            const int x = x0 + t - 1;
+            const bool valid = t >= 1 && t <= kRwStrip && x < P;
+            for (int j = 0; j < n; ++j, ++o) {
+                if (((o >> 1) & 1) != e) continue;
+                const int q = o & 3, y = r0 + j;
+                const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * q, (o >> 2) & 1, wl));
+                if (!ok && lane == 0) give_up();
+                uint32_t qq;
+                asm volatile(
+                    "{\n.reg .pred p, r;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred r, %2, 128, p;\nselp.u32 %0, 1, 0, r;\n}\n"
+                    : "=r"(qq)
+                    : "r"((!ok || *abort_flag) ? 1u : 0u), "r"(1 + e)
+                    : "memory");
+                if (qq) {
+                    quit = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                float* xb = xl + (o & 1) * 2 * 4 * 16;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    float v0[16], v1[16], v2[16];
+                    const uint32_t ta = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)(q * 128 + 16 * h);
+                    tc_ld16(ta, v0);
+                    tc_ld16(ta + 32, v1);
+                    tc_ld16(ta + 64, v2);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                    if (h == 1) {
+                        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(acce0 + 8 * q);
+                    }
+                    // the warp's edge values for its neighbours
+                    if (lane == 31)
+#pragma unroll
+                        for (int c = 0; c < 16; ++c) xb[(0 * 4 + wq) * 16 + c] = v0[c];
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < 16; ++c) xb[(1 * 4 + wq) * 16 + c] = v2[c];
+                    asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
+                    float r[16];
+#pragma unroll
+                    for (int c = 0; c < 16; ++c) {
+                        float l = __shfl_up_sync(kFull, v0[c], 1);
+                        float rr = __shfl_down_sync(kFull, v2[c], 1);
+                        if (lane == 0) l = wq > 0 ? xb[(0 * 4 + wq - 1) * 16 + c] : 0.f;
+                        if (lane == 31) rr = wq < 3 ? xb[(1 * 4 + wq + 1) * 16 + c] : 0.f;
+                        r[c] = fmaxf(l + v1[c] + rr + sbias[16 * h + c], 0.f);
+                    }
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) pk[c] = pack_bf16x2(r[2 * c], r[2 * c + 1]);
+                    if (valid) {
+                        uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
+                        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                    }
+                    if (pool) {
+                        if ((y & 1) == 0) {
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) prev[8 * h + c] = pk[c];
+                        } else {
+                            // 0.25 (v(y-1, x) + v(y-1, x+1) + v(y, x) + v(y, x+1)) of the bf16 values
+                            float s[16];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) {
+                                const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&prev[8 * h + c]));
+                                const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[c]));
+                                s[2 * c] = a.x;
+                                s[2 * c + 1] = a.y;
+                                r[2 * c] = b.x;
+                                r[2 * c + 1] = b.y;
+                            }
+                            // right neighbour's pair (lane 31: the next warp's lane 0, via xb)
+                            asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
+                            if (lane == 0)
+#pragma unroll
+                                for (int c = 0; c < 16; ++c) {
+                                    xb[(0 * 4 + wq) * 16 + c] = s[c];
+                                    xb[(1 * 4 + wq) * 16 + c] = r[c];
+                                }
+                            asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
+                            uint32_t pp[8];
+#pragma unroll
+                            for (int c = 0; c < 16; c += 2) {
+                                float sa = __shfl_down_sync(kFull, s[c], 1), sb = __shfl_down_sync(kFull, s[c + 1], 1);
+                                float ra = __shfl_down_sync(kFull, r[c], 1), rb = __shfl_down_sync(kFull, r[c + 1], 1);
+                                if (lane == 31 && wq < 3) {
+                                    sa = xb[(0 * 4 + wq + 1) * 16 + c];
+                                    sb = xb[(0 * 4 + wq + 1) * 16 + c + 1];
+                                    ra = xb[(1 * 4 + wq + 1) * 16 + c];
+                                    rb = xb[(1 * 4 + wq + 1) * 16 + c + 1];
+                                }
+                                pp[c / 2] = pack_bf16x2(0.25f * (s[c] + sa + r[c] + ra),
+                                                        0.25f * (s[c + 1] + sb + r[c + 1] + rb));
+                            }
+                            if (valid && (x & 1) == 0 && (x >> 1) < Q) {
+                                uint4* dst = reinterpret_cast<uint4*>(A.pool + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + 16 * h);
+                                dst[0] = make_uint4(pp[0], pp[1], pp[2], pp[3]);
+                                dst[1] = make_uint4(pp[4], pp[5], pp[6], pp[7]);
+                            }
+                        }
+                    }
+                    // the exchange slots are reused by the next half / row
+                    asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
+                }
+            }
+            g += n;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem) : "memory");
+    }
+}
+
+// FP32 masters [tap][ci][co] of one 32->32 layer -> the B operand layout
+// [dy][kc][g][n = 32 dx + co][8 ci] in bf16 (ci = 16 kc + 8 g + e).
+__global__ void k_pack_rows_w(const float* w, __nv_bfloat16* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 6 * 2 * 96 * 8) return;
+    const int e = i & 7, n = (i >> 3) % 96, gk = i / (8 * 96);  // gk = (dy * 2 + kc) * 2 + g
+    const int g = gk & 1, kc = (gk >> 1) & 1, dy = gk >> 2;
+    const int dx = n / 32, co = n % 32, ci = 16 * kc + 8 * g + e;
+    out[i] = __float2bfloat16_rn(w[((dy * 3 + dx) * C + ci) * C + co]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1120,6 +1523,10 @@ struct Net {
     // bf16 B fragments of the input and output convolutions (k_pack_frags)
     uint2* in_frag = nullptr;
     uint2* out_frag = nullptr;
+    // the forward 32->32 layers' weights in k_conv_rows' B layout, and the
+    // TMA descriptors of their inputs (a1, p1, a3, p2, a5, u1, a7, u0, a9)
+    __nv_bfloat16* wrows = nullptr;
+    CUtensorMap tm_in[9];
     // activations (P = fine, Q = P/2, R = P/4)
     __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
     float* out = nullptr;
@@ -1155,7 +1562,7 @@ static int64_t param_off(int block) {
 
 static void net_free(Net& N) {
     cudaFree(N.w); cudaFree(N.m); cudaFree(N.v); cudaFree(N.g);
-    cudaFree(N.w16); cudaFree(N.w16t); cudaFree(N.in_frag); cudaFree(N.out_frag);
+    cudaFree(N.w16); cudaFree(N.w16t); cudaFree(N.in_frag); cudaFree(N.out_frag); cudaFree(N.wrows);
     cudaFree(N.x0);
     for (auto* p : N.a) cudaFree(p);
     cudaFree(N.p1); cudaFree(N.p2); cudaFree(N.u0); cudaFree(N.u1); cudaFree(N.out);
@@ -1196,6 +1603,34 @@ struct pic_ws {
 };
 
 namespace picb200 {
+
+// TMA descriptor of an NHWC bf16 image of P x P pixels and 32 channels,
+// read in boxes of 8 channels x 128 pixels x 1 row (zero filled outside).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P) {
+    static EncodeTiledFn encode = nullptr;
+    if (!encode) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !f)
+            return fail(PIC_ERR_CUDA, "warm start: cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<EncodeTiledFn>(f);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)P, (cuuint64_t)P};
+    const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)P * C * 2};
+    const cuuint32_t box[3] = {8, 128, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dims,
+                              strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(PIC_ERR_CUDA, "warm start: TMA descriptor encoding failed (" + std::to_string((int)r) + ")");
+    return PIC_OK;
+}
 
 static int ws_alloc(pic_ctx* c) {
     if (c->ws) return PIC_OK;
@@ -1247,6 +1682,14 @@ static int ws_alloc(pic_ctx* c) {
     PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
     PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     PIC_CUDA(cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    PIC_CUDA(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kRwSmem));
+    if (cudaMalloc(&N.wrows, (size_t)kNumConv32 * kRwWBytes))
+        return fail(PIC_ERR_CUDA, "warm start: parameter allocation failed");
+    {
+        const __nv_bfloat16* ins[9] = {N.a[1], N.p1, N.a[3], N.p2, N.a[5], N.u1, N.a[7], N.u0, N.a[9]};
+        const int sz[9] = {(int)P, (int)Q, (int)Q, (int)R, (int)R, (int)Q, (int)Q, (int)P, (int)P};
+        for (int l = 0; l < 9; ++l) PIC_TRY(make_row_tmap(&N.tm_in[l], ins[l], sz[l]));
+    }
     PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
     return PIC_OK;
 }
@@ -1296,7 +1739,10 @@ static int ws_pack(pic_ctx* c) {
                                                                        N.w16, N.w16t);
     k_pack_frags<<<g1((kInSteps * 4 + kOutSteps) * 32), 256, 0, c->stream>>>(
         N.w, N.w + param_off(kNumConv32 + 1), N.in_frag, N.out_frag);
-    c->launches += 2;
+    for (int l = 0; l < kNumConv32; ++l)
+        k_pack_rows_w<<<g1(kRwWBytes / 2), 256, 0, c->stream>>>(N.w + param_off(l + 1),
+                                                                 N.wrows + (int64_t)l * (kRwWBytes / 2));
+    c->launches += 2 + kNumConv32;
     PIC_CUDA(cudaGetLastError());
     N.packed = true;
     return PIC_OK;
@@ -1333,10 +1779,42 @@ static void conv32_tc(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloa
         in, N.w16 + (int64_t)layer * kW32, N.w + param_off(layer + 1) + kW32, P, out, pool_out);
 }
 
+// Forward 32->32 convolution `layer` on the row-streaming tcgen05 kernel,
+// its input being the layer's TMA descriptor's image; the decoder's
+// upsample-and-skip sum u = up2(up) + skip is formed first when `up` is given.
+static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfloat16* pool,
+                      const __nv_bfloat16* up = nullptr, const __nv_bfloat16* skip = nullptr,
+                      __nv_bfloat16* u = nullptr) {
+    Net& N = c->ws->net;
+    if (up) {
+        k_up_add8<<<g1((int64_t)P * P * 4), 256, 0, c->stream>>>(up, skip, P, u);
+        c->launches += 1;
+    }
+    const int units = ((P + kRwStrip - 1) / kRwStrip) * P;
+    // at least 16 rows a CTA: the two halo rows of a CTA's share stay small
+    const int grid = std::max(1, std::min(N.sms, units / 16));
+    RowConvArgs A;
+    A.w = N.wrows + (int64_t)layer * (kRwWBytes / 2);
+    A.bias = N.w + param_off(layer + 1) + kW32;
+    A.out = out;
+    A.pool = pool;
+    A.P = P;
+    k_conv_rows<<<grid, kRwThreads, kRwSmem, c->stream>>>(N.tm_in[layer], A);
+    c->launches += 1;
+}
+
 // The solve's guess buffer, allocated when a network becomes usable (so
 // that no allocation falls inside a timed solve).
 static int ws_guess_buffer(pic_ctx* c) {
     if (!c->ps.net_guess) PIC_CUDA(cudaMalloc(&c->ps.net_guess, (size_t)c->nodes * 4));
+    return PIC_OK;
+}
+
+// Bound of the tensor-core kernels' waits on the current device; cycles <= 0
+// restores the default.
+int ws_set_wait_limit(int64_t cycles) {
+    const long long v = cycles > 0 ? (long long)cycles : kWsWaitCycles;
+    PIC_CUDA(cudaMemcpyToSymbol(g_ws_wait_cycles, &v, sizeof(v)));
     return PIC_OK;
 }
 
@@ -1381,18 +1859,18 @@ static void forward(pic_ctx* c) {
     const int P = N.P, Q = P / 2, R = P / 4;
     const dim3 gP((P + TW - 1) / TW, (P + TH - 1) / TH);
     k_conv_in<<<gP, 256, 0, c->stream>>>(N.xin, N.in_frag, N.w + kInW, P, N.a[1]);
-    conv32_tc(c, 0, N.a[1], N.a[2], P, nullptr, nullptr, N.p1);
-    conv32_tc(c, 1, N.p1, N.a[3], Q);
-    conv32_tc(c, 2, N.a[3], N.a[4], Q, nullptr, nullptr, N.p2);
-    conv32_tc(c, 3, N.p2, N.a[5], R);
-    conv32_tc(c, 4, N.a[5], N.a[6], R);
-    conv32_tc(c, 5, N.a[4], N.a[7], Q, N.a[6], N.u1);
-    conv32_tc(c, 6, N.a[7], N.a[8], Q);
-    conv32_tc(c, 7, N.a[2], N.a[9], P, N.a[8], N.u0);
-    conv32_tc(c, 8, N.a[9], N.a[10], P);
+    conv_rows(c, 0, N.a[2], P, N.p1);
+    conv_rows(c, 1, N.a[3], Q, nullptr);
+    conv_rows(c, 2, N.a[4], Q, N.p2);
+    conv_rows(c, 3, N.a[5], R, nullptr);
+    conv_rows(c, 4, N.a[6], R, nullptr);
+    conv_rows(c, 5, N.a[7], Q, nullptr, N.a[6], N.a[4], N.u1);
+    conv_rows(c, 6, N.a[8], Q, nullptr);
+    conv_rows(c, 7, N.a[9], P, nullptr, N.a[8], N.a[2], N.u0);
+    conv_rows(c, 8, N.a[10], P, nullptr);
     const int64_t ob = param_off(kNumConv32 + 1);
     k_conv_out<<<gP, 256, 0, c->stream>>>(N.a[10], N.out_frag, N.w + ob + kOutW, P, N.out);
-    c->launches += 11;
+    c->launches += 2;
 }
 
 // Loss of the guess N.out against the scaled right-hand-side change rhs

@@ -163,6 +163,8 @@ def lib():
         "pic_autotune": (cint, [vp, P(cint), P(dbl)]),
         "pic_ws_debug_step": (cint, [vp, vp, vp, vp, vp, P(dbl)]),
         "pic_deposit_points_noalloc": (cint, [vp, i64, i32, i32, dbl, dbl, vp, dbl, dbl, vp, vp, vp]),
+        "pic_write_diagnostics": (cint, [vp, ctypes.c_char_p, cint, dbl]),
+        "pic_debug_set_wait_limits": (cint, [vp, i64, i64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -363,6 +365,10 @@ class Pic:
     def set_bz(self, bz: np.ndarray):
         bz = np.ascontiguousarray(bz, dtype=np.float64)
         _check(lib().pic_set_bz(self.h, _p(bz)))
+
+    def write_diagnostics(self, directory: str, iteration: int, scale_factor: float = 1.0):
+        """The reference's text snapshots (pic_write_diagnostics)."""
+        _check(lib().pic_write_diagnostics(self.h, directory.encode(), iteration, scale_factor))
 
     def set_poisson(self, solver=SOLVER_MG_PCG, warm=WARM_PREVIOUS, tol=1e-8, maxit=500):
         _check(lib().pic_set_poisson(self.h, solver, warm, tol, maxit))

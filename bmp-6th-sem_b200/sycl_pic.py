@@ -50,6 +50,7 @@ def _lib():
             "sycl_pic_cleanup_map": (dbl, [cint]), "sycl_pic_generate_new_particles": (dbl, []),
             "sycl_pic_update_fields_from_phi": (None, []),
             "sycl_pic_print_diagnostics": (None, [cp, cint]), "sycl_pic_save_meshes": (None, []),
+            "sycl_pic_last_status": (cint, []),
             "sycl_pic_finalize": (None, []),
         }
         for name, (res, args) in sig.items():
@@ -167,12 +168,21 @@ def generate_new_particles() -> float:
     return _checked_seconds(_lib().sycl_pic_generate_new_particles(), "generate_new_particles")
 
 
+def _checked_status(what: str) -> None:
+    if _lib().sycl_pic_last_status() != 0:
+        _err(what)
+
+
 def print_diagnostics(directory: str, iteration: int) -> None:
+    """Text snapshots (printNumberDensity/printEnergy/printElectricField/
+    printPhi); raises where the reference would print and exit."""
     _lib().sycl_pic_print_diagnostics(directory.encode(), int(iteration))
+    _checked_status("print_diagnostics")
 
 
 def save_meshes() -> None:
     _lib().sycl_pic_save_meshes()
+    _checked_status("save_meshes")
 
 
 def dump_rho_phi_cpp(prefix: str) -> None:

@@ -234,6 +234,14 @@ int pic_set_phi(pic_ctx* ctx, const double* host);
  * (calculateElectricField, src/poissonSolver.cpp:433-456). */
 int pic_update_fields_from_phi(pic_ctx* ctx);
 int pic_set_bz(pic_ctx* ctx, const double* host);
+/* The reference's text snapshots (printNumberDensity, printEnergy,
+ * printElectricField, printPhi: src/utils.cpp:829-991): one file per
+ * quantity, dir/<quantity>/<iteration>, GRID_Y lines of GRID_X "%lf" values
+ * separated by single spaces, for electronDensity and ionDensity (final_mesh
+ * times scale_factor), electronenergy and ionenergy (0.66667 energy/(n+1)),
+ * Ex, Ey and potential.  Folders are created as needed.  PIC_ERR_IO when a
+ * folder or file cannot be created or written (the reference exits). */
+int pic_write_diagnostics(pic_ctx* ctx, const char* dir, int iteration, double scale_factor);
 
 /* ---- instrumentation (no reference counterpart; the reference returns
  * host wall seconds per operator, src/sycl_pic_ctypes.cpp:127-236) ------- */
@@ -250,6 +258,16 @@ int pic_set_profiling(pic_ctx* ctx, int on);
 int pic_profile_read(pic_ctx* ctx, double* ms, int64_t* calls, int reset);
 /* Kernel launches issued by this context since creation. */
 int pic_launch_count(pic_ctx* ctx, int64_t* n);
+/* Test hook (no reference counterpart).  The library's only device-side
+ * waits are bounded: the batched ensemble solve's block barriers give up
+ * after a number of polls (default 2^26), the learned warm start's
+ * tensor-core pipeline waits after a number of SM clock cycles (default
+ * 2^31, about a second); either then records a flag and lets its kernel
+ * finish, and the operator returns PIC_ERR_TIMEOUT.  This lowers the two
+ * bounds on the context's device so that a test can make the waits run out
+ * without any fault; values <= 0 restore the defaults.  Device-wide: it
+ * affects every context on that device. */
+int pic_debug_set_wait_limits(pic_ctx* ctx, int64_t barrier_polls, int64_t tensor_wait_cycles);
 
 /* ---- tuning (no reference counterpart) -----------------------------------
  * The particle kernels are built for PIC_NUM_TILE_SHAPES tile shapes of 256

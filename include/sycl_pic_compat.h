@@ -48,9 +48,17 @@ double sycl_pic_cleanup_map(int species);                /* :201 */
  * ions' and ionisation pairs (pic_generate_new_particles with the reference's
  * constants, temperatures from M_PICDAT.DAT). */
 double sycl_pic_generate_new_particles(void);
-/* :239 text snapshots into dir/{electronDensity,ionDensity,potential,Ex,Ey}/<iter>. */
+/* :239 text snapshots into dir/{electronDensity,ionDensity,electronenergy,
+ * ionenergy,potential,Ex,Ey}/<iter> (printNumberDensity, printEnergy,
+ * printElectricField, printPhi: src/utils.cpp:829-991).  Where the reference
+ * exits on a file it cannot create, this returns with the reason in
+ * pic_last_error() and the status in sycl_pic_last_status(). */
 void sycl_pic_print_diagnostics(const char* dir, int iteration);
 void sycl_pic_save_meshes(void);         /* :247 Mesh_<s>.out              */
+/* No reference counterpart: PIC_OK or the PIC_ERR_* status of the last
+ * sycl_pic_print_diagnostics / sycl_pic_save_meshes call (the reference's
+ * signatures return nothing). */
+int sycl_pic_last_status(void);
 void sycl_pic_finalize(void);            /* :267                          */
 /* sycl_pic_module.cpp:216-223 (Python extension): E from host phi. */
 void sycl_pic_update_fields_from_phi(void);

@@ -122,6 +122,9 @@ def lib():
             "orc_ref_mover": (i64, [vp, P(Grid), vp, i64, dbl, dbl, vp, vp, vp, P(i64), P(i64)]),
             "orc_ref_cleanup": (None, [vp, vp]),
             "orc_ref_compact": (i64, [vp, vp, i64, vp, i64]),
+            "orc_plasma_counts": (i64, [i32, i32, i32, dbl, dbl, dbl, dbl, ctypes.c_uint64, vp]),
+            "orc_plasma_fill": (None, [i32, i32, dbl, dbl, i32, dbl, dbl, dbl, ctypes.c_uint64, vp,
+                                       vp, i64, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -473,3 +476,23 @@ def ref_lib():
 def ref_grid_params(nx: int, ny: int, width: float, height: float) -> RefGridParams:
     """The reference's params1 (src/particles.cpp:357-368): dx = XMAX/NX."""
     return RefGridParams(nx, ny, nx + 1, ny + 1, width / nx, height / ny, width, height)
+
+
+def generate_plasma(nx: int, ny: int, dx: float, dy: float, ppc: int, v_th: float,
+                    blob_peak: float = 0.0, blob_cx: float = 0.0, blob_cy: float = 0.0,
+                    blob_sigma: float = 1.0, drift_vx: float = 0.0, drift_vy: float = 0.0,
+                    seed: int = 1) -> np.ndarray:
+    """Seeded reference-layout Points of one species (C, OpenMP): ppc per cell
+    plus floor(blob_peak exp(-r^2/(2 sigma^2)) + u) blob particles, uniform in
+    the cell, Maxwellian velocities (sigma v_th per component, blob particles
+    drifting), in an order random with respect to the cells."""
+    L = lib()
+    counts = np.zeros(nx * ny, np.int64)
+    n = int(L.orc_plasma_counts(nx, ny, ppc, blob_peak, blob_cx, blob_cy, blob_sigma, seed,
+                                _ptr(counts)))
+    start = np.zeros(nx * ny, np.int64)
+    np.cumsum(counts[:-1], out=start[1:])
+    pts = np.empty(n, POINT_DTYPE)
+    L.orc_plasma_fill(nx, ny, dx, dy, ppc, v_th, drift_vx, drift_vy, seed, _ptr(counts),
+                      _ptr(start), n, _ptr(pts))
+    return pts

@@ -821,3 +821,92 @@ int64_t orc_ref_compact(orc_hmap* m, orc_point* p, int64_t end, const int32_t* e
     free(dst); free(src);
     return keep;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Synthetic plasma for the CPU baseline (bench.py's reference arm)           */
+/* ------------------------------------------------------------------------- */
+
+/* splitmix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
+ * generators", OOPSLA 2014) as a counter-based generator: the value of
+ * counter c under key k. */
+static inline uint64_t sm64(uint64_t k, uint64_t c) {
+    uint64_t z = k + (c + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static inline double u01(uint64_t k, uint64_t c) { return (double)(sm64(k, c) >> 11) * 0x1.0p-53; }
+
+/* Particles per cell of the workload description: ppc background plus
+ * floor(blob_peak * exp(-r^2/(2 sigma^2)) + u), r from the blob centre in
+ * cells (cell centres).  Writes counts[nx*ny]; returns the total. */
+int64_t orc_plasma_counts(int32_t nx, int32_t ny, int32_t ppc, double blob_peak, double cx,
+                          double cy, double sigma, uint64_t seed, int64_t* counts) {
+    int64_t total = 0;
+#pragma omp parallel for schedule(static) reduction(+ : total)
+    for (int64_t c = 0; c < (int64_t)nx * ny; ++c) {
+        int64_t k = ppc;
+        if (blob_peak > 0) {
+            const double rx = (double)(c % nx) + 0.5 - cx, ry = (double)(c / nx) + 0.5 - cy;
+            k += (int64_t)floor(blob_peak * exp(-(rx * rx + ry * ry) / (2 * sigma * sigma)) +
+                                u01(seed ^ 0xB10Bull, (uint64_t)c));
+        }
+        counts[c] = k;
+        total += k;
+    }
+    return total;
+}
+
+/* Fills the Points of the cells' counts (start = exclusive prefix of the
+ * counts): positions uniform in the cell, velocities Maxwellian with sigma
+ * v_th per component (Box-Muller), blob particles (index in cell >= ppc)
+ * adding (drift_vx, drift_vy).  Point i goes to out[perm(i)], perm a
+ * bijection of [0, n) (a 4-round Feistel network on the next power of two,
+ * cycle-walked), so that the array order is random with respect to the
+ * cells, as the reference's initParticlesRandomly leaves it. */
+void orc_plasma_fill(int32_t nx, int32_t ny, double dx, double dy, int32_t ppc, double v_th,
+                     double drift_vx, double drift_vy, uint64_t seed, const int64_t* counts,
+                     const int64_t* start, int64_t n, orc_point* out) {
+    int bits = 1;
+    while ((1ll << bits) < n) ++bits;
+    const int lo = bits / 2, hi = bits - lo;
+    const uint64_t lmask = (1ull << lo) - 1, hmask = (1ull << hi) - 1;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t c = 0; c < (int64_t)nx * ny; ++c) {
+        const int gx = (int)(c % nx), gy = (int)(c / nx);
+        for (int64_t j = 0; j < counts[c]; ++j) {
+            const uint64_t i = (uint64_t)(start[c] + j);
+            /* Feistel permutation of i within [0, 2^bits), walked until < n */
+            uint64_t x = i;
+            do {
+                uint64_t L = x >> lo, R = x & lmask;
+                for (int r = 0; r < 4; ++r) {
+                    /* alternate halves of width hi and lo */
+                    const uint64_t F = sm64(seed + (uint64_t)r, R);
+                    const uint64_t nL = R, nR = (L ^ F) & ((r & 1) ? lmask : hmask);
+                    L = nL;
+                    R = nR;
+                }
+                x = ((L & hmask) << lo) | (R & lmask);
+            } while (x >= (uint64_t)n);
+            orc_point* p = &out[x];
+            const uint64_t k = seed ^ 0x5EEDull;
+            p->x = (gx + u01(k, 8 * i)) * dx;
+            p->y = (gy + u01(k, 8 * i + 1)) * dy;
+            p->z = 0.0;
+            double g[4];
+            for (int h = 0; h < 2; ++h) {
+                const double u1 = 1.0 - u01(k, 8 * i + 2 + 2 * h), u2 = u01(k, 8 * i + 3 + 2 * h);
+                const double rr = sqrt(-2.0 * log(u1));
+                g[2 * h] = rr * cos(6.283185307179586 * u2);
+                g[2 * h + 1] = rr * sin(6.283185307179586 * u2);
+            }
+            const int blob = j >= ppc;
+            p->vx = v_th * g[0] + (blob ? drift_vx : 0.0);
+            p->vy = v_th * g[1] + (blob ? drift_vy : 0.0);
+            p->vz = v_th * g[2];
+            p->pointer = 0;
+            p->pad_ = 0;
+        }
+    }
+}

@@ -12,7 +12,9 @@ run statistics:
     max|<phi>|;
   * time-averaged electron density, averaged over y: within 1e-4 of its
     maximum at every x;
-  * relative kinetic-energy change over the run: within 1e-4 of the oracle's.
+  * relative kinetic-energy change over the run: within 1e-4 of the oracle's;
+  * relative total-energy change (kinetic + 1/2 sum rho phi dA, the field
+    energy on the node grid) over the run: within 1e-4 of the oracle's.
 Measured on a B200: identical lost counts, 2e-7 (potential), 2e-8
 (density), 1e-8 (energy change): over this run the FP32 state follows the
 FP64 trajectories closely.
@@ -44,14 +46,21 @@ def test_cfg1_run_statistics(oracle):
     ke0 = [O.kinetic_energy(pts[s], ctom[s]) for s in range(2)]
     acc = dict(phi_g=0.0, phi_o=0.0, ne_g=0.0, ne_o=0.0)
     n_avg = 0
+    import test_gpu_config_parity as CP
+    tot_g, tot_o = [], []
     with P.Pic(C.library_config(w)) as pic:
         for s in range(2):
             pic.import_points(s, pts[s])
         for it in range(steps):
+            cur = [pic.export_points(s) for s in range(2)] if it in (0, steps - 1) else None
             pic.step(it)
             rho = np.zeros(g.nodes)
             fin_o = [O.deposit(g, ref[s], sps[s], wgt[s], EPS0, rho)[0] for s in range(2)]
             phi_o, ef_o = D.step(rho)
+            if cur is not None:
+                # state, density and potential of the same step on both sides
+                tot_g.append(sum(CP._energy(w, cur, [pic.final_mesh(s) for s in range(2)], pic.phi())))
+                tot_o.append(sum(CP._energy(w, ref, fin_o, phi_o)))
             for s in range(2):
                 O.push(g, ref[s], ctom[s], w.dt, ef_o, bz)
             if it >= steps // 2:
@@ -82,3 +91,8 @@ def test_cfg1_run_statistics(oracle):
     assert dphi <= 1e-4
     assert dne <= 1e-4
     assert max(dke) <= 1e-4
+    dtot_g = (tot_g[1] - tot_g[0]) / tot_g[0]
+    dtot_o = (tot_o[1] - tot_o[0]) / tot_o[0]
+    print(f"total energy change gpu {dtot_g:.6e} oracle {dtot_o:.6e}")
+    assert abs(tot_g[0] - tot_o[0]) <= 1e-5 * abs(tot_o[0])
+    assert abs(dtot_g - dtot_o) <= 1e-4

@@ -6,7 +6,8 @@ place; operators return elapsed seconds; after poisson_solve the (in place
 overwritten) right-hand side and phi satisfy the reduced system to 1e-8
 relative residual, measured by the FP64 oracle; writes through get_phi()
 reach the E field via update_fields_from_phi(); the diagnostics writers
-create their files; particle counts never grow.
+create their files and raise on a folder they cannot create; particle
+counts never grow.
 """
 import os
 
@@ -62,6 +63,10 @@ def test_reference_driver_loop(oracle, tmp_path, monkeypatch):
         sp.save_meshes()
         assert any(f.startswith("Mesh") for f in os.listdir(tmp_path))
         assert os.path.isdir(tmp_path / "out")
+        # where the reference prints and exits, the module raises
+        (tmp_path / "a_file").write_text("x")
+        with pytest.raises(RuntimeError):
+            sp.print_diagnostics(str(tmp_path / "a_file" / "out"), 0)
         ne1, ni1 = sp.get_particle_counts()
         assert sp.generate_new_particles() >= 0     # band inside the 16 mm domain
         ne2, ni2 = sp.get_particle_counts()
