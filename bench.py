@@ -67,10 +67,12 @@ def parse():
                     help="skip the energy-weighted mesh (deposit_energy = 0)")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned warm-start comparison")
-    ap.add_argument("--ws-pairs", type=int, default=64,
+    ap.add_argument("--ws-pairs", type=int, default=512,
                     help="pairs recorded for the learned warm start")
-    ap.add_argument("--ws-epochs", type=int, default=6)
-    ap.add_argument("--ws-eval", type=int, default=12,
+    ap.add_argument("--ws-epochs", type=int, default=12)
+    ap.add_argument("--ws-lr", type=float, default=1e-3,
+                    help="Adam step size, decaying along a half cosine to 1/100 of it")
+    ap.add_argument("--ws-eval", type=int, default=24,
                     help="evaluation steps, each solved from both guesses")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-instance batched ensemble measurement")
@@ -425,8 +427,8 @@ def run_learned(pic, args, it):
         it += 1
     pic.ws_record(0)
     t0 = time.perf_counter()
-    loss0 = pic.ws_train(1, 1e-3)
-    loss = pic.ws_train(max(args.ws_epochs - 1, 1), 1e-3)
+    loss0 = pic.ws_train(1, args.ws_lr)
+    loss = pic.ws_train_cosine(max(args.ws_epochs - 1, 1), args.ws_lr, args.ws_lr / 100)
     train_s = time.perf_counter() - t0
     ml, mp, il, ip, dphi = [], [], [], [], []
     for _ in range(args.ws_eval):
@@ -559,7 +561,8 @@ def run_cfg4(args):
     pic.ws_record(0)
     rec_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    losses = [pic.ws_train(1, 1e-3) for _ in range(args.cfg4_epochs)]
+    losses = [pic.ws_train(1, args.ws_lr)]
+    losses.append(pic.ws_train_cosine(max(args.cfg4_epochs - 1, 1), args.ws_lr, args.ws_lr / 100))
     train_s = time.perf_counter() - t0
     pic.ws_record(-1)
     ml, mp, il, ip, dphi = [], [], [], [], []

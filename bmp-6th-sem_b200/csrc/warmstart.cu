@@ -580,49 +580,52 @@ __global__ void k_up_add8(const __nv_bfloat16* coarse, const __nv_bfloat16* skip
 // Row-streaming 32->32 convolution on tcgen05 (the forward 32->32 layers).
 //
 // Implicit GEMM with the pixels of one input row as M and (column tap dx,
-// output channel co) as N.  For output row y of a column strip whose first
-// output column is x0 (a multiple of 126), tile pixel i = 0..127 being input
-// column x0 - 1 + i:
-//   D[i][32 dx + co] = sum_{dy, ci} in[y + dy - 1][x0 - 1 + i][ci] W[dy][dx][ci][co]
+// output channel co) as N.  A column strip of 120 output columns starting at
+// x0 (a multiple of 120) is read as four 32-pixel groups, group w holding
+// input columns x0 + 30 w - 1 .. x0 + 30 w + 30 in tile rows 32 w .. 32 w + 31
+// (neighbouring groups overlap by two columns).  For output row y:
+//   D[i][32 dx + co] = sum_{dy, ci} in[y + dy - 1][col(i)][ci] W[dy][dx][ci][co]
 // -- six MMAs of M = 128, N = 96, K = 16 (three row taps x two halves of the
 // input channels), FP32 accumulators in TMEM.  The column taps are summed in
-// the epilogue, where TMEM lane i holds tile pixel i:
-//   out[y][x0 + j][co] = D[j][co] + D[j + 1][32 + co] + D[j + 2][64 + co],
-// the neighbours' values taken by warp shuffles (and across the four warps
-// of a warpgroup through shared memory).  126 outputs a strip row.
+// the epilogue, where TMEM lane i holds tile row i: lane l of warp w (l = 1..30)
+// outputs column x0 + 30 w + l - 1,
+//   out[co] = D[i - 1][co] + D[i][32 + co] + D[i + 1][64 + co],
+// the neighbours' values taken by warp shuffles -- the overlap keeps every
+// neighbour inside the warp, so the four epilogue warps never wait on each
+// other.  The 2x2 average pool of the encoder layers pairs lanes (l, l + 1)
+// for odd l, again inside the warp.
 //
-// Every input row is loaded once by TMA (four boxes of 8 channels x 128
-// pixels, zero filled outside the image) into a ring of row slots and used
-// by three consecutive output rows: each CTA walks down its share of the
-// (strip, row) units.  Roles, 12 warps:
+// Every input row is loaded once by TMA (four boxes of 32 channels x 32
+// pixels, 64-byte swizzle, zero filled outside the image) into a ring of row
+// slots and used by three consecutive output rows: each CTA walks down its
+// share of the (strip, row) units.  Roles, 12 warps:
 //   warp 0   TMA producer (one lane);
 //   warp 1   TMEM allocation, MMA issue (one lane);
-//   warps 4-7 and 8-11  two epilogue warpgroups, each taking output rows in
-//            pairs (2m, 2m + 1) with accumulators 2e, 2e + 1 (four in TMEM):
-//            bias, relu, bf16 store and, for the encoder layers, the 2x2
-//            average pool of the pair.
+//   warps 4-7 and 8-11  two epilogue warpgroups, each taking every output
+//            row (accumulators in turn, four in TMEM) for one half of the
+//            output channels: bias, relu, bf16 store and, for the encoder
+//            layers, the pool.
 // Every wait is bounded (g_ws_wait_cycles); a role that gives up records
-// g_ws_fault, the CTA's roles leave their loops together, the MMA lane waits
-// (fixed bound) for the MMAs it issued and the producer for its copies before
-// the tensor memory is freed.
+// g_ws_fault, the CTA's roles leave their loops, the MMA lane waits (fixed
+// bound) for the MMAs it issued and the producer for its copies before the
+// tensor memory is freed.
 // ---------------------------------------------------------------------------
-constexpr int kRwStrip = 126;                 // output columns a strip
-constexpr int kRwSlots = 8;                   // input row slots
-constexpr int kRwRowBytes = 4 * 128 * 16;     // one input row: 4 boxes [128 px][8 ch] bf16
+constexpr int kRwStrip = 120;                 // output columns a strip
+constexpr int kRwSlots = 12;                  // input row slots
+constexpr int kRwRowBytes = 128 * 64;         // one input row: [128 tile rows][32 ch] bf16, swizzled
 constexpr int kRwWBytes = 6 * 2 * 96 * 16;    // weights: [dy][kc][g][n 96][8 ci] bf16
 constexpr int kRwThreads = 12 * 32;
-// shared memory: head @0 (full[8] @0, empty[8] @64, accf[4] @128, acce[4]
-// @160, drain @192, TMEM address @200, abort @204), weights @1024, row slots
-// (1024-aligned), edge exchange [wg][buf][side][warp][16] floats, bias
-constexpr int kRwXchg = 2 * 2 * 2 * 4 * 16 * 4;
+// shared memory: head @0 (full[16] @0, empty[16] @128, accf[4] @256, acce[4]
+// @288, drain @320, TMEM address @328, abort @332), bias @512, weights @1024,
+// row slots (1024-aligned)
+constexpr int kRwOffBias = 512;
 constexpr int kRwOffW = 1024;
 constexpr int kRwOffRows = kRwOffW + kRwWBytes;
-constexpr int kRwOffX = kRwOffRows + kRwSlots * kRwRowBytes;
-constexpr int kRwOffBias = kRwOffX + kRwXchg;
-constexpr int kRwSmemUsed = kRwOffBias + 32 * 4;
+constexpr int kRwSmemUsed = kRwOffRows + kRwSlots * kRwRowBytes;
 static_assert(kRwOffRows % 1024 == 0, "row slots 1024-aligned");
+static_assert(kRwSlots <= 16, "barrier head layout");
 // more than half an SM's shared memory: one CTA an SM (its TMEM is all 512 columns)
-constexpr int kRwSmem = 120 * 1024;
+constexpr int kRwSmem = 140 * 1024;
 static_assert(kRwSmemUsed + 1024 <= kRwSmem, "row-conv shared memory");
 // kind::f16: FP32 accumulator, bf16 A and B, both K-major, N = 96, M = 128
 constexpr uint32_t kRwIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((96u >> 3) << 17) | ((128u >> 4) << 24);
@@ -646,6 +649,15 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, int 
         : "memory");
 }
 
+// K-major operand in the 64-byte swizzle layout (rows of 64 bytes, 16-byte
+// chunks permuted within each 512-byte group of 8 rows, as TMA's 64-byte
+// swizzle writes them): stride between 8-row groups 512 bytes; a K block of
+// 16 bf16 at byte k * 32 of the row is addressed by the start address.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(512u >> 4) << 32) |
+           (1ull << 46) | (4ull << 61);
+}
+
 __device__ __forceinline__ void rw_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
     asm volatile(
         "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
@@ -666,7 +678,7 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // The CTA's share of the (strip, row) units [g0, g1), in pairs of rows when
-// pooling (P is a multiple of 4, so a pair never straddles two strips).
+// pooling (P is even, so a pair never straddles two strips).
 __device__ __forceinline__ void rw_share(int units, int pool, int& g0, int& g1) {
     const int b = blockIdx.x, n = gridDim.x;
     g0 = (int)(((int64_t)units * b) / n);
@@ -683,14 +695,13 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     // offsets below are from the first 1024-byte boundary of the buffer
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
-    const uint32_t full0 = sbase, empty0 = sbase + 64, accf0 = sbase + 128, acce0 = sbase + 160;
-    const uint32_t drain = sbase + 192;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 200);
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 204);
+    const uint32_t full0 = sbase, empty0 = sbase + 128, accf0 = sbase + 256, acce0 = sbase + 288;
+    const uint32_t drain = sbase + 320;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 328);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 332);
+    float* sbias = reinterpret_cast<float*>(smem + kRwOffBias);
     unsigned char* wsm = smem + kRwOffW;
     unsigned char* rows = smem + kRwOffRows;
-    float* xch = reinterpret_cast<float*>(smem + kRwOffX);
-    float* sbias = reinterpret_cast<float*>(smem + kRwOffBias);
     const long long wl = g_ws_wait_cycles;
     const int P = A.P;
     const int strips = (P + kRwStrip - 1) / kRwStrip;
@@ -712,7 +723,7 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
         }
         for (int a = 0; a < 4; ++a) {
             mbar_init(accf0 + 8 * a, 1);
-            mbar_init(acce0 + 8 * a, 4);
+            mbar_init(acce0 + 8 * a, 8);  // the eight epilogue warps
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -755,8 +766,8 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
                     const uint32_t dst = smem_u32(rows + s * kRwRowBytes);
                     mbar_expect_tx(full0 + 8 * s, kRwRowBytes);
 #pragma unroll
-                    for (int gch = 0; gch < 4; ++gch)
-                        tma_load_3d(dst + gch * 2048, &tmap, 8 * gch, x0 - 1, r0 - 1 + i, full0 + 8 * s);
+                    for (int w = 0; w < 4; ++w)
+                        tma_load_3d(dst + w * 2048, &tmap, 0, x0 + 30 * w - 1, r0 - 1 + i, full0 + 8 * s);
                 }
                 g += r1 - r0;
             }
@@ -796,7 +807,7 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
                         const uint32_t rb = rows_u32 + ((ld + j + dy) % kRwSlots) * kRwRowBytes;
 #pragma unroll
                         for (int kc = 0; kc < 2; ++kc)
-                            rw_mma(tmem + q * 128, tc_desc(rb + kc * 4096, 2048, 128),
+                            rw_mma(tmem + q * 128, sw64_desc(rb + kc * 32),
                                    tc_desc(w_u32 + (dy * 2 + kc) * 3072, 1536, 128), (dy | kc) ? 1u : 0u);
                     }
                     tc_commit(accf0 + 8 * q);
@@ -814,124 +825,79 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
             }
         }
         __syncwarp();
-    } else if (warp >= 4) {
+    }
+    else if (warp >= 4) {
         // ---------------- epilogue ----------------
-        const int e = (warp - 4) >> 2;    // warpgroup
-        const int wq = warp & 3;          // TMEM lanes 32 wq .. 32 wq + 31
-        const int t = 32 * wq + lane;     // tile pixel
+        // both warpgroups take every row, warpgroup h the output channels
+        // 16 h .. 16 h + 15
+        const int h = (warp - 4) >> 2;
+        const int wq = warp & 3;          // TMEM lanes 32 wq .. 32 wq + 31 = the warp's pixel group
         const int Q = P / 2;
-        float* xl = xch + (e * 2) * 2 * 4 * 16;  // [buf][side][warp][16]
-        uint32_t prev[16];                       // even row of a pooled pair, bf16x2
+        float bias[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) bias[c] = sbias[16 * h + c];
+        uint32_t prev[8];                 // even row of a pooled pair, bf16x2
         int o = 0;
         bool quit = false;
         for (int g = g0; g < g1 && !quit;) {
             const int strip = g / P, r0 = g % P, r1 = min(P, r0 + (g1 - g)), n = r1 - r0;
-            const int x0 = strip * kRwStrip;
-            const int x = x0 + t - 1;
-            const bool valid = t >= 1 && t <= kRwStrip && x < P;
+            const int x = strip * kRwStrip + 30 * wq + lane - 1;
+            const bool valid = lane >= 1 && lane <= 30 && x < P;
             for (int j = 0; j < n; ++j, ++o) {
-                if (((o >> 1) & 1) != e) continue;
                 const int q = o & 3, y = r0 + j;
                 const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * q, (o >> 2) & 1, wl));
-                if (!ok && lane == 0) give_up();
-                uint32_t qq;
-                asm volatile(
-                    "{\n.reg .pred p, r;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred r, %2, 128, p;\nselp.u32 %0, 1, 0, r;\n}\n"
-                    : "=r"(qq)
-                    : "r"((!ok || *abort_flag) ? 1u : 0u), "r"(1 + e)
-                    : "memory");
-                if (qq) {
+                if (!ok) {
+                    if (lane == 0) give_up();
                     quit = true;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                float* xb = xl + (o & 1) * 2 * 4 * 16;
+                float v0[16], v1[16], v2[16];
+                const uint32_t ta = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)(q * 128 + 16 * h);
+                tc_ld16(ta, v0);
+                tc_ld16(ta + 32, v1);
+                tc_ld16(ta + 64, v2);
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acce0 + 8 * q);  // this warp's part of the accumulator is read
+                uint32_t pk[8];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float v0[16], v1[16], v2[16];
-                    const uint32_t ta = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)(q * 128 + 16 * h);
-                    tc_ld16(ta, v0);
-                    tc_ld16(ta + 32, v1);
-                    tc_ld16(ta + 64, v2);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                    if (h == 1) {
-                        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(acce0 + 8 * q);
-                    }
-                    // the warp's edge values for its neighbours
-                    if (lane == 31)
+                for (int c = 0; c < 16; c += 2) {
+                    const float l0 = __shfl_up_sync(kFull, v0[c], 1), l1 = __shfl_up_sync(kFull, v0[c + 1], 1);
+                    const float r0v = __shfl_down_sync(kFull, v2[c], 1), r1v = __shfl_down_sync(kFull, v2[c + 1], 1);
+                    pk[c / 2] = pack_bf16x2(fmaxf(l0 + v1[c] + r0v + bias[c], 0.f),
+                                            fmaxf(l1 + v1[c + 1] + r1v + bias[c + 1], 0.f));
+                }
+                if (valid) {
+                    uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
+                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                }
+                if (pool) {
+                    if ((y & 1) == 0) {
 #pragma unroll
-                        for (int c = 0; c < 16; ++c) xb[(0 * 4 + wq) * 16 + c] = v0[c];
-                    if (lane == 0)
+                        for (int c = 0; c < 8; ++c) prev[c] = pk[c];
+                    } else {
+                        // 0.25 (v(y-1, x) + v(y-1, x+1) + v(y, x) + v(y, x+1)) of the
+                        // bf16 values; lane l + 1 holds column x + 1
+                        uint32_t pp[8];
 #pragma unroll
-                        for (int c = 0; c < 16; ++c) xb[(1 * 4 + wq) * 16 + c] = v2[c];
-                    asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
-                    float r[16];
-#pragma unroll
-                    for (int c = 0; c < 16; ++c) {
-                        float l = __shfl_up_sync(kFull, v0[c], 1);
-                        float rr = __shfl_down_sync(kFull, v2[c], 1);
-                        if (lane == 0) l = wq > 0 ? xb[(0 * 4 + wq - 1) * 16 + c] : 0.f;
-                        if (lane == 31) rr = wq < 3 ? xb[(1 * 4 + wq + 1) * 16 + c] : 0.f;
-                        r[c] = fmaxf(l + v1[c] + rr + sbias[16 * h + c], 0.f);
-                    }
-                    uint32_t pk[8];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) pk[c] = pack_bf16x2(r[2 * c], r[2 * c + 1]);
-                    if (valid) {
-                        uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
-                        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                    }
-                    if (pool) {
-                        if ((y & 1) == 0) {
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) prev[8 * h + c] = pk[c];
-                        } else {
-                            // 0.25 (v(y-1, x) + v(y-1, x+1) + v(y, x) + v(y, x+1)) of the bf16 values
-                            float s[16];
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) {
-                                const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&prev[8 * h + c]));
-                                const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[c]));
-                                s[2 * c] = a.x;
-                                s[2 * c + 1] = a.y;
-                                r[2 * c] = b.x;
-                                r[2 * c + 1] = b.y;
-                            }
-                            // right neighbour's pair (lane 31: the next warp's lane 0, via xb)
-                            asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
-                            if (lane == 0)
-#pragma unroll
-                                for (int c = 0; c < 16; ++c) {
-                                    xb[(0 * 4 + wq) * 16 + c] = s[c];
-                                    xb[(1 * 4 + wq) * 16 + c] = r[c];
-                                }
-                            asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
-                            uint32_t pp[8];
-#pragma unroll
-                            for (int c = 0; c < 16; c += 2) {
-                                float sa = __shfl_down_sync(kFull, s[c], 1), sb = __shfl_down_sync(kFull, s[c + 1], 1);
-                                float ra = __shfl_down_sync(kFull, r[c], 1), rb = __shfl_down_sync(kFull, r[c + 1], 1);
-                                if (lane == 31 && wq < 3) {
-                                    sa = xb[(0 * 4 + wq + 1) * 16 + c];
-                                    sb = xb[(0 * 4 + wq + 1) * 16 + c + 1];
-                                    ra = xb[(1 * 4 + wq + 1) * 16 + c];
-                                    rb = xb[(1 * 4 + wq + 1) * 16 + c + 1];
-                                }
-                                pp[c / 2] = pack_bf16x2(0.25f * (s[c] + sa + r[c] + ra),
-                                                        0.25f * (s[c + 1] + sb + r[c + 1] + rb));
-                            }
-                            if (valid && (x & 1) == 0 && (x >> 1) < Q) {
-                                uint4* dst = reinterpret_cast<uint4*>(A.pool + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + 16 * h);
-                                dst[0] = make_uint4(pp[0], pp[1], pp[2], pp[3]);
-                                dst[1] = make_uint4(pp[4], pp[5], pp[6], pp[7]);
-                            }
+                        for (int c = 0; c < 8; ++c) {
+                            const uint32_t pr = __shfl_down_sync(kFull, prev[c], 1);
+                            const uint32_t cr = __shfl_down_sync(kFull, pk[c], 1);
+                            const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&prev[c]));
+                            const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pr));
+                            const float2 d = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[c]));
+                            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&cr));
+                            pp[c] = pack_bf16x2(0.25f * (a.x + b.x + d.x + f.x), 0.25f * (a.y + b.y + d.y + f.y));
+                        }
+                        if (valid && (lane & 1) && (x >> 1) < Q) {
+                            uint4* dst = reinterpret_cast<uint4*>(A.pool + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + 16 * h);
+                            dst[0] = make_uint4(pp[0], pp[1], pp[2], pp[3]);
+                            dst[1] = make_uint4(pp[4], pp[5], pp[6], pp[7]);
                         }
                     }
-                    // the exchange slots are reused by the next half / row
-                    asm volatile("bar.sync %0, 128;\n" ::"r"(1 + e) : "memory");
                 }
             }
             g += n;
@@ -1605,7 +1571,8 @@ struct pic_ws {
 namespace picb200 {
 
 // TMA descriptor of an NHWC bf16 image of P x P pixels and 32 channels,
-// read in boxes of 8 channels x 128 pixels x 1 row (zero filled outside).
+// read in boxes of 32 channels x 32 pixels x 1 row (64 bytes a pixel,
+// 64-byte swizzle, zero filled outside).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1622,10 +1589,10 @@ static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P) {
     }
     const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)P, (cuuint64_t)P};
     const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)P * C * 2};
-    const cuuint32_t box[3] = {8, 128, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)C, 32, 1};
     const cuuint32_t es[3] = {1, 1, 1};
     const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dims,
-                              strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return fail(PIC_ERR_CUDA, "warm start: TMA descriptor encoding failed (" + std::to_string((int)r) + ")");
@@ -2078,21 +2045,42 @@ int pic_ws_pairs(pic_ctx* c, int64_t* n) {
     return PIC_OK;
 }
 
-int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
-    if (!c || epochs < 0 || !(lr > 0)) return fail(PIC_ERR_ARG, "warm start: bad training arguments");
+// Adam over the recorded pairs, one pair a step, the pairs of each epoch in
+// an order drawn afresh (a seeded permutation: training is repeatable); the
+// step size follows lr(t) = lr_min + (lr_max - lr_min) (1 + cos(pi t / T)) / 2
+// over the T steps of the call (constant when lr_min == lr_max).
+static int ws_train(pic_ctx* c, int epochs, double lr_max, double lr_min, double* loss_out) {
+    if (!c || epochs < 0 || !(lr_max > 0) || !(lr_min > 0) || lr_min > lr_max)
+        return fail(PIC_ERR_ARG, "warm start: bad training arguments");
     if (!c->ws || c->ws->net.n_pairs == 0) return fail(PIC_ERR_STATE, "warm start: no recorded pairs");
     Net& N = c->ws->net;
     const int P = N.P;
+    const int64_t np = N.n_pairs, total = (int64_t)epochs * np;
+    std::vector<int64_t> order((size_t)np);
     double last = 0;
+    int64_t t = 0;
     for (int e = 0; e < epochs; ++e) {
+        for (int64_t s = 0; s < np; ++s) order[(size_t)s] = s;
+        uint64_t z = 0x9E3779B97F4A7C15ull * (uint64_t)(N.adam_t + 1) + (uint64_t)e;
+        for (int64_t s = np - 1; s > 0; --s) {  // Fisher-Yates with splitmix64 draws
+            z += 0x9E3779B97F4A7C15ull;
+            uint64_t r = z;
+            r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ull;
+            r = (r ^ (r >> 27)) * 0x94D049BB133111EBull;
+            r ^= r >> 31;
+            std::swap(order[(size_t)s], order[(size_t)(r % (uint64_t)(s + 1))]);
+        }
         double ep = 0;
-        for (int64_t s = 0; s < N.n_pairs; ++s) {
+        for (int64_t k = 0; k < np; ++k, ++t) {
+            const int64_t s = order[(size_t)k];
             PIC_TRY(ws_pack(c));
             N.xin = N.ds_x + s * (int64_t)P * P * 4;
             forward(c);
             enqueue_loss(c, N.ds_t + s * c->nodes, N.loss_acc + s);
             backward(c);
             N.adam_t += 1;
+            const double lr = lr_min + (lr_max - lr_min) * 0.5 *
+                                           (1.0 + std::cos(3.141592653589793 * (double)t / (double)std::max<int64_t>(total, 1)));
             const float b1 = 0.9f, b2 = 0.999f;
             const float c1 = 1.f / (1.f - std::pow(b1, (float)N.adam_t));
             const float c2 = 1.f / (1.f - std::pow(b2, (float)N.adam_t));
@@ -2101,18 +2089,26 @@ int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
             N.packed = false;
             c->launches += 1;
         }
-        std::vector<float> ls((size_t)N.n_pairs);
+        std::vector<float> ls((size_t)np);
         PIC_CUDA(cudaMemcpyAsync(ls.data(), N.loss_acc, ls.size() * 4, cudaMemcpyDeviceToHost, c->stream));
         PIC_CUDA(cudaStreamSynchronize(c->stream));
         PIC_TRY(ws_check_fault());
         for (float v : ls) ep += v;
-        last = ep / (double)N.n_pairs;
+        last = ep / (double)np;
     }
     N.trained = true;
     PIC_TRY(ws_guess_buffer(c));
     if (loss_out) *loss_out = last;
     PIC_CUDA(cudaGetLastError());
     return PIC_OK;
+}
+
+int pic_ws_train(pic_ctx* c, int epochs, double lr, double* loss_out) {
+    return ws_train(c, epochs, lr, lr, loss_out);
+}
+
+int pic_ws_train_cosine(pic_ctx* c, int epochs, double lr_max, double lr_min, double* loss_out) {
+    return ws_train(c, epochs, lr_max, lr_min, loss_out);
 }
 
 int pic_ws_get_params(pic_ctx* c, float* host, int64_t n) {

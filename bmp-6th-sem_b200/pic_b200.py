@@ -143,6 +143,7 @@ def lib():
         "pic_ws_record": (cint, [vp, i64, dbl, dbl, dbl]),
         "pic_ws_pairs": (cint, [vp, P(i64)]),
         "pic_ws_train": (cint, [vp, cint, dbl, P(dbl)]),
+        "pic_ws_train_cosine": (cint, [vp, cint, dbl, dbl, P(dbl)]),
         "pic_ws_num_params": (i64, []),
         "pic_ws_get_params": (cint, [vp, vp, i64]),
         "pic_ws_set_params": (cint, [vp, vp, i64, dbl, dbl, dbl]),
@@ -386,6 +387,11 @@ class Pic:
     def ws_train(self, epochs: int, lr: float) -> float:
         loss = ctypes.c_double(0)
         _check(lib().pic_ws_train(self.h, epochs, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def ws_train_cosine(self, epochs: int, lr_max: float, lr_min: float) -> float:
+        loss = ctypes.c_double(0)
+        _check(lib().pic_ws_train_cosine(self.h, epochs, lr_max, lr_min, ctypes.byref(loss)))
         return loss.value
 
     def ws_params(self) -> np.ndarray:

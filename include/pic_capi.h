@@ -334,6 +334,10 @@ int pic_ws_pairs(pic_ctx* ctx, int64_t* n);
 /* Adam epochs over the recorded pairs (one pair per step); *loss = mean
  * normalised squared error of the last epoch. */
 int pic_ws_train(pic_ctx* ctx, int epochs, double lr, double* loss);
+/* The same with the step size decaying over the call's steps from lr_max to
+ * lr_min along a half cosine.  Each epoch visits the pairs in a new seeded
+ * order (both entry points). */
+int pic_ws_train_cosine(pic_ctx* ctx, int epochs, double lr_max, double lr_min, double* loss);
 int64_t pic_ws_num_params(void);
 int pic_ws_get_params(pic_ctx* ctx, float* host, int64_t n);
 int pic_ws_set_params(pic_ctx* ctx, const float* host, int64_t n, double phi_scale,
