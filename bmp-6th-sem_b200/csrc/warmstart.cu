@@ -577,53 +577,56 @@ __global__ void k_up_add8(const __nv_bfloat16* coarse, const __nv_bfloat16* skip
 }
 
 // ---------------------------------------------------------------------------
-// Row-streaming 32->32 convolution on tcgen05 (the forward 32->32 layers).
+// Block-streaming 32->32 convolution on tcgen05 (the forward 32->32 layers).
 //
-// Implicit GEMM with the pixels of one input row as M and (column tap dx,
-// output channel co) as N.  A column strip of 120 output columns starting at
-// x0 (a multiple of 120) is read as four 32-pixel groups, group w holding
-// input columns x0 + 30 w - 1 .. x0 + 30 w + 30 in tile rows 32 w .. 32 w + 31
-// (neighbouring groups overlap by two columns).  For output row y:
-//   D[i][32 dx + co] = sum_{dy, ci} in[y + dy - 1][col(i)][ci] W[dy][dx][ci][co]
-// -- six MMAs of M = 128, N = 96, K = 16 (three row taps x two halves of the
+// Implicit GEMM over blocks of 4 output rows x 30 output columns.  Its input,
+// image rows y - 1 .. y + 4 by columns x0 - 1 .. x0 + 30 (x0 = 30 s for column
+// strip s, y a multiple of 4), arrives as ONE TMA box of 6 rows x 32 pixels x
+// 32 channels (64 bytes a pixel, 64-byte swizzle, zero filled outside the
+// image): tile row i = 32 r + p holds row y - 1 + r, column x0 - 1 + p.  The
+// four-row window starting at box row dy is the A operand of row tap dy -- a
+// 2 KB offset in shared memory -- so for every block
+//   D[32 r + p][32 dx + co] = sum_{dy, ci} in[y + r + dy - 1][x0 - 1 + p][ci] W[dy][dx][ci][co]
+// is six MMAs of M = 128, N = 96, K = 16 (three row taps x two halves of the
 // input channels), FP32 accumulators in TMEM.  The column taps are summed in
-// the epilogue, where TMEM lane i holds tile row i: lane l of warp w (l = 1..30)
-// outputs column x0 + 30 w + l - 1,
+// the epilogue, where warp r of a warpgroup reads TMEM lanes 32 r .. 32 r + 31
+// (output row y + r, one pixel a lane): lane p = 1..30 outputs column
+// x0 + p - 1,
 //   out[co] = D[i - 1][co] + D[i][32 + co] + D[i + 1][64 + co],
-// the neighbours' values taken by warp shuffles -- the overlap keeps every
-// neighbour inside the warp, so the four epilogue warps never wait on each
-// other.  The 2x2 average pool of the encoder layers pairs lanes (l, l + 1)
-// for odd l, again inside the warp.
+// the neighbours' values taken by warp shuffles.  One TMA box per 120
+// outputs keeps the copy engine's per-box cost off the critical path (1.6x
+// the output's bytes are read, the halo rows and columns mostly from L2).
 //
-// Every input row is loaded once by TMA (four boxes of 32 channels x 32
-// pixels, 64-byte swizzle, zero filled outside the image) into a ring of row
-// slots and used by three consecutive output rows: each CTA walks down its
-// share of the (strip, row) units.  Roles, 12 warps:
-//   warp 0   TMA producer (one lane);
-//   warp 1   TMEM allocation, MMA issue (one lane);
-//   warps 4-7 and 8-11  two epilogue warpgroups, each taking every output
-//            row (accumulators in turn, four in TMEM) for one half of the
-//            output channels: bias, relu, bf16 store and, for the encoder
-//            layers, the pool.
+// Roles, 12 warps:
+//   warp 0   TMA producer (one lane), a ring of block slots;
+//   warp 1   TMEM allocation, MMA issue (one lane), four accumulators;
+//   warps 4-7 and 8-11  two epilogue warpgroups, each taking every block for
+//            one half of the output channels: bias, relu, bf16 store and,
+//            for the encoder layers, the 2x2 average pool (rows y + 2k and
+//            y + 2k + 1 meet through shared memory, columns through a
+//            shuffle).
 // Every wait is bounded (g_ws_wait_cycles); a role that gives up records
 // g_ws_fault, the CTA's roles leave their loops, the MMA lane waits (fixed
 // bound) for the MMAs it issued and the producer for its copies before the
 // tensor memory is freed.
 // ---------------------------------------------------------------------------
-constexpr int kRwStrip = 120;                 // output columns a strip
-constexpr int kRwSlots = 12;                  // input row slots
-constexpr int kRwRowBytes = 128 * 64;         // one input row: [128 tile rows][32 ch] bf16, swizzled
+constexpr int kRwCols = 30;                   // output columns a strip
+constexpr int kRwBlk = 4;                     // output rows a block
+constexpr int kRwSlots = 8;                   // block slots
+constexpr int kRwBoxRows = kRwBlk + 2;
+constexpr int kRwSlotBytes = kRwBoxRows * 32 * 64;   // 6 rows x 32 px x 32 ch bf16 (12 KB)
 constexpr int kRwWBytes = 6 * 2 * 96 * 16;    // weights: [dy][kc][g][n 96][8 ci] bf16
 constexpr int kRwThreads = 12 * 32;
-// shared memory: head @0 (full[16] @0, empty[16] @128, accf[4] @256, acce[4]
-// @288, drain @320, TMEM address @328, abort @332), bias @512, weights @1024,
-// row slots (1024-aligned)
+// shared memory: head @0 (full[8] @0, empty[8] @64, accf[4] @128, acce[4]
+// @160, drain @192, TMEM address @200, abort @204), bias @512, weights
+// @1024, block slots (1024-aligned), pool exchange [half][buf][pair][32][8] words
 constexpr int kRwOffBias = 512;
 constexpr int kRwOffW = 1024;
-constexpr int kRwOffRows = kRwOffW + kRwWBytes;
-constexpr int kRwSmemUsed = kRwOffRows + kRwSlots * kRwRowBytes;
-static_assert(kRwOffRows % 1024 == 0, "row slots 1024-aligned");
-static_assert(kRwSlots <= 16, "barrier head layout");
+constexpr int kRwOffSlots = kRwOffW + kRwWBytes;
+constexpr int kRwOffX = kRwOffSlots + kRwSlots * kRwSlotBytes;
+constexpr int kRwXchgBytes = 2 * 2 * 2 * 32 * 8 * 4;
+constexpr int kRwSmemUsed = kRwOffX + kRwXchgBytes;
+static_assert(kRwOffSlots % 1024 == 0 && kRwSlotBytes % 1024 == 0, "block slots 1024-aligned");
 // more than half an SM's shared memory: one CTA an SM (its TMEM is all 512 columns)
 constexpr int kRwSmem = 140 * 1024;
 static_assert(kRwSmemUsed + 1024 <= kRwSmem, "row-conv shared memory");
@@ -677,16 +680,11 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// The CTA's share of the (strip, row) units [g0, g1), in pairs of rows when
-// pooling (P is even, so a pair never straddles two strips).
-__device__ __forceinline__ void rw_share(int units, int pool, int& g0, int& g1) {
+// The CTA's share [g0, g1) of the (strip, block) units, strip-major.
+__device__ __forceinline__ void rw_share(int units, int& g0, int& g1) {
     const int b = blockIdx.x, n = gridDim.x;
     g0 = (int)(((int64_t)units * b) / n);
     g1 = (int)(((int64_t)units * (b + 1)) / n);
-    if (pool) {
-        g0 &= ~1;
-        g1 = b + 1 == n ? units : (g1 & ~1);
-    }
 }
 
 __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_constant__ CUtensorMap tmap,
@@ -695,20 +693,21 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     // offsets below are from the first 1024-byte boundary of the buffer
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
-    const uint32_t full0 = sbase, empty0 = sbase + 128, accf0 = sbase + 256, acce0 = sbase + 288;
-    const uint32_t drain = sbase + 320;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 328);
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 332);
+    const uint32_t full0 = sbase, empty0 = sbase + 64, accf0 = sbase + 128, acce0 = sbase + 160;
+    const uint32_t drain = sbase + 192;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 200);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 204);
     float* sbias = reinterpret_cast<float*>(smem + kRwOffBias);
     unsigned char* wsm = smem + kRwOffW;
-    unsigned char* rows = smem + kRwOffRows;
+    unsigned char* slots = smem + kRwOffSlots;
+    uint32_t* xch = reinterpret_cast<uint32_t*>(smem + kRwOffX);
     const long long wl = g_ws_wait_cycles;
     const int P = A.P;
-    const int strips = (P + kRwStrip - 1) / kRwStrip;
-    const int units = strips * P;
+    const int nblk = (P + kRwBlk - 1) / kRwBlk;
+    const int units = ((P + kRwCols - 1) / kRwCols) * nblk;
     const int pool = A.pool != nullptr;
     int g0, g1;
-    rw_share(units, pool, g0, g1);
+    rw_share(units, g0, g1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 1) {
@@ -729,6 +728,11 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    // launched with programmatic stream serialisation: everything above ran
+    // while the kernel before was finishing; from here on its results are
+    // read (the weights too: the packing kernel may be the one before)
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     // weights and bias into shared memory (generic stores, then a fence to
     // the async proxy the MMAs read through)
     for (int i = threadIdx.x; i < kRwWBytes / 16; i += kRwThreads)
@@ -747,33 +751,21 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     if (warp == 0) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
-            int ld = 0;
-            bool quit = false;
-            for (int g = g0; g < g1 && !quit;) {
-                const int strip = g / P, r0 = g % P, r1 = min(P, r0 + (g1 - g));
-                const int x0 = strip * kRwStrip;
-                for (int i = 0; i < r1 - r0 + 2; ++i, ++ld) {
-                    const int s = ld % kRwSlots;
-                    if (ld >= kRwSlots && !mbar_wait_bounded(empty0 + 8 * s, ((ld / kRwSlots) & 1) ^ 1, wl)) {
-                        give_up();
-                        quit = true;
-                        break;
-                    }
-                    if (*abort_flag) {
-                        quit = true;
-                        break;
-                    }
-                    const uint32_t dst = smem_u32(rows + s * kRwRowBytes);
-                    mbar_expect_tx(full0 + 8 * s, kRwRowBytes);
-#pragma unroll
-                    for (int w = 0; w < 4; ++w)
-                        tma_load_3d(dst + w * 2048, &tmap, 0, x0 + 30 * w - 1, r0 - 1 + i, full0 + 8 * s);
+            int k = 0;
+            for (int u = g0; u < g1; ++u, ++k) {
+                const int s = k % kRwSlots;
+                if (k >= kRwSlots && !mbar_wait_bounded(empty0 + 8 * s, ((k / kRwSlots) & 1) ^ 1, wl)) {
+                    give_up();
+                    break;
                 }
-                g += r1 - r0;
+                if (*abort_flag) break;
+                const int x0 = (u / nblk) * kRwCols, y = (u % nblk) * kRwBlk;
+                mbar_expect_tx(full0 + 8 * s, kRwSlotBytes);
+                tma_load_3d(smem_u32(slots + s * kRwSlotBytes), &tmap, 0, x0 - 1, y - 1, full0 + 8 * s);
             }
             // every copy issued has landed before the CTA leaves (the last
             // use of each slot; fixed bound)
-            for (int j = max(0, ld - kRwSlots); j < ld; ++j)
+            for (int j = max(0, k - kRwSlots); j < k; ++j)
                 if (!mbar_wait_bounded(full0 + 8 * (j % kRwSlots), (j / kRwSlots) & 1, kWsWaitCycles))
                     atomicExch(&g_ws_fault, 1);
         }
@@ -781,43 +773,31 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     } else if (warp == 1) {
         // ---------------- MMA issue ----------------
         if (lane == 0) {
-            const uint32_t rows_u32 = smem_u32(rows), w_u32 = smem_u32(wsm);
-            int ld = 0, o = 0, waited = 0;  // loads [0, waited) are known to have landed
+            const uint32_t slots_u32 = smem_u32(slots), w_u32 = smem_u32(wsm);
             bool quit = false;
-            for (int g = g0; g < g1 && !quit;) {
-                const int r0 = g % P, r1 = min(P, r0 + (g1 - g)), n = r1 - r0;
-                for (int j = 0; j < n; ++j, ++o) {
-                    for (; waited < ld + j + 3 && !quit; ++waited)
-                        if (!mbar_wait_bounded(full0 + 8 * (waited % kRwSlots), (waited / kRwSlots) & 1, wl)) {
-                            give_up();
-                            quit = true;
-                        }
-                    const int q = o & 3;
-                    if (!quit && o >= 4 && !mbar_wait_bounded(acce0 + 8 * q, ((o >> 2) & 1) ^ 1, wl)) {
-                        give_up();
-                        quit = true;
-                    }
-                    if (quit || *abort_flag) {
-                        quit = true;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-#pragma unroll
-                    for (int dy = 0; dy < 3; ++dy) {
-                        const uint32_t rb = rows_u32 + ((ld + j + dy) % kRwSlots) * kRwRowBytes;
-#pragma unroll
-                        for (int kc = 0; kc < 2; ++kc)
-                            rw_mma(tmem + q * 128, sw64_desc(rb + kc * 32),
-                                   tc_desc(w_u32 + (dy * 2 + kc) * 3072, 1536, 128), (dy | kc) ? 1u : 0u);
-                    }
-                    tc_commit(accf0 + 8 * q);
-                    tc_commit(empty0 + 8 * ((ld + j) % kRwSlots));  // row y - 1 is done with
+            int k = 0;
+            for (int u = g0; u < g1; ++u, ++k) {
+                const int s = k % kRwSlots, q = k & 3;
+                if (!mbar_wait_bounded(full0 + 8 * s, (k / kRwSlots) & 1, wl) ||
+                    (k >= 4 && !mbar_wait_bounded(acce0 + 8 * q, ((k >> 2) & 1) ^ 1, wl))) {
+                    give_up();
+                    quit = true;
+                    break;
                 }
-                if (quit) break;
-                tc_commit(empty0 + 8 * ((ld + n) % kRwSlots));
-                tc_commit(empty0 + 8 * ((ld + n + 1) % kRwSlots));
-                ld += n + 2;
-                g += n;
+                if (*abort_flag) {
+                    quit = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t sb = slots_u32 + s * kRwSlotBytes;
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                    for (int kc = 0; kc < 2; ++kc)
+                        rw_mma(tmem + q * 128, sw64_desc(sb + dy * 2048 + kc * 32),
+                               tc_desc(w_u32 + (dy * 2 + kc) * 3072, 1536, 128), (dy | kc) ? 1u : 0u);
+                tc_commit(accf0 + 8 * q);
+                tc_commit(empty0 + 8 * s);
             }
             if (quit) {  // MMAs the epilogue will not wait for may still run
                 tc_commit(drain);
@@ -828,79 +808,82 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     }
     else if (warp >= 4) {
         // ---------------- epilogue ----------------
-        // both warpgroups take every row, warpgroup h the output channels
-        // 16 h .. 16 h + 15
-        const int h = (warp - 4) >> 2;
-        const int wq = warp & 3;          // TMEM lanes 32 wq .. 32 wq + 31 = the warp's pixel group
+        const int h = (warp - 4) >> 2;    // output channels 16 h .. 16 h + 15
+        const int r = warp & 3;           // TMEM lanes 32 r .. 32 r + 31 = output row y + r
         const int Q = P / 2;
         float bias[16];
 #pragma unroll
         for (int c = 0; c < 16; ++c) bias[c] = sbias[16 * h + c];
-        uint32_t prev[8];                 // even row of a pooled pair, bf16x2
-        int o = 0;
-        bool quit = false;
-        for (int g = g0; g < g1 && !quit;) {
-            const int strip = g / P, r0 = g % P, r1 = min(P, r0 + (g1 - g)), n = r1 - r0;
-            const int x = strip * kRwStrip + 30 * wq + lane - 1;
-            const bool valid = lane >= 1 && lane <= 30 && x < P;
-            for (int j = 0; j < n; ++j, ++o) {
-                const int q = o & 3, y = r0 + j;
-                const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * q, (o >> 2) & 1, wl));
-                if (!ok) {
-                    if (lane == 0) give_up();
-                    quit = true;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                float v0[16], v1[16], v2[16];
-                const uint32_t ta = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)(q * 128 + 16 * h);
-                tc_ld16(ta, v0);
-                tc_ld16(ta + 32, v1);
-                tc_ld16(ta + 64, v2);
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(acce0 + 8 * q);  // this warp's part of the accumulator is read
-                uint32_t pk[8];
+        int k = 0;
+        for (int u = g0; u < g1; ++u, ++k) {
+            const int q = k & 3;
+            const int x = (u / nblk) * kRwCols + lane - 1, y = (u % nblk) * kRwBlk + r;
+            const bool valid = lane >= 1 && lane <= kRwCols && x < P && y < P;
+            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * q, (k >> 2) & 1, wl));
+            if (!ok && lane == 0) give_up();
+            uint32_t quit;  // the same decision in the whole warpgroup (it meets at barriers below)
+            asm volatile(
+                "{\n.reg .pred p, t;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred t, %2, 128, p;\nselp.u32 %0, 1, 0, t;\n}\n"
+                : "=r"(quit)
+                : "r"(ok ? 0u : 1u), "r"(1 + h)
+                : "memory");
+            if (quit) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            float v0[16], v1[16], v2[16];
+            const uint32_t ta = tmem + ((uint32_t)(32 * r) << 16) + (uint32_t)(q * 128 + 16 * h);
+            tc_ld16(ta, v0);
+            tc_ld16(ta + 32, v1);
+            tc_ld16(ta + 64, v2);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce0 + 8 * q);  // this warp's part of the accumulator is read
+            uint32_t pk[8];
 #pragma unroll
-                for (int c = 0; c < 16; c += 2) {
-                    const float l0 = __shfl_up_sync(kFull, v0[c], 1), l1 = __shfl_up_sync(kFull, v0[c + 1], 1);
-                    const float r0v = __shfl_down_sync(kFull, v2[c], 1), r1v = __shfl_down_sync(kFull, v2[c + 1], 1);
-                    pk[c / 2] = pack_bf16x2(fmaxf(l0 + v1[c] + r0v + bias[c], 0.f),
-                                            fmaxf(l1 + v1[c + 1] + r1v + bias[c + 1], 0.f));
+            for (int c = 0; c < 16; c += 2) {
+                const float l0 = __shfl_up_sync(kFull, v0[c], 1), l1 = __shfl_up_sync(kFull, v0[c + 1], 1);
+                const float r0v = __shfl_down_sync(kFull, v2[c], 1), r1v = __shfl_down_sync(kFull, v2[c + 1], 1);
+                pk[c / 2] = pack_bf16x2(fmaxf(l0 + v1[c] + r0v + bias[c], 0.f),
+                                        fmaxf(l1 + v1[c + 1] + r1v + bias[c + 1], 0.f));
+            }
+            if (valid) {
+                uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+            if (pool) {
+                // rows y (r even) and y + 1 meet in shared memory (double
+                // buffered by block: one barrier a block)
+                uint4* xb = reinterpret_cast<uint4*>(xch + (((h * 2 + (k & 1)) * 2 + (r >> 1)) * 32 + lane) * 8);
+                if ((r & 1) == 0) {
+                    xb[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    xb[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
                 }
-                if (valid) {
-                    uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
-                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                }
-                if (pool) {
-                    if ((y & 1) == 0) {
+                asm volatile("bar.sync %0, 128;\n" ::"r"(1 + h) : "memory");
+                if (r & 1) {
+                    // 0.25 (v(y-1, x) + v(y-1, x+1) + v(y, x) + v(y, x+1)) of the
+                    // bf16 values; lane l + 1 holds column x + 1
+                    uint32_t pp[8], pe[8];
+                    *reinterpret_cast<uint4*>(pe) = xb[0];
+                    *reinterpret_cast<uint4*>(pe + 4) = xb[1];
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) prev[c] = pk[c];
-                    } else {
-                        // 0.25 (v(y-1, x) + v(y-1, x+1) + v(y, x) + v(y, x+1)) of the
-                        // bf16 values; lane l + 1 holds column x + 1
-                        uint32_t pp[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            const uint32_t pr = __shfl_down_sync(kFull, prev[c], 1);
-                            const uint32_t cr = __shfl_down_sync(kFull, pk[c], 1);
-                            const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&prev[c]));
-                            const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pr));
-                            const float2 d = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[c]));
-                            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&cr));
-                            pp[c] = pack_bf16x2(0.25f * (a.x + b.x + d.x + f.x), 0.25f * (a.y + b.y + d.y + f.y));
-                        }
-                        if (valid && (lane & 1) && (x >> 1) < Q) {
-                            uint4* dst = reinterpret_cast<uint4*>(A.pool + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + 16 * h);
-                            dst[0] = make_uint4(pp[0], pp[1], pp[2], pp[3]);
-                            dst[1] = make_uint4(pp[4], pp[5], pp[6], pp[7]);
-                        }
+                    for (int c = 0; c < 8; ++c) {
+                        const uint32_t pv = pe[c];
+                        const uint32_t pr = __shfl_down_sync(kFull, pv, 1);
+                        const uint32_t cr = __shfl_down_sync(kFull, pk[c], 1);
+                        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pv));
+                        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pr));
+                        const float2 d = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[c]));
+                        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&cr));
+                        pp[c] = pack_bf16x2(0.25f * (a.x + b.x + d.x + f.x), 0.25f * (a.y + b.y + d.y + f.y));
+                    }
+                    if (valid && (lane & 1) && (x >> 1) < Q) {
+                        uint4* dst = reinterpret_cast<uint4*>(A.pool + ((int64_t)(y >> 1) * Q + (x >> 1)) * C + 16 * h);
+                        dst[0] = make_uint4(pp[0], pp[1], pp[2], pp[3]);
+                        dst[1] = make_uint4(pp[4], pp[5], pp[6], pp[7]);
                     }
                 }
             }
-            g += n;
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -1571,7 +1554,7 @@ struct pic_ws {
 namespace picb200 {
 
 // TMA descriptor of an NHWC bf16 image of P x P pixels and 32 channels,
-// read in boxes of 32 channels x 32 pixels x 1 row (64 bytes a pixel,
+// read in boxes of 32 channels x 32 pixels x 6 rows (64 bytes a pixel,
 // 64-byte swizzle, zero filled outside).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -1589,7 +1572,7 @@ static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P) {
     }
     const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)P, (cuuint64_t)P};
     const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)P * C * 2};
-    const cuuint32_t box[3] = {(cuuint32_t)C, 32, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)C, 32, (cuuint32_t)kRwBoxRows};
     const cuuint32_t es[3] = {1, 1, 1};
     const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dims,
                               strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
@@ -1746,7 +1729,7 @@ static void conv32_tc(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloa
         in, N.w16 + (int64_t)layer * kW32, N.w + param_off(layer + 1) + kW32, P, out, pool_out);
 }
 
-// Forward 32->32 convolution `layer` on the row-streaming tcgen05 kernel,
+// Forward 32->32 convolution `layer` on the block-streaming tcgen05 kernel,
 // its input being the layer's TMA descriptor's image; the decoder's
 // upsample-and-skip sum u = up2(up) + skip is formed first when `up` is given.
 static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfloat16* pool,
@@ -1757,16 +1740,25 @@ static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfl
         k_up_add8<<<g1((int64_t)P * P * 4), 256, 0, c->stream>>>(up, skip, P, u);
         c->launches += 1;
     }
-    const int units = ((P + kRwStrip - 1) / kRwStrip) * P;
-    // at least 16 rows a CTA: the two halo rows of a CTA's share stay small
-    const int grid = std::max(1, std::min(N.sms, units / 16));
+    const int units = ((P + kRwCols - 1) / kRwCols) * ((P + kRwBlk - 1) / kRwBlk);
+    const int grid = std::max(1, std::min(N.sms, (units + 3) / 4));
     RowConvArgs A;
     A.w = N.wrows + (int64_t)layer * (kRwWBytes / 2);
     A.bias = N.w + param_off(layer + 1) + kW32;
     A.out = out;
     A.pool = pool;
     A.P = P;
-    k_conv_rows<<<grid, kRwThreads, kRwSmem, c->stream>>>(N.tm_in[layer], A);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kRwThreads);
+    cfg.dynamicSmemBytes = kRwSmem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_conv_rows, N.tm_in[layer], A);
     c->launches += 1;
 }
 
