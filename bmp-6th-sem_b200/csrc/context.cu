@@ -880,6 +880,13 @@ int pic_debug_set_wait_limits(pic_ctx* c, int64_t barrier_polls, int64_t tensor_
     return PIC_OK;
 }
 
+int pic_debug_vcycle(pic_ctx* c, const float* rhs, float* out, int per_sweep) {
+    if (!c || !rhs || !out) return fail(PIC_ERR_ARG, "null argument");
+    PIC_CUDA(cudaSetDevice(c->cfg.device));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    return poisson_debug_vcycle(c, rhs, out, per_sweep);
+}
+
 int pic_launch_count(pic_ctx* c, int64_t* n) {
     if (!c || !n) return fail(PIC_ERR_ARG, "null argument");
     *n = c->launches;
@@ -898,6 +905,12 @@ int pic_set_poisson(pic_ctx* c, int solver, int warm, double tol, int maxit) {
     c->ps.warm = warm;
     c->ps.tol = tol;
     c->ps.maxit = maxit;
+    return PIC_OK;
+}
+
+int pic_set_poisson_graph(pic_ctx* c, int enable) {
+    if (!c) return fail(PIC_ERR_ARG, "null context");
+    c->ps.graph_off = enable == 0;
     return PIC_OK;
 }
 

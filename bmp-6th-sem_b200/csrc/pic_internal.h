@@ -138,6 +138,7 @@ struct MGLevel {
     uint8_t* mask;     // 1 = Dirichlet
     float* x;
     float* b;
+    float* xo;         // the up sweep's output (its tiles read x around them)
 };
 
 struct PoissonState {
@@ -173,6 +174,7 @@ struct PoissonState {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int body_nodes[2] = {0, 0};
     bool graph_failed = false;
+    bool graph_off = false;  // pic_set_poisson_graph(ctx, 0): direct launches
 };
 
 }  // namespace picb200
@@ -282,6 +284,7 @@ int ws_after_solve(pic_ctx* c, bool record);
 // poisson.cu
 int poisson_setup(pic_ctx* c);
 void poisson_free(pic_ctx* c);
+int poisson_debug_vcycle(pic_ctx* c, const float* rhs, float* out, int per_sweep);
 int poisson_solve(pic_ctx* c);
 int fields_from_phi(pic_ctx* c);
 int overwrite_phi(pic_ctx* c);  // electrode nodes take their potential

@@ -245,23 +245,26 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t nodes, const uin
 // previous direction), so one pass reads z's neighbours and no kernel
 // boundary is needed between the two; partial p.q.  beta = rz/rz_old, 0 on
 // the first iteration after a (re)start (marked by rz_old == 0).
+// z is FP64 (k_pcg_rz's) or the V-cycle's FP32 output (0 at electrodes)
+template <typename Z>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_pq(Grid64 g, const uint8_t* mask,
-                                                        const double* z, double* p, double* q,
+                                                        const Z* zs, double* p, double* q,
                                                         double* partials, int nblocks,
                                                         unsigned* arrive, double* scal) {
     pdl_enter();
     const double ro = scal[S_RZ_OLD];
     const double beta = ro == 0.0 ? 0.0 : scal[S_RZ] / ro;
     const int64_t nodes = g.n;
+    auto z = [&](int64_t k) { return (double)zs[k]; };
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes;
          i += (int64_t)gridDim.x * blockDim.x) {
         double pi = 0.0, qi = 0.0;
         if (!mask[i]) {
-            const double az = g.cd * z[i] - g.cx * (z[i - 1] + z[i + 1]) -
-                              g.cy * (z[row_dn(i, nodes, g.GX)] + z[row_up(i, nodes, g.GX)]);
+            const double az = g.cd * z(i) - g.cx * (z(i - 1) + z(i + 1)) -
+                              g.cy * (z(row_dn(i, nodes, g.GX)) + z(row_up(i, nodes, g.GX)));
             // (after a restart p and q are not read: beta == 0)
-            pi = beta == 0.0 ? z[i] : z[i] + beta * p[i];
+            pi = beta == 0.0 ? z(i) : z(i) + beta * p[i];
             qi = beta == 0.0 ? az : az + beta * q[i];
         }
         p[i] = pi;
@@ -358,6 +361,16 @@ __global__ void k_mg_rbgs(LevelDev L, int color) {
     L.x[k] = s / L.cd;
 }
 
+// b - A x at one node from its value c and its neighbours west, east, down,
+// up; every operation rounded as written (no contraction), so each kernel
+// that computes a residual gets the same bits
+__device__ __forceinline__ float mg_residual(float b, float c, float w, float e, float d, float u,
+                                             float cx, float cy, float cd) {
+    const float ax = __fsub_rn(__fsub_rn(__fmul_rn(cd, c), __fmul_rn(cx, __fadd_rn(w, e))),
+                               __fmul_rn(cy, __fadd_rn(d, u)));
+    return __fsub_rn(b, ax);
+}
+
 // Residual at fine node (i, j); 0 outside the x range and at electrodes.
 // Rows wrap (only reached periodic in y: with walls the restriction of an
 // interior coarse node stays inside the fine rows).
@@ -366,9 +379,8 @@ __device__ __forceinline__ float fine_residual(const LevelDev& F, int i, int j) 
     j = j < 0 ? j + F.GY : (j >= F.GY ? j - F.GY : j);
     const int k = j * F.GX + i, n = F.GX * F.GY;
     if (F.mask[k]) return 0.0f;
-    const float ax = F.cd * F.x[k] - F.cx * (F.x[k - 1] + F.x[k + 1]) -
-                     F.cy * (F.x[row_dn(k, n, F.GX)] + F.x[row_up(k, n, F.GX)]);
-    return F.b[k] - ax;
+    return mg_residual(F.b[k], F.x[k], F.x[k - 1], F.x[k + 1], F.x[row_dn(k, n, F.GX)],
+                       F.x[row_up(k, n, F.GX)], F.cx, F.cy, F.cd);
 }
 
 // b_coarse = full weighting of the fine residual
@@ -446,6 +458,163 @@ __global__ void k_mg_prolong_black(LevelDev F, LevelDev C) {
     const float s = __fmaf_rn(F.cx, prolonged(F, C, i - 1, j) + prolonged(F, C, i + 1, j),
                               __fmaf_rn(F.cy, prolonged(F, C, i, jd) + prolonged(F, C, i, ju), F.b[k]));
     F.x[k] = s / F.cd;
+}
+
+
+// ---- a whole level a kernel (temporal blocking) ----------------------------
+//
+// The per-sweep kernels above take 4 kNu launches a level, each a full pass
+// over the level's nodes.  Here a block copies a tile of the level, with a
+// halo, into shared memory and runs all of the level's sweeps there, the
+// region it has right shrinking by one node a sweep; only the tile's core is
+// written back.  Every node goes through the operations of the per-sweep
+// kernels in the same order, so the iterates are the same bits; the halo
+// nodes are recomputed by each neighbouring tile.
+//   k_mg_down: zero start, black, (red, black) x (kNu - 1), residual and its
+//     full weighting into the coarse right-hand side.  Core 32 x 32 fine
+//     nodes (16 x 16 coarse), halo 2 kNu + 1 (sweeps, residual, weighting).
+//   k_mg_up: coarse correction, black, red, (black, red) x (kNu - 1).  Core
+//     32 x 32, halo 2 kNu.  Its halo reads the level's x where neighbouring
+//     tiles write their cores, so it writes a second array (MGLevel::xo).
+// Region rows wrap at the level's row count like row_up / row_dn (only
+// periodic in y matters: with walls the first and last rows are electrodes,
+// never updated, so nothing crosses them); a level smaller than the region
+// just appears more than once in it, each copy updated alike.  Columns left
+// and right of the level are electrodes of value 0 (the x walls are
+// electrodes, so their values are never used).
+constexpr int kTileCore = 32;
+constexpr int kDownHalo = 2 * kNu + 1;
+constexpr int kUpHalo = 2 * kNu;
+constexpr int kDownSide = kTileCore + 2 * kDownHalo;
+constexpr int kUpSide = kTileCore + 2 * kUpHalo;
+constexpr int kTileThreads = 256;
+static_assert(kDownSide % 2 == 0 && kUpSide % 2 == 0, "tile rows hold as many nodes of each colour");
+
+// node index of level coordinates (i, j), rows wrapped; -1 outside the columns
+__device__ __forceinline__ int tile_node(const LevelDev& L, int i, int j) {
+    if (i < 0 || i >= L.GX) return -1;
+    j %= L.GY;
+    return j < 0 ? (j + L.GY) * L.GX + i : j * L.GX + i;
+}
+
+// one colour over the region's inner nodes (k_mg_rbgs's arithmetic); region
+// node (li, lj) is level node (i0 + li, j0 + lj), colour (i + j) & 1 (rows
+// wrap only at an even row count, so wrapping keeps the colour)
+template <int S>
+__device__ __forceinline__ void tile_half_sweep(float* x, const float* b, const uint8_t* m, float cx,
+                                                float cy, float cd, int color, int i0, int j0) {
+    constexpr int HS = S / 2;
+    for (int h = threadIdx.x; h < HS * S; h += kTileThreads) {
+        const int lj = h / HS;
+        const int li = 2 * (h - lj * HS) + ((i0 + j0 + lj + color) & 1);
+        const int t = lj * S + li;
+        if (li == 0 || lj == 0 || li == S - 1 || lj == S - 1 || m[t]) continue;
+        const float s = __fmaf_rn(cx, x[t - 1] + x[t + 1], __fmaf_rn(cy, x[t - S] + x[t + S], b[t]));
+        x[t] = s / cd;
+    }
+    __syncthreads();
+}
+
+// level F's smoothing from a zero start, then C.b = restriction of F's residual
+__global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C) {
+    constexpr int S = kDownSide, H = kDownHalo, CC = kTileCore / 2;
+    __shared__ float sx[S * S], sb[S * S], sr[S * S];
+    __shared__ uint8_t sm[S * S];
+    pdl_enter();
+    const int I0 = blockIdx.x * CC, J0 = blockIdx.y * CC;  // first coarse node of the tile
+    const int i0 = 2 * I0 - H, j0 = 2 * J0 - H;            // level node of region node (0, 0)
+    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
+        const int li = t % S, lj = t / S;
+        const int k = tile_node(F, i0 + li, j0 + lj);
+        const bool msk = k < 0 || F.mask[k];
+        const float bv = k < 0 ? 0.0f : F.b[k];
+        sm[t] = msk;
+        sb[t] = bv;
+        // zero start: the black sweep reads red x = b / cd (electrodes 0);
+        // black values are written before anything reads them
+        sx[t] = (!msk && ((i0 + li + j0 + lj) & 1) == 0) ? bv / F.cd : 0.0f;
+    }
+    __syncthreads();
+    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    for (int s = 1; s < kNu; ++s) {
+        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    }
+    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
+        const int li = t % S, lj = t / S;
+        float rv = 0.0f;
+        if (li > 0 && lj > 0 && li < S - 1 && lj < S - 1 && !sm[t])
+            rv = mg_residual(sb[t], sx[t], sx[t - 1], sx[t + 1], sx[t - S], sx[t + S], F.cx, F.cy, F.cd);
+        sr[t] = rv;
+        const int i = i0 + li, j = j0 + lj;
+        if (li >= H && lj >= H && li < H + kTileCore && lj < H + kTileCore && !sm[t] && j < F.GY)
+            F.x[j * F.GX + i] = sx[t];
+    }
+    __syncthreads();
+    // full weighting, in k_mg_restrict's order
+    for (int t = threadIdx.x; t < CC * CC; t += kTileThreads) {
+        const int I = I0 + t % CC, J = J0 + t / CC;
+        if (I >= C.GX || J >= C.GY) continue;
+        const int64_t kc = (int64_t)J * C.GX + I;
+        if (C.mask[kc]) {
+            C.b[kc] = 0.0f;
+            continue;
+        }
+        const int c = (2 * J - j0) * S + (2 * I - i0);
+        float s = 4.0f * sr[c];
+        s += 2.0f * (sr[c - 1] + sr[c + 1] + sr[c - S] + sr[c + S]);
+        s += sr[c - S - 1] + sr[c - S + 1] + sr[c + S - 1] + sr[c + S + 1];
+        C.b[kc] = s * 0.0625f;
+    }
+}
+
+// Where the finest level's k_mg_up also starts the PCG iteration: z is its
+// output (FP32, electrodes 0), and it reduces r.z into scal[S_RZ] like
+// k_pcg_rz (per-block partials over the tile cores, summed in block order).
+struct RzArgs {
+    const double* r;
+    double* partials;
+    unsigned* arrive;
+    double* scal;
+};
+static_assert(kTileThreads == kRedThreads, "k_mg_up's reduction uses the PCG block reduction");
+
+// xo = level F's x corrected by C.x and smoothed; with kRz also r.z
+template <bool kRz>
+__global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, float* xo, RzArgs R) {
+    constexpr int S = kUpSide, H = kUpHalo;
+    __shared__ float sx[S * S], sb[S * S];
+    __shared__ uint8_t sm[S * S];
+    pdl_enter();
+    const int i0 = blockIdx.x * kTileCore - H, j0 = blockIdx.y * kTileCore - H;
+    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
+        const int i = i0 + t % S;
+        int j = (j0 + t / S) % F.GY;
+        if (j < 0) j += F.GY;
+        const bool in = i >= 0 && i < F.GX;
+        const int k = j * F.GX + i;
+        const bool msk = !in || F.mask[k];
+        sm[t] = msk;
+        sb[t] = in ? F.b[k] : 0.0f;
+        sx[t] = msk ? (in ? F.x[k] : 0.0f) : prolonged(F, C, i, j);
+    }
+    __syncthreads();
+    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+    for (int s = 1; s < kNu; ++s) {
+        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+    }
+    double acc[1] = {0.0};
+    for (int t = threadIdx.x; t < kTileCore * kTileCore; t += kTileThreads) {
+        const int li = H + t % kTileCore, lj = H + t / kTileCore;
+        const int i = i0 + li, j = j0 + lj;
+        if (i >= F.GX || j >= F.GY || sm[lj * S + li]) continue;
+        const float z = sx[lj * S + li];
+        xo[j * F.GX + i] = z;
+        if (kRz) acc[0] += R.r[j * F.GX + i] * (double)z;
+    }
+    if (kRz) reduce_finalize<1>(acc, R.partials, gridDim.x * gridDim.y, R.arrive, R.scal, S_RZ);
 }
 
 
@@ -694,11 +863,50 @@ void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_
     cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
-int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
+// One V-cycle on st from levels[0].b; the result is in vcycle_out().
+// Returns the number of kernels.  Levels above the fused ones take two
+// kernels each (k_mg_down, k_mg_up); with with_rz the finest k_mg_up also
+// reduces r.z for the PCG iteration.
+int enqueue_vcycle(pic_ctx* c, cudaStream_t st, bool with_rz) {
+    PoissonState& ps = c->ps;
+    const int kf = ps.fused_first;
+    const dim3 tb(kTileThreads);
+    int launches = 0;
+    for (int l = 0; l < kf; ++l) {
+        const LevelDev F = as_dev(ps.levels[l]);
+        const LevelDev C = as_dev(ps.levels[l + 1]);
+        const int cc = kTileCore / 2;
+        launch_pdl(k_mg_down, dim3((C.GX + cc - 1) / cc, (C.GY + cc - 1) / cc), tb, 0, st, F, C);
+        launches += 1;
+    }
+    launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
+               *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    launches += 1;
+    for (int l = kf - 1; l >= 0; --l) {
+        const LevelDev F = as_dev(ps.levels[l]);
+        LevelDev C = as_dev(ps.levels[l + 1]);
+        if (l + 1 < kf) C.x = ps.levels[l + 1].xo;  // what the coarser k_mg_up wrote
+        const dim3 grid((F.GX + kTileCore - 1) / kTileCore, (F.GY + kTileCore - 1) / kTileCore);
+        if (l == 0 && with_rz)
+            launch_pdl(k_mg_up<true>, grid, tb, 0, st, F, C, ps.levels[l].xo,
+                       RzArgs{ps.r, ps.partials, arrive_ptr(ps), ps.scal});
+        else
+            launch_pdl(k_mg_up<false>, grid, tb, 0, st, F, C, ps.levels[l].xo, RzArgs{});
+        launches += 1;
+    }
+    return launches;
+}
+
+const float* vcycle_out(const PoissonState& ps) {
+    return ps.fused_first > 0 ? ps.levels[0].xo : ps.levels[0].x;
+}
+
+// The same V-cycle with one kernel a half sweep, updating each level's x in
+// place (the result in levels[0].x): the check of the tiled one.
+void enqueue_vcycle_per_sweep(pic_ctx* c, cudaStream_t st) {
     PoissonState& ps = c->ps;
     const int kf = ps.fused_first;
     const dim3 b2(32, 8);
-    int launches = 0;
     for (int l = 0; l < kf; ++l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
@@ -709,11 +917,9 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
         }
         launch_pdl(k_mg_restrict, grid2d(C.GX, C.GY, b2), b2, 0, st, F, C);
-        launches += 2 * kNu;
     }
     launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
                *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
-    launches += 1;
     for (int l = kf - 1; l >= 0; --l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
@@ -724,9 +930,23 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st) {
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 1);
             launch_pdl(k_mg_rbgs, gh, b2, 0, st, F, 0);
         }
-        launches += 2 * kNu;
     }
-    return launches;
+}
+
+// One V-cycle applied to a host right-hand side (FP32, one value a node),
+// tiled (per_sweep 0) or one kernel a half sweep (1); the result into out.
+int debug_vcycle(pic_ctx* c, const float* rhs, float* out, int per_sweep) {
+    PoissonState& ps = c->ps;
+    if (!ps.mg_ok) return fail(PIC_ERR_CONFIG, "no multigrid hierarchy on this grid");
+    const size_t bytes = (size_t)ps.levels[0].nodes * sizeof(float);
+    PIC_CUDA(cudaMemcpyAsync(ps.levels[0].b, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (per_sweep) enqueue_vcycle_per_sweep(c, c->stream);
+    else enqueue_vcycle(c, c->stream, false);
+    PIC_CUDA(cudaGetLastError());
+    PIC_CUDA(cudaMemcpyAsync(out, per_sweep ? ps.levels[0].x : vcycle_out(ps), bytes, cudaMemcpyDeviceToHost,
+                             c->stream));
+    PIC_CUDA(cudaStreamSynchronize(c->stream));
+    return PIC_OK;
 }
 
 // One PCG iteration enqueued on st; returns the number of kernels.
@@ -737,15 +957,24 @@ int enqueue_iteration(pic_ctx* c, cudaStream_t st, bool jacobi,
     const int nb = ps.nblocks;
     unsigned* arrive = arrive_ptr(ps);
     int launches = 0;
-    if (!jacobi) launches += enqueue_vcycle(c, st);
     const dim3 gb(nb), tb(kRedThreads);
-    launch_pdl(k_pcg_rz, gb, tb, 0, st, g.n, c->mask, ps.r, ps.levels[0].x, 1.0 / g.cd,
-               jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
-    launch_pdl(k_pcg_pq, gb, tb, 0, st, g, c->mask, ps.z, ps.p[0], ps.q, ps.partials, nb, arrive,
-               ps.scal);
+    // with tiled levels the finest k_mg_up computes r.z and pq reads its
+    // FP32 output; otherwise k_pcg_rz makes z
+    const bool rz_in_vcycle = !jacobi && ps.fused_first > 0;
+    if (!jacobi) launches += enqueue_vcycle(c, st, rz_in_vcycle);
+    if (rz_in_vcycle) {
+        launch_pdl(k_pcg_pq<float>, gb, tb, 0, st, g, c->mask, vcycle_out(ps), ps.p[0], ps.q, ps.partials,
+                   nb, arrive, ps.scal);
+    } else {
+        launch_pdl(k_pcg_rz, gb, tb, 0, st, g.n, c->mask, ps.r, vcycle_out(ps), 1.0 / g.cd,
+                   jacobi ? 1 : 0, ps.z, ps.partials, nb, arrive, ps.scal);
+        launch_pdl(k_pcg_pq<double>, gb, tb, 0, st, g, c->mask, (const double*)ps.z, ps.p[0], ps.q,
+                   ps.partials, nb, arrive, ps.scal);
+        launches += 1;
+    }
     launch_pdl(k_pcg_update, gb, tb, 0, st, g.n, c->mask, ps.p[0], ps.q, c->phi, ps.r,
                ps.levels[0].b, ps.partials, nb, arrive, ps.scal, handle, use_handle);
-    return launches + 3;
+    return launches + 2;
 }
 
 __global__ void k_cond_init(const double* scal, cudaGraphConditionalHandle handle) {
@@ -796,6 +1025,10 @@ int build_graph(pic_ctx* c, bool jacobi) {
 
 }  // namespace
 
+int poisson_debug_vcycle(pic_ctx* c, const float* rhs, float* out, int per_sweep) {
+    return debug_vcycle(c, rhs, out, per_sweep);
+}
+
 // ---------------------------------------------------------------------------
 
 int poisson_setup(pic_ctx* c) {
@@ -814,7 +1047,10 @@ int poisson_setup(pic_ctx* c) {
     PIC_CUDA(cudaMemsetAsync(ps.p[1], 0, n * 8, c->stream));
     PIC_CUDA(cudaMemsetAsync(ps.q, 0, n * 8, c->stream));
     ps.nblocks = (int)std::min<int64_t>((c->nodes + kRedThreads - 1) / kRedThreads, 148 * 8);
-    PIC_CUDA(cudaMalloc(&ps.partials, (size_t)ps.nblocks * 4 * sizeof(double)));
+    // room for the PCG kernels' partials and for the finest k_mg_up's (one per tile)
+    const size_t up_tiles = (size_t)((c->GX + kTileCore - 1) / kTileCore) *
+                            (size_t)((c->solve_rows + kTileCore - 1) / kTileCore);
+    PIC_CUDA(cudaMalloc(&ps.partials, std::max((size_t)ps.nblocks * 4, up_tiles) * sizeof(double)));
     PIC_CUDA(cudaMalloc(&ps.scal, 16 * sizeof(double)));
     PIC_CUDA(cudaMemsetAsync(ps.scal, 0, 16 * sizeof(double), c->stream));
     PIC_CUDA(cudaMallocHost(&ps.host_scal, 16 * sizeof(double)));
@@ -841,7 +1077,9 @@ int poisson_setup(pic_ctx* c) {
         L.cd = 2.0f * (L.cx + L.cy);
         PIC_CUDA(cudaMalloc(&L.x, (size_t)L.nodes * 4));
         PIC_CUDA(cudaMalloc(&L.b, (size_t)L.nodes * 4));
+        PIC_CUDA(cudaMalloc(&L.xo, (size_t)L.nodes * 4));
         PIC_CUDA(cudaMemsetAsync(L.x, 0, (size_t)L.nodes * 4, c->stream));
+        PIC_CUDA(cudaMemsetAsync(L.xo, 0, (size_t)L.nodes * 4, c->stream));
         PIC_CUDA(cudaMemsetAsync(L.b, 0, (size_t)L.nodes * 4, c->stream));
         if (l == 0) {
             L.mask = c->mask;
@@ -930,6 +1168,7 @@ void poisson_free(pic_ctx* c) {
     PoissonState& ps = c->ps;
     for (size_t l = 0; l < ps.levels.size(); ++l) {
         cudaFree(ps.levels[l].x);
+        cudaFree(ps.levels[l].xo);
         cudaFree(ps.levels[l].b);
         if (l > 0) cudaFree(ps.levels[l].mask);
     }
@@ -991,7 +1230,7 @@ int poisson_solve(pic_ctx* c) {
         k_fix_bb<<<1, 1, 0, c->stream>>>(ps.scal, tol2, ps.maxit, restarts > 0 ? 1 : 0);
         c->launches += 2;
         PIC_CUDA(cudaGetLastError());
-        if (ps.gexec[slot]) {
+        if (ps.gexec[slot] && !ps.graph_off) {
             PIC_CUDA(cudaGraphLaunch(ps.gexec[slot], c->stream));
         } else {
             // host-driven loop: one synchronisation per iteration
@@ -1030,7 +1269,7 @@ int poisson_solve(pic_ctx* c) {
         ++restarts;
     }
     const int it = (int)ps.host_scal[S_IT];
-    if (ps.gexec[slot]) c->launches += (int64_t)it * ps.body_nodes[slot] + 1;
+    if (ps.gexec[slot] && !ps.graph_off) c->launches += (int64_t)it * ps.body_nodes[slot] + 1;
     if (ws_active && status == PIC_OK) PIC_TRY(ws_after_solve(c, c->ws_record));
     if (c->periodic) PIC_TRY(overwrite_phi(c));  // the last row repeats row 0
     PIC_TRY(fields_from_phi(c));

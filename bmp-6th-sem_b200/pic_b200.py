@@ -166,6 +166,8 @@ def lib():
         "pic_deposit_points_noalloc": (cint, [vp, i64, i32, i32, dbl, dbl, vp, dbl, dbl, vp, vp, vp]),
         "pic_write_diagnostics": (cint, [vp, ctypes.c_char_p, cint, dbl]),
         "pic_debug_set_wait_limits": (cint, [vp, i64, i64]),
+        "pic_debug_vcycle": (cint, [vp, vp, vp, cint]),
+        "pic_set_poisson_graph": (cint, [vp, cint]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -268,6 +268,15 @@ int pic_launch_count(pic_ctx* ctx, int64_t* n);
  * without any fault; values <= 0 restore the defaults.  Device-wide: it
  * affects every context on that device. */
 int pic_debug_set_wait_limits(pic_ctx* ctx, int64_t barrier_polls, int64_t tensor_wait_cycles);
+/* Test hook (no reference counterpart).  Applies one multigrid V-cycle (the
+ * PCG's preconditioner) to rhs, one FP32 value per node in the context's
+ * node order, and writes the result to out (host buffers).  per_sweep = 0
+ * runs the solver's own V-cycle (a level's sweeps in one kernel, on tiles in
+ * shared memory), 1 the same V-cycle with one kernel per half sweep; the
+ * two give the same bits.  PIC_ERR_CONFIG when the grid has no multigrid
+ * hierarchy.  Overwrites the solver's multigrid work arrays: not during a
+ * solve in flight on another stream. */
+int pic_debug_vcycle(pic_ctx* ctx, const float* rhs, float* out, int per_sweep);
 
 /* ---- tuning (no reference counterpart) -----------------------------------
  * The particle kernels are built for PIC_NUM_TILE_SHAPES tile shapes of 256
@@ -390,6 +399,11 @@ int pic_ensemble_info(pic_ensemble* ens, int* graph_active, int* tile_shape, int
 
 /* ---- Poisson controls -------------------------------------------------- */
 int pic_set_poisson(pic_ctx* ctx, int solver, int warm_start, double tol, int maxit);
+/* (no reference counterpart) enable = 0: run the PCG iterations as direct
+ * launches with one host synchronisation per iteration instead of one CUDA
+ * graph per solve (same kernels, same results; slower).  For profilers that
+ * do not follow the kernels of a graph's conditional node.  Default 1. */
+int pic_set_poisson_graph(pic_ctx* ctx, int enable);
 /* Iterations, achieved relative residual and device milliseconds of the most
  * recent solve. */
 int pic_poisson_stats(pic_ctx* ctx, int* iterations, double* relres, double* ms);
