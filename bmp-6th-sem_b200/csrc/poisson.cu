@@ -490,12 +490,17 @@ constexpr int kUpSide = kTileCore + 2 * kUpHalo;
 constexpr int kTileThreads = 256;
 static_assert(kDownSide % 2 == 0 && kUpSide % 2 == 0, "tile rows hold as many nodes of each colour");
 
-// node index of level coordinates (i, j), rows wrapped; -1 outside the columns
-__device__ __forceinline__ int tile_node(const LevelDev& L, int i, int j) {
-    if (i < 0 || i >= L.GX) return -1;
-    j %= L.GY;
-    return j < 0 ? (j + L.GY) * L.GX + i : j * L.GX + i;
+// level row of region row j (rows wrap at the level's row count)
+__device__ __forceinline__ int tile_row(int j, int GY) {
+    j %= GY;
+    return j < 0 ? j + GY : j;
 }
+
+// Region nodes a thread loads: all its loads are issued before the first
+// result is used (the load phase is one round trip to memory, not one per
+// node).
+template <int S>
+constexpr int tile_loads() { return (S * S + kTileThreads - 1) / kTileThreads; }
 
 // one colour over the region's inner nodes (k_mg_rbgs's arithmetic); region
 // node (li, lj) is level node (i0 + li, j0 + lj), colour (i + j) & 1 (rows
@@ -523,16 +528,31 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C
     pdl_enter();
     const int I0 = blockIdx.x * CC, J0 = blockIdx.y * CC;  // first coarse node of the tile
     const int i0 = 2 * I0 - H, j0 = 2 * J0 - H;            // level node of region node (0, 0)
-    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
-        const int li = t % S, lj = t / S;
-        const int k = tile_node(F, i0 + li, j0 + lj);
-        const bool msk = k < 0 || F.mask[k];
-        const float bv = k < 0 ? 0.0f : F.b[k];
-        sm[t] = msk;
-        sb[t] = bv;
-        // zero start: the black sweep reads red x = b / cd (electrodes 0);
-        // black values are written before anything reads them
-        sx[t] = (!msk && ((i0 + li + j0 + lj) & 1) == 0) ? bv / F.cd : 0.0f;
+    {
+        constexpr int NL = tile_loads<S>();
+        int kk[NL];
+        uint8_t mv[NL];
+        float bv[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int t = threadIdx.x + u * kTileThreads, li = t % S, lj = t / S, i = i0 + li;
+            kk[u] = (t < S * S && i >= 0 && i < F.GX) ? tile_row(j0 + lj, F.GY) * F.GX + i : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            mv[u] = kk[u] < 0 ? 1 : F.mask[kk[u]];
+            bv[u] = kk[u] < 0 ? 0.0f : F.b[kk[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int t = threadIdx.x + u * kTileThreads, li = t % S, lj = t / S;
+            if (t >= S * S) break;
+            sm[t] = mv[u];
+            sb[t] = bv[u];
+            // zero start: the black sweep reads red x = b / cd (electrodes 0);
+            // black values are written before anything reads them
+            sx[t] = (!mv[u] && ((i0 + li + j0 + lj) & 1) == 0) ? bv[u] / F.cd : 0.0f;
+        }
     }
     __syncthreads();
     tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
@@ -587,16 +607,58 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, 
     __shared__ uint8_t sm[S * S];
     pdl_enter();
     const int i0 = blockIdx.x * kTileCore - H, j0 = blockIdx.y * kTileCore - H;
-    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
-        const int i = i0 + t % S;
-        int j = (j0 + t / S) % F.GY;
-        if (j < 0) j += F.GY;
-        const bool in = i >= 0 && i < F.GX;
-        const int k = j * F.GX + i;
-        const bool msk = !in || F.mask[k];
-        sm[t] = msk;
-        sb[t] = in ? F.b[k] : 0.0f;
-        sx[t] = msk ? (in ? F.x[k] : 0.0f) : prolonged(F, C, i, j);
+    {
+        // the node's mask, b, x and the four coarse values prolonged() reads
+        // (column I + 1 clamped: only read for odd i < GX - 1), all loaded
+        // before any is used
+        constexpr int NL = tile_loads<S>();
+        int kk[NL], c00[NL], c10[NL], c01[NL], c11[NL];
+        uint8_t mv[NL];
+        float bv[NL], xv[NL], x00[NL], x10[NL], x01[NL], x11[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int t = threadIdx.x + u * kTileThreads, i = i0 + t % S;
+            const int j = tile_row(j0 + t / S, F.GY);
+            const bool in = t < S * S && i >= 0 && i < F.GX;
+            kk[u] = in ? j * F.GX + i : -1;
+            const int I = i >> 1, J = j >> 1;
+            const int I1 = min(I + 1, C.GX - 1), J1 = J + 1 == C.GY ? 0 : J + 1;  // wraps only periodic in y
+            c00[u] = J * C.GX + I;
+            c10[u] = J * C.GX + I1;
+            c01[u] = J1 * C.GX + I;
+            c11[u] = J1 * C.GX + I1;
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const bool in = kk[u] >= 0;
+            mv[u] = in ? F.mask[kk[u]] : 1;
+            bv[u] = in ? F.b[kk[u]] : 0.0f;
+            xv[u] = in ? F.x[kk[u]] : 0.0f;
+            x00[u] = in ? C.x[c00[u]] : 0.0f;
+            x10[u] = in ? C.x[c10[u]] : 0.0f;
+            x01[u] = in ? C.x[c01[u]] : 0.0f;
+            x11[u] = in ? C.x[c11[u]] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int t = threadIdx.x + u * kTileThreads, i = i0 + t % S;
+            if (t >= S * S) break;
+            const int j = tile_row(j0 + t / S, F.GY);  // as prolonged() gets it
+            sm[t] = mv[u];
+            sb[t] = bv[u];
+            float v = xv[u];
+            if (!mv[u]) {
+                // prolonged(): x + the bilinear interpolation of the coarse correction
+                const bool ox = i & 1, oy = j & 1;
+                float cv;
+                if (!ox && !oy) cv = x00[u];
+                else if (ox && !oy) cv = 0.5f * (x00[u] + x10[u]);
+                else if (!ox && oy) cv = 0.5f * (x00[u] + x01[u]);
+                else cv = 0.25f * (x00[u] + x10[u] + x01[u] + x11[u]);
+                v = xv[u] + cv;
+            }
+            sx[t] = v;
+        }
     }
     __syncthreads();
     tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
@@ -635,6 +697,7 @@ struct FusedLevels {
     const float* gb;  // right-hand side of the first fused level
     float* gx;        // its solution (output)
     int sweeps;
+    int small;  // first level worked by warp 0 alone (n: none)
 };
 
 __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* smem) {
@@ -651,6 +714,15 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
         for (int k = tid; k < n; k += kFusedThreads) B(0)[k] = F.gb[k];
     }
     __syncthreads();
+    // Levels from F.small on are worked by warp 0 alone, with warp barriers
+    // between the phases (a block barrier of 1024 threads costs more than
+    // the few hundred nodes of such a level); the others by the whole block.
+    const int ls = F.small;
+    auto stride = [&](int l) { return l >= ls ? 32 : kFusedThreads; };
+    auto sync = [&](int l) {
+        if (l >= ls) __syncwarp();
+        else __syncthreads();
+    };
     // one colour: h enumerates (row, half-column); hw = ceil(GX/2), and
     // h / hw comes from a 32-bit reciprocal (exact for these sizes)
     auto sweep = [&](int l, int color) {
@@ -660,7 +732,7 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
         const float* b = B(l);
         const uint8_t* m = M(l);
         const float cx = F.cx[l], cy = F.cy[l], icd = 1.0f / F.cd[l];
-        for (int h = tid; h < hw * GY; h += kFusedThreads) {
+        for (int h = tid; h < hw * GY; h += stride(l)) {
             const int j = (int)__umulhi((uint32_t)h, rcp);
             const int i = 2 * (h - j * hw) + ((j + color) & 1);
             if (i >= GX) continue;
@@ -669,7 +741,7 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
             x[k] = __fmaf_rn(cx, x[k - 1] + x[k + 1],
                              __fmaf_rn(cy, x[row_dn(k, n, GX)] + x[row_up(k, n, GX)], b[k])) * icd;
         }
-        __syncthreads();
+        sync(l);
     };
     auto residual = [&](int l, int i, int j) -> float {
         const int GX = F.GX[l], GY = F.GY[l];
@@ -682,20 +754,21 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
                          F.cy[l] * (x[row_dn(k, n, GX)] + x[row_up(k, n, GX)]);
         return B(l)[k] - ax;
     };
-    for (int l = 0; l < F.n - 1; ++l) {
+    // zero start, smoothing, restriction into level l + 1
+    auto down = [&](int l) {
         const int GX = F.GX[l], n = GX * F.GY[l];
-        for (int k = tid; k < n; k += kFusedThreads) {
+        for (int k = tid; k < n; k += stride(l)) {
             const int i = k % GX, j = k / GX;
             X(l)[k] = (((i + j) & 1) == 0 && !M(l)[k]) ? B(l)[k] / F.cd[l] : 0.0f;
         }
-        __syncthreads();
+        sync(l);
         sweep(l, 1);
         for (int s = 1; s < kNu; ++s) {
             sweep(l, 0);
             sweep(l, 1);
         }
         const int CGX = F.GX[l + 1], cn = CGX * F.GY[l + 1];
-        for (int kc = tid; kc < cn; kc += kFusedThreads) {
+        for (int kc = tid; kc < cn; kc += stride(l)) {
             if (M(l + 1)[kc]) {
                 B(l + 1)[kc] = 0.0f;
                 continue;
@@ -708,12 +781,13 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
                  residual(l, i + 1, j + 1);
             B(l + 1)[kc] = s * 0.0625f;
         }
-        __syncthreads();
-    }
-    {
+        sync(l);
+    };
+    // coarsest level: symmetric sweeps from zero
+    auto coarsest = [&]() {
         const int l = F.n - 1, n = F.GX[l] * F.GY[l];
-        for (int k = tid; k < n; k += kFusedThreads) X(l)[k] = 0.0f;
-        __syncthreads();
+        for (int k = tid; k < n; k += stride(l)) X(l)[k] = 0.0f;
+        sync(l);
         for (int s = 0; s < F.sweeps; ++s) {
             sweep(l, 0);
             sweep(l, 1);
@@ -722,11 +796,12 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
             sweep(l, 1);
             sweep(l, 0);
         }
-    }
-    for (int l = F.n - 2; l >= 0; --l) {
+    };
+    // coarse correction from level l + 1, then smoothing
+    auto up = [&](int l) {
         const int GX = F.GX[l], n = GX * F.GY[l], CGX = F.GX[l + 1];
         const float* xc = X(l + 1);
-        for (int k = tid; k < n; k += kFusedThreads) {
+        for (int k = tid; k < n; k += stride(l)) {
             if (M(l)[k]) continue;
             const int i = k % GX, j = k / GX, I = i >> 1, J = j >> 1;
             const int J1 = J + 1 == F.GY[l + 1] ? 0 : J + 1;  // wraps only periodic in y
@@ -738,12 +813,22 @@ __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* 
             else v = 0.25f * (xc[J * CGX + I] + xc[J * CGX + I + 1] + xc[J1 * CGX + I] + xc[J1 * CGX + I + 1]);
             X(l)[k] += v;
         }
-        __syncthreads();
+        sync(l);
         for (int s = 0; s < kNu; ++s) {
             sweep(l, 1);
             sweep(l, 0);
         }
+    };
+    const int last = F.n - 1;
+    for (int l = 0; l < last && l < ls; ++l) down(l);
+    if (tid < 32) {  // the small levels (a no-op when there are none)
+        for (int l = ls; l < last; ++l) down(l);
+        if (last >= ls) coarsest();
+        for (int l = last - 1; l >= ls; --l) up(l);
     }
+    if (last < ls) coarsest();
+    __syncthreads();
+    for (int l = min(ls, last) - 1; l >= 0; --l) up(l);
     {
         const int n = F.GX[0] * F.GY[0];
         for (int k = tid; k < n; k += kFusedThreads) F.gx[k] = X(0)[k];
@@ -1150,7 +1235,24 @@ int poisson_setup(pic_ctx* c) {
     }
     F.gb = ps.levels[kf].b;
     F.gx = ps.levels[kf].x;
-    F.sweeps = kCoarseSweeps;
+    // levels of at most 512 nodes: warp 0 alone
+    F.small = F.n;
+    for (int i = 0; i < F.n; ++i)
+        if ((int64_t)F.GX[i] * F.GY[i] <= 512) {
+            F.small = i;
+            break;
+        }
+    // The coarsest level's sweeps: a single free node is exact after one
+    // sweep pair (later ones recompute the same value), so one pair does
+    {
+        const MGLevel& Lc = ps.levels[L - 1];
+        std::vector<uint8_t> m((size_t)Lc.nodes);
+        PIC_CUDA(cudaMemcpyAsync(m.data(), Lc.mask, m.size(), cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        int64_t free_nodes = 0;
+        for (uint8_t v : m) free_nodes += v ? 0 : 1;
+        F.sweeps = free_nodes <= 1 ? 1 : kCoarseSweeps;
+    }
     static_assert(sizeof(FusedLevels) <= sizeof(ps.fused_desc), "fused level table");
     std::memcpy(ps.fused_desc, &F, sizeof(F));
     ps.fused_smem = off;

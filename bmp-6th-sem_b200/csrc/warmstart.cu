@@ -22,13 +22,14 @@
 // Storage: activations and their gradients NHWC bf16 (32 channels), weights
 // bf16 with FP32 master copies and Adam moments.  Convolutions are implicit
 // GEMMs on the tensor cores, bf16 operands and FP32 accumulation (K = 9 taps
-// x 32 channels for the 32->32 layers): the forward 32->32 layers on tcgen05
-// with TMEM accumulators (k_conv32_tc, the average pools fused into its
-// epilogue); the forward 3->32 input and 32->1 output layers with
+// x 32 channels for the 32->32 layers): the 32->32 layers forward and their
+// data gradients on tcgen05 with TMEM accumulators (k_conv_rows: the average
+// pools fused into the forward epilogue, the relu gates into the gradient
+// one); the forward 3->32 input and 32->1 output layers with
 // mma.sync.m16n8k16 (K = 12 taps x 4 channels, and N = 8 of which one column
-// is used), their bf16 weights prepacked as B fragments; the training-only
-// data and weight gradients of the 32->32 layers with mma.sync, those of the
-// outer layers on the FP32 cores.
+// is used), their bf16 weights prepacked as B fragments; the weight
+// gradients of the 32->32 layers with mma.sync, those of the outer layers on
+// the FP32 cores.
 // Weight gradients are reduced through per-block partials in a fixed order,
 // so training is deterministic.
 #include <cuda.h>
@@ -108,10 +109,6 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// every committed group but the newest N has landed
-template <int N>
-__device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Start the copy of a (TH+2) x (TW+2) x 32 halo tile of an NHWC bf16 image
 // into shared memory ([row][col][CP]); pixels outside the image read as zero.
@@ -128,169 +125,8 @@ __device__ __forceinline__ void load_halo_async(__nv_bfloat16* dst, const __nv_b
 }
 
 // ---------------------------------------------------------------------------
-// 32 -> 32 3x3 convolution (forward, or data gradient with transformed
-// weights).  Weights in global memory as [tap][n][k] bf16 (n = output
-// channel, k = input channel).  Epilogue: out = act(acc + bias), where act is
-// relu (forward) or a gate (out *= gate[p] > 0, data gradient).  Training
-// uses it for the data gradients; the forward pass runs k_conv32_tc.
+// tcgen05 / mbarrier helpers
 // ---------------------------------------------------------------------------
-struct ConvArgs {
-    const __nv_bfloat16* in;
-    const __nv_bfloat16* w;   // [9][32][32]
-    const float* bias;        // [32] or null
-    const __nv_bfloat16* gate;  // [P][P][32] or null: multiply by (gate > 0)
-    __nv_bfloat16* out;
-    int P;
-    int relu;
-};
-
-constexpr int kConvSmem = ((TH + 2) * (TW + 2) * CP + 9 * C * CP) * 2;
-
-__global__ void __launch_bounds__(256) k_conv32(ConvArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* in_s = reinterpret_cast<__nv_bfloat16*>(smem);
-    __nv_bfloat16* w_s = in_s + (TH + 2) * (TW + 2) * CP;
-    const int y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
-    load_halo_async(in_s, A.in, A.P, y0, x0);
-    for (int i = threadIdx.x; i < 9 * C * (C / 8); i += blockDim.x) {
-        const int q = i & 3, row = i >> 2;  // row = tap*32 + n
-        cp_async16(w_s + row * CP + q * 8, A.w + row * C + q * 8, true);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // warp = output row in the tile
-    float acc[2][4][4];
-#pragma unroll
-    for (int m = 0; m < 2; ++m)
-#pragma unroll
-        for (int n = 0; n < 4; ++n)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
-#pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3, dx = tap % 3;
-#pragma unroll
-        for (int kc = 0; kc < 2; ++kc) {
-            uint32_t a[2][4];
-#pragma unroll
-            for (int m = 0; m < 2; ++m) {
-                const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
-                const int koff = (lane >> 4) * 8;
-                const __nv_bfloat16* pa = in_s + ((warp + dy) * (TW + 2) + m * 16 + r + dx) * CP + kc * 16 + koff;
-                ldsm_x4(smem_u32(pa), a[m][0], a[m][1], a[m][2], a[m][3]);
-            }
-            uint32_t b[4][2];
-#pragma unroll
-            for (int nh = 0; nh < 2; ++nh) {
-                const int n = nh * 16 + (lane & 7) + (lane >> 4) * 8;
-                const int koff = ((lane >> 3) & 1) * 8;
-                const __nv_bfloat16* pb = w_s + (tap * C + n) * CP + kc * 16 + koff;
-                ldsm_x4(smem_u32(pb), b[nh * 2][0], b[nh * 2][1], b[nh * 2 + 1][0], b[nh * 2 + 1][1]);
-            }
-#pragma unroll
-            for (int m = 0; m < 2; ++m)
-#pragma unroll
-                for (int n = 0; n < 4; ++n)
-                    mma_bf16(acc[m][n], a[m][0], a[m][1], a[m][2], a[m][3], b[n][0], b[n][1]);
-        }
-    }
-    // epilogue: stage the tile in shared memory, then write 16-byte chunks
-    __syncthreads();
-    __nv_bfloat16* o_s = in_s;  // [TH*TW][CP]
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int m = 0; m < 2; ++m)
-#pragma unroll
-        for (int n = 0; n < 4; ++n)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int px = m * 16 + g + h * 8;
-                const int ch = n * 8 + t * 2;
-                float v0 = acc[m][n][h * 2], v1 = acc[m][n][h * 2 + 1];
-                if (A.bias) {
-                    v0 += A.bias[ch];
-                    v1 += A.bias[ch + 1];
-                }
-                if (A.relu) {
-                    v0 = fmaxf(v0, 0.f);
-                    v1 = fmaxf(v1, 0.f);
-                }
-                *reinterpret_cast<__nv_bfloat162*>(o_s + (warp * TW + px) * CP + ch) =
-                    __floats2bfloat162_rn(v0, v1);
-            }
-    __syncthreads();
-    for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
-        const int q = i & 3, pix = i >> 2;
-        const int y = y0 + pix / TW, x = x0 + pix % TW;
-        if (y >= A.P || x >= A.P) continue;
-        const int64_t go = ((int64_t)y * A.P + x) * C + q * 8;
-        uint4 v = *reinterpret_cast<const uint4*>(o_s + pix * CP + q * 8);
-        if (A.gate) {
-            const uint4 gv = *reinterpret_cast<const uint4*>(A.gate + go);
-            __nv_bfloat162* pv = reinterpret_cast<__nv_bfloat162*>(&v);
-            const __nv_bfloat162* pg = reinterpret_cast<const __nv_bfloat162*>(&gv);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float2 f = __bfloat1622float2(pv[e]);
-                const float2 gg = __bfloat1622float2(pg[e]);
-                pv[e] = __floats2bfloat162_rn(gg.x > 0.f ? f.x : 0.f, gg.y > 0.f ? f.y : 0.f);
-            }
-        }
-        *reinterpret_cast<uint4*>(A.out + go) = v;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// 32 -> 32 3x3 convolution, forward pass, on the fifth-generation tensor
-// cores (tcgen05), warp-specialised and persistent (one CTA per SM).
-// Work unit: output rows y0, y0 + 1 (y0 even) x kTcW pixels from x0.  Per row
-// and k16 step one tcgen05.mma (M = 128 pixels, N = 32 channels, K = 16),
-// both operands in shared memory in the no-swizzle K-major layout:
-//   A: the unit's 4-row halo tile as [chunk q of 8 channels][row][pixel], 16
-//      bytes a pixel, so the A tile of tap (dy, dx) for row r starts at halo
-//      row r + dy, pixel dx; 8-pixel groups 128 bytes apart (SBO), the two
-//      chunk planes of a k16 step kTcPlane apart (LBO);
-//   B: the weights as [tap][chunk][n][8]: SBO 128 bytes (eight n), LBO 512.
-// Roles (warps):
-//   0-2  producers: copy unit k's halo into ring stage k % kTcStages with
-//        cp.async, then wait for the copies of unit k - kTcLag, fence them to
-//        the async proxy and arrive on that stage's `full` barrier;
-//   3    MMA: waits `full[s]` and `acc_empty[a]`, issues the 36 MMAs into
-//        TMEM accumulator a (64 columns: row r in 32r .. 32r+31) and commits
-//        them to `empty[s]` and `acc_full[a]`;
-//   4-11 epilogue, a warpgroup a row (TMEM lanes 32(w%4)..): tcgen05.ld of
-//        its 32 pixels, releases the accumulator, adds the bias, relu, bf16
-//        into a double-buffered shared stage; after a named barrier of the
-//        two warpgroups, 16-byte stores of both rows and the 2x2 average pool
-//        read from the stage.
-// Every wait is bounded (about a second): a role that gives up records
-// g_ws_fault and all roles leave their loops.
-// ---------------------------------------------------------------------------
-constexpr int kTcW = 128;                                // pixels of a unit row
-constexpr int kTcRows = 4;                               // halo rows
-constexpr int kTcPix = kTcW + 2;                         // halo pixels a row
-constexpr int kTcPlane = kTcRows * kTcPix * 16 + 32;     // bytes a chunk plane (+32: bank offset)
-constexpr int kTcHalo = 4 * kTcPlane;
-constexpr int kTcW16 = 9 * 4 * 32 * 16;                  // weight bytes
-constexpr int kTcStages = 3;
-constexpr int kTcLag = 1;                                // units in flight behind the one handed over
-// Accumulation chains a row: the taps split into kTcHalves partial sums
-// (taps 0-4 and 5-8 when 2), so that 2 * kTcHalves independent MMA chains
-// interleave; the epilogue adds the partials.
-constexpr int kTcHalves = 1;
-constexpr int kTcAccCols = 2 * kTcHalves * 32;           // TMEM columns of one accumulator set
-constexpr int kTcTmemCols = 2 * kTcAccCols;              // two sets (power of two, >= 32)
-constexpr int kTcProducers = 3 * 32;                     // producer threads (warps 0-2)
-constexpr int kTcStage = 2 * kTcW * C * 2;               // epilogue stage: 2 rows x kTcW px x 64 B
-constexpr int kTcEpi = 8 * 32;                           // epilogue threads (warps 4-11)
-constexpr int kTcThreads = 4 * 32 + kTcEpi;
-constexpr int kTcHead = 128;                             // barriers, TMEM address, abort flag
-constexpr int kTcSmem = kTcHead + kTcW16 + kTcStages * kTcHalo + 2 * kTcStage;
-// kind::f16 instruction descriptor: FP32 accumulator, bf16 A and B, both
-// K-major, N = 32, M = 128
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
-static_assert(kTcSmem <= 227 * 1024, "shared memory of one CTA");
-
 __device__ int g_ws_fault;  // a bounded wait of the warm-start kernels gave up
 // Bound of the tensor-core kernels' pipeline waits, in SM clock cycles (about
 // a second by default); a test lowers it to make the waits give up.
@@ -323,249 +159,10 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
-    asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
-        : "memory");
-}
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-          "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-          "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-          "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-}
-
-__global__ void __launch_bounds__(kTcThreads, 1) k_conv32_tc(const __nv_bfloat16* __restrict__ in,
-                                                      const __nv_bfloat16* __restrict__ w,
-                                                      const float* __restrict__ bias, int P,
-                                                      __nv_bfloat16* __restrict__ out,
-                                                      __nv_bfloat16* __restrict__ pool_out) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    // head: full[4] @0, empty[4] @32, acc_full[2] @64, acc_empty[2] @80, TMEM address @96, abort @100,
-    // drain @104 (the MMA warp's last commit: every MMA issued has completed)
-    static_assert(kTcStages <= 4, "barrier head layout");
-    const uint32_t sbase = smem_u32(smem);
-    const uint32_t full0 = sbase, empty0 = sbase + 32, accf0 = sbase + 64, acce0 = sbase + 80;
-    const uint32_t drain = sbase + 104;
-    const long long wl = g_ws_wait_cycles;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 96);
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 100);
-    unsigned char* wsm = smem + kTcHead;
-    unsigned char* ring = wsm + kTcW16;
-    unsigned char* stage0 = ring + kTcStages * kTcHalo;
-    const int Q = P / 2;
-    const int units_x = (P + kTcW - 1) / kTcW, units = ((P + 1) / 2) * units_x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 3) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
-                     "n"(kTcTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-    }
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
-            mbar_init(full0 + 8 * s, kTcProducers);
-            mbar_init(empty0 + 8 * s, 1);
-        }
-        for (int a = 0; a < 2; ++a) {
-            mbar_init(accf0 + 8 * a, 1);
-            mbar_init(acce0 + 8 * a, kTcEpi / 32);
-        }
-        mbar_init(drain, 1);
-        *abort_flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem = *tslot;
-    auto give_up = [&]() {
-        if (!*abort_flag) atomicExch(&g_ws_fault, 1);
-        *abort_flag = 1;
-    };
-
-    if (warp < 3) {
-        // ---------------- producers ----------------
-        const int pt = threadIdx.x;  // 0 .. kTcProducers-1
-        int k = 0;
-        for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
-            const int s = k % kTcStages;
-            if (k >= kTcStages && !mbar_wait_bounded(empty0 + 8 * s, ((k / kTcStages) & 1) ^ 1, wl)) {
-                give_up();
-                break;
-            }
-            if (*abort_flag) break;
-            if (k == 0)  // weights [tap][n][k] -> [tap][chunk][n][8], with the first unit
-                for (int i = pt; i < 9 * 32 * 4; i += kTcProducers) {
-                    const int q = i & 3, n = (i >> 2) & 31, tap = i >> 7;
-                    cp_async16(wsm + ((tap * 4 + q) * 32 + n) * 16, w + (tap * 32 + n) * C + q * 8, true);
-                }
-            const int y0 = (u / units_x) * 2, x0 = (u % units_x) * kTcW;
-            unsigned char* halo = ring + s * kTcHalo;
-            for (int i = pt; i < kTcRows * kTcPix * 4; i += kTcProducers) {
-                const int q = i & 3, pix = i >> 2;
-                const int y = y0 - 1 + pix / kTcPix, x = x0 - 1 + pix % kTcPix;
-                const bool ok = y >= 0 && x >= 0 && y < P && x < P;
-                cp_async16(halo + q * kTcPlane + pix * 16, ok ? in + ((int64_t)y * P + x) * C + q * 8 : in, ok);
-            }
-            cp_async_commit();
-            if (k >= kTcLag) {  // unit k - kTcLag has landed: hand it to the tensor cores
-                cp_async_wait_groups<kTcLag>();
-                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-                mbar_arrive(full0 + 8 * ((k - kTcLag) % kTcStages));
-            }
-        }
-        cp_async_wait_all();
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        for (int j = std::max(k - kTcLag, 0); j < k; ++j) mbar_arrive(full0 + 8 * (j % kTcStages));
-    } else if (warp == 3) {
-        // ---------------- MMA issue ----------------
-        if (lane == 0) {
-            const uint64_t bd = tc_desc(smem_u32(wsm), 512, 128);
-            int k = 0;
-            bool quit = false;
-            for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
-                const int s = k % kTcStages, a = k & 1;
-                if (!mbar_wait_bounded(full0 + 8 * s, (k / kTcStages) & 1, wl) ||
-                    (k >= 2 && !mbar_wait_bounded(acce0 + 8 * a, ((k >> 1) & 1) ^ 1, wl))) {
-                    give_up();
-                    quit = true;
-                    break;
-                }
-                if (*abort_flag) {
-                    quit = true;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                // descriptors differ only in the start address field (addresses >> 4 stay below 2^14)
-                const uint64_t ad = tc_desc(smem_u32(ring + s * kTcHalo), kTcPlane, 128);
-                // k16 step j of chain h covers tap h * 5 + j / 2 (chain 1: taps 5-8), chunk pair j % 2;
-                // the chains of both rows are issued in turn
-#pragma unroll
-                for (int j = 0; j < 18 / kTcHalves + 1; ++j)
-#pragma unroll
-                    for (int h = 0; h < kTcHalves; ++h) {
-                        const int tap = (kTcHalves == 1 ? 0 : h * 5) + j / 2, kc = j % 2;
-                        if (j >= (kTcHalves == 1 ? 18 : (h == 0 ? 10 : 8))) continue;
-#pragma unroll
-                        for (int r = 0; r < 2; ++r)
-                            tc_mma(tmem + a * kTcAccCols + (r * kTcHalves + h) * 32,
-                                   ad + (uint64_t)((2 * kc * kTcPlane + ((r + tap / 3) * kTcPix + tap % 3) * 16) >> 4),
-                                   bd + (uint64_t)(((tap * 4 + 2 * kc) * 512) >> 4), j ? 1u : 0u);
-                    }
-                tc_commit(empty0 + 8 * s);
-                tc_commit(accf0 + 8 * a);
-            }
-            // Leaving early, MMAs whose accumulator the epilogue will not
-            // wait for may still be running: no MMA may write TMEM when it is
-            // freed below.  One more commit tracks every MMA issued; its wait
-            // has the fixed bound, not the test's.  (On the normal path the
-            // epilogue has waited for every accumulator.)
-            if (quit) {
-                tc_commit(drain);
-                if (!mbar_wait_bounded(drain, 0, kWsWaitCycles)) atomicExch(&g_ws_fault, 1);
-            }
-        }
-        __syncwarp();
-    } else {
-        // ---------------- epilogue ----------------
-        const int row = (warp - 4) >> 2;  // unit row of this warpgroup
-        const int wl = warp & 3;          // TMEM lanes 32 wl .. 32 wl + 31 = pixels of the row
-        const int et = threadIdx.x - 4 * 32;
-        float bz[C];
-#pragma unroll
-        for (int ch = 0; ch < C; ++ch) bz[ch] = bias[ch];
-        int k = 0;
-        for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
-            const int a = k & 1;
-            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(accf0 + 8 * a, (k >> 1) & 1, wl));
-            if (!ok && lane == 0) give_up();
-            __nv_bfloat16* st = reinterpret_cast<__nv_bfloat16*>(stage0 + (k & 1) * kTcStage);
-            if (ok) {
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                uint32_t v[32];
-                tc_ld32(tmem + ((uint32_t)(32 * wl) << 16) + (uint32_t)(a * kTcAccCols + row * 32), v);
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(acce0 + 8 * a);
-                // bias, relu, bf16 into stage k & 1: [row][pixel][32 ch], chunk q of pixel p at
-                // position q ^ ((p >> 1) & 3) so that the eight lanes of a store phase hit distinct banks
-                const int px = 32 * wl + lane;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    uint32_t w4[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int ch = 8 * q + 2 * e;
-                        w4[e] = pack_bf16x2(fmaxf(__uint_as_float(v[ch]) + bz[ch], 0.f),
-                                            fmaxf(__uint_as_float(v[ch + 1]) + bz[ch + 1], 0.f));
-                    }
-                    *reinterpret_cast<uint4*>(st + (row * kTcW + px) * C + (q ^ ((px >> 1) & 3)) * 8) =
-                        make_uint4(w4[0], w4[1], w4[2], w4[3]);
-                }
-            }
-            // both rows staged; every epilogue thread takes the same quit decision here
-            uint32_t quit;
-            asm volatile(
-                "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred q, 1, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
-                : "=r"(quit)
-                : "r"((!ok || *abort_flag) ? 1u : 0u), "n"(kTcEpi)
-                : "memory");
-            if (quit) break;
-            const int y0 = (u / units_x) * 2, x0 = (u % units_x) * kTcW;
-            // 2 rows x kTcW pixels x 4 chunks, consecutive threads consecutive 16-byte chunks
-#pragma unroll
-            for (int j = 0; j < 2 * kTcW * 4 / kTcEpi; ++j) {
-                const int i = j * kTcEpi + et, r = i / (kTcW * 4), pix = (i >> 2) % kTcW, q = i & 3;
-                const int y = y0 + r, x = x0 + pix;
-                if (y < P && x < P)
-                    *reinterpret_cast<uint4*>(out + ((int64_t)y * P + x) * C + q * 8) =
-                        *reinterpret_cast<const uint4*>(st + (r * kTcW + pix) * C + (q ^ ((pix >> 1) & 3)) * 8);
-            }
-            if (pool_out) {
-                // 0.25 (v(y0, x) + v(y0, x+1) + v(y0+1, x) + v(y0+1, x+1)) of the bf16 outputs
-                const int q = et & 3, pxp = et >> 2;  // kTcW / 2 pooled pixels x 4 chunks
-                const int X = x0 / 2 + pxp, Y = y0 / 2;
-                if (X < Q && Y < Q) {
-                    auto at = [&](int r, int p) {
-                        return *reinterpret_cast<const uint4*>(st + (r * kTcW + p) * C + (q ^ ((p >> 1) & 3)) * 8);
-                    };
-                    const uint4 c4[4] = {at(0, 2 * pxp), at(0, 2 * pxp + 1), at(1, 2 * pxp), at(1, 2 * pxp + 1)};
-                    uint4 o;
-                    __nv_bfloat162* po = reinterpret_cast<__nv_bfloat162*>(&o);
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float2 f0 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[0])[e]);
-                        const float2 f1 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[1])[e]);
-                        const float2 f2 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[2])[e]);
-                        const float2 f3 = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(&c4[3])[e]);
-                        po[e] = __floats2bfloat162_rn(0.25f * (f0.x + f1.x + f2.x + f3.x), 0.25f * (f0.y + f1.y + f2.y + f3.y));
-                    }
-                    *reinterpret_cast<uint4*>(pool_out + ((int64_t)Y * Q + X) * C + q * 8) = o;
-                }
-            }
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    if (warp == 3) {
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(kTcTmemCols) : "memory");
-    }
-}
-
 // u = up2(coarse) + skip, 16 bytes a thread (P = fine size; each sum rounded to bf16)
 __global__ void k_up_add8(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, int P, __nv_bfloat16* u) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -633,12 +230,17 @@ static_assert(kRwSmemUsed + 1024 <= kRwSmem, "row-conv shared memory");
 // kind::f16: FP32 accumulator, bf16 A and B, both K-major, N = 96, M = 128
 constexpr uint32_t kRwIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((96u >> 3) << 17) | ((128u >> 4) << 24);
 
+// Forward layers: out = relu(conv + bias) (and its pool).  Data gradients
+// (weights flipped and transposed, see k_pack_rows_w): out = conv, each
+// value kept where gate > 0 (the forward activation), else 0.
 struct RowConvArgs {
-    const __nv_bfloat16* w;   // packed [dy][kc][g][n][8]
-    const float* bias;        // [32]
-    __nv_bfloat16* out;       // [P][P][32]
-    __nv_bfloat16* pool;      // [P/2][P/2][32] or null
+    const __nv_bfloat16* w;     // packed [dy][kc][g][n][8]
+    const float* bias;          // [32] or null (0)
+    __nv_bfloat16* out;         // [P][P][32]
+    __nv_bfloat16* pool;        // [P/2][P/2][32] or null
+    const __nv_bfloat16* gate;  // [P][P][32] or null
     int P;
+    int relu;
 };
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
@@ -737,7 +339,7 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     // the async proxy the MMAs read through)
     for (int i = threadIdx.x; i < kRwWBytes / 16; i += kRwThreads)
         reinterpret_cast<uint4*>(wsm)[i] = reinterpret_cast<const uint4*>(A.w)[i];
-    if (threadIdx.x < 32) sbias[threadIdx.x] = A.bias[threadIdx.x];
+    if (threadIdx.x < 32) sbias[threadIdx.x] = A.bias ? A.bias[threadIdx.x] : 0.f;
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -843,8 +445,19 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
             for (int c = 0; c < 16; c += 2) {
                 const float l0 = __shfl_up_sync(kFull, v0[c], 1), l1 = __shfl_up_sync(kFull, v0[c + 1], 1);
                 const float r0v = __shfl_down_sync(kFull, v2[c], 1), r1v = __shfl_down_sync(kFull, v2[c + 1], 1);
-                pk[c / 2] = pack_bf16x2(fmaxf(l0 + v1[c] + r0v + bias[c], 0.f),
-                                        fmaxf(l1 + v1[c + 1] + r1v + bias[c + 1], 0.f));
+                const float s0 = l0 + v1[c] + r0v + bias[c], s1 = l1 + v1[c + 1] + r1v + bias[c + 1];
+                pk[c / 2] = A.relu ? pack_bf16x2(fmaxf(s0, 0.f), fmaxf(s1, 0.f)) : pack_bf16x2(s0, s1);
+            }
+            if (A.gate && valid) {
+                const uint4* gp = reinterpret_cast<const uint4*>(A.gate + ((int64_t)y * P + x) * C + 16 * h);
+                const uint4 ga = gp[0], gb = gp[1];
+                const uint32_t gw[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[e]));
+                    const float2 g = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&gw[e]));
+                    pk[e] = pack_bf16x2(g.x > 0.f ? f.x : 0.f, g.y > 0.f ? f.y : 0.f);
+                }
             }
             if (valid) {
                 uint4* dst = reinterpret_cast<uint4*>(A.out + ((int64_t)y * P + x) * C + 16 * h);
@@ -894,15 +507,25 @@ __global__ void __launch_bounds__(kRwThreads, 1) k_conv_rows(const __grid_consta
     }
 }
 
-// FP32 masters [tap][ci][co] of one 32->32 layer -> the B operand layout
-// [dy][kc][g][n = 32 dx + co][8 ci] in bf16 (ci = 16 kc + 8 g + e).
-__global__ void k_pack_rows_w(const float* w, __nv_bfloat16* out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 6 * 2 * 96 * 8) return;
+// FP32 masters [tap][ci][co] of the 32->32 layers (stride apart) -> the B
+// operand layout [dy][kc][g][n = 32 dx + co][8 ci] in bf16 (ci = 16 kc + 8 g
+// + e), for the forward layers (out) and for their data gradients (out_t:
+// taps flipped, channels swapped, W'[tap][ci][co] = W[8 - tap][co][ci], since
+// dX[p][ci] = sum_tap sum_co dY[p - d(tap)][co] W[tap][ci][co] and
+// d(8 - tap) = -d(tap)).
+constexpr int kRwWElems = 6 * 2 * 96 * 8;
+__global__ void k_pack_rows_w(const float* w, int64_t stride, int layers, __nv_bfloat16* out,
+                              __nv_bfloat16* out_t) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (int64_t)layers * kRwWElems) return;
+    const int l = (int)(j / kRwWElems), i = (int)(j % kRwWElems);
     const int e = i & 7, n = (i >> 3) % 96, gk = i / (8 * 96);  // gk = (dy * 2 + kc) * 2 + g
     const int g = gk & 1, kc = (gk >> 1) & 1, dy = gk >> 2;
     const int dx = n / 32, co = n % 32, ci = 16 * kc + 8 * g + e;
-    out[i] = __float2bfloat16_rn(w[((dy * 3 + dx) * C + ci) * C + co]);
+    const int tap = dy * 3 + dx;
+    const float* wl = w + l * stride;
+    out[j] = __float2bfloat16_rn(wl[(tap * C + ci) * C + co]);
+    out_t[j] = __float2bfloat16_rn(wl[((8 - tap) * C + co) * C + ci]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1465,17 +1088,18 @@ struct Net {
     float* v = nullptr;
     float* g = nullptr;
     int64_t adam_t = 0;
-    // bf16 working copies of the 32->32 weights, [layer][tap][n][k], and
-    // their data-gradient transposes
-    __nv_bfloat16* w16 = nullptr;
-    __nv_bfloat16* w16t = nullptr;
     // bf16 B fragments of the input and output convolutions (k_pack_frags)
     uint2* in_frag = nullptr;
     uint2* out_frag = nullptr;
-    // the forward 32->32 layers' weights in k_conv_rows' B layout, and the
-    // TMA descriptors of their inputs (a1, p1, a3, p2, a5, u1, a7, u0, a9)
+    // the 32->32 layers' weights in k_conv_rows' B layout (forward, and
+    // flipped and transposed for the data gradients), the TMA descriptors of
+    // the forward inputs (a1, p1, a3, p2, a5, u1, a7, u0, a9) and of the
+    // gradient buffers the backward convolutions read (d_big[0..1],
+    // d_mid[0..1], d_small[0..1])
     __nv_bfloat16* wrows = nullptr;
+    __nv_bfloat16* wrows_t = nullptr;
     CUtensorMap tm_in[9];
+    CUtensorMap tm_grad[6];
     // activations (P = fine, Q = P/2, R = P/4)
     __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
     float* out = nullptr;
@@ -1499,7 +1123,7 @@ struct Net {
     double* db = nullptr;
     bool have_prev = false;
     bool trained = false;
-    bool packed = false;      // w16/w16t match the masters
+    bool packed = false;      // the bf16 weights match the masters
     bool auto_scale = false;  // take s0, s1, s2 from the first recorded pair
 };
 
@@ -1511,7 +1135,7 @@ static int64_t param_off(int block) {
 
 static void net_free(Net& N) {
     cudaFree(N.w); cudaFree(N.m); cudaFree(N.v); cudaFree(N.g);
-    cudaFree(N.w16); cudaFree(N.w16t); cudaFree(N.in_frag); cudaFree(N.out_frag); cudaFree(N.wrows);
+    cudaFree(N.in_frag); cudaFree(N.out_frag); cudaFree(N.wrows); cudaFree(N.wrows_t);
     cudaFree(N.x0);
     for (auto* p : N.a) cudaFree(p);
     cudaFree(N.p1); cudaFree(N.p2); cudaFree(N.u0); cudaFree(N.u1); cudaFree(N.out);
@@ -1598,7 +1222,6 @@ static int ws_alloc(pic_ctx* c) {
     };
     if (cudaMalloc(&N.w, kParams * 4) || cudaMalloc(&N.m, kParams * 4) ||
         cudaMalloc(&N.v, kParams * 4) || cudaMalloc(&N.g, kParams * 4) ||
-        balloc(&N.w16, (int64_t)kNumConv32 * kW32) || balloc(&N.w16t, (int64_t)kNumConv32 * kW32) ||
         cudaMalloc(&N.in_frag, kInSteps * 4 * 32 * sizeof(uint2)) ||
         cudaMalloc(&N.out_frag, kOutSteps * 32 * sizeof(uint2)) ||
         balloc(&N.x0, P * P * 4))
@@ -1630,29 +1253,19 @@ static int ws_alloc(pic_ctx* c) {
     PIC_CUDA(cudaMemcpy(N.w, w.data(), kParams * 4, cudaMemcpyHostToDevice));
     PIC_CUDA(cudaMemset(N.m, 0, kParams * 4));
     PIC_CUDA(cudaMemset(N.v, 0, kParams * 4));
-    PIC_CUDA(cudaFuncSetAttribute(k_conv32, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
-    PIC_CUDA(cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     PIC_CUDA(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kRwSmem));
-    if (cudaMalloc(&N.wrows, (size_t)kNumConv32 * kRwWBytes))
+    if (cudaMalloc(&N.wrows, (size_t)kNumConv32 * kRwWBytes) || cudaMalloc(&N.wrows_t, (size_t)kNumConv32 * kRwWBytes))
         return fail(PIC_ERR_CUDA, "warm start: parameter allocation failed");
     {
         const __nv_bfloat16* ins[9] = {N.a[1], N.p1, N.a[3], N.p2, N.a[5], N.u1, N.a[7], N.u0, N.a[9]};
         const int sz[9] = {(int)P, (int)Q, (int)Q, (int)R, (int)R, (int)Q, (int)Q, (int)P, (int)P};
         for (int l = 0; l < 9; ++l) PIC_TRY(make_row_tmap(&N.tm_in[l], ins[l], sz[l]));
+        const __nv_bfloat16* gr[6] = {N.d_big[0], N.d_big[1], N.d_mid[0], N.d_mid[1], N.d_small[0], N.d_small[1]};
+        const int gs[6] = {(int)P, (int)P, (int)Q, (int)Q, (int)R, (int)R};
+        for (int i = 0; i < 6; ++i) PIC_TRY(make_row_tmap(&N.tm_grad[i], gr[i], gs[i]));
     }
     PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
     return PIC_OK;
-}
-
-// w: 9 blocks of [tap][ci][co] fp32 (stride apart) -> w16: [layer][tap][n=co][k=ci]
-// bf16 and its data-gradient form w16t[layer][tap][n=ci][k=co] = w16[layer][8-tap][co][ci].
-__global__ void k_pack_w16(const float* w, int64_t stride, __nv_bfloat16* w16, __nv_bfloat16* w16t) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)kNumConv32 * kW32) return;
-    const int l = (int)(i / kW32), r = (int)(i % kW32);
-    const int tap = r / (C * C), n = (r / C) % C, k = r % C;
-    w16[i] = __float2bfloat16_rn(w[l * stride + (tap * C + k) * C + n]);
-    w16t[i] = __float2bfloat16_rn(w[l * stride + ((8 - tap) * C + n) * C + k]);
 }
 
 // B fragments (m16n8k16, per lane: {k 2t, 2t+1 | k 2t+8, 2t+9} of column g)
@@ -1685,53 +1298,16 @@ __global__ void k_pack_frags(const float* w_in, const float* w_out, uint2* in_fr
 static int ws_pack(pic_ctx* c) {
     Net& N = c->ws->net;
     if (N.packed) return PIC_OK;
-    k_pack_w16<<<g1((int64_t)kNumConv32 * kW32), 256, 0, c->stream>>>(N.w + param_off(1), kW32 + kB32,
-                                                                       N.w16, N.w16t);
     k_pack_frags<<<g1((kInSteps * 4 + kOutSteps) * 32), 256, 0, c->stream>>>(
         N.w, N.w + param_off(kNumConv32 + 1), N.in_frag, N.out_frag);
-    for (int l = 0; l < kNumConv32; ++l)
-        k_pack_rows_w<<<g1(kRwWBytes / 2), 256, 0, c->stream>>>(N.w + param_off(l + 1),
-                                                                 N.wrows + (int64_t)l * (kRwWBytes / 2));
-    c->launches += 2 + kNumConv32;
+    k_pack_rows_w<<<g1((int64_t)kNumConv32 * kRwWElems), 256, 0, c->stream>>>(
+        N.w + param_off(1), kW32 + kB32, kNumConv32, N.wrows, N.wrows_t);
+    c->launches += 2;
     PIC_CUDA(cudaGetLastError());
     N.packed = true;
     return PIC_OK;
 }
 
-static void conv32(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
-                   bool transposed, const __nv_bfloat16* gate) {
-    Net& N = c->ws->net;
-    ConvArgs A;
-    A.in = in;
-    A.w = (transposed ? N.w16t : N.w16) + (int64_t)layer * kW32;
-    A.bias = transposed ? nullptr : N.w + param_off(layer + 1) + kW32;
-    A.gate = gate;
-    A.out = out;
-    A.P = P;
-    A.relu = transposed ? 0 : 1;
-    const dim3 grid((P + TW - 1) / TW, (P + TH - 1) / TH);
-    k_conv32<<<grid, 256, kConvSmem, c->stream>>>(A);
-}
-
-// Forward 32->32 convolution on the tcgen05 tensor cores (k_conv32_tc), the
-// decoder's upsample-and-skip sum (into u) first when `up` is given.
-static void conv32_tc(pic_ctx* c, int layer, const __nv_bfloat16* in, __nv_bfloat16* out, int P,
-                      const __nv_bfloat16* up = nullptr, __nv_bfloat16* u = nullptr,
-                      __nv_bfloat16* pool_out = nullptr) {
-    Net& N = c->ws->net;
-    if (up) {
-        k_up_add8<<<g1((int64_t)P * P * 4), 256, 0, c->stream>>>(up, in, P, u);
-        in = u;
-        c->launches += 1;
-    }
-    const int units = ((P + 1) / 2) * ((P + kTcW - 1) / kTcW);
-    k_conv32_tc<<<std::min(units, N.sms), kTcThreads, kTcSmem, c->stream>>>(
-        in, N.w16 + (int64_t)layer * kW32, N.w + param_off(layer + 1) + kW32, P, out, pool_out);
-}
-
-// Forward 32->32 convolution `layer` on the block-streaming tcgen05 kernel,
-// its input being the layer's TMA descriptor's image; the decoder's
-// upsample-and-skip sum u = up2(up) + skip is formed first when `up` is given.
 static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfloat16* pool,
                       const __nv_bfloat16* up = nullptr, const __nv_bfloat16* skip = nullptr,
                       __nv_bfloat16* u = nullptr) {
@@ -1747,7 +1323,9 @@ static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfl
     A.bias = N.w + param_off(layer + 1) + kW32;
     A.out = out;
     A.pool = pool;
+    A.gate = nullptr;
     A.P = P;
+    A.relu = 1;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kRwThreads);
@@ -1759,6 +1337,34 @@ static void conv_rows(pic_ctx* c, int layer, __nv_bfloat16* out, int P, __nv_bfl
     cfg.attrs = at;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, k_conv_rows, N.tm_in[layer], A);
+    c->launches += 1;
+}
+
+// Data gradient of 32->32 layer `layer` on tcgen05: out = conv(grad input
+// tm_grad[g], flipped and transposed weights), kept where gate > 0.
+static void conv_rows_grad(pic_ctx* c, int layer, int g, __nv_bfloat16* out, int P, const __nv_bfloat16* gate) {
+    Net& N = c->ws->net;
+    const int units = ((P + kRwCols - 1) / kRwCols) * ((P + kRwBlk - 1) / kRwBlk);
+    const int grid = std::max(1, std::min(N.sms, (units + 3) / 4));
+    RowConvArgs A;
+    A.w = N.wrows_t + (int64_t)layer * (kRwWBytes / 2);
+    A.bias = nullptr;
+    A.out = out;
+    A.pool = nullptr;
+    A.gate = gate;
+    A.P = P;
+    A.relu = 0;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kRwThreads);
+    cfg.dynamicSmemBytes = kRwSmem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_conv_rows, N.tm_grad[g], A);
     c->launches += 1;
 }
 
@@ -1863,27 +1469,27 @@ static void backward(pic_ctx* c) {
     k_conv_out_dx<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.dout, N.w + ob, N.a[10], P, B0);
     // B0 = dPre10
     wgrad32(c, 8, N.a[9], B0, P);
-    conv32(c, 8, B0, B1, P, true, N.a[9]);        // B1 = dPre9
+    conv_rows_grad(c, 8, 0, B1, P, N.a[9]);        // B1 = dPre9
     wgrad32(c, 7, N.u0, B1, P);
-    conv32(c, 7, B1, B2, P, true, nullptr);       // B2 = dU0
+    conv_rows_grad(c, 7, 1, B2, P, nullptr);       // B2 = dU0
     k_down_sum_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(B2, N.a[8], P, M0);  // M0 = dPre8
     wgrad32(c, 6, N.a[7], M0, Q);
-    conv32(c, 6, M0, M1, Q, true, N.a[7]);        // M1 = dPre7
+    conv_rows_grad(c, 6, 2, M1, Q, N.a[7]);        // M1 = dPre7
     wgrad32(c, 5, N.u1, M1, Q);
-    conv32(c, 5, M1, M2, Q, true, nullptr);       // M2 = dU1
+    conv_rows_grad(c, 5, 3, M2, Q, nullptr);       // M2 = dU1
     k_down_sum_gate<<<g1((int64_t)R * R * C), 256, 0, c->stream>>>(M2, N.a[6], Q, S0);  // S0 = dPre6
     wgrad32(c, 4, N.a[5], S0, R);
-    conv32(c, 4, S0, S1, R, true, N.a[5]);        // S1 = dPre5
+    conv_rows_grad(c, 4, 4, S1, R, N.a[5]);        // S1 = dPre5
     wgrad32(c, 3, N.p2, S1, R);
-    conv32(c, 3, S1, S0, R, true, nullptr);       // S0 = dP2
+    conv_rows_grad(c, 3, 5, S0, R, nullptr);       // S0 = dP2
     k_skip_pool_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(M2, S0, N.a[4], Q, M0);  // M0 = dPre4
     wgrad32(c, 2, N.a[3], M0, Q);
-    conv32(c, 2, M0, M1, Q, true, N.a[3]);        // M1 = dPre3
+    conv_rows_grad(c, 2, 2, M1, Q, N.a[3]);        // M1 = dPre3
     wgrad32(c, 1, N.p1, M1, Q);
-    conv32(c, 1, M1, M0, Q, true, nullptr);       // M0 = dP1
+    conv_rows_grad(c, 1, 3, M0, Q, nullptr);       // M0 = dP1
     k_skip_pool_gate<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(B2, M0, N.a[2], P, B0);  // B0 = dPre2
     wgrad32(c, 0, N.a[1], B0, P);
-    conv32(c, 0, B0, B1, P, true, N.a[1]);        // B1 = dPre1
+    conv_rows_grad(c, 0, 0, B1, P, N.a[1]);        // B1 = dPre1
     k_wgrad_in<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.xin, B1, P, N.partial);
     k_sum_partials<<<g1(kInOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kInOut, N.g);
     c->launches += 2 + 1 + 10 * 3 + 4 + 2;
