@@ -487,7 +487,8 @@ constexpr int kDownHalo = 2 * kNu + 1;
 constexpr int kUpHalo = 2 * kNu;
 constexpr int kDownSide = kTileCore + 2 * kDownHalo;
 constexpr int kUpSide = kTileCore + 2 * kUpHalo;
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 256;      // the finest level's kernels (and r.z)
+constexpr int kTileThreadsSmall = 1024; // levels of fewer tiles than two per SM: shorter chains
 static_assert(kDownSide % 2 == 0 && kUpSide % 2 == 0, "tile rows hold as many nodes of each colour");
 
 // level row of region row j (rows wrap at the level's row count)
@@ -499,17 +500,17 @@ __device__ __forceinline__ int tile_row(int j, int GY) {
 // Region nodes a thread loads: all its loads are issued before the first
 // result is used (the load phase is one round trip to memory, not one per
 // node).
-template <int S>
-constexpr int tile_loads() { return (S * S + kTileThreads - 1) / kTileThreads; }
+template <int S, int NT>
+constexpr int tile_loads() { return (S * S + NT - 1) / NT; }
 
 // one colour over the region's inner nodes (k_mg_rbgs's arithmetic); region
 // node (li, lj) is level node (i0 + li, j0 + lj), colour (i + j) & 1 (rows
 // wrap only at an even row count, so wrapping keeps the colour)
-template <int S>
+template <int S, int NT>
 __device__ __forceinline__ void tile_half_sweep(float* x, const float* b, const uint8_t* m, float cx,
                                                 float cy, float cd, int color, int i0, int j0) {
     constexpr int HS = S / 2;
-    for (int h = threadIdx.x; h < HS * S; h += kTileThreads) {
+    for (int h = threadIdx.x; h < HS * S; h += NT) {
         const int lj = h / HS;
         const int li = 2 * (h - lj * HS) + ((i0 + j0 + lj + color) & 1);
         const int t = lj * S + li;
@@ -521,7 +522,8 @@ __device__ __forceinline__ void tile_half_sweep(float* x, const float* b, const 
 }
 
 // level F's smoothing from a zero start, then C.b = restriction of F's residual
-__global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C) {
+template <int NT>
+__global__ void __launch_bounds__(NT) k_mg_down(LevelDev F, LevelDev C) {
     constexpr int S = kDownSide, H = kDownHalo, CC = kTileCore / 2;
     __shared__ float sx[S * S], sb[S * S], sr[S * S];
     __shared__ uint8_t sm[S * S];
@@ -529,13 +531,13 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C
     const int I0 = blockIdx.x * CC, J0 = blockIdx.y * CC;  // first coarse node of the tile
     const int i0 = 2 * I0 - H, j0 = 2 * J0 - H;            // level node of region node (0, 0)
     {
-        constexpr int NL = tile_loads<S>();
+        constexpr int NL = tile_loads<S, NT>();
         int kk[NL];
         uint8_t mv[NL];
         float bv[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
-            const int t = threadIdx.x + u * kTileThreads, li = t % S, lj = t / S, i = i0 + li;
+            const int t = threadIdx.x + u * NT, li = t % S, lj = t / S, i = i0 + li;
             kk[u] = (t < S * S && i >= 0 && i < F.GX) ? tile_row(j0 + lj, F.GY) * F.GX + i : -1;
         }
 #pragma unroll
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C
         }
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
-            const int t = threadIdx.x + u * kTileThreads, li = t % S, lj = t / S;
+            const int t = threadIdx.x + u * NT, li = t % S, lj = t / S;
             if (t >= S * S) break;
             sm[t] = mv[u];
             sb[t] = bv[u];
@@ -555,12 +557,12 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C
         }
     }
     __syncthreads();
-    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
     for (int s = 1; s < kNu; ++s) {
-        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
-        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
     }
-    for (int t = threadIdx.x; t < S * S; t += kTileThreads) {
+    for (int t = threadIdx.x; t < S * S; t += NT) {
         const int li = t % S, lj = t / S;
         float rv = 0.0f;
         if (li > 0 && lj > 0 && li < S - 1 && lj < S - 1 && !sm[t])
@@ -572,7 +574,7 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_down(LevelDev F, LevelDev C
     }
     __syncthreads();
     // full weighting, in k_mg_restrict's order
-    for (int t = threadIdx.x; t < CC * CC; t += kTileThreads) {
+    for (int t = threadIdx.x; t < CC * CC; t += NT) {
         const int I = I0 + t % CC, J = J0 + t / CC;
         if (I >= C.GX || J >= C.GY) continue;
         const int64_t kc = (int64_t)J * C.GX + I;
@@ -597,11 +599,12 @@ struct RzArgs {
     unsigned* arrive;
     double* scal;
 };
-static_assert(kTileThreads == kRedThreads, "k_mg_up's reduction uses the PCG block reduction");
+
 
 // xo = level F's x corrected by C.x and smoothed; with kRz also r.z
-template <bool kRz>
-__global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, float* xo, RzArgs R) {
+template <bool kRz, int NT>
+__global__ void __launch_bounds__(NT) k_mg_up(LevelDev F, LevelDev C, float* xo, RzArgs R) {
+    static_assert(!kRz || NT == kRedThreads, "the r.z reduction is the PCG block reduction");
     constexpr int S = kUpSide, H = kUpHalo;
     __shared__ float sx[S * S], sb[S * S];
     __shared__ uint8_t sm[S * S];
@@ -611,13 +614,13 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, 
         // the node's mask, b, x and the four coarse values prolonged() reads
         // (column I + 1 clamped: only read for odd i < GX - 1), all loaded
         // before any is used
-        constexpr int NL = tile_loads<S>();
+        constexpr int NL = tile_loads<S, NT>();
         int kk[NL], c00[NL], c10[NL], c01[NL], c11[NL];
         uint8_t mv[NL];
         float bv[NL], xv[NL], x00[NL], x10[NL], x01[NL], x11[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
-            const int t = threadIdx.x + u * kTileThreads, i = i0 + t % S;
+            const int t = threadIdx.x + u * NT, i = i0 + t % S;
             const int j = tile_row(j0 + t / S, F.GY);
             const bool in = t < S * S && i >= 0 && i < F.GX;
             kk[u] = in ? j * F.GX + i : -1;
@@ -641,7 +644,7 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, 
         }
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
-            const int t = threadIdx.x + u * kTileThreads, i = i0 + t % S;
+            const int t = threadIdx.x + u * NT, i = i0 + t % S;
             if (t >= S * S) break;
             const int j = tile_row(j0 + t / S, F.GY);  // as prolonged() gets it
             sm[t] = mv[u];
@@ -661,14 +664,14 @@ __global__ void __launch_bounds__(kTileThreads) k_mg_up(LevelDev F, LevelDev C, 
         }
     }
     __syncthreads();
-    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
-    tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
     for (int s = 1; s < kNu; ++s) {
-        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
-        tile_half_sweep<S>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
     }
     double acc[1] = {0.0};
-    for (int t = threadIdx.x; t < kTileCore * kTileCore; t += kTileThreads) {
+    for (int t = threadIdx.x; t < kTileCore * kTileCore; t += NT) {
         const int li = H + t % kTileCore, lj = H + t / kTileCore;
         const int i = i0 + li, j = j0 + lj;
         if (i >= F.GX || j >= F.GY || sm[lj * S + li]) continue;
@@ -698,20 +701,37 @@ struct FusedLevels {
     float* gx;        // its solution (output)
     int sweeps;
     int small;  // first level worked by warp 0 alone (n: none)
+    int mpre[kMaxFused + 1];  // prefix sums of the levels' node counts
 };
+// every thread's share of the masks and of the first level's b, loaded in
+// one round trip (the setup keeps the fused levels within this)
+constexpr int kFusedLoads = 8;
 
 __device__ __forceinline__ void fused_body(const FusedLevels& F, unsigned char* smem) {
     auto X = [&](int l) { return reinterpret_cast<float*>(smem + F.ox[l]); };
     auto B = [&](int l) { return reinterpret_cast<float*>(smem + F.ob[l]); };
     auto M = [&](int l) { return reinterpret_cast<uint8_t*>(smem + F.om[l]); };
     const int tid = threadIdx.x;
-    for (int l = 0; l < F.n; ++l) {
-        const int n = F.GX[l] * F.GY[l];
-        for (int k = tid; k < n; k += kFusedThreads) M(l)[k] = F.gmask[l][k];
-    }
     {
-        const int n = F.GX[0] * F.GY[0];
-        for (int k = tid; k < n; k += kFusedThreads) B(0)[k] = F.gb[k];
+        const int n0 = F.GX[0] * F.GY[0], total = F.mpre[F.n];
+        uint8_t mv[kFusedLoads];
+        float bv[kFusedLoads];
+        int lv[kFusedLoads];
+#pragma unroll
+        for (int u = 0; u < kFusedLoads; ++u) {
+            const int k = tid + u * kFusedThreads;
+            int l = 0;
+            while (l + 1 < F.n && k >= F.mpre[l + 1]) ++l;
+            lv[u] = l;
+            mv[u] = k < total ? F.gmask[l][k - F.mpre[l]] : 0;
+            bv[u] = k < n0 ? F.gb[k] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kFusedLoads; ++u) {
+            const int k = tid + u * kFusedThreads;
+            if (k < total) M(lv[u])[k - F.mpre[lv[u]]] = mv[u];
+            if (k < n0) B(0)[k] = bv[u];
+        }
     }
     __syncthreads();
     // Levels from F.small on are worked by warp 0 alone, with warp barriers
@@ -952,6 +972,10 @@ void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_
 // Returns the number of kernels.  Levels above the fused ones take two
 // kernels each (k_mg_down, k_mg_up); with with_rz the finest k_mg_up also
 // reduces r.z for the PCG iteration.
+// fewer tiles than two per SM: blocks of kTileThreadsSmall (the level's time
+// is one block's latency, which more threads a tile shorten)
+static bool small_grid(dim3 g) { return (int64_t)g.x * g.y < 2 * 148; }
+
 int enqueue_vcycle(pic_ctx* c, cudaStream_t st, bool with_rz) {
     PoissonState& ps = c->ps;
     const int kf = ps.fused_first;
@@ -961,7 +985,11 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st, bool with_rz) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
         const int cc = kTileCore / 2;
-        launch_pdl(k_mg_down, dim3((C.GX + cc - 1) / cc, (C.GY + cc - 1) / cc), tb, 0, st, F, C);
+        const dim3 grid((C.GX + cc - 1) / cc, (C.GY + cc - 1) / cc);
+        if (small_grid(grid))
+            launch_pdl(k_mg_down<kTileThreadsSmall>, grid, dim3(kTileThreadsSmall), 0, st, F, C);
+        else
+            launch_pdl(k_mg_down<kTileThreads>, grid, tb, 0, st, F, C);
         launches += 1;
     }
     launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
@@ -973,10 +1001,13 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st, bool with_rz) {
         if (l + 1 < kf) C.x = ps.levels[l + 1].xo;  // what the coarser k_mg_up wrote
         const dim3 grid((F.GX + kTileCore - 1) / kTileCore, (F.GY + kTileCore - 1) / kTileCore);
         if (l == 0 && with_rz)
-            launch_pdl(k_mg_up<true>, grid, tb, 0, st, F, C, ps.levels[l].xo,
+            launch_pdl(k_mg_up<true, kTileThreads>, grid, tb, 0, st, F, C, ps.levels[l].xo,
                        RzArgs{ps.r, ps.partials, arrive_ptr(ps), ps.scal});
+        else if (small_grid(grid))
+            launch_pdl(k_mg_up<false, kTileThreadsSmall>, grid, dim3(kTileThreadsSmall), 0, st, F, C,
+                       ps.levels[l].xo, RzArgs{});
         else
-            launch_pdl(k_mg_up<false>, grid, tb, 0, st, F, C, ps.levels[l].xo, RzArgs{});
+            launch_pdl(k_mg_up<false, kTileThreads>, grid, tb, 0, st, F, C, ps.levels[l].xo, RzArgs{});
         launches += 1;
     }
     return launches;
@@ -1235,13 +1266,17 @@ int poisson_setup(pic_ctx* c) {
     }
     F.gb = ps.levels[kf].b;
     F.gx = ps.levels[kf].x;
-    // levels of at most 512 nodes: warp 0 alone
+    // levels of at most 64 nodes: warp 0 alone
     F.small = F.n;
     for (int i = 0; i < F.n; ++i)
-        if ((int64_t)F.GX[i] * F.GY[i] <= 512) {
+        if ((int64_t)F.GX[i] * F.GY[i] <= 64) {
             F.small = i;
             break;
         }
+    F.mpre[0] = 0;
+    for (int i = 0; i < F.n; ++i) F.mpre[i + 1] = F.mpre[i] + F.GX[i] * F.GY[i];
+    if (F.mpre[F.n] > kFusedLoads * kFusedThreads)
+        return fail(PIC_ERR_CONFIG, "coarse multigrid levels too large for the one-block kernel");
     // The coarsest level's sweeps: a single free node is exact after one
     // sweep pair (later ones recompute the same value), so one pair does
     {
