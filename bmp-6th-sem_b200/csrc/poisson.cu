@@ -1224,13 +1224,19 @@ int poisson_setup(pic_ctx* c) {
         const size_t n = (size_t)ps.levels[l].nodes;
         return ((n * 4 + 15) & ~(size_t)15) * 2 + ((n + 15) & ~(size_t)15);
     };
-    const size_t kSmemBudget = 64 * 1024;  // small levels only: one SM does them
-    size_t total = 0;
+    // small levels only (33^2 and below): one SM does them, and a level of
+    // 65^2 runs faster as tiled kernels over many SMs; a coarsest level too
+    // large for that budget (periodic in y, coarsening stopped early) may
+    // take up to 64 KB
     int kf = L;
-    for (int l = L - 1; l >= 0; --l) {
-        if (total + level_bytes(l) > kSmemBudget || L - l > kMaxFused) break;
-        total += level_bytes(l);
-        kf = l;
+    for (size_t budget : {(size_t)16 * 1024, (size_t)64 * 1024}) {
+        size_t total = 0;
+        for (int l = L - 1; l >= 0; --l) {
+            if (total + level_bytes(l) > budget || L - l > kMaxFused) break;
+            total += level_bytes(l);
+            kf = l;
+        }
+        if (kf < L) break;
     }
     if (kf == L && ps.mg_ok) {
         // only periodic in y can stop coarsening early (rows no longer even)
