@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--cfg4-eval", type=int, default=2000)
     ap.add_argument("--cfg4-epochs", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="profiling aid: W steps of the workload, then K Poisson solves from the same "
+                         "state (phi of the previous step as the start); prints their statistics")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="with --solve-only: PCG iterations as direct launches (for profilers)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-energy", action="store_true",
@@ -312,7 +317,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     l0 = launches()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
     iters = []
     t_wall0 = time.perf_counter()
     for k in range(args.steps):
@@ -324,8 +329,9 @@ def run_ours(args, rank, world, local_rank):
         e[1].record(stream)
         pic.poisson_solve(it)
         e[2].record(stream)
-        for s in range(2):
-            pic.move_particles(s, it)
+        pic.move_particles(0, it)
+        e[4].record(stream)
+        pic.move_particles(1, it)
         e[3].record(stream)
         iters.append(pic.poisson_stats()[0])
         it += 1
@@ -378,6 +384,7 @@ def run_ours(args, rank, world, local_rank):
                      "achieved_GBs": BYTES_STEP * n_part / (step_particle_ms * 1e-3) / 1e9,
                      "survey_112B_equivalent_GBs": BYTES_SURVEY_FP32 * n_part / (step_particle_ms * 1e-3) / 1e9}
     roofline_step["frac"] = roofline_step["achieved_GBs"] / peak
+    roofline["kernels"] = kernel_rooflines(w, counts, ev, pois_ms, iters, phases, peak, peak_kind)
 
     learned = None
     if not args.no_learned:
@@ -411,6 +418,51 @@ def run_ours(args, rank, world, local_rank):
 
 
 P_PHASES = 6
+
+# Algorithmic bytes of one MG-PCG iteration per fine node: the finest
+# level's down kernel (read b, mask; write x and the coarse b: 10 B), up
+# kernel (read x, b, mask, the coarse x, r; write z: 22 B), p/q update (read
+# z, mask, p, q; write p, q: 37 B) and x/r update (read p, q, x, r, mask;
+# write x, r, r32: 53 B), plus the coarser tiled levels (24 B a node at a
+# quarter, a sixteenth ... of the nodes: about 8 B).
+POISSON_BYTES_NODE_ITER = 130
+# k_flush per node and species: read the two accumulators and rho, write
+# them back (accumulators cleared) with final_mesh and energy_mesh.
+FLUSH_BYTES_NODE = 64
+
+
+def kernel_rooflines(w, counts, ev, pois_ms, iters, phases, peak, peak_kind):
+    """HBM roofline of each kernel class of the step, from the timed steps'
+    CUDA events (per-species push passes, the solve) and the profiled
+    steps' phase timers (flush): algorithmic bytes / device time against
+    the copy bandwidth.  The push passes include their side-list fix-up
+    (~8 us); the solve's vectors (8 MB each at 1025^2) stay in L2, so it is
+    latency-bound far below HBM, which the fraction shows."""
+    steps = len(ev)
+    nodes = (w.nx + 1) * (w.ny + 1)
+    out = []
+    for s, name in ((0, "electrons"), (1, "Ar+")):
+        ms = sum((e[4].elapsed_time(e[3]) if s == 1 else e[2].elapsed_time(e[4])) for e in ev) / steps
+        gbs = BYTES_PUSH_PASS * counts[s] / (ms * 1e-3) / 1e9
+        out.append({"kernel": f"k_cells<kPush> {name} pass (+ k_fixup)", "ms": ms,
+                    "bytes": BYTES_PUSH_PASS * counts[s], "achieved_GBs": gbs, "frac": gbs / peak})
+    fl = phases["flush"]
+    if fl["calls_per_step"]:
+        ms = fl["ms_per_step"] / fl["calls_per_step"]
+        gbs = FLUSH_BYTES_NODE * nodes / (ms * 1e-3) / 1e9
+        out.append({"kernel": "k_flush (accumulators -> meshes, rho)", "ms": ms, "bytes": FLUSH_BYTES_NODE * nodes,
+                    "achieved_GBs": gbs, "frac": gbs / peak})
+    ms = statistics.mean(pois_ms)
+    it = statistics.mean(iters)
+    b = POISSON_BYTES_NODE_ITER * nodes * it
+    gbs = b / (ms * 1e-3) / 1e9
+    out.append({"kernel": "Poisson MG-PCG solve (k_mg_down, k_mg_fused, k_mg_up, k_pcg_pq, k_pcg_update per "
+                "iteration; setup, true residual, E field)", "ms": ms, "iterations": it, "bytes": b,
+                "bytes_per_node_iteration": POISSON_BYTES_NODE_ITER, "achieved_GBs": gbs, "frac": gbs / peak})
+    for k in out:
+        k["peak_GBs"] = peak
+        k["peak_kind"] = f"{peak_kind} hbm_gbs"
+    return out
 
 
 def run_learned(pic, args, it):
@@ -463,7 +515,7 @@ def run_learned(pic, args, it):
             "train_s": train_s, "loss_first_epoch": loss0, "loss_last_epoch": loss,
             "eval_steps": args.ws_eval, "scales": list(pic.ws_scales()),
             "what": "residual loss |db - A guess|^2 (scaled); network: 3-level conv encoder-decoder, "
-                    "32 channels, 32->32 forward convolutions on tcgen05 (TMEM accumulators), the rest on mma.sync; bf16 operands, FP32 accumulation"}, it
+                    "32 channels, 32->32 convolutions (forward and data gradients) on tcgen05 (TMEM accumulators), the 3->32 / 32->1 forward layers and the 32->32 weight gradients on mma.sync; bf16 operands, FP32 accumulation"}, it
 
 
 def run_ensemble(args, rank, world, local_rank):
@@ -650,6 +702,33 @@ def run_e2e(pic, steps, n_part, it0):
                     "from the last solve (Poisson excluded, as in the metric)"}
 
 
+def run_solve_only(args):
+    """K solves of the workload's Poisson problem from one state, for a
+    kernel launch list; not a bench line."""
+    import pic_b200 as P
+    import pic_configs as C
+    w = workload(args.config)
+    with P.Pic(C.library_config(w, deposit_energy=not args.no_energy)) as pic:
+        C.load_plasma(pic, w)
+        for it in range(args.warmup):
+            pic.step(it)
+        phi_prev = pic.phi()
+        pic.zero_rho()
+        for s in range(2):
+            pic.charge_deposition(s)
+        rho = pic.rho()
+        P._check(P.lib().pic_set_poisson_graph(pic.h, 0 if args.no_graph else 1))
+        st = []
+        for _ in range(args.steps):
+            pic.set_rho(rho)
+            pic.set_phi(phi_prev)
+            pic.poisson_solve(args.warmup)
+            st.append(pic.poisson_stats())
+    print(json.dumps({"solve_only": describe(w), "graph": not args.no_graph, "iters": [x[0] for x in st],
+                      "relres": st[-1][1], "ms_median": statistics.median([x[2] for x in st])}))
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -682,6 +761,8 @@ def main():
 
     if args.config == "cfg4":
         return run_cfg4(args) if rank == 0 else 0
+    if args.solve_only:
+        return run_solve_only(args) if rank == 0 else 0
     if world > 1:
         import datetime
         import torch
