@@ -482,7 +482,7 @@ def run_learned(pic, args, it):
     loss0 = pic.ws_train(1, args.ws_lr)
     loss = pic.ws_train_cosine(max(args.ws_epochs - 1, 1), args.ws_lr, args.ws_lr / 100)
     train_s = time.perf_counter() - t0
-    ml, mp, il, ip, dphi = [], [], [], [], []
+    ml, mp, il, ip, dphi, r0l, r0p = [], [], [], [], [], [], []
     for _ in range(args.ws_eval):
         pic.zero_rho()
         for s in range(2):
@@ -491,12 +491,14 @@ def run_learned(pic, args, it):
         pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_LEARNED, 1e-8, 500)
         pic.poisson_solve(it)
         n_l, r_l, ms_l = pic.poisson_stats()
+        r0l.append(pic.poisson_start_relres())
         phi_l = pic.phi()
         pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_PREVIOUS, 1e-8, 500)
         pic.set_phi(phi_prev)
         pic.set_rho(rho)
         pic.poisson_solve(it)
         n_p, r_p, ms_p = pic.poisson_stats()
+        r0p.append(pic.poisson_start_relres())
         dphi.append(float(np.abs(phi_l - pic.phi()).max()))
         for s in range(2):
             pic.move_particles(s, it)
@@ -511,6 +513,7 @@ def run_learned(pic, args, it):
     return {"ms_per_step_learned": statistics.median(ml), "ms_per_step_plain_same_state": statistics.median(mp),
             "ms_mean_learned": statistics.mean(ml), "ms_mean_plain_same_state": statistics.mean(mp),
             "iters_learned": statistics.mean(il), "iters_plain_same_state": statistics.mean(ip),
+            "start_relres_learned": statistics.mean(r0l), "start_relres_plain_same_state": statistics.mean(r0p),
             "max_abs_dphi_V": max(dphi), "train_pairs": args.ws_pairs, "train_epochs": args.ws_epochs,
             "train_s": train_s, "loss_first_epoch": loss0, "loss_last_epoch": loss,
             "eval_steps": args.ws_eval, "scales": list(pic.ws_scales()),
@@ -617,7 +620,7 @@ def run_cfg4(args):
     losses.append(pic.ws_train_cosine(max(args.cfg4_epochs - 1, 1), args.ws_lr, args.ws_lr / 100))
     train_s = time.perf_counter() - t0
     pic.ws_record(-1)
-    ml, mp, il, ip, dphi = [], [], [], [], []
+    ml, mp, il, ip, dphi, r0l, r0p = [], [], [], [], [], [], []
     it = T + 1
     for _ in range(E):
         pic.zero_rho()
@@ -627,12 +630,14 @@ def run_cfg4(args):
         pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_LEARNED, 1e-8, 500)
         pic.poisson_solve(it)
         n_l, r_l, ms_l = pic.poisson_stats()
+        r0l.append(pic.poisson_start_relres())
         phi_l = pic.phi()
         pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_PREVIOUS, 1e-8, 500)
         pic.set_phi(phi_prev)
         pic.set_rho(rho)
         pic.poisson_solve(it)
         n_p, r_p, ms_p = pic.poisson_stats()
+        r0p.append(pic.poisson_start_relres())
         dphi.append(float(np.abs(phi_l - pic.phi()).max()))
         for s in range(2):
             pic.move_particles(s, it)
@@ -648,6 +653,7 @@ def run_cfg4(args):
                        "epochs": args.cfg4_epochs},
             "plain_ms_per_step_same_state": statistics.mean(mp),
             "iters_learned": statistics.mean(il), "iters_plain_same_state": statistics.mean(ip),
+            "start_relres_learned": statistics.mean(r0l), "start_relres_plain_same_state": statistics.mean(r0p),
             "iters_learned_hist": {str(k): il.count(k) for k in sorted(set(il))},
             "iters_plain_hist": {str(k): ip.count(k) for k in sorted(set(ip))},
             "max_abs_dphi_V": max(dphi), "loss_per_epoch": losses,

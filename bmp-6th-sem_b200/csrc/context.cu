@@ -914,6 +914,12 @@ int pic_set_poisson_graph(pic_ctx* c, int enable) {
     return PIC_OK;
 }
 
+int pic_poisson_start_relres(pic_ctx* c, double* relres0) {
+    if (!c || !relres0) return fail(PIC_ERR_ARG, "null argument");
+    *relres0 = c->ps.last_relres0;
+    return PIC_OK;
+}
+
 int pic_poisson_stats(pic_ctx* c, int* iters, double* relres, double* ms) {
     if (!c) return fail(PIC_ERR_ARG, "null context");
     if (iters) *iters = c->ps.last_iters;

@@ -159,6 +159,7 @@ struct PoissonState {
     bool have_prev = false;
     int last_iters = 0;
     double last_relres = 0, last_ms = 0;
+    double last_relres0 = 0;  // relative residual of the last solve's starting guess
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float* net_guess = nullptr;  // learned warm start output (nodes), optional
     // false: no multigrid hierarchy (periodic in y with an odd row count, or

@@ -70,7 +70,8 @@ enum {
     S_IT = 7,     // iterations done
     S_TOL2 = 8,   // tol^2
     S_MAXIT = 9,  // iteration limit
-    S_STATUS = 10 // 0 running/converged, 1 iteration limit, 2 not finite
+    S_STATUS = 10, // 0 running/converged, 1 iteration limit, 2 not finite
+    S_RR0 = 11     // r.r of the solve's starting guess
 };
 
 struct Grid64 {
@@ -220,7 +221,10 @@ __global__ void k_fix_bb(double* scal, double tol2, int maxit, int restart) {
     scal[S_TOL2] = tol2;
     scal[S_MAXIT] = (double)maxit;
     scal[S_STATUS] = 0.0;
-    if (!restart) scal[S_IT] = 0.0;
+    if (!restart) {
+        scal[S_IT] = 0.0;
+        scal[S_RR0] = scal[S_RR];
+    }
 }
 
 // z = M^-1 r (from the MG output or the diagonal); partial r.z
@@ -1424,6 +1428,7 @@ int poisson_solve(pic_ctx* c) {
     ps.last_ms = ms;
     ps.last_iters = it;
     ps.last_relres = bb > 0 ? std::sqrt(true_rr / bb) : 0.0;
+    ps.last_relres0 = bb > 0 ? std::sqrt(ps.host_scal[S_RR0] / bb) : 0.0;
     ps.have_prev = true;
     if (learned) PIC_TRY(ws_check_fault());  // the guess's kernels gave up a bounded wait
     if (status != PIC_OK)

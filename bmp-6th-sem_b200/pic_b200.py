@@ -168,6 +168,7 @@ def lib():
         "pic_debug_set_wait_limits": (cint, [vp, i64, i64]),
         "pic_debug_vcycle": (cint, [vp, vp, vp, cint]),
         "pic_set_poisson_graph": (cint, [vp, cint]),
+        "pic_poisson_start_relres": (cint, [vp, P(dbl)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -442,6 +443,12 @@ class Pic:
         it, rr, ms = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)
         _check(lib().pic_poisson_stats(self.h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(ms)))
         return it.value, rr.value, ms.value
+
+    def poisson_start_relres(self):
+        """Relative residual of the last solve's starting guess."""
+        r = ctypes.c_double(0)
+        _check(lib().pic_poisson_start_relres(self.h, ctypes.byref(r)))
+        return r.value
 
 
 class _Instance(Pic):

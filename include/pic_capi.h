@@ -407,6 +407,10 @@ int pic_set_poisson_graph(pic_ctx* ctx, int enable);
 /* Iterations, achieved relative residual and device milliseconds of the most
  * recent solve. */
 int pic_poisson_stats(pic_ctx* ctx, int* iterations, double* relres, double* ms);
+/* (no reference counterpart) Relative residual ||b - A x0|| / ||b|| of the
+ * starting guess x0 of the most recent single-context solve (the previous
+ * phi, zero, or the learned guess), on the reduced system. */
+int pic_poisson_start_relres(pic_ctx* ctx, double* relres0);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,12 @@
   from the network's guess reaches the same 1e-8 relative residual as PCG
   started from phi_{n-1} on the same state: the converged potentials agree
   to 1e-6 of max|phi| (both are 1e-8-residual solutions of one system).
+  The guess is strictly the better start: its starting residual
+  (pic_poisson_start_relres) is below phi_{n-1}'s on every evaluation step
+  and below half of it on average; it never costs iterations.
+* The data gradients run on the tcgen05 row convolution (flipped,
+  transposed weights, relu gate in its epilogue), the forward 32->32 layers
+  too; the gradient check covers both.
 """
 import numpy as np
 import pytest
@@ -150,7 +156,7 @@ def test_training_and_same_state_guess(oracle):
         assert last < 0.5 * first, (first, last)
         GX = w.GX
         mask = oracle.electrode_mask(GX, GX, oracle.Electrodes(w.rects))
-        it_l, it_p = [], []
+        it_l, it_p, ratio = [], [], []
         for it in range(59, 65):
             pic.zero_rho()
             for s in range(2):
@@ -159,12 +165,14 @@ def test_training_and_same_state_guess(oracle):
             pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_LEARNED, 1e-8, 500)
             pic.poisson_solve(it)
             nl, rl, _ = pic.poisson_stats()
+            r0_l = pic.poisson_start_relres()
             phi_l, b = pic.phi(), pic.rho()
             pic.set_poisson(P.SOLVER_MG_PCG, P.WARM_PREVIOUS, 1e-8, 500)
             pic.set_phi(phi_prev)
             pic.set_rho(rho)
             pic.poisson_solve(it)
             npl, rp, _ = pic.poisson_stats()
+            r0_p = pic.poisson_start_relres()
             phi_p = pic.phi()
             assert rl <= 1e-8 and rp <= 1e-8
             dxl = w.xmax / w.nx
@@ -173,6 +181,12 @@ def test_training_and_same_state_guess(oracle):
             assert np.abs(phi_l - phi_p).max() <= 1e-6 * np.abs(phi_p).max()
             it_l.append(nl)
             it_p.append(npl)
+            ratio.append(r0_l / r0_p)
             for s in range(2):
                 pic.move_particles(s, it)
+    # the trained guess is a strictly better start: its starting residual is
+    # below half of phi_{n-1}'s on average and below it on every step; the
+    # iteration count may not move (the gain is in components the first
+    # V-cycle removes), but it never grows
+    assert np.mean(ratio) < 0.5 and max(ratio) < 1.0, ratio
     assert np.mean(it_l) <= np.mean(it_p), (it_l, it_p)
