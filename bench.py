@@ -518,7 +518,7 @@ def run_learned(pic, args, it):
             "train_s": train_s, "loss_first_epoch": loss0, "loss_last_epoch": loss,
             "eval_steps": args.ws_eval, "scales": list(pic.ws_scales()),
             "what": "residual loss |db - A guess|^2 (scaled); network: 3-level conv encoder-decoder, "
-                    "32 channels, 32->32 convolutions (forward and data gradients) on tcgen05 (TMEM accumulators), the 3->32 / 32->1 forward layers and the 32->32 weight gradients on mma.sync; bf16 operands, FP32 accumulation"}, it
+                    "32 channels, 32->32 convolutions (forward, data and weight gradients) on tcgen05 (TMEM accumulators), the 3->32 / 32->1 layers on mma.sync and FP32 cores; bf16 operands, FP32 accumulation"}, it
 
 
 def run_ensemble(args, rank, world, local_rank):

@@ -25,11 +25,11 @@
 // x 32 channels for the 32->32 layers): the 32->32 layers forward and their
 // data gradients on tcgen05 with TMEM accumulators (k_conv_rows: the average
 // pools fused into the forward epilogue, the relu gates into the gradient
-// one); the forward 3->32 input and 32->1 output layers with
+// one) and their weight gradients on tcgen05 as well (k_wgrad_rows, MN-major
+// operands); the forward 3->32 input and 32->1 output layers with
 // mma.sync.m16n8k16 (K = 12 taps x 4 channels, and N = 8 of which one column
-// is used), their bf16 weights prepacked as B fragments; the weight
-// gradients of the 32->32 layers with mma.sync, those of the outer layers on
-// the FP32 cores.
+// is used), their bf16 weights prepacked as B fragments; the outer layers'
+// gradients on the FP32 cores.
 // Weight gradients are reduced through per-block partials in a fixed order,
 // so training is deterministic.
 #include <cuda.h>
@@ -60,13 +60,6 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2,
                                         uint32_t& r3) {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-                 : "r"(addr));
-}
-
-__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2,
-                                          uint32_t& r3) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                  : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
                  : "r"(addr));
 }
@@ -529,107 +522,255 @@ __global__ void k_pack_rows_w(const float* w, int64_t stride, int layers, __nv_b
 }
 
 // ---------------------------------------------------------------------------
-// 32 -> 32 weight gradient: dW[tap][co][ci] = sum_p dY[p][co] * X[p+tap][ci],
-// db[co] = sum_p dY[p][co].  Persistent blocks over output tiles; warp w
-// owns tap w (warp 0 also tap 8); per-block partials are summed afterwards.
+// 32 -> 32 weight gradient on tcgen05 (training).
+//
+//   dW[dy][dx][ci][co] = sum_{y, x} X[y + dy - 1][x + dx - 1][ci] dY[y][x][co],
+//   db[co] = sum_{y, x} dY[y][x][co]
+//
+// The reduction runs over pixels, so both operands are MN-major: a pixel's
+// 32 channels (64 bytes) are the M (or N) extent of one swizzle atom and
+// consecutive pixels its K rows, which is exactly how the TMA boxes of the
+// NHWC images land in shared memory (64-byte swizzle, 8 pixels a 512-byte
+// atom).  A unit is 4 rows x 32 pixels of dY (rows y0 .. y0 + 3, pixels
+// x0 .. x0 + 31): its dY box (4 rows) and, for each column tap dx, a box of
+// X rows y0 - 1 .. y0 + 5 shifted by dx - 1 pixels (zero filled outside the
+// image).  For dY row r the A operand is X rows r .. r + 3 of the dx box --
+// four 32-channel atoms 2 KB apart (LBO), so M = 128 = (dy = 0..3) x 32 ci,
+// the fourth row tap unused -- and B is dY row r (N = 32 co); K = 16 pixels
+// an MMA (two 8-pixel groups 512 bytes apart, SBO).  Every unit adds its
+// 24 MMAs (4 rows x 3 dx x 2 K blocks) into three TMEM accumulators
+// (D_dx[dy ci][co]), which the CTA writes out once at the end as its
+// per-block partial; the partials are summed in a fixed order afterwards.
+//
+// Roles, 8 warps: warp 0 TMA producer (one lane), warp 1 TMEM allocation and
+// MMA issue (one lane), warps 4-7 the bias gradient (each unit's dY box from
+// shared memory, a channel and a quarter of the pixels a thread) and the
+// final TMEM read-out (warp 4 + dy reads lanes 32 dy ..).  Every wait is
+// bounded as in k_conv_rows.
 // ---------------------------------------------------------------------------
-constexpr int kWgradSmem = ((TH + 2) * (TW + 2) * CP + TH * TW * CP) * 2;
+constexpr int kWgStages = 3;
+constexpr int kWgXRows = 7;                              // X rows of a box
+constexpr int kWgXBytes = kWgXRows * 32 * 64;            // 14 KB
+constexpr int kWgDBytes = 4 * 32 * 64;                   // 8 KB
+constexpr int kWgStageBytes = 3 * kWgXBytes + kWgDBytes; // 50 KB
+constexpr int kWgOffStages = 2048;
+// a 4 KB pad after the ring keeps every operand address an MMA can form
+// inside the allocation
+constexpr int kWgSmemUsed = kWgOffStages + kWgStages * kWgStageBytes + 4096;
+constexpr int kWgSmem = kWgSmemUsed + 1024;              // + alignment slack
+static_assert(kWgStageBytes % 1024 == 0, "stages 1024-aligned");
+static_assert(kWgSmem <= 227 * 1024, "weight-gradient shared memory");
+constexpr int kWgThreads = 8 * 32;
+// kind::f16: FP32 accumulator, bf16 A and B, both MN-major, N = 32, M = 128
+constexpr uint32_t kWgIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                              ((32u >> 3) << 17) | ((128u >> 4) << 24);
 
-__global__ void __launch_bounds__(256) k_wgrad32(const __nv_bfloat16* X, const __nv_bfloat16* dY,
-                                                 int P, float* partial) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* x_s = reinterpret_cast<__nv_bfloat16*>(smem);
-    __nv_bfloat16* d_s = x_s + (TH + 2) * (TW + 2) * CP;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tiles_x = (P + TW - 1) / TW, tiles_y = (P + TH - 1) / TH;
-    float acc[2][2][4][4];  // [tap slot][m][n][e]
-    float bsum = 0.f;       // bias gradient: thread t < 32 owns channel t
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int n = 0; n < 4; ++n)
-#pragma unroll
-                for (int e = 0; e < 4; ++e) acc[s][m][n][e] = 0.f;
-    for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
-        const int y0 = (tile / tiles_x) * TH, x0 = (tile % tiles_x) * TW;
-        __syncthreads();
-        load_halo_async(x_s, X, P, y0, x0);
-        for (int i = threadIdx.x; i < TH * TW * (C / 8); i += blockDim.x) {
-            const int q = i & 3, pix = i >> 2;
-            const int y = y0 + pix / TW, x = x0 + pix % TW;
-            const bool in = y < P && x < P;
-            cp_async16(d_s + pix * CP + q * 8, in ? dY + ((int64_t)y * P + x) * C + q * 8 : dY, in);
+// MN-major operand, 64-byte swizzle: 32-element atoms `lbo` bytes apart in
+// M/N, 8-row K groups `sbo` bytes apart
+__device__ __forceinline__ uint64_t sw64_mn_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (4ull << 61);
+}
+
+__device__ __forceinline__ void wg_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kWgIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kWgThreads, 1) k_wgrad_rows(const __grid_constant__ CUtensorMap tmx,
+                                                             const __grid_constant__ CUtensorMap tmd,
+                                                             int P, float* partial) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t sbase = smem_u32(smem);
+    // head: full[3] @0, empty[3] @32, accf @64, TMEM address @80, abort @84;
+    // bias exchange [4][32] floats @1024; stages from @2048
+    const uint32_t full0 = sbase, empty0 = sbase + 32, accf = sbase + 64;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 80);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 84);
+    float* sdb = reinterpret_cast<float*>(smem + 1024);
+    unsigned char* stages = smem + kWgOffStages;
+    const long long wl = g_ws_wait_cycles;
+    const int nrb = (P + 3) / 4;  // row blocks; rows past P read as zero
+    const int units = nrb * ((P + 31) / 32);
+    int g0, g1;
+    rw_share(units, g0, g1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(smem_u32(tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWgStages; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 5);  // the MMA commit and the four bias warps
         }
-        cp_async_wait_all();
-        __syncthreads();
-        if (threadIdx.x < C) {
-            float s = 0.f;
-            for (int pix = 0; pix < TH * TW; ++pix) s += __bfloat162float(d_s[pix * CP + threadIdx.x]);
-            bsum += s;
-        }
+        mbar_init(accf, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+    auto give_up = [&]() {
+        if (!*abort_flag) atomicExch(&g_ws_fault, 1);
+        *abort_flag = 1;
+    };
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int k = 0;
+            for (int u = g0; u < g1; ++u, ++k) {
+                const int s = k % kWgStages;
+                if (k >= kWgStages && !mbar_wait_bounded(empty0 + 8 * s, ((k / kWgStages) & 1) ^ 1, wl)) {
+                    give_up();
+                    break;
+                }
+                if (*abort_flag) break;
+                const int x0 = (u / nrb) * 32, y0 = (u % nrb) * 4;
+                const uint32_t st = smem_u32(stages + s * kWgStageBytes);
+                mbar_expect_tx(full0 + 8 * s, kWgStageBytes);
 #pragma unroll
-        for (int slot = 0; slot < 2; ++slot) {
-            const int tap = slot == 0 ? warp : 8;
-            if (slot == 1 && warp != 0) break;
-            const int dy = tap / 3, dx = tap % 3;
+                for (int dx = 0; dx < 3; ++dx)
+                    tma_load_3d(st + dx * kWgXBytes, &tmx, 0, x0 + dx - 1, y0 - 1, full0 + 8 * s);
+                tma_load_3d(st + 3 * kWgXBytes, &tmd, 0, x0, y0, full0 + 8 * s);
+            }
+            // every copy issued has landed before the CTA leaves (fixed bound)
+            for (int j = max(0, k - kWgStages); j < k; ++j)
+                if (!mbar_wait_bounded(full0 + 8 * (j % kWgStages), (j / kWgStages) & 1, kWsWaitCycles))
+                    atomicExch(&g_ws_fault, 1);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMA issue ----------------
+        if (lane == 0) {
+            int k = 0;
+            for (int u = g0; u < g1; ++u, ++k) {
+                const int s = k % kWgStages;
+                if (!mbar_wait_bounded(full0 + 8 * s, (k / kWgStages) & 1, wl)) {
+                    give_up();
+                    break;
+                }
+                if (*abort_flag) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t st = smem_u32(stages + s * kWgStageBytes);
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                        for (int kb = 0; kb < 2; ++kb)
+                            wg_mma(tmem + dx * 32, sw64_mn_desc(st + dx * kWgXBytes + r * 2048 + kb * 1024, 2048, 512),
+                                   sw64_mn_desc(st + 3 * kWgXBytes + r * 2048 + kb * 1024, 2048, 512),
+                                   (k | r | kb) ? 1u : 0u);
+                tc_commit(empty0 + 8 * s);
+            }
+            // all issued MMAs have completed when this arrives (also on the
+            // give-up path, before the tensor memory is freed)
+            tc_commit(accf);
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // ---------------- bias gradient, then the read-out ----------------
+        const int q = warp - 4;  // pixels 8q .. 8q + 7 of each row; TMEM lanes 32q ..
+        const int chunk = lane >> 3, e = lane & 7;
+        float dbs = 0.f;
+        int k = 0;
+        for (int u = g0; u < g1; ++u, ++k) {
+            const int s = k % kWgStages;
+            const bool ok = __all_sync(kFull, !*abort_flag && mbar_wait_bounded(full0 + 8 * s, (k / kWgStages) & 1, wl));
+            if (!ok) {
+                if (lane == 0) give_up();
+                break;
+            }
+            const unsigned char* dyb = stages + s * kWgStageBytes + 3 * kWgXBytes;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int p = 0; p < 8; ++p) {
+                    // channel `lane` of pixel 8q + p in row r: 64-byte rows,
+                    // 16-byte chunk index XOR (row >> 1) & 3 (the 64-byte swizzle)
+                    const int row = r * 32 + 8 * q + p;
+                    const int off = row * 64 + ((chunk ^ ((row >> 1) & 3)) << 4) + 2 * e;
+                    dbs += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(dyb + off));
+                }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        }
+        sdb[q * 32 + lane] = dbs;
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        float* out = partial + (int64_t)blockIdx.x * (9 * C * C + C);
+        if (q == 0) out[9 * C * C + lane] = ((sdb[lane] + sdb[32 + lane]) + sdb[64 + lane]) + sdb[96 + lane];
+        const bool done = __all_sync(kFull, mbar_wait_bounded(accf, 0, kWsWaitCycles));
+        const bool good = __all_sync(kFull, done && !*abort_flag && g1 > g0);
+        if (!done && lane == 0) give_up();
+        if (q < 3) {
+            // row tap dy = q, input channel ci = lane; column dx * 32 + co
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16);
+            float v[16];
 #pragma unroll 1
-            for (int kp = 0; kp < TH * TW; kp += 16) {  // 16 pixels of one tile row
-                const int prow = kp / TW, pcol = kp % TW;
-                uint32_t a[2][4];
+            for (int cb = 0; cb < 6; ++cb) {
+                if (good) {
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    tc_ld16(ta + cb * 16, v);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                } else {
 #pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    // A = dY^T: rows co, cols pixels; stored [pixel][co] -> transposed load
-                    const int p = kp + (lane & 7) + (lane >> 4) * 8;
-                    const int co = m * 16 + ((lane >> 3) & 1) * 8;
-                    ldsm_x4_t(smem_u32(d_s + p * CP + co), a[m][0], a[m][1], a[m][2], a[m][3]);
-                }
-                uint32_t b[4][2];
-#pragma unroll
-                for (int nh = 0; nh < 2; ++nh) {
-                    const int pl = (lane & 7) + ((lane >> 3) & 1) * 8;  // pixel within the 16
-                    const int ci = nh * 16 + (lane >> 4) * 8;
-                    const __nv_bfloat16* pb = x_s + ((prow + dy) * (TW + 2) + pcol + pl + dx) * CP + ci;
-                    ldsm_x4_t(smem_u32(pb), b[nh * 2][0], b[nh * 2][1], b[nh * 2 + 1][0], b[nh * 2 + 1][1]);
+                    for (int j = 0; j < 16; ++j) v[j] = 0.f;
                 }
 #pragma unroll
-                for (int m = 0; m < 2; ++m)
-#pragma unroll
-                    for (int n = 0; n < 4; ++n)
-                        mma_bf16(acc[slot][m][n], a[m][0], a[m][1], a[m][2], a[m][3], b[n][0], b[n][1]);
+                for (int j = 0; j < 16; ++j) {
+                    const int col = cb * 16 + j, dx = col >> 5, co = col & 31;
+                    out[((q * 3 + dx) * C + co) * C + lane] = v[j];
+                }
             }
         }
     }
-    // partial[block][tap][co][ci] and partial[block][9*32*32 + co]
-    float* out = partial + (int64_t)blockIdx.x * (9 * C * C + C);
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int slot = 0; slot < 2; ++slot) {
-        const int tap = slot == 0 ? warp : 8;
-        if (slot == 1 && warp != 0) break;
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int n = 0; n < 4; ++n)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int co = m * 16 + g + h * 8, ci = n * 8 + t * 2;
-                    out[(tap * C + co) * C + ci] = acc[slot][m][n][h * 2];
-                    out[(tap * C + co) * C + ci + 1] = acc[slot][m][n][h * 2 + 1];
-                }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem) : "memory");
     }
-    if (threadIdx.x < C) out[9 * C * C + threadIdx.x] = bsum;
 }
 
-// Sums per-block partials (fixed order) into grad[n] (n values per block).
+// Sums per-block partials into grad[n] (n values per block) in a fixed
+// order.  Many outputs: a thread an output, eight interleaved running sums
+// (block b into sum b % 8, combined in order) so that eight loads are in
+// flight; few outputs: a warp an output, lane l summing blocks l, l + 32,
+// ..., then a fixed shuffle tree.
+constexpr int kSumWide = 1024;  // outputs from which a thread takes one
 __global__ void k_sum_partials(const float* partial, int nblocks, int n, float* grad) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float s = 0.f;
-    for (int b = 0; b < nblocks; ++b) s += partial[(int64_t)b * n + i];
-    grad[i] = s;
+    if (n >= kSumWide) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int b = 0;
+        for (; b + 8 <= nblocks; b += 8)
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s[u] += partial[(int64_t)(b + u) * n + i];
+        for (int u = 0; b < nblocks; ++b, ++u) s[u] += partial[(int64_t)b * n + i];
+        grad[i] = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+        return;
+    }
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i >= n) return;  // whole warps leave together
+    float v = 0.f;
+    for (int b = lane; b < nblocks; b += 32) v += partial[(int64_t)b * n + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if (lane == 0) grad[i] = v;
 }
+
+// launch shape of k_sum_partials for n outputs
+inline unsigned sum_blocks(int n) { return n >= kSumWide ? (unsigned)((n + 255) / 256) : (unsigned)((n * 32 + 255) / 256); }
 
 // ---------------------------------------------------------------------------
 // Input conv 3->32, output conv 32->1
@@ -1100,6 +1241,7 @@ struct Net {
     __nv_bfloat16* wrows_t = nullptr;
     CUtensorMap tm_in[9];
     CUtensorMap tm_grad[6];
+    CUtensorMap tm_wx[9], tm_wd[6];  // the same images in k_wgrad_rows' boxes
     // activations (P = fine, Q = P/2, R = P/4)
     __nv_bfloat16 *x0 = nullptr, *a[11] = {}, *p1 = nullptr, *p2 = nullptr, *u0 = nullptr, *u1 = nullptr;
     float* out = nullptr;
@@ -1184,7 +1326,7 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P) {
+static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P, int rows = kRwBoxRows) {
     static EncodeTiledFn encode = nullptr;
     if (!encode) {
         void* f = nullptr;
@@ -1196,7 +1338,7 @@ static int make_row_tmap(CUtensorMap* tm, const __nv_bfloat16* base, int P) {
     }
     const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)P, (cuuint64_t)P};
     const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)P * C * 2};
-    const cuuint32_t box[3] = {(cuuint32_t)C, 32, (cuuint32_t)kRwBoxRows};
+    const cuuint32_t box[3] = {(cuuint32_t)C, 32, (cuuint32_t)rows};
     const cuuint32_t es[3] = {1, 1, 1};
     const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dims,
                               strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
@@ -1263,8 +1405,11 @@ static int ws_alloc(pic_ctx* c) {
         const __nv_bfloat16* gr[6] = {N.d_big[0], N.d_big[1], N.d_mid[0], N.d_mid[1], N.d_small[0], N.d_small[1]};
         const int gs[6] = {(int)P, (int)P, (int)Q, (int)Q, (int)R, (int)R};
         for (int i = 0; i < 6; ++i) PIC_TRY(make_row_tmap(&N.tm_grad[i], gr[i], gs[i]));
+        // the weight gradients' boxes: X rows y0 - 1 .. y0 + 5, dY rows y0 .. y0 + 3
+        for (int l = 0; l < 9; ++l) PIC_TRY(make_row_tmap(&N.tm_wx[l], ins[l], sz[l], kWgXRows));
+        for (int i = 0; i < 6; ++i) PIC_TRY(make_row_tmap(&N.tm_wd[i], gr[i], gs[i], 4));
     }
-    PIC_CUDA(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
+    PIC_CUDA(cudaFuncSetAttribute(k_wgrad_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
     return PIC_OK;
 }
 
@@ -1408,10 +1553,14 @@ __global__ void k_scatter_wgrad(const float* src, float* g) {
     }
 }
 
-static void wgrad32(pic_ctx* c, int layer, const __nv_bfloat16* X, const __nv_bfloat16* dY, int P) {
+// Weight gradient of 32->32 layer `layer` from its forward input (tm_wx)
+// and the gradient image tm_wd[g] of its output, on tcgen05.
+static void wgrad32(pic_ctx* c, int layer, int g, int P) {
     Net& N = c->ws->net;
-    k_wgrad32<<<kWgradBlocks, 256, kWgradSmem, c->stream>>>(X, dY, P, N.partial);
-    k_sum_partials<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.partial, kWgradBlocks, 9 * C * C + C,
+    const int units = ((P + 3) / 4) * ((P + 31) / 32);
+    const int grid = std::max(1, std::min(N.sms, units));
+    k_wgrad_rows<<<grid, kWgThreads, kWgSmem, c->stream>>>(N.tm_wx[layer], N.tm_wd[g], P, N.partial);
+    k_sum_partials<<<sum_blocks(9 * C * C + C), 256, 0, c->stream>>>(N.partial, grid, 9 * C * C + C,
                                                              N.gsum);
     k_scatter_wgrad<<<g1(9 * C * C + C), 256, 0, c->stream>>>(N.gsum, N.g + param_off(layer + 1));
 }
@@ -1449,7 +1598,7 @@ static void enqueue_loss(pic_ctx* c, const float* rhs, float* loss_slot) {
     const float inv_count = 1.f / (float)nodes;
     k_resid<<<g1(nodes), 256, 0, c->stream>>>(N.out, rhs, c->mask, N.GX, N.GY, N.P, kappa, beta,
                                               inv_count, N.resid, N.loss_partial);
-    k_sum_partials<<<1, 32, 0, c->stream>>>(N.loss_partial, (int)g1(nodes), 1, loss_slot);
+    k_sum_partials<<<sum_blocks(1), 256, 0, c->stream>>>(N.loss_partial, (int)g1(nodes), 1, loss_slot);
     k_resid_grad<<<g1((int64_t)N.P * N.P), 256, 0, c->stream>>>(N.resid, c->mask, N.GX, N.GY, N.P,
                                                                 kappa, beta, inv_count, N.dout);
     c->launches += 3;
@@ -1465,33 +1614,33 @@ static void backward(pic_ctx* c) {
     __nv_bfloat16 *S0 = N.d_small[0], *S1 = N.d_small[1];
     // output conv
     k_wgrad_out<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.a[10], N.dout, P, N.partial);
-    k_sum_partials<<<g1(kOutOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kOutOut, N.g + ob);
+    k_sum_partials<<<sum_blocks(kOutOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kOutOut, N.g + ob);
     k_conv_out_dx<<<g1((int64_t)P * P, 128), 128, 0, c->stream>>>(N.dout, N.w + ob, N.a[10], P, B0);
     // B0 = dPre10
-    wgrad32(c, 8, N.a[9], B0, P);
+    wgrad32(c, 8, 0, P);
     conv_rows_grad(c, 8, 0, B1, P, N.a[9]);        // B1 = dPre9
-    wgrad32(c, 7, N.u0, B1, P);
+    wgrad32(c, 7, 1, P);
     conv_rows_grad(c, 7, 1, B2, P, nullptr);       // B2 = dU0
     k_down_sum_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(B2, N.a[8], P, M0);  // M0 = dPre8
-    wgrad32(c, 6, N.a[7], M0, Q);
+    wgrad32(c, 6, 2, Q);
     conv_rows_grad(c, 6, 2, M1, Q, N.a[7]);        // M1 = dPre7
-    wgrad32(c, 5, N.u1, M1, Q);
+    wgrad32(c, 5, 3, Q);
     conv_rows_grad(c, 5, 3, M2, Q, nullptr);       // M2 = dU1
     k_down_sum_gate<<<g1((int64_t)R * R * C), 256, 0, c->stream>>>(M2, N.a[6], Q, S0);  // S0 = dPre6
-    wgrad32(c, 4, N.a[5], S0, R);
+    wgrad32(c, 4, 4, R);
     conv_rows_grad(c, 4, 4, S1, R, N.a[5]);        // S1 = dPre5
-    wgrad32(c, 3, N.p2, S1, R);
+    wgrad32(c, 3, 5, R);
     conv_rows_grad(c, 3, 5, S0, R, nullptr);       // S0 = dP2
     k_skip_pool_gate<<<g1((int64_t)Q * Q * C), 256, 0, c->stream>>>(M2, S0, N.a[4], Q, M0);  // M0 = dPre4
-    wgrad32(c, 2, N.a[3], M0, Q);
+    wgrad32(c, 2, 2, Q);
     conv_rows_grad(c, 2, 2, M1, Q, N.a[3]);        // M1 = dPre3
-    wgrad32(c, 1, N.p1, M1, Q);
+    wgrad32(c, 1, 3, Q);
     conv_rows_grad(c, 1, 3, M0, Q, nullptr);       // M0 = dP1
     k_skip_pool_gate<<<g1((int64_t)P * P * C), 256, 0, c->stream>>>(B2, M0, N.a[2], P, B0);  // B0 = dPre2
-    wgrad32(c, 0, N.a[1], B0, P);
+    wgrad32(c, 0, 0, P);
     conv_rows_grad(c, 0, 0, B1, P, N.a[1]);        // B1 = dPre1
     k_wgrad_in<<<kSmallWgradBlocks, 256, 0, c->stream>>>(N.xin, B1, P, N.partial);
-    k_sum_partials<<<g1(kInOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kInOut, N.g);
+    k_sum_partials<<<sum_blocks(kInOut), 256, 0, c->stream>>>(N.partial, kSmallWgradBlocks, kInOut, N.g);
     c->launches += 2 + 1 + 10 * 3 + 4 + 2;
 }
 
