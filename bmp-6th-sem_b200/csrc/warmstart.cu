@@ -742,25 +742,27 @@ __global__ void __launch_bounds__(kWgThreads, 1) k_wgrad_rows(const __grid_const
 }
 
 // Sums per-block partials into grad[n] (n values per block) in a fixed
-// order.  Many outputs: a thread an output, eight interleaved running sums
-// (block b into sum b % 8, combined in order) so that eight loads are in
-// flight; few outputs: a warp an output, lane l summing blocks l, l + 32,
-// ..., then a fixed shuffle tree.
-constexpr int kSumWide = 1024;  // outputs from which a thread takes one
-__global__ void k_sum_partials(const float* partial, int nblocks, int n, float* grad) {
+// order.  Many outputs: a block takes 32 consecutive outputs, its warp w
+// sums blocks w, w + 8, ... (coalesced rows), and the eight warp sums are
+// added in order; few outputs: a warp an output, lane l summing blocks l,
+// l + 32, ..., then a fixed shuffle tree.
+constexpr int kSumWide = 1024;  // outputs from which the first form is used
+__global__ void __launch_bounds__(256) k_sum_partials(const float* partial, int nblocks, int n, float* grad) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (n >= kSumWide) {
-        const int i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= n) return;
-        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        int b = 0;
-        for (; b + 8 <= nblocks; b += 8)
-#pragma unroll
-            for (int u = 0; u < 8; ++u) s[u] += partial[(int64_t)(b + u) * n + i];
-        for (int u = 0; b < nblocks; ++b, ++u) s[u] += partial[(int64_t)b * n + i];
-        grad[i] = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+        __shared__ float red[8][32];
+        const int i = blockIdx.x * 32 + lane;
+        float v = 0.f;
+        if (i < n)
+            for (int b = warp; b < nblocks; b += 8) v += partial[(int64_t)b * n + i];
+        red[warp][lane] = v;
+        __syncthreads();
+        if (warp == 0 && i < n)
+            grad[i] = ((red[0][lane] + red[1][lane]) + (red[2][lane] + red[3][lane])) +
+                      ((red[4][lane] + red[5][lane]) + (red[6][lane] + red[7][lane]));
         return;
     }
-    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= n) return;  // whole warps leave together
     float v = 0.f;
     for (int b = lane; b < nblocks; b += 32) v += partial[(int64_t)b * n + i];
@@ -769,8 +771,8 @@ __global__ void k_sum_partials(const float* partial, int nblocks, int n, float* 
     if (lane == 0) grad[i] = v;
 }
 
-// launch shape of k_sum_partials for n outputs
-inline unsigned sum_blocks(int n) { return n >= kSumWide ? (unsigned)((n + 255) / 256) : (unsigned)((n * 32 + 255) / 256); }
+// launch shape of k_sum_partials (256 threads a block) for n outputs
+inline unsigned sum_blocks(int n) { return n >= kSumWide ? (unsigned)((n + 31) / 32) : (unsigned)((n * 32 + 255) / 256); }
 
 // ---------------------------------------------------------------------------
 // Input conv 3->32, output conv 32->1
