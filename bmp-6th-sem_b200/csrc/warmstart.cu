@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(kWgThreads, 1) k_wgrad_rows(const __grid_const
 // sums blocks w, w + 8, ... (coalesced rows), and the eight warp sums are
 // added in order; few outputs: a warp an output, lane l summing blocks l,
 // l + 32, ..., then a fixed shuffle tree.
-constexpr int kSumWide = 1024;  // outputs from which the first form is used
+constexpr int kSumWide = 256;  // outputs from which the first form is used
 __global__ void __launch_bounds__(256) k_sum_partials(const float* partial, int nblocks, int n, float* grad) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (n >= kSumWide) {
@@ -908,20 +908,34 @@ __global__ void k_conv_out_dx(const float* dout, const float* w, const __nv_bflo
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (int64_t)P * P) return;
     const int y = (int)(p / P), x = (int)(p % P);
-    float acc[C];
+    float d[9];
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[c] = 0.f;
     for (int tap = 0; tap < 9; ++tap) {
         const int yy = y - (tap / 3 - 1), xx = x - (tap % 3 - 1);
-        if (yy < 0 || xx < 0 || yy >= P || xx >= P) continue;
-        const float d = dout[(int64_t)yy * P + xx];
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] = fmaf(ws[tap * C + c], d, acc[c]);
+        d[tap] = (yy < 0 || xx < 0 || yy >= P || xx >= P) ? 0.f : dout[(int64_t)yy * P + xx];
     }
-    const __nv_bfloat16* ap = a + p * C;
-    __nv_bfloat16* dst = da + p * C;
+    const uint4* ap = reinterpret_cast<const uint4*>(a + p * C);
+    uint4* dst = reinterpret_cast<uint4*>(da + p * C);
 #pragma unroll
-    for (int c = 0; c < C; ++c) dst[c] = __float2bfloat16_rn(__bfloat162float(ap[c]) > 0.f ? acc[c] : 0.f);
+    for (int q = 0; q < 4; ++q) {  // channels 8q .. 8q + 7
+        const uint4 av = ap[q];
+        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+        uint32_t o[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int c0 = 8 * q + 2 * h;
+            float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+            for (int tap = 0; tap < 9; ++tap) {
+                // (a tap outside the image adds 0: the same sum)
+                s0 = fmaf(ws[tap * C + c0], d[tap], s0);
+                s1 = fmaf(ws[tap * C + c0 + 1], d[tap], s1);
+            }
+            const float2 g = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&aw[h]));
+            o[h] = pack_bf16x2(g.x > 0.f ? s0 : 0.f, g.y > 0.f ? s1 : 0.f);
+        }
+        dst[q] = make_uint4(o[0], o[1], o[2], o[3]);
+    }
 }
 
 // Small weight gradients on FP32 cores, persistent blocks over TH x TW tiles
@@ -1024,6 +1038,7 @@ __global__ void __launch_bounds__(256) k_wgrad_out(const __nv_bfloat16* a, const
         if (o < kOutOut) partial[(int64_t)blockIdx.x * kOutOut + o] = acc[j];
     }
 }
+
 
 // ---------------------------------------------------------------------------
 // Pooling, upsampling, gates
@@ -1384,6 +1399,8 @@ static int ws_alloc(pic_ctx* c) {
         if (balloc(&p, Q * Q * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
     for (auto*& p : N.d_small)
         if (balloc(&p, R * R * C)) return fail(PIC_ERR_CUDA, "warm start: gradient allocation failed");
+    // per-block partials of the 32->32 weight gradients; per-row partials of
+    // the outer layers'
     N.partial_floats = (size_t)std::max(kWgradBlocks, kSmallWgradBlocks) * (9 * C * C + C);
     if (cudaMalloc(&N.partial, N.partial_floats * 4) || cudaMalloc(&N.loss_partial, g1(std::max<int64_t>(P * P, c->nodes)) * 4) ||
         cudaMalloc(&N.gsum, (9 * C * C + C) * 4))
