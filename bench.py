@@ -45,7 +45,7 @@ UNIT = "particle-steps/s"
 # its slot in the other buffer.  Binning and the deposit ride on this pass.
 BYTES_PUSH_PASS = 40
 BYTES_STEP = 40           # whole particle phase of one step
-BYTES_SURVEY_FP32 = 112   # the blueprint's per-particle-step figure (push 48 + deposit 12 + bin 52)
+BYTES_THREE_PASS_FP32 = 112   # separate push / deposit / bin passes: 48 + 12 + 52 bytes a particle-step
 
 
 def parse():
@@ -382,7 +382,7 @@ def run_ours(args, rank, world, local_rank):
     step_particle_ms = (ms6[0] + ms6[1] + ms6[2] + ms6[4]) / prof_steps
     roofline_step = {"bytes_per_particle_step": BYTES_STEP,
                      "achieved_GBs": BYTES_STEP * n_part / (step_particle_ms * 1e-3) / 1e9,
-                     "survey_112B_equivalent_GBs": BYTES_SURVEY_FP32 * n_part / (step_particle_ms * 1e-3) / 1e9}
+                     "three_pass_112B_equivalent_GBs": BYTES_THREE_PASS_FP32 * n_part / (step_particle_ms * 1e-3) / 1e9}
     roofline_step["frac"] = roofline_step["achieved_GBs"] / peak
     roofline["kernels"] = kernel_rooflines(w, counts, ev, pois_ms, iters, phases, peak, peak_kind)
 
