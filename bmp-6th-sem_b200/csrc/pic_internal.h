@@ -176,6 +176,11 @@ struct PoissonState {
     int body_nodes[2] = {0, 0};
     bool graph_failed = false;
     bool graph_off = false;  // pic_set_poisson_graph(ctx, 0): direct launches
+    // exact coarse solve of levels[fused_first] (single contexts; poisson.cu)
+    bool direct = false;
+    int direct_nf = 0;
+    float* direct_inv = nullptr;  // [nf][nf] FP32 inverse over the level's free nodes
+    int* direct_free = nullptr;   // level node index of each free node
 };
 
 }  // namespace picb200

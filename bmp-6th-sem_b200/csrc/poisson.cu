@@ -865,6 +865,109 @@ __global__ void __launch_bounds__(kFusedThreads) k_mg_fused(FusedLevels F) {
     fused_body(F, smem);
 }
 
+// ---- exact solve of the first fused level (single contexts) -------------------
+//
+// Below the tiled levels the V-cycle needs the coarse-grid correction, the
+// solution of that level's own system A x = b (Dirichlet 0 at its
+// electrodes).  When the level has at most kDirectMax free nodes the
+// library inverts A once at set-up (FP64 Cholesky on the host, the inverse
+// kept in FP32 on the device) and the correction is one dense product in a
+// multi-block kernel (k_mg_direct), in place of the one-block chain of
+// smaller levels (k_mg_fused, still used by the batched ensemble solve).
+// The exact coarse solve is symmetric positive definite, so the
+// preconditioner stays a valid one for CG.
+constexpr int kDirectMax = 1200;
+
+// inverse of the level's operator over its free nodes (row-major, nf x nf),
+// or false when Cholesky breaks down (not positive definite)
+static bool invert_level(int GX, int GY, double cx, double cy, double cd, const std::vector<uint8_t>& mask,
+                         std::vector<int>& freen, std::vector<float>& inv) {
+    const int n = GX * GY;
+    std::vector<int> fidx(n, -1);
+    freen.clear();
+    for (int k = 0; k < n; ++k)
+        if (!mask[k]) {
+            fidx[k] = (int)freen.size();
+            freen.push_back(k);
+        }
+    const int nf = (int)freen.size();
+    std::vector<double> A((size_t)nf * nf, 0.0);
+    for (int f = 0; f < nf; ++f) {
+        const int k = freen[f];
+        A[(size_t)f * nf + f] += cd;
+        const int up = k + GX >= n ? k + GX - n : k + GX, dn = k - GX < 0 ? k - GX + n : k - GX;
+        const int nb[4] = {k - 1, k + 1, dn, up};
+        const double cf[4] = {cx, cx, cy, cy};
+        for (int e = 0; e < 4; ++e) {
+            const int g = (nb[e] >= 0 && nb[e] < n) ? fidx[nb[e]] : -1;
+            if (g >= 0) A[(size_t)f * nf + g] -= cf[e];
+        }
+    }
+    // envelope: first nonzero column of each row (fill-in stays inside it)
+    std::vector<int> first(nf);
+    for (int i = 0; i < nf; ++i) {
+        int j = 0;
+        while (j < i && A[(size_t)i * nf + j] == 0.0) ++j;
+        first[i] = j;
+    }
+    // in-place Cholesky, lower triangle: A = L L^T
+    for (int j = 0; j < nf; ++j) {
+        double* Lj = &A[(size_t)j * nf];
+        double s = Lj[j];
+        for (int k = first[j]; k < j; ++k) s -= Lj[k] * Lj[k];
+        if (!(s > 0.0)) return false;
+        Lj[j] = std::sqrt(s);
+        for (int i = j + 1; i < nf; ++i) {
+            if (first[i] > j) continue;
+            double* Li = &A[(size_t)i * nf];
+            double t = Li[j];
+            for (int k = std::max(first[i], first[j]); k < j; ++k) t -= Li[k] * Lj[k];
+            Li[j] = t / Lj[j];
+        }
+    }
+    // columns of the inverse: L y = e_c, then L^T x = y
+    std::vector<std::vector<int>> below(nf);  // rows k > i with L[k][i] in the envelope
+    for (int k = 0; k < nf; ++k)
+        for (int i = first[k]; i < k; ++i) below[i].push_back(k);
+    inv.assign((size_t)nf * nf, 0.f);
+    std::vector<double> y(nf), x(nf);
+    for (int c = 0; c < nf; ++c) {
+        for (int i = 0; i < c; ++i) y[i] = 0.0;
+        for (int i = c; i < nf; ++i) {
+            const double* Li = &A[(size_t)i * nf];
+            double t = i == c ? 1.0 : 0.0;
+            for (int k = std::max(first[i], c); k < i; ++k) t -= Li[k] * y[k];
+            y[i] = t / Li[i];
+        }
+        for (int i = nf - 1; i >= 0; --i) {
+            double t = y[i];
+            for (int k : below[i]) t -= A[(size_t)k * nf + i] * x[k];
+            x[i] = t / A[(size_t)i * nf + i];
+        }
+        for (int i = 0; i < nf; ++i) inv[(size_t)i * nf + c] = (float)x[i];
+    }
+    return true;
+}
+
+// x[free_idx[i]] = sum_j inv[i][j] b[free_idx[j]]: a warp a row (lanes over
+// j, then a fixed shuffle tree), b's free values staged in shared memory
+__global__ void __launch_bounds__(256) k_mg_direct(const float* __restrict__ inv, const int* __restrict__ freen,
+                                                   int nf, const float* __restrict__ b, float* __restrict__ x) {
+    extern __shared__ float bs[];
+    pdl_enter();
+    for (int j = threadIdx.x; j < nf; j += 256) bs[j] = b[freen[j]];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= nf) return;
+    const float* row = inv + (int64_t)i * nf;
+    float s = 0.f;
+#pragma unroll 4
+    for (int j = lane; j < nf; j += 32) s = fmaf(row[j], bs[j], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (lane == 0) x[freen[i]] = s;
+}
+
 // injected Dirichlet mask of a coarse level: the x walls (and, unless
 // periodic in y, the y walls) are Dirichlet, inner nodes take the fine
 // node's flag
@@ -976,6 +1079,20 @@ void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_
 // Returns the number of kernels.  Levels above the fused ones take two
 // kernels each (k_mg_down, k_mg_up); with with_rz the finest k_mg_up also
 // reduces r.z for the PCG iteration.
+// The V-cycle's coarsest step, from levels[fused_first].b into its x: the
+// exact solve when set up, else the one-block chain of the small levels.
+static void enqueue_coarse(pic_ctx* c, cudaStream_t st) {
+    PoissonState& ps = c->ps;
+    if (ps.direct) {
+        const MGLevel& L = ps.levels[ps.fused_first];
+        launch_pdl(k_mg_direct, dim3((unsigned)((ps.direct_nf + 7) / 8)), dim3(256), (size_t)ps.direct_nf * 4, st,
+                   (const float*)ps.direct_inv, (const int*)ps.direct_free, ps.direct_nf, (const float*)L.b, L.x);
+    } else {
+        launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
+                   *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    }
+}
+
 // fewer tiles than two per SM: blocks of kTileThreadsSmall (the level's time
 // is one block's latency, which more threads a tile shorten)
 static bool small_grid(dim3 g) { return (int64_t)g.x * g.y < 2 * 148; }
@@ -996,8 +1113,7 @@ int enqueue_vcycle(pic_ctx* c, cudaStream_t st, bool with_rz) {
             launch_pdl(k_mg_down<kTileThreads>, grid, tb, 0, st, F, C);
         launches += 1;
     }
-    launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
-               *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    enqueue_coarse(c, st);
     launches += 1;
     for (int l = kf - 1; l >= 0; --l) {
         const LevelDev F = as_dev(ps.levels[l]);
@@ -1038,8 +1154,7 @@ void enqueue_vcycle_per_sweep(pic_ctx* c, cudaStream_t st) {
         }
         launch_pdl(k_mg_restrict, grid2d(C.GX, C.GY, b2), b2, 0, st, F, C);
     }
-    launch_pdl(k_mg_fused, dim3(1), dim3(kFusedThreads), ps.fused_smem, st,
-               *reinterpret_cast<const FusedLevels*>(ps.fused_desc));
+    enqueue_coarse(c, st);
     for (int l = kf - 1; l >= 0; --l) {
         const LevelDev F = as_dev(ps.levels[l]);
         const LevelDev C = as_dev(ps.levels[l + 1]);
@@ -1307,6 +1422,23 @@ int poisson_setup(pic_ctx* c) {
     PIC_CUDA(cudaFuncGetAttributes(&fa, k_mg_fused));
     if ((int)off > fa.maxDynamicSharedSizeBytes)
         PIC_CUDA(cudaFuncSetAttribute(k_mg_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
+    // the exact coarse solve of the first fused level, when it is small
+    if (ps.levels[kf].nodes <= kDirectMax) {
+        const MGLevel& Lk = ps.levels[kf];
+        std::vector<uint8_t> m((size_t)Lk.nodes);
+        PIC_CUDA(cudaMemcpyAsync(m.data(), Lk.mask, m.size(), cudaMemcpyDeviceToHost, c->stream));
+        PIC_CUDA(cudaStreamSynchronize(c->stream));
+        std::vector<int> freen;
+        std::vector<float> inv;
+        if (invert_level(Lk.GX, Lk.GY, Lk.cx, Lk.cy, Lk.cd, m, freen, inv) && !freen.empty()) {
+            ps.direct_nf = (int)freen.size();
+            PIC_CUDA(cudaMalloc(&ps.direct_inv, inv.size() * sizeof(float)));
+            PIC_CUDA(cudaMalloc(&ps.direct_free, freen.size() * sizeof(int)));
+            PIC_CUDA(cudaMemcpy(ps.direct_inv, inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice));
+            PIC_CUDA(cudaMemcpy(ps.direct_free, freen.data(), freen.size() * sizeof(int), cudaMemcpyHostToDevice));
+            ps.direct = true;
+        }
+    }
     PIC_CUDA(cudaStreamCreateWithFlags(&ps.cap_stream, cudaStreamNonBlocking));
     return PIC_OK;
 }
@@ -1320,6 +1452,11 @@ void poisson_free(pic_ctx* c) {
         if (l > 0) cudaFree(ps.levels[l].mask);
     }
     ps.levels.clear();
+    cudaFree(ps.direct_inv);
+    cudaFree(ps.direct_free);
+    ps.direct_inv = nullptr;
+    ps.direct_free = nullptr;
+    ps.direct = false;
     cudaFree(ps.r);
     cudaFree(ps.z);
     cudaFree(ps.p[0]);
