@@ -491,6 +491,8 @@ constexpr int kDownHalo = 2 * kNu + 1;
 constexpr int kUpHalo = 2 * kNu;
 constexpr int kDownSide = kTileCore + 2 * kDownHalo;
 constexpr int kUpSide = kTileCore + 2 * kUpHalo;
+constexpr int kUpCoarse = kUpSide / 2 + 1;  // coarse nodes under an up tile, a side
+static_assert(kUpHalo % 2 == 0, "up tiles start on an even node");
 constexpr int kTileThreads = 256;      // the finest level's kernels (and r.z)
 constexpr int kTileThreadsSmall = 1024; // levels of fewer tiles than two per SM: shorter chains
 static_assert(kDownSide % 2 == 0 && kUpSide % 2 == 0, "tile rows hold as many nodes of each colour");
@@ -610,30 +612,30 @@ template <bool kRz, int NT>
 __global__ void __launch_bounds__(NT) k_mg_up(LevelDev F, LevelDev C, float* xo, RzArgs R) {
     static_assert(!kRz || NT == kRedThreads, "the r.z reduction is the PCG block reduction");
     constexpr int S = kUpSide, H = kUpHalo;
-    __shared__ float sx[S * S], sb[S * S];
+    __shared__ float sx[S * S], sb[S * S], sc[kUpCoarse * kUpCoarse];
     __shared__ uint8_t sm[S * S];
     pdl_enter();
     const int i0 = blockIdx.x * kTileCore - H, j0 = blockIdx.y * kTileCore - H;
     {
-        // the node's mask, b, x and the four coarse values prolonged() reads
-        // (column I + 1 clamped: only read for odd i < GX - 1), all loaded
-        // before any is used
+        // the coarse correction's tile first: coarse nodes (i0 / 2 + a,
+        // j0 / 2 + b), rows wrapped like the fine ones (periodic in y the row
+        // counts are even, so (j mod GY) / 2 = (j / 2) mod (GY / 2)); columns
+        // outside the level read 0 (only electrode or outside nodes use them)
+        const int I0 = i0 >> 1, J0 = j0 >> 1;
+        for (int t = threadIdx.x; t < kUpCoarse * kUpCoarse; t += NT) {
+            const int I = I0 + t % kUpCoarse, J = tile_row(J0 + t / kUpCoarse, C.GY);
+            sc[t] = (I >= 0 && I < C.GX) ? C.x[J * C.GX + I] : 0.0f;
+        }
+        // the node's mask, b and x, all loaded before any is used
         constexpr int NL = tile_loads<S, NT>();
-        int kk[NL], c00[NL], c10[NL], c01[NL], c11[NL];
+        int kk[NL];
         uint8_t mv[NL];
-        float bv[NL], xv[NL], x00[NL], x10[NL], x01[NL], x11[NL];
+        float bv[NL], xv[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int t = threadIdx.x + u * NT, i = i0 + t % S;
             const int j = tile_row(j0 + t / S, F.GY);
-            const bool in = t < S * S && i >= 0 && i < F.GX;
-            kk[u] = in ? j * F.GX + i : -1;
-            const int I = i >> 1, J = j >> 1;
-            const int I1 = min(I + 1, C.GX - 1), J1 = J + 1 == C.GY ? 0 : J + 1;  // wraps only periodic in y
-            c00[u] = J * C.GX + I;
-            c10[u] = J * C.GX + I1;
-            c01[u] = J1 * C.GX + I;
-            c11[u] = J1 * C.GX + I1;
+            kk[u] = (t < S * S && i >= 0 && i < F.GX) ? j * F.GX + i : -1;
         }
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
@@ -641,27 +643,25 @@ __global__ void __launch_bounds__(NT) k_mg_up(LevelDev F, LevelDev C, float* xo,
             mv[u] = in ? F.mask[kk[u]] : 1;
             bv[u] = in ? F.b[kk[u]] : 0.0f;
             xv[u] = in ? F.x[kk[u]] : 0.0f;
-            x00[u] = in ? C.x[c00[u]] : 0.0f;
-            x10[u] = in ? C.x[c10[u]] : 0.0f;
-            x01[u] = in ? C.x[c01[u]] : 0.0f;
-            x11[u] = in ? C.x[c11[u]] : 0.0f;
         }
+        __syncthreads();
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
-            const int t = threadIdx.x + u * NT, i = i0 + t % S;
+            const int t = threadIdx.x + u * NT, li = t % S, lj = t / S, i = i0 + li;
             if (t >= S * S) break;
-            const int j = tile_row(j0 + t / S, F.GY);  // as prolonged() gets it
             sm[t] = mv[u];
             sb[t] = bv[u];
             float v = xv[u];
             if (!mv[u]) {
                 // prolonged(): x + the bilinear interpolation of the coarse correction
+                const int j = j0 + lj;
                 const bool ox = i & 1, oy = j & 1;
+                const float* c = sc + ((j >> 1) - J0) * kUpCoarse + ((i >> 1) - I0);
                 float cv;
-                if (!ox && !oy) cv = x00[u];
-                else if (ox && !oy) cv = 0.5f * (x00[u] + x10[u]);
-                else if (!ox && oy) cv = 0.5f * (x00[u] + x01[u]);
-                else cv = 0.25f * (x00[u] + x10[u] + x01[u] + x11[u]);
+                if (!ox && !oy) cv = c[0];
+                else if (ox && !oy) cv = 0.5f * (c[0] + c[1]);
+                else if (!ox && oy) cv = 0.5f * (c[0] + c[kUpCoarse]);
+                else cv = 0.25f * (c[0] + c[1] + c[kUpCoarse] + c[kUpCoarse + 1]);
                 v = xv[u] + cv;
             }
             sx[t] = v;
