@@ -339,16 +339,17 @@ __global__ void __launch_bounds__(kRedThreads) k_true_residual(Grid64 g, const u
 
 // ---- multigrid (FP32) ------------------------------------------------------
 
+// icd = 1 / cd (rounded once): the Gauss-Seidel updates multiply by it
 struct LevelDev {
     int nx, ny, GX, GY;
-    float cx, cy, cd;
+    float cx, cy, cd, icd;
     const uint8_t* mask;
     float* x;
     float* b;
 };
 
 __host__ __device__ __forceinline__ LevelDev as_dev(const MGLevel& L) {
-    return LevelDev{L.nx, L.ny, L.GX, L.GY, L.cx, L.cy, L.cd, L.mask, L.x, L.b};
+    return LevelDev{L.nx, L.ny, L.GX, L.GY, L.cx, L.cy, L.cd, 1.0f / L.cd, L.mask, L.x, L.b};
 }
 
 // one Gauss-Seidel half sweep over the nodes of one colour
@@ -362,7 +363,7 @@ __global__ void k_mg_rbgs(LevelDev L, int color) {
     if (L.mask[k]) return;
     const float s = __fmaf_rn(L.cx, L.x[k - 1] + L.x[k + 1],
                               __fmaf_rn(L.cy, L.x[row_dn(k, n, L.GX)] + L.x[row_up(k, n, L.GX)], L.b[k]));
-    L.x[k] = s / L.cd;
+    L.x[k] = s * L.icd;
 }
 
 // b - A x at one node from its value c and its neighbours west, east, down,
@@ -426,10 +427,10 @@ __global__ void k_mg_init_black(LevelDev L) {
     if (i >= L.GX || j >= L.GY) return;
     const int k = j * L.GX + i, n = L.GX * L.GY;
     if (L.mask[k]) return;
-    auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] / L.cd; };
+    auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] * L.icd; };
     const float s = __fmaf_rn(L.cx, xr(k - 1) + xr(k + 1),
                               __fmaf_rn(L.cy, xr(row_dn(k, n, L.GX)) + xr(row_up(k, n, L.GX)), L.b[k]));
-    L.x[k] = s / L.cd;
+    L.x[k] = s * L.icd;
 }
 
 // x at fine node (i, j) plus the bilinear interpolation of the coarse
@@ -461,7 +462,7 @@ __global__ void k_mg_prolong_black(LevelDev F, LevelDev C) {
     const int jd = j == 0 ? F.GY - 1 : j - 1, ju = j + 1 == F.GY ? 0 : j + 1;
     const float s = __fmaf_rn(F.cx, prolonged(F, C, i - 1, j) + prolonged(F, C, i + 1, j),
                               __fmaf_rn(F.cy, prolonged(F, C, i, jd) + prolonged(F, C, i, ju), F.b[k]));
-    F.x[k] = s / F.cd;
+    F.x[k] = s * F.icd;
 }
 
 
@@ -514,7 +515,7 @@ constexpr int tile_loads() { return (S * S + NT - 1) / NT; }
 // wrap only at an even row count, so wrapping keeps the colour)
 template <int S, int NT>
 __device__ __forceinline__ void tile_half_sweep(float* x, const float* b, const uint8_t* m, float cx,
-                                                float cy, float cd, int color, int i0, int j0) {
+                                                float cy, float icd, int color, int i0, int j0) {
     constexpr int HS = S / 2;
     for (int h = threadIdx.x; h < HS * S; h += NT) {
         const int lj = h / HS;
@@ -522,7 +523,7 @@ __device__ __forceinline__ void tile_half_sweep(float* x, const float* b, const 
         const int t = lj * S + li;
         if (li == 0 || lj == 0 || li == S - 1 || lj == S - 1 || m[t]) continue;
         const float s = __fmaf_rn(cx, x[t - 1] + x[t + 1], __fmaf_rn(cy, x[t - S] + x[t + S], b[t]));
-        x[t] = s / cd;
+        x[t] = s * icd;
     }
     __syncthreads();
 }
@@ -557,16 +558,17 @@ __global__ void __launch_bounds__(NT) k_mg_down(LevelDev F, LevelDev C) {
             if (t >= S * S) break;
             sm[t] = mv[u];
             sb[t] = bv[u];
-            // zero start: the black sweep reads red x = b / cd (electrodes 0);
+            // zero start: the black sweep reads red x = b / cd (electrodes 0;
+            // as a product with icd, like every update);
             // black values are written before anything reads them
-            sx[t] = (!mv[u] && ((i0 + li + j0 + lj) & 1) == 0) ? bv[u] / F.cd : 0.0f;
+            sx[t] = (!mv[u] && ((i0 + li + j0 + lj) & 1) == 0) ? bv[u] * F.icd : 0.0f;
         }
     }
     __syncthreads();
-    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 1, i0, j0);
     for (int s = 1; s < kNu; ++s) {
-        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
-        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 0, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 1, i0, j0);
     }
     for (int t = threadIdx.x; t < S * S; t += NT) {
         const int li = t % S, lj = t / S;
@@ -668,11 +670,11 @@ __global__ void __launch_bounds__(NT) k_mg_up(LevelDev F, LevelDev C, float* xo,
         }
     }
     __syncthreads();
-    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
-    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 1, i0, j0);
+    tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 0, i0, j0);
     for (int s = 1; s < kNu; ++s) {
-        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 1, i0, j0);
-        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.cd, 0, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 1, i0, j0);
+        tile_half_sweep<S, NT>(sx, sb, sm, F.cx, F.cy, F.icd, 0, i0, j0);
     }
     double acc[1] = {0.0};
     for (int t = threadIdx.x; t < kTileCore * kTileCore; t += NT) {
@@ -1837,7 +1839,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
                                      : 0.0f;
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
-                        if (ok[u]) L.x[k[u]] = v[u] / L.cd;
+                        if (ok[u]) L.x[k[u]] = v[u] * L.icd;
                 }
             }
             grid.sync();
@@ -1858,7 +1860,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
                     if (L.mask[k]) continue;
                     float w, e, d, u;
                     if (mode == 0) {
-                        auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] / L.cd; };
+                        auto xr = [&](int m) { return L.mask[m] ? 0.0f : L.b[m] * L.icd; };
                         w = xr(k - 1);
                         e = xr(k + 1);
                         d = xr(row_dn(k, nl, L.GX));
@@ -1870,7 +1872,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_poisson_batch(const BatchInst
                         d = prolonged(L, C, x, jd);
                         u = prolonged(L, C, x, ju);
                     }
-                    L.x[k] = __fmaf_rn(L.cx, w + e, __fmaf_rn(L.cy, d + u, L.b[k])) / L.cd;
+                    L.x[k] = __fmaf_rn(L.cx, w + e, __fmaf_rn(L.cy, d + u, L.b[k])) * L.icd;
                 }
             }
             grid.sync();
