@@ -27,17 +27,20 @@
 // when it falls outside the fine grid.  Operators are rediscretised with
 // spacing 2^l*dx; restriction is full weighting, prolongation bilinear, the
 // smoother red-black Gauss-Seidel with the colour order reversed after the
-// coarse correction, so the V-cycle is a symmetric preconditioner.  The
-// coarsest level (min(nx,ny) <= 2: one unknown per row or column) gets
-// symmetric RB-GS sweeps.  All levels
-// from the first one whose hierarchy fits in shared memory down to the
-// coarsest run inside one thread block (k_mg_fused).
+// coarse correction, so the V-cycle is a symmetric preconditioner.  A level
+// above the small ones is two kernels, all of its sweeps on shared-memory
+// tiles with recomputed halos (k_mg_down, k_mg_up).  The small levels (from
+// the first whose hierarchy fits a 16 KB budget) are either solved exactly
+// -- the first of them inverted once at set-up, applied as one dense product
+// (k_mg_direct) -- or, in the batched ensemble solve and when that level is
+// too large, run inside one thread block (k_mg_fused: RB-GS on each, the
+// coarsest with symmetric sweeps).
 //
 // The PCG loop is one CUDA graph: a while-conditional node whose body is one
-// iteration (V-cycle, z.r, p update, A p, x/r update, convergence test); the
-// test kernel sets the condition on the device, so a solve costs one graph
-// launch and one host synchronisation.  Without conditional-node support the
-// same kernels run from a host loop.
+// iteration (V-cycle with r.z, p update with A p, x/r update with the
+// convergence test); the last kernel sets the condition on the device, so a
+// solve costs one graph launch and one host synchronisation.  Without
+// conditional-node support the same kernels run from a host loop.
 #include <cooperative_groups.h>
 #include <utility>
 #include <cuda_runtime.h>
