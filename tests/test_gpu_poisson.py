@@ -110,6 +110,37 @@ def test_poisson_internal_electrode_vs_direct(oracle, n):
     assert np.allclose(ef, ef_same, rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("n,inner", [(32, False), (30, True), (60, True)])
+def test_exact_coarse_solve(oracle, n, inner):
+    """The multigrid's coarse-grid correction is an exact solve of the first
+    small level (inverted once at set-up).  On grids of at most 1,200 nodes
+    that level is the grid itself (n = 32, 30: the preconditioner is the
+    exact inverse in FP32, so PCG needs a few iterations at most to 1e-12);
+    on 61^2 it is the 31^2 level below one tiled level.  Both against the
+    direct solve to 1e-8 of max|phi|, an inner electrode included."""
+    import pic_b200 as P
+    import pic_configs as C
+    dx = 2.5e-4
+    c = n // 2
+    rects = C.wall_rects(n, n, left=40.0)
+    if inner:
+        rects = rects + [(c - 3, c - 2, c + 4, c + 3, 90.0)]
+    GX = n + 1
+    rho = np.random.default_rng(n).normal(0, 1e7, GX * GX)
+    cfg = P.make_config(n, n, n * dx, n * dx, 5e-11, [(-1.6e-19, 9.1e-31, 1.0, 1.0)], rects,
+                        tol=1e-12, maxit=200)
+    with P.Pic(cfg) as pic:
+        pic.set_rho(rho)
+        pic.poisson_solve(0)
+        phi = pic.phi()
+        iters = pic.poisson_stats()[0]
+    D = oracle.DirectPoisson(GX, GX, dx, dx, oracle.Electrodes(rects))
+    phi_o, _ = D.step(rho.copy())
+    assert np.abs(phi - phi_o).max() <= 1e-8 * np.abs(phi_o).max()
+    if GX * GX <= 1200:
+        assert iters <= 4, iters
+
+
 def test_warm_start_cuts_iterations():
     d0, d1 = np.load(FIXTURES[0]), np.load(FIXTURES[1])
     with golden_pic(0, 1e-8, warm=1) as pic:
